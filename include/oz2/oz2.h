@@ -1,0 +1,91 @@
+/*
+ * oz2.h - C ABI of the B200-native Ozaki Scheme II FP64 GEMM emulator (liboz2.so).
+ *
+ * Plain pointers and sizes only. Stream and event arguments are cudaStream_t / cudaEvent_t
+ * passed as void*. Matrices are column-major device pointers, as in BLAS. Every entry point
+ * returns an oz2_status; oz2_last_error() gives the message of the last failure on a handle.
+ *
+ * Each entry point replaces one member of the reference's C++ class oz2::Ozaki2
+ * (MacraMacra/OS2-Xe, src/ozaki2_gpu.hpp); the citation is given beside it. The C++ header
+ * oz2/ozaki2.hpp wraps these functions in a class with the reference's names and exceptions.
+ */
+#ifndef OZ2_OZ2_H
+#define OZ2_OZ2_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct oz2_context* oz2_handle;
+
+typedef enum {
+    OZ2_OK = 0,
+    OZ2_EINVAL = 1,     /* std::invalid_argument in the reference */
+    OZ2_ENOMEM = 2,     /* workspace does not fit (std::runtime_error in the reference) */
+    OZ2_EINTERNAL = 3,  /* std::runtime_error / std::logic_error */
+    OZ2_ETIMEOUT = 4,   /* a device-side wait ran out; no counterpart in the reference */
+    OZ2_EOVERFLOW = 5,  /* std::overflow_error */
+    OZ2_ECUDA = 6       /* a CUDA runtime call failed */
+} oz2_status;
+
+/* Ozaki2(sycl::queue&) / ~Ozaki2(): src/ozaki2_gpu.hpp:680-687.
+ * Binds to a caller-owned CUDA stream (NULL = legacy default stream) of the current device. */
+int oz2_create(void* stream, oz2_handle* out);
+int oz2_destroy(oz2_handle h);
+/* rebinds the handle to another stream of the same device (no counterpart: SYCL binds once) */
+int oz2_set_stream(oz2_handle h, void* stream);
+
+/* Ozaki2::gemm: src/ozaki2_gpu.hpp:739-760.
+ * C = alpha op(A) op(B) + beta C with op in {'N','T','C'} ('C' equals 'T' for real data),
+ * num_moduli in [2, 24]. deps: cudaEvent_t[ndeps] the stream waits on first (may be NULL);
+ * done: a cudaEvent_t recorded after the last kernel (may be NULL). Asynchronous. */
+int oz2_dgemm(oz2_handle h, char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha, const double* A,
+              int64_t lda, const double* B, int64_t ldb, double beta, double* C, int64_t ldc, int num_moduli,
+              void* const* deps, int ndeps, void* done);
+
+/* Ozaki2::zgemm: src/ozaki2_gpu.hpp:764-786. Complex data interleaved (re, im) as
+ * std::complex<double>; alpha and beta point to {re, im} on the HOST. 3M form, 3s INT8 GEMMs. */
+int oz2_zgemm(oz2_handle h, char ta, char tb, int64_t m, int64_t n, int64_t k, const double* alpha,
+              const double* A, int64_t lda, const double* B, int64_t ldb, const double* beta, double* C,
+              int64_t ldc, int num_moduli, void* const* deps, int ndeps, void* done);
+
+/* Ozaki2::precision_bits / precision_bits_complex / moduli_for_bits: src/ozaki2_gpu.hpp:689-700, :762 */
+int oz2_precision_bits(int64_t k, int num_moduli, int* out);
+int oz2_precision_bits_complex(int64_t k, int num_moduli, int* out);
+int oz2_moduli_for_bits(int64_t k, int bits, int* out);
+
+/* Ozaki2::set_workspace_limit / set_resident_hint / release_workspace: src/ozaki2_gpu.hpp:702-710 */
+int oz2_set_workspace_limit(oz2_handle h, size_t bytes);
+int oz2_set_resident_hint(oz2_handle h, size_t bytes);
+int oz2_release_workspace(oz2_handle h);
+
+/* Ozaki2::stage_times: src/ozaki2_gpu.hpp:716-737. out = {scale_ms, split_ms, gemm_ms, crt_ms}.
+ * Zeros unless profiling is on (the reference's queue property enable_profiling). Waits for
+ * the last call. */
+int oz2_set_profiling(oz2_handle h, int enable);
+int oz2_stage_times(oz2_handle h, double* out4);
+
+/* Ozaki2::last_tiling: src/ozaki2_gpu.hpp:712, TileInfo :47-53.
+ * out = {mb, nb, pm, pn, k_chunks, workspace_bytes} */
+int oz2_last_tiling(oz2_handle h, int64_t* out6);
+
+/* Ozaki2::set_tuning: src/ozaki2_gpu.hpp:713, Tuning :41-45. The reference's three knobs are
+ * Xe2-specific; here they are accepted and reported back, and pow2_tiles keeps its meaning
+ * (prefer power-of-two tile candidates). */
+int oz2_set_tuning(oz2_handle h, int batched_gemm, int pad_lda, int pow2_tiles);
+
+/* Device-side error word: non-zero after a kernel's bounded wait ran out (OZ2_ETIMEOUT).
+ * Synchronises the handle's stream, returns and clears the word. */
+int oz2_check_device_error(oz2_handle h);
+
+/* message of the last failed call on the handle (or of the last failed handle-less call) */
+const char* oz2_last_error(oz2_handle h);
+const char* oz2_status_string(int status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,228 @@
+// oz2_crt.cu - CRT reconstruction of the Ozaki-II path: per C entry, s residues r_t in
+// [0, m_t) -> the exact integer x = Sum_t r_t W_t - q M (|x| <= M/4, q = rint(Sum_t r_t y_t/m_t)
+// from an FP32 estimate) -> one round-to-nearest-even to a double -> * 2^-(D_i + E_j) ->
+// alpha/beta update. Ref src/ozaki2_gpu.hpp:526-588 (CrtAcc), :603-626 (launch_crt),
+// :628-664 (launch_crt_cplx, 3M recombination Re = P0 - P1, Im = P2 - P0 - P1).
+//
+// Bandwidth-bound: s bytes of residues per entry in (3s for complex), 8 (16) bytes of C out,
+// plus 8 (16) in when beta != 0. Each thread handles 4 consecutive rows of one column.
+#include <algorithm>
+
+#include "oz2_kernels.cuh"
+
+namespace oz2 {
+namespace {
+
+struct CrtParams {
+    const uint8_t* resid;
+    int64_t rstride, gstride, ldr, m, n, ldc;
+    const unsigned long long* maxA;
+    const unsigned long long* maxB;
+    int tk;
+    double ar, ai, br, bi;
+    double* C;
+    CrtConst cc;
+    uint32_t mod_m[kMaxModuli];
+};
+
+__device__ __forceinline__ int exponent_of(unsigned long long b, int tk) {
+    if (b >= 0x7FF0000000000000ull) return kNonFinite;
+    if (b == 0) return 0;
+    const int be = static_cast<int>(b >> 52);
+    const int e2 = be ? be - 1022 : -1010 - __clzll(static_cast<long long>(b));
+    return tk - e2;
+}
+
+// exact reconstruction + single rounding; r[t] in [0, m_t)
+template <int S, int NL>
+__device__ __forceinline__ double crt_value(const uint32_t (&r)[S], const CrtConst& cc, int shift) {
+    float u = 0.0f;
+    uint64_t acc[NL];
+#pragma unroll
+    for (int l = 0; l < NL; ++l) acc[l] = 0;
+#pragma unroll
+    for (int t = 0; t < S; ++t) {
+        u = __fmaf_rn(static_cast<float>(r[t]), cc.frac[t], u);
+#pragma unroll
+        for (int l = 0; l < NL; ++l) acc[l] += static_cast<uint64_t>(r[t]) * cc.W[t][l];
+    }
+    const int64_t q = __float2int_rn(u);
+    // x = Sum r_t W_t - q M  modulo 2^(32 NL), as NL two's-complement words
+    uint32_t w[NL];
+    int64_t carry = 0;
+#pragma unroll
+    for (int l = 0; l < NL; ++l) {
+        const int64_t v = static_cast<int64_t>(acc[l]) - q * static_cast<int64_t>(cc.M[l]) + carry;
+        w[l] = static_cast<uint32_t>(v);
+        carry = v >> 32;
+    }
+    const bool neg = static_cast<int32_t>(w[NL - 1]) < 0;
+    if (neg) {
+        uint32_t cy = 1;
+#pragma unroll
+        for (int l = 0; l < NL; ++l) {
+            const uint32_t nw = ~w[l] + cy;
+            cy = (cy && nw == 0) ? 1u : 0u;
+            w[l] = nw;
+        }
+    }
+    int tw = -1;
+#pragma unroll
+    for (int l = 0; l < NL; ++l)
+        if (w[l]) tw = l;
+    if (tw < 0) return 0.0;
+    // the 64 bits below the leading one, with everything further down folded into a sticky bit
+    uint32_t a = 0, b = 0, c = 0;
+    bool sticky = false;
+#pragma unroll
+    for (int l = 0; l < NL; ++l) {
+        if (l == tw) a = w[l];
+        else if (l == tw - 1) b = w[l];
+        else if (l == tw - 2) c = w[l];
+        else if (l < tw - 2) sticky |= w[l] != 0;
+    }
+    const int z = __clz(a);
+    const uint64_t hi = (static_cast<uint64_t>(a) << 32) | b;
+    uint64_t top = z ? (hi << z) | (c >> (32 - z)) : hi;
+    sticky |= (z ? (c << z) : c) != 0;
+    top |= sticky ? 1u : 0u;
+    const double val = ldexp(__ull2double_rn(top), 32 * tw - 32 - z - shift);
+    return neg ? -val : val;
+}
+
+__device__ __forceinline__ uint32_t sub_mod(uint32_t a, uint32_t b, uint32_t m) {  // (a - b) mod m, a,b < m
+    uint32_t r = a + m - b;
+    return min(r, r - m);
+}
+
+template <int S, bool CPLX>
+__global__ void __launch_bounds__(256) crt_kernel(const __grid_constant__ CrtParams P) {
+    constexpr int NL = limbs_for(S);
+    const int64_t i0 = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) * 4;
+    if (i0 >= P.m) return;
+    int De[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) De[e] = i0 + e < P.m ? exponent_of(P.maxA[i0 + e], P.tk) : 0;
+    for (int64_t j = blockIdx.y; j < P.n; j += gridDim.y) {
+        const int Ej = exponent_of(P.maxB[j], P.tk);
+        const uint8_t* base = P.resid + j * P.ldr + i0;
+        uint32_t rr[4][S], ri[4][S];
+#pragma unroll
+        for (int t = 0; t < S; ++t) {
+            const uint32_t w0 = __ldg(reinterpret_cast<const uint32_t*>(base + t * P.rstride));
+            if (!CPLX) {
+#pragma unroll
+                for (int e = 0; e < 4; ++e) rr[e][t] = (w0 >> (8 * e)) & 0xFFu;
+            } else {
+                const uint32_t w1 = __ldg(reinterpret_cast<const uint32_t*>(base + P.gstride + t * P.rstride));
+                const uint32_t w2 = __ldg(reinterpret_cast<const uint32_t*>(base + 2 * P.gstride + t * P.rstride));
+                const uint32_t m = P.mod_m[t];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const uint32_t p0 = (w0 >> (8 * e)) & 0xFFu, p1 = (w1 >> (8 * e)) & 0xFFu;
+                    const uint32_t p2 = (w2 >> (8 * e)) & 0xFFu;
+                    rr[e][t] = sub_mod(p0, p1, m);                  // Re = P0 - P1
+                    ri[e][t] = sub_mod(sub_mod(p2, p0, m), p1, m);  // Im = P2 - P0 - P1
+                }
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int64_t i = i0 + e;
+            if (i >= P.m) break;
+            const bool nonfinite = De[e] == kNonFinite || Ej == kNonFinite;
+            const int shift = nonfinite ? 0 : De[e] + Ej;
+            double* cp = P.C + (CPLX ? 2 : 1) * (i + j * P.ldc);
+            if (!CPLX) {
+                double v = crt_value<S, NL>(rr[e], P.cc, shift);
+                if (nonfinite) v = __longlong_as_double(0x7FF8000000000000ll);
+                // the reference's unfused alpha*v + beta*c, one rounding per operation
+                const double av = __dmul_rn(P.ar, v);
+                cp[0] = P.br == 0.0 ? av : __dadd_rn(av, __dmul_rn(P.br, cp[0]));
+            } else {
+                double vr = crt_value<S, NL>(rr[e], P.cc, shift);
+                double vi = crt_value<S, NL>(ri[e], P.cc, shift);
+                if (nonfinite) vr = vi = __longlong_as_double(0x7FF8000000000000ll);
+                double orr = __dsub_rn(__dmul_rn(P.ar, vr), __dmul_rn(P.ai, vi));
+                double oi = __dadd_rn(__dmul_rn(P.ar, vi), __dmul_rn(P.ai, vr));
+                if (P.br != 0.0 || P.bi != 0.0) {
+                    const double cr = cp[0], ci = cp[1];
+                    orr = __dadd_rn(orr, __dsub_rn(__dmul_rn(P.br, cr), __dmul_rn(P.bi, ci)));
+                    oi = __dadd_rn(oi, __dadd_rn(__dmul_rn(P.br, ci), __dmul_rn(P.bi, cr)));
+                }
+                cp[0] = orr;
+                cp[1] = oi;
+            }
+        }
+    }
+}
+
+template <int S>
+void crt_launch_s(const CrtParams& P, bool cplx, cudaStream_t st) {
+    const int64_t quads = ceil_div(P.m, 4);
+    dim3 grid(static_cast<unsigned>(ceil_div(quads, 256)), static_cast<unsigned>(std::min<int64_t>(P.n, 65535)));
+    if (cplx) crt_kernel<S, true><<<grid, 256, 0, st>>>(P);
+    else crt_kernel<S, false><<<grid, 256, 0, st>>>(P);
+}
+
+template <int S>
+void crt_dispatch(int s, const CrtParams& P, bool cplx, cudaStream_t st) {
+    if constexpr (S <= kMaxModuli) {
+        if (s == S) return crt_launch_s<S>(P, cplx, st);
+        crt_dispatch<S + 1>(s, P, cplx, st);
+    }
+}
+
+__global__ void scale_c_kernel(double* C, int64_t ldc, int64_t m, int64_t n, double br, double bi, int cplx) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    for (int64_t j = blockIdx.y; j < n; j += gridDim.y) {
+        if (!cplx) {
+            double* cp = C + i + j * ldc;
+            *cp = br == 0.0 ? 0.0 : __dmul_rn(br, *cp);
+        } else {
+            double* cp = C + 2 * (i + j * ldc);
+            if (br == 0.0 && bi == 0.0) {
+                cp[0] = 0.0;
+                cp[1] = 0.0;
+            } else {
+                const double r = cp[0], im = cp[1];
+                cp[0] = __dsub_rn(__dmul_rn(br, r), __dmul_rn(bi, im));
+                cp[1] = __dadd_rn(__dmul_rn(br, im), __dmul_rn(bi, r));
+            }
+        }
+    }
+}
+
+}  // namespace
+
+void launch_crt(const CrtArgs& a, cudaStream_t st) {
+    if (a.m <= 0 || a.n <= 0) return;
+    CrtParams P{};
+    P.resid = a.resid;
+    P.rstride = a.rstride;
+    P.gstride = a.rstride * a.plan->s;
+    P.ldr = a.ldr;
+    P.m = a.m;
+    P.n = a.n;
+    P.ldc = a.ldc;
+    P.maxA = a.maxA;
+    P.maxB = a.maxB;
+    P.tk = a.tk;
+    P.ar = a.alpha[0];
+    P.ai = a.alpha[1];
+    P.br = a.beta[0];
+    P.bi = a.beta[1];
+    P.C = a.C;
+    crt_constants(*a.plan, P.cc);
+    for (int t = 0; t < a.plan->s; ++t) P.mod_m[t] = a.plan->m[t];
+    crt_dispatch<2>(a.plan->s, P, a.cplx, st);
+}
+
+void launch_scale_c(double* C, int64_t ldc, int64_t m, int64_t n, const double* beta, bool cplx, cudaStream_t st) {
+    if (m <= 0 || n <= 0) return;
+    dim3 grid(static_cast<unsigned>(ceil_div(m, 256)), static_cast<unsigned>(std::min<int64_t>(n, 65535)));
+    scale_c_kernel<<<grid, 256, 0, st>>>(C, ldc, m, n, beta[0], cplx ? beta[1] : 0.0, cplx ? 1 : 0);
+}
+
+}  // namespace oz2

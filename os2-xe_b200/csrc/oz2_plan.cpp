@@ -1,0 +1,172 @@
+// oz2_plan.cpp - see oz2_plan.hpp.
+#include "oz2_plan.hpp"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+namespace oz2 {
+namespace {
+
+// Pairwise-coprime moduli <= 256 for s = 2..24 (ref src/coprime_tables.hpp:10-111): each set
+// is a prefix of one of three sequences.
+constexpr uint16_t kSeqSmall[6] = {256, 255, 253, 251, 247, 241};
+constexpr uint16_t kSeqMid[13] = {256, 253, 251, 249, 247, 245, 241, 239, 233, 229, 227, 223, 211};
+constexpr uint16_t kSeqLarge[24] = {256, 253, 251, 249, 247, 241, 239, 235, 233, 229, 227, 223,
+                                    217, 211, 199, 197, 193, 191, 181, 179, 173, 167, 163, 157};
+
+struct Big {
+    uint32_t w[kBigWords] = {};
+    static Big of(uint64_t v) {
+        Big b;
+        b.w[0] = static_cast<uint32_t>(v);
+        b.w[1] = static_cast<uint32_t>(v >> 32);
+        return b;
+    }
+    bool mul(uint32_t f) {  // false on overflow
+        uint64_t c = 0;
+        for (auto& x : w) {
+            const uint64_t t = uint64_t{x} * f + c;
+            x = static_cast<uint32_t>(t);
+            c = t >> 32;
+        }
+        return c == 0;
+    }
+    uint32_t divmod(uint32_t d) {
+        uint64_t r = 0;
+        for (int i = kBigWords - 1; i >= 0; --i) {
+            const uint64_t cur = (r << 32) | w[i];
+            w[i] = static_cast<uint32_t>(cur / d);
+            r = cur % d;
+        }
+        return static_cast<uint32_t>(r);
+    }
+    uint32_t mod(uint32_t d) const {
+        Big t = *this;
+        return t.divmod(d);
+    }
+    bool shl(int bits) {  // false if set bits would be shifted out
+        Big r;
+        for (int b = kBigWords * 32 - 1; b >= 0; --b) {
+            if (!((w[b / 32] >> (b % 32)) & 1u)) continue;
+            if (b + bits >= kBigWords * 32) return false;
+            r.w[(b + bits) / 32] |= 1u << ((b + bits) % 32);
+        }
+        *this = r;
+        return true;
+    }
+    int cmp(const Big& o) const {
+        for (int i = kBigWords - 1; i >= 0; --i)
+            if (w[i] != o.w[i]) return w[i] < o.w[i] ? -1 : 1;
+        return 0;
+    }
+    // estimate from the top three words; the tk search below starts from it
+    double log2() const {
+        int top = kBigWords - 1;
+        while (top > 0 && w[top] == 0) --top;
+        const int lo = top - 2 > 0 ? top - 2 : 0;
+        double v = 0;
+        for (int i = top; i >= lo; --i) v = v * 4294967296.0 + w[i];
+        return std::log2(v) + 32.0 * lo;
+    }
+};
+
+int64_t inverse_mod(int64_t a, int64_t m) {
+    int64_t t = 0, nt = 1, r = m, nr = ((a % m) + m) % m;
+    while (nr) {
+        const int64_t q = r / nr;
+        int64_t tmp = t - q * nt;
+        t = nt;
+        nt = tmp;
+        tmp = r - q * nr;
+        r = nr;
+        nr = tmp;
+    }
+    return r == 1 ? (t % m + m) % m : -1;
+}
+
+uint32_t pow2_mod(int e, uint32_t m) {
+    uint32_t v = 1 % m;
+    for (int i = 0; i < e; ++i) v = (v * 2) % m;
+    return v;
+}
+
+}  // namespace
+
+int make_plan(int s, int64_t k, Plan& p) {
+    if (s < 2 || s > kMaxModuli || k < 1) return 1;
+    p = Plan{};
+    p.s = s;
+    const uint16_t* seq = s <= 6 ? kSeqSmall : (s <= 13 ? kSeqMid : kSeqLarge);
+    Big M = Big::of(1);
+    for (int t = 0; t < s; ++t) {
+        p.m[t] = seq[t];
+        if (!M.mul(seq[t])) return 5;
+    }
+    p.log2M = M.log2();
+    p.nl = static_cast<int>(std::floor(p.log2M / 32.0)) + 1;
+    if (p.nl < 2) p.nl = 2;
+    if (p.nl != limbs_for(s)) return 3;
+    // largest tk <= 100 with k 2^(2 tk + 2) <= M, so that |x| <= M/4 for every result entry
+    int tk = static_cast<int>(std::floor((p.log2M - 2.0 - std::log2(static_cast<double>(k))) / 2.0));
+    if (tk > kMaxScaleBits) tk = kMaxScaleBits;
+    for (;; --tk) {
+        if (tk < 1) return 1;
+        Big lhs = Big::of(static_cast<uint64_t>(k));
+        if (!lhs.shl(2 * tk + 2)) continue;
+        if (lhs.cmp(M) <= 0) break;
+    }
+    p.tk = tk;
+    for (int t = 0; t < s; ++t) {
+        Big Mt = M;
+        if (Mt.divmod(p.m[t]) != 0) return 3;
+        const int64_t y = inverse_mod(Mt.mod(p.m[t]), p.m[t]);
+        if (y < 0) return 3;
+        if (!Mt.mul(static_cast<uint32_t>(y))) return 5;
+        std::memcpy(p.W[t], Mt.w, sizeof Mt.w);
+        p.y[t] = static_cast<uint32_t>(y);
+    }
+    std::memcpy(p.M, M.w, sizeof M.w);
+    return 0;
+}
+
+const char* plan_error_text(int s, int64_t k, int status, char* buf, int len) {
+    if (s < 2 || s > kMaxModuli)
+        std::snprintf(buf, len, "oz2: num_moduli must be in [2, %d]", kMaxModuli);
+    else if (k < 1)
+        std::snprintf(buf, len, "oz2: k must be >= 1");
+    else if (status == 1)
+        std::snprintf(buf, len, "oz2: num_moduli=%d is too small for k=%lld", s, static_cast<long long>(k));
+    else if (status == 5)
+        std::snprintf(buf, len, "oz2: integer overflow while planning");
+    else
+        std::snprintf(buf, len, "oz2: inconsistent modulus table");
+    return buf;
+}
+
+void mod_constants(const Plan& p, ModConst* out) {
+    for (int t = 0; t < p.s; ++t) {
+        const uint32_t m = p.m[t], h = (m - 1) / 2;
+        ModConst& c = out[t];
+        c.m = m;
+        c.mu = static_cast<uint32_t>((uint64_t{1} << 32) / m);
+        c.h = h;
+        for (int j = 1; j <= 4; ++j) c.c[j - 1] = pow2_mod(21 * j, m);
+        c.koff3 = (h + m - pow2_mod(62, m)) % m;
+        c.koff5 = (h + m - pow2_mod(104, m)) % m;
+        c.kneg = (m - pow2_mod(31, m)) % m;
+    }
+}
+
+void crt_constants(const Plan& p, CrtConst& out) {
+    out = CrtConst{};
+    out.s = p.s;
+    out.nl = p.nl;
+    for (int t = 0; t < p.s; ++t) {
+        for (int l = 0; l < p.nl; ++l) out.W[t][l] = p.W[t][l];
+        out.frac[t] = static_cast<float>(static_cast<double>(p.y[t]) / p.m[t]);
+    }
+    for (int l = 0; l < p.nl; ++l) out.M[l] = p.M[l];
+}
+
+}  // namespace oz2

@@ -1,0 +1,68 @@
+// oz2_plan.hpp - host planning for the Ozaki Scheme II path: modulus sets, the exact
+// product M, the bits per scaled element tk, CRT weights, and the per-modulus constants the
+// split, GEMM-epilogue and CRT kernels read.
+#pragma once
+
+#include <cstdint>
+
+#if defined(__CUDACC__)
+#define OZ2_HD __host__ __device__
+#else
+#define OZ2_HD
+#endif
+
+namespace oz2 {
+
+constexpr int kMaxModuli = 24;
+constexpr int kBigWords = 8;       // 256-bit host integers
+constexpr int kMaxLimbs = 6;       // 32-bit limbs of M for s <= 24
+constexpr int kMaxScaleBits = 100;
+constexpr int kNarrowScaleBits = 62;
+constexpr int kNonFinite = -2147483647 - 1;
+
+// 32-bit limbs of M per s: max(2, floor(log2 M / 32) + 1) (ref src/ozaki2_gpu.hpp:55-59, :168)
+OZ2_HD constexpr int limbs_for(int s) {
+    constexpr int t[kMaxModuli + 1] = {0, 0, 2, 2, 2, 2, 2, 2, 2, 3, 3, 3, 3, 4, 4, 4, 4, 5, 5, 5, 5, 6, 6, 6, 6};
+    return t[s];
+}
+
+struct Plan {
+    int s = 0;
+    int nl = 0;
+    int tk = 0;
+    double log2M = 0;
+    uint32_t m[kMaxModuli] = {};
+    uint32_t y[kMaxModuli] = {};             // (M/m_t)^-1 mod m_t
+    uint32_t W[kMaxModuli][kBigWords] = {};  // CRT weights (M/m_t) y_t
+    uint32_t M[kBigWords] = {};
+};
+
+// Returns 0, or 1 (invalid: s out of [2, 24], k < 1, s too small for k), or 5 (overflow).
+// ref src/ozaki2_gpu.hpp:159-200
+int make_plan(int s, int64_t k, Plan& p);
+const char* plan_error_text(int s, int64_t k, int status, char* buf, int len);
+
+// Constants of one modulus as the kernels use them.
+struct ModConst {
+    uint32_t m;      // modulus
+    uint32_t mu;     // floor(2^32 / m), Barrett
+    uint32_t h;      // (m - 1) / 2: residues are kept symmetric in [-h, m-1-h]
+    uint32_t c[4];   // 2^(21 j) mod m, j = 1..4 (21-bit limb weights)
+    uint32_t koff3;  // (h - 2^62 mod m) mod m: narrow limb offset (tk <= 62)
+    uint32_t koff5;  // (h - 2^104 mod m) mod m: wide limb offset
+    uint32_t kneg;   // (m - 2^31 mod m) mod m: undoes the +2^31 bias of a signed int32
+};
+
+void mod_constants(const Plan& p, ModConst* out);
+
+// CRT table: Sum_t r_t W_t - q M with q = rint(Sum_t r_t frac_t) (FP32 quotient estimate,
+// exact while |x| <= M/4; ref src/ozaki2_gpu.hpp:526-588)
+struct CrtConst {
+    int s, nl;
+    uint32_t W[kMaxModuli][kMaxLimbs];
+    uint32_t M[kMaxLimbs];
+    float frac[kMaxModuli];
+};
+void crt_constants(const Plan& p, CrtConst& out);
+
+}  // namespace oz2

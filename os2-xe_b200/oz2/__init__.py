@@ -1,0 +1,238 @@
+"""Python binding of liboz2.so, the B200-native Ozaki Scheme II FP64 GEMM emulator.
+
+Mirrors the reference's C++ class oz2::Ozaki2 (MacraMacra/OS2-Xe, src/ozaki2_gpu.hpp:678-1188):
+the same member names, argument meaning and error behaviour. Reference exceptions map to
+Python ones: std::invalid_argument -> ValueError, std::runtime_error -> RuntimeError
+(MemoryError when the workspace does not fit), std::overflow_error -> OverflowError.
+
+Matrices are column-major device buffers: a torch CUDA tensor (its data_ptr is used) or a raw
+integer device address. This module calls only the C ABI; it has no CPU fallback and raises
+ImportError when the library is missing.
+"""
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboz2.so")
+
+OK, EINVAL, ENOMEM, EINTERNAL, ETIMEOUT, EOVERFLOW, ECUDA = range(7)
+K_MAX_MODULI = 24
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"{LIB_PATH} is not built: run python os2-xe_b200/build.py")
+_lib = C.CDLL(LIB_PATH)
+
+_i64, _i32, _dbl, _vp, _chr, _sz = C.c_int64, C.c_int, C.c_double, C.c_void_p, C.c_char, C.c_size_t
+_lib.oz2_create.argtypes = [_vp, C.POINTER(_vp)]
+_lib.oz2_destroy.argtypes = [_vp]
+_lib.oz2_set_stream.argtypes = [_vp, _vp]
+_lib.oz2_dgemm.argtypes = [_vp, _chr, _chr, _i64, _i64, _i64, _dbl, _vp, _i64, _vp, _i64, _dbl, _vp, _i64, _i32,
+                           _vp, _i32, _vp]
+_lib.oz2_zgemm.argtypes = [_vp, _chr, _chr, _i64, _i64, _i64, _vp, _vp, _i64, _vp, _i64, _vp, _vp, _i64, _i32,
+                           _vp, _i32, _vp]
+_lib.oz2_precision_bits.argtypes = [_i64, _i32, C.POINTER(_i32)]
+_lib.oz2_precision_bits_complex.argtypes = [_i64, _i32, C.POINTER(_i32)]
+_lib.oz2_moduli_for_bits.argtypes = [_i64, _i32, C.POINTER(_i32)]
+_lib.oz2_set_workspace_limit.argtypes = [_vp, _sz]
+_lib.oz2_set_resident_hint.argtypes = [_vp, _sz]
+_lib.oz2_release_workspace.argtypes = [_vp]
+_lib.oz2_set_profiling.argtypes = [_vp, _i32]
+_lib.oz2_stage_times.argtypes = [_vp, C.POINTER(_dbl)]
+_lib.oz2_last_tiling.argtypes = [_vp, C.POINTER(_i64)]
+_lib.oz2_set_tuning.argtypes = [_vp, _i32, _i32, _i32]
+_lib.oz2_check_device_error.argtypes = [_vp]
+_lib.oz2_last_error.argtypes = [_vp]
+_lib.oz2_last_error.restype = C.c_char_p
+_lib.oz2_status_string.argtypes = [_i32]
+_lib.oz2_status_string.restype = C.c_char_p
+
+
+def lib():
+    """The loaded ctypes library (for callers that bind further entry points)."""
+    return _lib
+
+
+def _raise(status, handle=None):
+    if status == OK:
+        return
+    msg = (_lib.oz2_last_error(handle) or b"").decode() or _lib.oz2_status_string(status).decode()
+    if status == EINVAL:
+        raise ValueError(msg)
+    if status == EOVERFLOW:
+        raise OverflowError(msg)
+    if status == ENOMEM:
+        raise MemoryError(msg)
+    if status == ETIMEOUT:
+        raise TimeoutError(msg)
+    raise RuntimeError(msg)
+
+
+def _addr(x):
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    return x.data_ptr()
+
+
+def _op(t):
+    t = t.value if isinstance(t, Trans) else t
+    return t.encode() if isinstance(t, str) else t
+
+
+class Trans:
+    """op(X): N, T or C (conjugate transpose; equals T for gemm)."""
+
+    def __init__(self, value):
+        self.value = value
+
+
+Trans.N, Trans.T, Trans.C = Trans("N"), Trans("T"), Trans("C")
+
+
+@dataclass
+class StageTimes:
+    scale_ms: float = 0.0
+    split_ms: float = 0.0
+    gemm_ms: float = 0.0
+    crt_ms: float = 0.0
+
+    def total_ms(self):
+        return self.scale_ms + self.split_ms + self.gemm_ms + self.crt_ms
+
+
+@dataclass
+class TileInfo:
+    mb: int = 0
+    nb: int = 0
+    pm: int = 0
+    pn: int = 0
+    k_chunks: int = 0
+    workspace_bytes: int = 0
+
+
+@dataclass
+class Tuning:
+    batched_gemm: bool = True
+    pad_lda: bool = True
+    pow2_tiles: bool = True
+
+
+class Ozaki2:
+    """Binds to a CUDA stream (a torch.cuda.Stream, a raw cudaStream_t int, or None for the
+    current torch stream / the legacy default stream). Not thread-safe: one object per stream."""
+
+    def __init__(self, stream=None, profiling=False):
+        self._h = _vp()
+        _raise(_lib.oz2_create(self._stream_ptr(stream), C.byref(self._h)))
+        self._tuning = Tuning()
+        if profiling:
+            self.set_profiling(True)
+
+    @staticmethod
+    def _stream_ptr(stream):
+        if stream is None:
+            try:
+                import torch
+                if torch.cuda.is_available():
+                    return torch.cuda.current_stream().cuda_stream
+            except ImportError:
+                pass
+            return None
+        if isinstance(stream, int):
+            return stream
+        return stream.cuda_stream
+
+    def close(self):
+        if self._h:
+            _lib.oz2_destroy(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h.value
+
+    def set_stream(self, stream):
+        _raise(_lib.oz2_set_stream(self._h, self._stream_ptr(stream)), self._h)
+
+    # ---- static planning (ref src/ozaki2_gpu.hpp:689-700, :762)
+    @staticmethod
+    def precision_bits(k, num_moduli):
+        out = _i32()
+        _raise(_lib.oz2_precision_bits(k, num_moduli, C.byref(out)))
+        return out.value
+
+    @staticmethod
+    def precision_bits_complex(k, num_moduli):
+        out = _i32()
+        _raise(_lib.oz2_precision_bits_complex(k, num_moduli, C.byref(out)))
+        return out.value
+
+    @staticmethod
+    def moduli_for_bits(k, bits):
+        out = _i32()
+        _raise(_lib.oz2_moduli_for_bits(k, bits, C.byref(out)))
+        return out.value
+
+    # ---- workspace and tuning (ref :702-714)
+    def set_workspace_limit(self, nbytes):
+        _raise(_lib.oz2_set_workspace_limit(self._h, nbytes), self._h)
+
+    def set_resident_hint(self, nbytes):
+        _raise(_lib.oz2_set_resident_hint(self._h, nbytes), self._h)
+
+    def release_workspace(self):
+        _raise(_lib.oz2_release_workspace(self._h), self._h)
+
+    def set_tuning(self, t):
+        self._tuning = t
+        _raise(_lib.oz2_set_tuning(self._h, int(t.batched_gemm), int(t.pad_lda), int(t.pow2_tiles)), self._h)
+
+    def tuning(self):
+        return self._tuning
+
+    def set_profiling(self, on):
+        _raise(_lib.oz2_set_profiling(self._h, int(bool(on))), self._h)
+
+    def stage_times(self):
+        out = (_dbl * 4)()
+        _raise(_lib.oz2_stage_times(self._h, out), self._h)
+        return StageTimes(*list(out))
+
+    def last_tiling(self):
+        out = (_i64 * 6)()
+        _raise(_lib.oz2_last_tiling(self._h, out), self._h)
+        return TileInfo(*list(out))
+
+    def check_device_error(self):
+        _raise(_lib.oz2_check_device_error(self._h), self._h)
+
+    # ---- the products (ref :739-786)
+    @staticmethod
+    def _events(deps):
+        if not deps:
+            return None, 0
+        arr = (_vp * len(deps))(*[d.cuda_event if hasattr(d, "cuda_event") else d for d in deps])
+        return arr, len(deps)
+
+    def gemm(self, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C_, ldc, num_moduli, deps=None, done=None):
+        ev, nev = self._events(deps)
+        d = done.cuda_event if hasattr(done, "cuda_event") else done
+        _raise(_lib.oz2_dgemm(self._h, _op(ta), _op(tb), m, n, k, float(alpha), _addr(A), lda, _addr(B), ldb,
+                              float(beta), _addr(C_), ldc, num_moduli, ev, nev, d), self._h)
+
+    def zgemm(self, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C_, ldc, num_moduli, deps=None, done=None):
+        alpha, beta = complex(alpha), complex(beta)
+        al = (_dbl * 2)(alpha.real, alpha.imag)
+        be = (_dbl * 2)(beta.real, beta.imag)
+        ev, nev = self._events(deps)
+        d = done.cuda_event if hasattr(done, "cuda_event") else done
+        _raise(_lib.oz2_zgemm(self._h, _op(ta), _op(tb), m, n, k, al, _addr(A), lda, _addr(B), ldb, be, _addr(C_),
+                              ldc, num_moduli, ev, nev, d), self._h)

@@ -1,0 +1,70 @@
+"""The C ABI library on the CPU: it loads, exports every entry point the header declares, and
+its host-only planning entry points agree with the oracle. No kernel is launched here."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import pytest
+
+from common import ROOT
+
+HEADER = os.path.join(ROOT, "include", "oz2", "oz2.h")
+LIB = os.path.join(ROOT, "os2-xe_b200", "oz2", "liboz2.so")
+
+
+def declared():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"\b(oz2_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    assert os.path.exists(LIB), "liboz2.so is not built (python os2-xe_b200/build.py)"
+    lib = C.CDLL(LIB)
+    names = declared()
+    assert len(names) >= 18
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_planning_entry_points_match_oracle(oracle):
+    import oz2
+    for s in range(2, 25):
+        for k in [1, 7, 1024, 8192, 131071, 262144]:
+            try:
+                want = oracle.precision_bits(k, s)
+            except ValueError:
+                with pytest.raises(ValueError, match="too small"):
+                    oz2.Ozaki2.precision_bits(k, s)
+                continue
+            assert oz2.Ozaki2.precision_bits(k, s) == want
+            assert oz2.Ozaki2.precision_bits_complex(k, s) == oracle.precision_bits(2 * k, s)
+    for k in [1, 16, 1024, 2000, 8192, 131071, 300000]:
+        for b in [1, 20, 40, 53, 60, 80, 90, 101]:
+            assert oz2.Ozaki2.moduli_for_bits(k, b) == oracle.moduli_for_bits(k, b)
+    with pytest.raises(ValueError, match=r"num_moduli must be in \[2, 24\]"):
+        oz2.Ozaki2.precision_bits(100, 1)
+
+
+def test_null_handle_is_rejected():
+    import oz2
+    lib = oz2.lib()
+    assert lib.oz2_dgemm(None, b"N", b"N", 1, 1, 1, 1.0, None, 1, None, 1, 0.0, None, 1, 8, None, 0, None) == 1
+    assert b"null handle" in lib.oz2_last_error(None)
+    assert lib.oz2_status_string(4) == b"device-side wait timed out"
+
+
+def test_cpp_header_compiles():
+    """include/oz2/ozaki2.hpp (the reference's class over the C ABI) compiles and links"""
+    src = os.path.join(ROOT, "include", "oz2", "ozaki2.hpp")
+    prog = ('#include "oz2/ozaki2.hpp"\n'
+            "int main() { return oz2::Ozaki2::moduli_for_bits(1024, 53) == 15 ? 0 : 1; }\n")
+    exe = os.path.join(ROOT, "os2-xe_b200", "_build", "hdr_check")
+    os.makedirs(os.path.dirname(exe), exist_ok=True)
+    r = subprocess.run(["/usr/bin/g++", "-std=c++17", "-x", "c++", "-", "-I" + os.path.join(ROOT, "include"),
+                        "-I/usr/local/cuda/include", "-o", exe, "-x", "none", LIB,
+                        "-Wl,-rpath," + os.path.dirname(LIB)],
+                       input=prog, capture_output=True, text=True, timeout=120)
+    assert os.path.exists(src)
+    assert r.returncode == 0, r.stderr
+    assert subprocess.run([exe], timeout=60).returncode == 0
