@@ -31,7 +31,7 @@ UNIT = "TFLOP/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="oz2", choices=["oz2", "reference"])
     ap.add_argument("--size", type=int, default=8192)
