@@ -81,6 +81,17 @@ int oz2_set_tuning(oz2_handle h, int batched_gemm, int pad_lda, int pow2_tiles);
  * Synchronises the handle's stream, returns and clears the word. */
 int oz2_check_device_error(oz2_handle h);
 
+/* Emulated DGEMM for callers that cannot allocate device memory. No counterpart in the
+ * reference. Same arguments, checks and results as oz2_dgemm, but no handle: it works on the
+ * given stream and the current device and allocates nothing. Its scratch is a 64 MiB static
+ * device array of the library (held by every GPU that loads it until the process exits), so
+ * problems needing more scratch are rejected with OZ2_EINVAL (m = n = k = 1024 at 16 moduli
+ * fits). The first call on each device looks the array up and should come before any stream
+ * capture. All calls share the array: calls that overlap on the GPU race. */
+int oz2_dgemm_noalloc(void* stream, char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha,
+                      const double* A, int64_t lda, const double* B, int64_t ldb, double beta, double* C,
+                      int64_t ldc, int num_moduli);
+
 /* message of the last failed call on the handle (or of the last failed handle-less call) */
 const char* oz2_last_error(oz2_handle h);
 const char* oz2_status_string(int status);

@@ -329,6 +329,11 @@ int run(oz2_context* h, char ta, char tb, int64_t m, int64_t n, int64_t k, const
 
 }  // namespace
 
+namespace oz2 {
+// lets entry points without a handle report a message through oz2_last_error(NULL)
+void set_last_error(const std::string& msg) { g_error = msg; }
+}  // namespace oz2
+
 extern "C" {
 
 int oz2_create(void* stream, oz2_handle* out) {
