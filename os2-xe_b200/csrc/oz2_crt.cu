@@ -33,21 +33,31 @@ __device__ __forceinline__ int exponent_of(unsigned long long b, int tk) {
     return tk - e2;
 }
 
-// exact reconstruction + single rounding; r[t] in [0, m_t)
+// 2^E * d for d in [2^63, 2^64]: exponent arithmetic on the bits while the result stays normal
+// (exact), ldexp otherwise (overflow, or one rounding into the subnormal range)
+__device__ __forceinline__ double scale_pow2(double d, int E) {
+    if (E >= -1022 - 63 && E <= 1023 - 64)
+        return __longlong_as_double(__double_as_longlong(d) + (static_cast<long long>(E) << 52));
+    return ldexp(d, E);
+}
+
+// Exact reconstruction + single rounding; r[t] in [0, m_t).
+// q = round(Sum r_t y_t / m_t) from 24-bit fixed-point fractions F_t (error < 2^-12, far
+// below the 1/4 margin that |x| <= M/4 leaves, so q is the reference's FP32 quotient), then
+// x = Sum r_t W_t - q M modulo 2^(32 NL) in 64-bit words, rounded once to double.
 template <int S, int NL>
 __device__ __forceinline__ double crt_value(const uint32_t (&r)[S], const CrtConst& cc, int shift) {
-    float u = 0.0f;
+    uint64_t uf = 0;
     uint64_t acc[NL];
 #pragma unroll
     for (int l = 0; l < NL; ++l) acc[l] = 0;
 #pragma unroll
     for (int t = 0; t < S; ++t) {
-        u = __fmaf_rn(static_cast<float>(r[t]), cc.frac[t], u);
+        uf += static_cast<uint64_t>(r[t]) * cc.F[t];
 #pragma unroll
         for (int l = 0; l < NL; ++l) acc[l] += static_cast<uint64_t>(r[t]) * cc.W[t][l];
     }
-    const int64_t q = __float2int_rn(u);
-    // x = Sum r_t W_t - q M  modulo 2^(32 NL), as NL two's-complement words
+    const int64_t q = static_cast<int64_t>((uf + (1u << 23)) >> 24);
     uint32_t w[NL];
     int64_t carry = 0;
 #pragma unroll
@@ -56,37 +66,42 @@ __device__ __forceinline__ double crt_value(const uint32_t (&r)[S], const CrtCon
         w[l] = static_cast<uint32_t>(v);
         carry = v >> 32;
     }
-    const bool neg = static_cast<int32_t>(w[NL - 1]) < 0;
-    if (neg) {
-        uint32_t cy = 1;
+    // 64-bit words, two's complement -> sign and magnitude
+    constexpr int NW = (NL + 1) / 2;
+    uint64_t X[NW];
 #pragma unroll
-        for (int l = 0; l < NL; ++l) {
-            const uint32_t nw = ~w[l] + cy;
-            cy = (cy && nw == 0) ? 1u : 0u;
-            w[l] = nw;
+    for (int i = 0; i < NW; ++i)
+        X[i] = static_cast<uint64_t>(w[2 * i]) | (2 * i + 1 < NL ? static_cast<uint64_t>(w[2 * i + 1]) << 32 : 0);
+    if (NL % 2)  // odd word count: sign-extend the top word into the last 64-bit word
+        X[NW - 1] = static_cast<uint64_t>(static_cast<int64_t>(static_cast<int32_t>(w[NL - 1])));
+    const bool neg = static_cast<int64_t>(X[NW - 1]) < 0;
+    if (neg) {
+        uint64_t borrow = 1;
+#pragma unroll
+        for (int i = 0; i < NW; ++i) {
+            const uint64_t nv = ~X[i] + borrow;
+            borrow = (borrow && nv == 0) ? 1 : 0;
+            X[i] = nv;
         }
     }
+    // leading 64 bits with a sticky bit for everything below
+    uint64_t hiw = 0, low = 0;
+    bool sticky = false;
     int tw = -1;
 #pragma unroll
-    for (int l = 0; l < NL; ++l)
-        if (w[l]) tw = l;
+    for (int i = NW - 1; i >= 0; --i)
+        if (tw < 0 && X[i]) tw = i;
     if (tw < 0) return 0.0;
-    // the 64 bits below the leading one, with everything further down folded into a sticky bit
-    uint32_t a = 0, b = 0, c = 0;
-    bool sticky = false;
 #pragma unroll
-    for (int l = 0; l < NL; ++l) {
-        if (l == tw) a = w[l];
-        else if (l == tw - 1) b = w[l];
-        else if (l == tw - 2) c = w[l];
-        else if (l < tw - 2) sticky |= w[l] != 0;
+    for (int i = 0; i < NW; ++i) {
+        if (i == tw) hiw = X[i];
+        else if (i == tw - 1) low = X[i];
+        else if (i < tw - 1) sticky |= X[i] != 0;
     }
-    const int z = __clz(a);
-    const uint64_t hi = (static_cast<uint64_t>(a) << 32) | b;
-    uint64_t top = z ? (hi << z) | (c >> (32 - z)) : hi;
-    sticky |= (z ? (c << z) : c) != 0;
-    top |= sticky ? 1u : 0u;
-    const double val = ldexp(__ull2double_rn(top), 32 * tw - 32 - z - shift);
+    const int z = __clzll(static_cast<long long>(hiw));
+    const uint64_t top = z ? (hiw << z) | (low >> (64 - z)) : hiw;
+    sticky |= (z ? (low << z) : low) != 0;
+    const double val = scale_pow2(__ull2double_rn(top | (sticky ? 1u : 0u)), 64 * tw - z - shift);
     return neg ? -val : val;
 }
 
@@ -100,48 +115,49 @@ __global__ void __launch_bounds__(256) crt_kernel(const __grid_constant__ CrtPar
     constexpr int NL = limbs_for(S);
     const int64_t i0 = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) * 4;
     if (i0 >= P.m) return;
-    int De[4];
-#pragma unroll
-    for (int e = 0; e < 4; ++e) De[e] = i0 + e < P.m ? exponent_of(P.maxA[i0 + e], P.tk) : 0;
     for (int64_t j = blockIdx.y; j < P.n; j += gridDim.y) {
         const int Ej = exponent_of(P.maxB[j], P.tk);
         const uint8_t* base = P.resid + j * P.ldr + i0;
-        uint32_t rr[4][S], ri[4][S];
+        // one 32-bit word per plane = the residues of the 4 entries i0..i0+3
+        uint32_t w0[S], w1[CPLX ? S : 1], w2[CPLX ? S : 1];
 #pragma unroll
         for (int t = 0; t < S; ++t) {
-            const uint32_t w0 = __ldg(reinterpret_cast<const uint32_t*>(base + t * P.rstride));
-            if (!CPLX) {
-#pragma unroll
-                for (int e = 0; e < 4; ++e) rr[e][t] = (w0 >> (8 * e)) & 0xFFu;
-            } else {
-                const uint32_t w1 = __ldg(reinterpret_cast<const uint32_t*>(base + P.gstride + t * P.rstride));
-                const uint32_t w2 = __ldg(reinterpret_cast<const uint32_t*>(base + 2 * P.gstride + t * P.rstride));
-                const uint32_t m = P.mod_m[t];
-#pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    const uint32_t p0 = (w0 >> (8 * e)) & 0xFFu, p1 = (w1 >> (8 * e)) & 0xFFu;
-                    const uint32_t p2 = (w2 >> (8 * e)) & 0xFFu;
-                    rr[e][t] = sub_mod(p0, p1, m);                  // Re = P0 - P1
-                    ri[e][t] = sub_mod(sub_mod(p2, p0, m), p1, m);  // Im = P2 - P0 - P1
-                }
+            w0[t] = __ldg(reinterpret_cast<const uint32_t*>(base + t * P.rstride));
+            if (CPLX) {
+                w1[t] = __ldg(reinterpret_cast<const uint32_t*>(base + P.gstride + t * P.rstride));
+                w2[t] = __ldg(reinterpret_cast<const uint32_t*>(base + 2 * P.gstride + t * P.rstride));
             }
         }
-#pragma unroll
+#pragma unroll 1
         for (int e = 0; e < 4; ++e) {
             const int64_t i = i0 + e;
             if (i >= P.m) break;
-            const bool nonfinite = De[e] == kNonFinite || Ej == kNonFinite;
-            const int shift = nonfinite ? 0 : De[e] + Ej;
+            const int De = exponent_of(P.maxA[i], P.tk);
+            const bool nonfinite = De == kNonFinite || Ej == kNonFinite;
+            const int shift = nonfinite ? 0 : De + Ej;
+            const uint32_t sel = 0x4440 + e;  // byte e of a word, zero-extended
             double* cp = P.C + (CPLX ? 2 : 1) * (i + j * P.ldc);
             if (!CPLX) {
-                double v = crt_value<S, NL>(rr[e], P.cc, shift);
+                uint32_t r[S];
+#pragma unroll
+                for (int t = 0; t < S; ++t) r[t] = __byte_perm(w0[t], 0, sel);
+                double v = crt_value<S, NL>(r, P.cc, shift);
                 if (nonfinite) v = __longlong_as_double(0x7FF8000000000000ll);
                 // the reference's unfused alpha*v + beta*c, one rounding per operation
                 const double av = __dmul_rn(P.ar, v);
                 cp[0] = P.br == 0.0 ? av : __dadd_rn(av, __dmul_rn(P.br, cp[0]));
             } else {
-                double vr = crt_value<S, NL>(rr[e], P.cc, shift);
-                double vi = crt_value<S, NL>(ri[e], P.cc, shift);
+                uint32_t rr[S], ri[S];
+#pragma unroll
+                for (int t = 0; t < S; ++t) {
+                    const uint32_t m = P.mod_m[t];
+                    const uint32_t p0 = __byte_perm(w0[t], 0, sel), p1 = __byte_perm(w1[t], 0, sel);
+                    const uint32_t p2 = __byte_perm(w2[t], 0, sel);
+                    rr[t] = sub_mod(p0, p1, m);                  // Re = P0 - P1
+                    ri[t] = sub_mod(sub_mod(p2, p0, m), p1, m);  // Im = P2 - P0 - P1
+                }
+                double vr = crt_value<S, NL>(rr, P.cc, shift);
+                double vi = crt_value<S, NL>(ri, P.cc, shift);
                 if (nonfinite) vr = vi = __longlong_as_double(0x7FF8000000000000ll);
                 double orr = __dsub_rn(__dmul_rn(P.ar, vr), __dmul_rn(P.ai, vi));
                 double oi = __dadd_rn(__dmul_rn(P.ar, vi), __dmul_rn(P.ai, vr));

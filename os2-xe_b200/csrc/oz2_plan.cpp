@@ -164,7 +164,7 @@ void crt_constants(const Plan& p, CrtConst& out) {
     out.nl = p.nl;
     for (int t = 0; t < p.s; ++t) {
         for (int l = 0; l < p.nl; ++l) out.W[t][l] = p.W[t][l];
-        out.frac[t] = static_cast<float>(static_cast<double>(p.y[t]) / p.m[t]);
+        out.F[t] = static_cast<uint32_t>(((static_cast<uint64_t>(p.y[t]) << 24) + p.m[t] / 2) / p.m[t]);
     }
     for (int l = 0; l < p.nl; ++l) out.M[l] = p.M[l];
 }

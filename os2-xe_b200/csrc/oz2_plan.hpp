@@ -55,13 +55,13 @@ struct ModConst {
 
 void mod_constants(const Plan& p, ModConst* out);
 
-// CRT table: Sum_t r_t W_t - q M with q = rint(Sum_t r_t frac_t) (FP32 quotient estimate,
-// exact while |x| <= M/4; ref src/ozaki2_gpu.hpp:526-588)
+// CRT table: Sum_t r_t W_t - q M with q = round(Sum_t r_t y_t / m_t) from an estimate whose
+// error is far below 1/4 (ref src/ozaki2_gpu.hpp:526-588 uses FP32; here 24-bit fixed point)
 struct CrtConst {
     int s, nl;
     uint32_t W[kMaxModuli][kMaxLimbs];
     uint32_t M[kMaxLimbs];
-    float frac[kMaxModuli];
+    uint32_t F[kMaxModuli];  // round(y_t / m_t * 2^24): fixed-point quotient weights
 };
 void crt_constants(const Plan& p, CrtConst& out);
 

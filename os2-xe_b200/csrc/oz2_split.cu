@@ -127,6 +127,23 @@ __device__ __forceinline__ void offset_limbs(double v, int e, uint32_t (&L)[NLIM
     }
 }
 
+// 2^k as a double for k in [-1022, 1023]
+__device__ __forceinline__ double pow2(int k) {
+    return __longlong_as_double(static_cast<long long>(k + 1023) << 52);
+}
+
+// Narrow path (tk <= 62) in floating point: y = v 2^e as two exact power-of-two products
+// (e = e1 + e2 keeps both factors normal for every e this path produces; a product that
+// underflows means |y| < 2^-1022, which rounds to 0 like the exact value), then one
+// round-to-nearest-even conversion to int64: the same integer as the bit-level RNE above.
+__device__ __forceinline__ void offset_limbs_fp(double v, double s1, double s2, uint32_t (&L)[3]) {
+    const long long x = __double2ll_rn((v * s1) * s2);
+    const uint64_t xo = static_cast<uint64_t>(x + (1ll << 62));
+    L[0] = static_cast<uint32_t>(xo) & kMask21;
+    L[1] = static_cast<uint32_t>(xo >> 21) & kMask21;
+    L[2] = static_cast<uint32_t>(xo >> 42) & kMask21;
+}
+
 // symmetric residue of the value whose offset limbs are L, as an int in [-h, m-1-h]
 template <int NLIMB>
 __device__ __forceinline__ int sym_residue(const uint32_t (&L)[NLIMB], const ModConst& c) {
@@ -137,6 +154,11 @@ __device__ __forceinline__ int sym_residue(const uint32_t (&L)[NLIMB], const Mod
     uint32_t r = v - q * c.m;
     r = min(r, r - c.m);
     return static_cast<int>(r) - static_cast<int>(c.h);
+}
+
+// low bytes of a, b, c, d as one little-endian word
+__device__ __forceinline__ uint32_t pack_bytes(uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+    return __byte_perm(__byte_perm(a, b, 0x0040), __byte_perm(c, d, 0x0040), 0x5410);
 }
 
 // Each thread: one plane row r and 16 consecutive inner indices k0..k0+15, i.e. one 16-byte
@@ -159,6 +181,8 @@ __global__ void __launch_bounds__(256) split_kernel(const __grid_constant__ Spli
 
     constexpr int NG = CPLX ? 2 : 1;
     uint32_t L[NG][16][NLIMB];
+    const int e1 = e >> 1;
+    const double s1 = pow2(live ? e1 : 0), s2 = pow2(live ? e - e1 : 0);
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
         const int64_t p = k0 + q;
@@ -173,8 +197,13 @@ __global__ void __launch_bounds__(256) split_kernel(const __grid_constant__ Spli
                 v0 = __ldg(P.X + idx);
             }
         }
-        offset_limbs<NLIMB>(v0, e, L[0][q]);
-        if (CPLX) offset_limbs<NLIMB>(v1, e, L[NG - 1][q]);
+        if constexpr (NLIMB == 3) {
+            offset_limbs_fp(v0, s1, s2, L[0][q]);
+            if (CPLX) offset_limbs_fp(v1, s1, s2, L[NG - 1][q]);
+        } else {
+            offset_limbs<NLIMB>(v0, e, L[0][q]);
+            if (CPLX) offset_limbs<NLIMB>(v1, e, L[NG - 1][q]);
+        }
     }
 
     const int64_t rb = r >> 7;
@@ -186,19 +215,40 @@ __global__ void __launch_bounds__(256) split_kernel(const __grid_constant__ Spli
 
     for (int t = 0; t < P.s; ++t) {
         const ModConst mc = P.mc[t];
-        uint32_t w0[4] = {0, 0, 0, 0}, w1[4] = {0, 0, 0, 0}, w2[4] = {0, 0, 0, 0};
+        uint32_t b0[16], b1[16], b2[16];  // residue bytes in the low 8 bits
+        if (mc.m == 256) {
+            // 2^21 j = 0 mod 256 and 2^62 = 0 mod 256: the residue byte is the low byte of 2^62 + x
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-            const int s0 = sym_residue<NLIMB>(L[0][q], mc);
-            w0[q >> 2] |= (static_cast<uint32_t>(s0) & 0xFFu) << (8 * (q & 3));
+            for (int q = 0; q < 16; ++q) {
+                b0[q] = L[0][q][0];
+                if (CPLX) {
+                    b1[q] = L[NG - 1][q][0];
+                    b2[q] = b0[q] + b1[q];
+                }
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                const int s0 = sym_residue<NLIMB>(L[0][q], mc);
+                b0[q] = static_cast<uint32_t>(s0);
+                if (CPLX) {
+                    const int s1 = sym_residue<NLIMB>(L[NG - 1][q], mc);
+                    const int m = static_cast<int>(mc.m), h = static_cast<int>(mc.h);
+                    int ss = s0 + s1;
+                    ss = ss > m - 1 - h ? ss - m : ss;
+                    ss = ss < -h ? ss + m : ss;
+                    b1[q] = static_cast<uint32_t>(s1);
+                    b2[q] = static_cast<uint32_t>(ss);
+                }
+            }
+        }
+        uint32_t w0[4], w1[4], w2[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            w0[q] = pack_bytes(b0[4 * q], b0[4 * q + 1], b0[4 * q + 2], b0[4 * q + 3]);
             if (CPLX) {
-                const int s1 = sym_residue<NLIMB>(L[NG - 1][q], mc);
-                const int m = static_cast<int>(mc.m), h = static_cast<int>(mc.h);
-                int ss = s0 + s1;
-                ss = ss > m - 1 - h ? ss - m : ss;
-                ss = ss < -h ? ss + m : ss;
-                w1[q >> 2] |= (static_cast<uint32_t>(s1) & 0xFFu) << (8 * (q & 3));
-                w2[q >> 2] |= (static_cast<uint32_t>(ss) & 0xFFu) << (8 * (q & 3));
+                w1[q] = pack_bytes(b1[4 * q], b1[4 * q + 1], b1[4 * q + 2], b1[4 * q + 3]);
+                w2[q] = pack_bytes(b2[4 * q], b2[4 * q + 1], b2[4 * q + 2], b2[4 * q + 3]);
             }
         }
         *reinterpret_cast<uint4*>(out + t * P.plane_bytes) = make_uint4(w0[0], w0[1], w0[2], w0[3]);
