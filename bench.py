@@ -151,6 +151,56 @@ def launches_per_call(t):
     return 2 + t.pn + (tiles if t.pm > 1 else 1) + tiles * t.k_chunks + tiles
 
 
+def grouped_leg(oz2, torch, dev, stream, reps=5):
+    """512 DGEMMs, m, n, k log-uniform in [32, 2048], ops uniform over NN/NT/TN/TT, s uniform in
+    14..20, U[-1,1): one grouped call (autotuned GEMM configuration, replayed from a CUDA graph)
+    against 512 sequential calls of the same problems. FP64-equivalent TFLOP/s = sum 2 m n k / t."""
+    import math
+    import random
+    rnd = random.Random(2024)
+    g = torch.Generator(device=dev)
+    g.manual_seed(77)
+    probs, flops = [], 0.0
+    for _ in range(512):
+        m, n, k = (int(math.exp(rnd.uniform(math.log(32), math.log(2048)))) for _ in range(3))
+        ta, tb = rnd.choice("NT"), rnd.choice("NT")
+        s = rnd.randint(14, 20)
+        lda, ldb = (m if ta == "N" else k), (k if tb == "N" else n)
+        A = torch.rand(m * k, dtype=torch.float64, device=dev, generator=g) * 2 - 1
+        B = torch.rand(k * n, dtype=torch.float64, device=dev, generator=g) * 2 - 1
+        C = torch.zeros(m * n, dtype=torch.float64, device=dev)
+        probs.append((ta, tb, m, n, k, 1.0, A, lda, B, ldb, 0.0, C, m, s))
+        flops += 2.0 * m * n * k
+    oz = oz2.Ozaki2(stream)
+    cfg = oz.autotune_grouped(probs)
+    oz.set_graph_mode(True)
+    oz.gemm_grouped(probs)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        oz.gemm_grouped(probs)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_grouped = e0.elapsed_time(e1) / reps
+    for p in probs:
+        oz.gemm(*p)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        for p in probs:
+            oz.gemm(*p)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_seq = e0.elapsed_time(e1) / reps
+    oz.check_device_error()
+    oz.close()
+    return {"workload": "512 dgemm, m,n,k log-uniform [32,2048], ops uniform NN/NT/TN/TT, s uniform 14..20, "
+                        "U[-1,1)", "grouped_tflops": flops / (t_grouped * 1e-3) / 1e12, "grouped_ms": t_grouped,
+            "sequential_tflops": flops / (t_seq * 1e-3) / 1e12, "sequential_ms": t_seq,
+            "speedup": t_seq / t_grouped, "gemm_config": cfg, "graph": True}
+
+
 def peaks():
     try:
         return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -307,6 +357,7 @@ def main():
         except Exception as e:  # noqa: BLE001
             extras["cublaslt_int8_tops"] = f"unavailable: {type(e).__name__}"
         line["vs_cublas_dgemm"] = value / world / extras["cublas_dgemm_tflops"]
+        extras["grouped_c4"] = grouped_leg(oz2, torch, dev, stream)
         if rank == 0:
             line["cpu_baseline"] = {k2: v for k2, v in cpu_sample(a, 1, 0).items() if k2 != "seconds_per_step"}
     line["extras"] = extras

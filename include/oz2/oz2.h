@@ -52,6 +52,40 @@ int oz2_zgemm(oz2_handle h, char ta, char tb, int64_t m, int64_t n, int64_t k, c
               const double* A, int64_t lda, const double* B, int64_t ldb, const double* beta, double* C,
               int64_t ldc, int num_moduli, void* const* deps, int ndeps, void* done);
 
+/* One problem of a grouped call: C = alpha op(A) op(B) + beta C (real). */
+typedef struct {
+    char ta, tb;     /* 'N', 'T' or 'C' */
+    int num_moduli;  /* s in [2, 24], per problem */
+    int64_t m, n, k;
+    double alpha, beta;
+    const double* A;
+    int64_t lda;
+    const double* B;
+    int64_t ldb;
+    double* C;
+    int64_t ldc;
+} oz2_dgemm_problem;
+
+/* Many independent emulated DGEMMs of uneven m, n, k, ops and s in one set of launches: one
+ * grouped scale and split per kernel variant, one persistent tcgen05 GEMM over every
+ * (problem, modulus, tile) job, one CRT per distinct s. No counterpart in the reference
+ * (equivalent to `count` calls of Ozaki2::gemm, src/ozaki2_gpu.hpp:739-760, with the same
+ * results bit for bit). Arguments are checked for every problem before anything runs; C
+ * blocks must not overlap. */
+int oz2_dgemm_grouped(oz2_handle h, int count, const oz2_dgemm_problem* problems, void* const* deps, int ndeps,
+                      void* done);
+/* Grouped calls are captured in a CUDA graph on first use and replayed when the same problem
+ * list (shapes, pointers, scalars) comes again; the workspace must not grow in between. */
+int oz2_set_graph_mode(oz2_handle h, int enable);
+/* GEMM kernel configuration: tile width along the rows of C (bn = 128 or 256), raster group of
+ * column tiles (group_j), persistent CTAs (ctas, 0 = one per SM); bn = 0 returns to the
+ * autotuned / heuristic choice. get returns the configuration of the last call. */
+int oz2_set_gemm_config(oz2_handle h, int bn, int group_j, int ctas);
+int oz2_get_gemm_config(oz2_handle h, int* out3);
+/* Times the candidate configurations on these problems (C is overwritten), remembers the
+ * fastest for problem lists of the same shapes and returns it in out3 (may be NULL). */
+int oz2_autotune_grouped(oz2_handle h, int count, const oz2_dgemm_problem* problems, int* out3);
+
 /* Ozaki2::precision_bits / precision_bits_complex / moduli_for_bits: src/ozaki2_gpu.hpp:689-700, :762 */
 int oz2_precision_bits(int64_t k, int num_moduli, int* out);
 int oz2_precision_bits_complex(int64_t k, int num_moduli, int* out);

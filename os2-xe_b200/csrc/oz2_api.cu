@@ -1,16 +1,21 @@
-// oz2_api.cu - the C ABI of liboz2.so (include/oz2/oz2.h) and the host orchestration of one
-// emulated GEMM: argument checks, plan cache, tiling and workspace, then the phases
-// scale -> split -> INT8 GEMM (+mod m) -> CRT on the handle's stream.
-// Mirrors the reference's class oz2::Ozaki2 (src/ozaki2_gpu.hpp:678-1188); the internals are
-// new: pre-tiled planes, tcgen05 products with residues fused, 1-byte residue planes.
+// oz2_api.cu - the C ABI of liboz2.so (include/oz2/oz2.h) and the host orchestration of the
+// emulated GEMMs: argument checks, plan cache, tiling and workspace, descriptor tables, then
+// the phases scale -> split -> INT8 GEMM (+mod m) -> CRT on the handle's stream.
+// Mirrors the reference's class oz2::Ozaki2 (src/ozaki2_gpu.hpp:678-1188) for single calls and
+// adds a grouped call (many independent DGEMMs in one set of launches, optionally replayed
+// from a CUDA graph) with a GEMM-configuration autotuner; the reference has neither.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <map>
+#include <memory>
 #include <string>
+#include <tuple>
 #include <utility>
 #include <vector>
 
@@ -23,6 +28,51 @@ using namespace oz2;
 namespace {
 enum Stage { kBegin = 0, kScale = 1, kSplit = 2, kGemm = 3, kCrt = 4 };
 thread_local std::string g_error;  // errors of calls without a usable handle
+constexpr int kRing = 4;
+
+// ---------------------------------------------------------------- launch program of one call
+// A call is planned on the host into a descriptor blob and a list of operations, then issued
+// on the stream (or captured into a CUDA graph and replayed).
+struct Op {
+    enum Kind { Memset, Scale, Split, Gemm, Crt, ScaleC, Mark } kind;
+    size_t off = 0;    // descriptor offset in the blob
+    int count = 0;     // items
+    int64_t blocks = 0;
+    void* ptr = nullptr;
+    size_t bytes = 0;  // memset
+    const Plan* plan = nullptr;
+    bool cplx = false;
+    GemmConfig cfg;
+    int64_t jobs = 0;
+    int64_t m = 0, n = 0, ldc = 0;  // scale_c
+    double beta[2] = {0, 0};
+    int stage = 0;
+};
+
+struct Program {
+    std::vector<unsigned char> blob;
+    std::vector<Op> ops;
+    size_t add(const void* p, size_t bytes) {
+        const size_t off = (blob.size() + 255) & ~size_t{255};
+        blob.resize(off + bytes);
+        std::memcpy(blob.data() + off, p, bytes);
+        return off;
+    }
+    size_t reserve(size_t bytes) {
+        const size_t off = (blob.size() + 255) & ~size_t{255};
+        blob.resize(off + bytes);
+        return off;
+    }
+};
+
+// one grouped call captured for replay: an executable graph per batch of problems, the device
+// copy of their descriptor tables, and the problem list it was built from
+struct GraphEntry {
+    std::vector<cudaGraphExec_t> execs;
+    std::vector<void*> dev_blobs;
+    std::vector<unsigned char> problems;
+};
+
 }  // namespace
 
 struct oz2_context {
@@ -32,15 +82,33 @@ struct oz2_context {
     size_t ws_limit = 0, resident_hint = 0;
     uint8_t* ws = nullptr;
     size_t ws_size = 0;
+    uint64_t ws_gen = 0;
     int* d_err = nullptr;
-    Plan plan;
-    int64_t plan_k = -1;
+    std::map<std::pair<int, int64_t>, std::unique_ptr<Plan>> plans;
     int64_t tiling[6] = {0, 0, 0, 0, 0, 0};
     int tuning[3] = {1, 1, 1};
     bool profiling = false;
     std::vector<std::pair<int, cudaEvent_t>> marks;
     std::vector<cudaEvent_t> pool;
     size_t pool_used = 0;
+    // pinned staging ring for large descriptor blobs
+    void* ring_host[kRing] = {};
+    size_t ring_cap[kRing] = {};
+    cudaEvent_t ring_ev[kRing] = {};
+    bool ring_used[kRing] = {};
+    int ring_next = 0;
+    // GEMM configuration: forced by the caller, tuned per problem-set shape, last used
+    GemmConfig forced;
+    bool has_forced = false;
+    std::map<std::string, GemmConfig> tuned;
+    GemmConfig last_cfg;
+    // CUDA graphs of grouped calls, captured on a private stream (the caller's stream may be
+    // the legacy default stream, which cannot be captured) and launched on the caller's stream
+    bool graph_mode = false;
+    cudaStream_t cap_stream = nullptr;
+    std::map<uint64_t, GraphEntry> graphs;
+    GraphEntry* capturing = nullptr;  // entry being filled by the current grouped call
+    bool capture_ok = true;           // false when part of the call ran outside the graphs
     std::string err;
 };
 
@@ -54,15 +122,16 @@ int fail(oz2_context* h, int status, const std::string& msg) {
 int cuda_fail(oz2_context* h, cudaError_t e, const char* where) {
     return fail(h, OZ2_ECUDA, std::string("oz2: ") + where + ": " + cudaGetErrorString(e));
 }
-#define OZ2_CUDA(h, call)                                     \
-    do {                                                      \
-        cudaError_t e_ = (call);                              \
+#define OZ2_CUDA(h, call)                                      \
+    do {                                                       \
+        cudaError_t e_ = (call);                               \
         if (e_ != cudaSuccess) return cuda_fail(h, e_, #call); \
     } while (0)
 
 bool op_ok(char t) { return t == 'N' || t == 'n' || t == 'T' || t == 't' || t == 'C' || t == 'c'; }
 bool is_n(char t) { return t == 'N' || t == 'n'; }
 bool is_c(char t) { return t == 'C' || t == 'c'; }
+size_t align256(size_t v) { return (v + 255) & ~size_t{255}; }
 
 void mark(oz2_context* h, int stage) {
     if (!h->profiling) return;
@@ -101,52 +170,24 @@ int end_call(oz2_context* h, void* done) {
     return OZ2_OK;
 }
 
-int ensure_plan(oz2_context* h, int s, int64_t k) {
-    if (h->plan.s == s && h->plan_k == k) return OZ2_OK;
-    Plan p;
-    const int st = make_plan(s, k, p);
+// plans are cached per (s, k); k is the plan's inner length (2k for complex)
+int get_plan(oz2_context* h, int s, int64_t k, const Plan** out) {
+    auto key = std::make_pair(s, k);
+    auto it = h->plans.find(key);
+    if (it != h->plans.end()) {
+        *out = it->second.get();
+        return OZ2_OK;
+    }
+    auto p = std::make_unique<Plan>();
+    const int st = make_plan(s, k, *p);
     if (st) {
         char buf[160];
         plan_error_text(s, k, st, buf, sizeof buf);
         return fail(h, st == 5 ? OZ2_EOVERFLOW : (st == 1 ? OZ2_EINVAL : OZ2_EINTERNAL), buf);
     }
-    h->plan = p;
-    h->plan_k = k;
+    *out = p.get();
+    h->plans.emplace(key, std::move(p));
     return OZ2_OK;
-}
-
-// ---------------------------------------------------------------- tiling / workspace
-struct Layout {
-    int64_t mb, nb, pm, pn, kchunks;
-    size_t bytes;
-    size_t o_maxA, o_maxB, o_A, o_B, o_R;
-};
-
-size_t align256(size_t v) { return (v + 255) & ~size_t{255}; }
-
-Layout layout_for(int64_t m, int64_t n, int64_t k, int s, int G, int64_t mb, int64_t nb) {
-    Layout L{};
-    L.mb = mb;
-    L.nb = nb;
-    L.pm = ceil_div(m, mb);
-    L.pn = ceil_div(n, nb);
-    const int64_t kb = ceil_div(k, kTileK);
-    L.kchunks = ceil_div(kb, kChunkKB);
-    const PlaneGeom ga = plane_geom(mb, k, kGemmI), gb = plane_geom(nb, k, kGemmJ);
-    const int64_t ldr = round_up(mb, 32);
-    size_t off = 0;
-    auto carve = [&](size_t bytes) {
-        const size_t o = off;
-        off = align256(off + bytes);
-        return o;
-    };
-    L.o_maxA = carve(static_cast<size_t>(m) * 8);
-    L.o_maxB = carve(static_cast<size_t>(n) * 8);
-    L.o_A = carve(static_cast<size_t>(G) * s * ga.plane_bytes);
-    L.o_B = carve(static_cast<size_t>(G) * s * gb.plane_bytes);
-    L.o_R = carve(static_cast<size_t>(G) * s * nb * ldr);
-    L.bytes = off;
-    return L;
 }
 
 size_t budget(oz2_context* h) {
@@ -161,6 +202,357 @@ size_t budget(oz2_context* h) {
     return lim;
 }
 
+void drop_graphs(oz2_context* h) {
+    for (auto& kv : h->graphs) {
+        for (auto e : kv.second.execs) cudaGraphExecDestroy(e);
+        for (auto b : kv.second.dev_blobs) cudaFree(b);
+    }
+    h->graphs.clear();
+    h->capturing = nullptr;
+}
+
+int ensure_workspace(oz2_context* h, size_t bytes) {
+    if (h->ws_size >= bytes) return OZ2_OK;
+    OZ2_CUDA(h, cudaStreamSynchronize(h->stream));
+    drop_graphs(h);
+    if (h->ws) cudaFree(h->ws);
+    h->ws = nullptr;
+    h->ws_size = 0;
+    ++h->ws_gen;
+    if (cudaMalloc(&h->ws, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        h->ws = nullptr;
+        return fail(h, OZ2_ENOMEM, "oz2: workspace allocation failed");
+    }
+    h->ws_size = bytes;
+    return OZ2_OK;
+}
+
+// ---------------------------------------------------------------- problem -> tasks -> program
+struct Prob {  // one validated problem with m, n, k > 0 and alpha != 0
+    char ta, tb;
+    int64_t m, n, k;
+    double alpha[2], beta[2];
+    const double* A;
+    int64_t lda;
+    const double* B;
+    int64_t ldb;
+    double* C;
+    int64_t ldc;
+    int G;  // 1 real, 3 complex (3M)
+    const Plan* plan;
+};
+
+// bytes of one problem (or one C tile of mb x nb) in the workspace
+struct Sizes {
+    size_t maxA, maxB, planesA, planesB, resid;
+    size_t total() const { return align256(maxA) + align256(maxB) + align256(planesA) + align256(planesB) + align256(resid); }
+};
+Sizes sizes_for(int64_t m, int64_t n, int64_t k, int s, int G, int64_t mb, int64_t nb) {
+    Sizes z;
+    z.maxA = static_cast<size_t>(m) * 8;
+    z.maxB = static_cast<size_t>(n) * 8;
+    z.planesA = static_cast<size_t>(G) * s * plane_geom(mb, k, kGemmIPad).plane_bytes;
+    z.planesB = static_cast<size_t>(G) * s * plane_geom(nb, k, kGemmJ).plane_bytes;
+    z.resid = static_cast<size_t>(G) * s * nb * round_up(mb, 32);
+    return z;
+}
+
+SplitItem side_item(const Prob& p, bool a_side, int64_t r0, int64_t rows, unsigned long long* maxbits,
+                    int8_t* planes, const ModConst* mc) {
+    SplitItem it{};
+    const bool cplx = p.G == 3;
+    const int w = cplx ? 2 : 1;
+    if (a_side) {
+        it.row_contig = is_n(p.ta);
+        it.X = p.A + w * (it.row_contig ? r0 : r0 * p.lda);
+        it.ldx = p.lda;
+        it.conj = cplx && is_c(p.ta);
+        it.rows_pad = plane_geom(rows, p.k, kGemmIPad).rows_pad;
+    } else {
+        it.row_contig = !is_n(p.tb);
+        it.X = p.B + w * (it.row_contig ? r0 : r0 * p.ldb);
+        it.ldx = p.ldb;
+        it.conj = cplx && is_c(p.tb);
+        it.rows_pad = plane_geom(rows, p.k, kGemmJ).rows_pad;
+    }
+    it.rows = rows;
+    it.k = p.k;
+    it.cplx = cplx;
+    it.tk = p.plan->tk;
+    it.s = p.plan->s;
+    it.maxbits = maxbits + r0;
+    it.planes = planes;
+    it.kb_total = ceil_div(p.k, kTileK);
+    it.plane_bytes = it.rows_pad * it.kb_total * kTileK;
+    for (int t = 0; t < it.s; ++t) it.mc[t] = mc[t];
+    return it;
+}
+
+ScaleItem scale_item(const Prob& p, bool a_side, unsigned long long* out) {
+    ScaleItem it{};
+    const bool cplx = p.G == 3;
+    it.X = a_side ? p.A : p.B;
+    it.ldx = a_side ? p.lda : p.ldb;
+    it.rows = a_side ? p.m : p.n;
+    it.k = p.k;
+    it.row_contig = a_side ? is_n(p.ta) : !is_n(p.tb);
+    it.cplx = cplx;
+    it.out = out;
+    return it;
+}
+
+// one GEMM + CRT unit: C rows [i0, i0+mb) x columns [j0, j0+nb) of a problem
+struct Task {
+    const Prob* p;
+    int64_t i0, j0, mb, nb;
+    bool split_a, split_b;
+    unsigned long long *maxA, *maxB;  // of the whole problem
+    int8_t *planesA, *planesB;
+    uint8_t* resid;
+    int64_t ldr;
+};
+
+template <class Item>
+void add_grouped(Program& prog, std::vector<Item>& items, Op::Kind kind, int64_t (*geom)(Item&, int64_t),
+                 const Plan* plan, bool cplx) {
+    int64_t blocks = 0;
+    for (auto& it : items) blocks += geom(it, blocks);
+    Op op;
+    op.kind = kind;
+    op.count = static_cast<int>(items.size());
+    op.blocks = blocks;
+    op.plan = plan;
+    op.cplx = cplx;
+    op.off = prog.add(items.data(), items.size() * sizeof(Item));
+    prog.ops.push_back(op);
+}
+
+int64_t split_geom(SplitItem& it, int64_t b0) { return split_item_blocks(it, b0); }
+int64_t crt_geom(CrtItem& it, int64_t b0) { return crt_item_blocks(it, b0); }
+
+// Appends split, GEMM and CRT operations for a list of tasks (launches grouped by kernel variant)
+void plan_tasks(Program& prog, const std::vector<Task>& tasks, const GemmConfig& cfg) {
+    // split: group by (row_contig, complex, wide limb path)
+    std::map<std::tuple<int, int, int>, std::vector<SplitItem>> split_groups;
+    for (const Task& t : tasks) {
+        const Prob& p = *t.p;
+        const ModConst* mc = p.plan->mc;
+        const bool wide = p.plan->tk > kNarrowScaleBits;
+        if (t.split_b) {
+            SplitItem it = side_item(p, false, t.j0, t.nb, t.maxB, t.planesB, mc);
+            split_groups[{it.row_contig, it.cplx, wide}].push_back(it);
+        }
+        if (t.split_a) {
+            SplitItem it = side_item(p, true, t.i0, t.mb, t.maxA, t.planesA, mc);
+            split_groups[{it.row_contig, it.cplx, wide}].push_back(it);
+        }
+    }
+    for (auto& kv : split_groups) add_grouped(prog, kv.second, Op::Split, split_geom, nullptr, false);
+    Op mk;
+    mk.kind = Op::Mark;
+    mk.stage = kSplit;
+    prog.ops.push_back(mk);
+
+    // GEMM: one persistent launch over every task; largest work first
+    std::vector<GemmItem> gi;
+    std::vector<size_t> order(tasks.size());
+    for (size_t i = 0; i < tasks.size(); ++i) order[i] = i;
+    auto work = [&](size_t i) {
+        const Task& t = tasks[i];
+        return static_cast<double>(t.p->G) * t.p->plan->s * gemm_tiles_i(t.mb, cfg.bn) * ceil_div(t.nb, kGemmJ) *
+               ceil_div(t.p->k, kTileK);
+    };
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return work(a) > work(b); });
+    int64_t jobs = 0;
+    for (size_t oi : order) {
+        const Task& t = tasks[oi];
+        const Prob& p = *t.p;
+        GemmItem g{};
+        g.planes_i = t.planesA;
+        g.planes_j = t.planesB;
+        g.resid = t.resid;
+        g.pstride_i = plane_geom(t.mb, p.k, kGemmIPad).plane_bytes;
+        g.pstride_j = plane_geom(t.nb, p.k, kGemmJ).plane_bytes;
+        g.rstride = t.nb * t.ldr;
+        g.ldr = t.ldr;
+        g.m = t.mb;
+        g.n = t.nb;
+        g.kb_total = ceil_div(p.k, kTileK);
+        g.tiles_i = static_cast<int>(gemm_tiles_i(t.mb, cfg.bn));
+        g.tiles_j = static_cast<int>(ceil_div(t.nb, kGemmJ));
+        g.tiles = static_cast<int64_t>(g.tiles_i) * g.tiles_j;
+        g.s = p.plan->s;
+        g.groups = p.G;
+        g.job0 = jobs;
+        const ModConst* mc = p.plan->mc;
+        for (int q = 0; q < g.s; ++q) {
+            g.mod_m[q] = mc[q].m;
+            g.mod_mu[q] = mc[q].mu;
+            g.mod_kneg[q] = mc[q].kneg;
+        }
+        jobs += g.tiles * p.G * g.s;
+        gi.push_back(g);
+    }
+    Op go;
+    go.kind = Op::Gemm;
+    go.count = static_cast<int>(gi.size());
+    go.jobs = jobs;
+    go.cfg = cfg;
+    go.off = prog.add(gi.data(), gi.size() * sizeof(GemmItem));
+    prog.ops.push_back(go);
+    mk.stage = kGemm;
+    prog.ops.push_back(mk);
+
+    // CRT: group by (s, complex); the CRT table of s is a kernel parameter
+    std::map<std::pair<int, int>, std::pair<const Plan*, std::vector<CrtItem>>> crt_groups;
+    for (const Task& t : tasks) {
+        const Prob& p = *t.p;
+        const bool cplx = p.G == 3;
+        const int w = cplx ? 2 : 1;
+        CrtItem c{};
+        c.resid = t.resid;
+        c.rstride = t.nb * t.ldr;
+        c.gstride = c.rstride * p.plan->s;
+        c.ldr = t.ldr;
+        c.m = t.mb;
+        c.n = t.nb;
+        c.ldc = p.ldc;
+        c.maxA = t.maxA + t.i0;
+        c.maxB = t.maxB + t.j0;
+        c.tk = p.plan->tk;
+        c.ar = p.alpha[0];
+        c.ai = p.alpha[1];
+        c.br = p.beta[0];
+        c.bi = p.beta[1];
+        c.C = p.C + w * (t.i0 + t.j0 * p.ldc);
+        auto& grp = crt_groups[{p.plan->s, cplx}];
+        grp.first = p.plan;
+        grp.second.push_back(c);
+    }
+    for (auto& kv : crt_groups)
+        add_grouped(prog, kv.second.second, Op::Crt, crt_geom, kv.second.first, kv.first.second != 0);
+    mk.stage = kCrt;
+    prog.ops.push_back(mk);
+}
+
+void plan_scale(oz2_context* h, Program& prog, std::vector<ScaleItem>& items) {
+    // group by (row_contig, complex)
+    std::map<std::pair<int, int>, std::vector<ScaleItem>> groups;
+    for (auto& it : items) groups[{it.row_contig, it.cplx}].push_back(it);
+    for (auto& kv : groups) {
+        int64_t blocks = 0;
+        for (auto& it : kv.second) blocks += scale_item_blocks(it, h->num_sms, blocks);
+        Op op;
+        op.kind = Op::Scale;
+        op.count = static_cast<int>(kv.second.size());
+        op.blocks = blocks;
+        op.off = prog.add(kv.second.data(), kv.second.size() * sizeof(ScaleItem));
+        prog.ops.push_back(op);
+    }
+    Op mk;
+    mk.kind = Op::Mark;
+    mk.stage = kScale;
+    prog.ops.push_back(mk);
+}
+
+// one-dimensional grids: every launch must stay below 2^31 blocks
+int check_grid(oz2_context* h, const Program& prog) {
+    for (const Op& op : prog.ops)
+        if (op.blocks > 0x7FFFFFFFll) return fail(h, OZ2_EINVAL, "oz2: problem too large for one launch");
+    return OZ2_OK;
+}
+
+// ---------------------------------------------------------------- issuing a program
+int upload(oz2_context* h, const Program& prog, unsigned char* dev) {
+    const size_t bytes = prog.blob.size();
+    if (bytes == 0) return OZ2_OK;
+    if (bytes <= kParamBlobBytes) {  // written by a kernel that takes the bytes as its parameter
+        launch_write_blob(prog.blob.data(), bytes, dev, h->stream);
+        return OZ2_OK;
+    }
+    const int slot = h->ring_next;
+    h->ring_next = (h->ring_next + 1) % kRing;
+    if (h->ring_used[slot]) OZ2_CUDA(h, cudaEventSynchronize(h->ring_ev[slot]));
+    if (!h->ring_ev[slot]) OZ2_CUDA(h, cudaEventCreateWithFlags(&h->ring_ev[slot], cudaEventDisableTiming));
+    if (h->ring_cap[slot] < bytes) {
+        if (h->ring_host[slot]) cudaFreeHost(h->ring_host[slot]);
+        h->ring_host[slot] = nullptr;
+        const size_t cap = std::max(bytes, h->ring_cap[slot] * 2);
+        OZ2_CUDA(h, cudaHostAlloc(&h->ring_host[slot], cap, cudaHostAllocDefault));
+        h->ring_cap[slot] = cap;
+    }
+    std::memcpy(h->ring_host[slot], prog.blob.data(), bytes);
+    OZ2_CUDA(h, cudaMemcpyAsync(dev, h->ring_host[slot], bytes, cudaMemcpyHostToDevice, h->stream));
+    OZ2_CUDA(h, cudaEventRecord(h->ring_ev[slot], h->stream));
+    h->ring_used[slot] = true;
+    return OZ2_OK;
+}
+
+void issue(oz2_context* h, const Program& prog, const unsigned char* dev) {
+    const unsigned char* hb = prog.blob.data();
+    for (const Op& op : prog.ops) {
+        switch (op.kind) {
+            case Op::Memset: cudaMemsetAsync(op.ptr, 0, op.bytes, h->stream); break;
+            case Op::Scale:
+                launch_scale(reinterpret_cast<const ScaleItem*>(dev + op.off), reinterpret_cast<const ScaleItem*>(hb + op.off),
+                             op.count, op.blocks, h->stream);
+                break;
+            case Op::Split:
+                launch_split(reinterpret_cast<const SplitItem*>(dev + op.off), reinterpret_cast<const SplitItem*>(hb + op.off),
+                             op.count, op.blocks, h->stream);
+                break;
+            case Op::Gemm:
+                launch_gemm(reinterpret_cast<const GemmItem*>(dev + op.off), op.count, op.jobs, op.cfg, h->num_sms, h->d_err,
+                            h->stream);
+                break;
+            case Op::Crt:
+                launch_crt(reinterpret_cast<const CrtItem*>(dev + op.off), op.count, op.blocks, *op.plan, op.cplx,
+                           h->stream);
+                break;
+            case Op::ScaleC: launch_scale_c(static_cast<double*>(op.ptr), op.ldc, op.m, op.n, op.beta, op.cplx, h->stream); break;
+            case Op::Mark: mark(h, op.stage); break;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- GEMM configuration
+GemmConfig heuristic_config(const std::vector<const Prob*>& probs) {
+    GemmConfig c;
+    // narrow problems waste less padding with 128-row tiles along i
+    std::vector<int64_t> ms;
+    for (auto* p : probs) ms.push_back(p->m);
+    std::sort(ms.begin(), ms.end());
+    const int64_t med = ms.empty() ? 0 : ms[ms.size() / 2];
+    c.bn = med > 0 && med <= 384 ? 128 : 256;
+    c.group_j = 16;
+    return c;
+}
+
+std::string shape_signature(const std::vector<const Prob*>& probs) {
+    std::string s;
+    char buf[96];
+    for (auto* p : probs) {
+        std::snprintf(buf, sizeof buf, "%c%c%lld,%lld,%lld,%d,%d;", p->ta, p->tb, static_cast<long long>(p->m),
+                      static_cast<long long>(p->n), static_cast<long long>(p->k), p->plan->s, p->G);
+        s += buf;
+    }
+    return s;
+}
+
+GemmConfig config_for(oz2_context* h, const std::vector<const Prob*>& probs) {
+    if (h->has_forced) return h->forced;
+    auto it = h->tuned.find(shape_signature(probs));
+    if (it != h->tuned.end()) return it->second;
+    return heuristic_config(probs);
+}
+
+// ---------------------------------------------------------------- one emulated GEMM (tiled)
+struct Layout {
+    int64_t mb, nb, pm, pn, kchunks;
+    size_t bytes;
+};
+
 std::vector<int64_t> tile_candidates(int64_t x, int64_t unit, bool pow2) {
     std::vector<int64_t> c{x};
     for (int64_t p = 2; p <= 256; ++p) {
@@ -174,27 +566,33 @@ std::vector<int64_t> tile_candidates(int64_t x, int64_t unit, bool pow2) {
     return c;
 }
 
+size_t desc_bytes_single(int64_t pm, int64_t pn) {
+    const int64_t tiles = pm * pn;
+    return 4096 + static_cast<size_t>(2 * tiles) * (sizeof(SplitItem) + 256) +
+           static_cast<size_t>(tiles) * (sizeof(GemmItem) + sizeof(CrtItem) + 512) + 2 * sizeof(ScaleItem);
+}
+
 // Largest column tile that fits for each row-tile candidate, scored by an analytic time model
-// of this implementation (tensor-core work on padded tiles, HBM traffic of split and CRT,
-// per-launch overhead).
+// of this implementation (tensor work on padded tiles, HBM traffic of split and CRT, launches).
 int choose_layout(oz2_context* h, int64_t m, int64_t n, int64_t k, int s, int G, Layout& out) {
     const size_t limit = budget(h);
     double best = std::numeric_limits<double>::infinity();
     const bool pow2 = h->tuning[2] != 0;
     const auto nbs = tile_candidates(n, kGemmJ, pow2);
-    for (int64_t mb : tile_candidates(m, kGemmI, pow2)) {
+    for (int64_t mb : tile_candidates(m, kGemmIPad, pow2)) {
         for (int64_t nb : nbs) {
-            const Layout L = layout_for(m, n, k, s, G, mb, nb);
-            if (L.bytes > limit) continue;
-            const double gemm = 2.0 * G * s * k * static_cast<double>(L.pm * round_up(mb, kGemmI)) *
-                                static_cast<double>(L.pn * round_up(nb, kGemmJ)) / 3.0e15;
-            const double split = G * (8.0 + s) * (static_cast<double>(k) * m * (L.pm > 1 ? L.pn : 1) +
+            const int64_t pm = ceil_div(m, mb), pn = ceil_div(n, nb);
+            const size_t bytes = sizes_for(m, n, k, s, G, mb, nb).total() + align256(desc_bytes_single(pm, pn));
+            if (bytes > limit) continue;
+            const double gemm = 2.0 * G * s * k * static_cast<double>(pm * round_up(mb, kGemmIPad)) *
+                                static_cast<double>(pn * round_up(nb, kGemmJ)) / 3.0e15;
+            const double split = G * (8.0 + s) * (static_cast<double>(k) * m * (pm > 1 ? pn : 1) +
                                                   static_cast<double>(k) * n) / 5.0e12;
             const double crt = G * (s + 16.0) * static_cast<double>(m) * n / 5.0e12;
-            const double t = gemm + split + crt + L.pm * L.pn * (L.kchunks + 3) * 5e-6;
+            const double t = gemm + split + crt + pm * pn * 4 * 5e-6;
             if (t < best) {
                 best = t;
-                out = L;
+                out = Layout{mb, nb, pm, pn, ceil_div(ceil_div(k, kTileK), kChunkKB), bytes};
             }
             break;
         }
@@ -207,32 +605,10 @@ int choose_layout(oz2_context* h, int64_t m, int64_t n, int64_t k, int s, int G,
     return OZ2_OK;
 }
 
-int ensure_workspace(oz2_context* h, size_t bytes) {
-    if (h->ws_size >= bytes) return OZ2_OK;
-    OZ2_CUDA(h, cudaStreamSynchronize(h->stream));
-    if (h->ws) cudaFree(h->ws);
-    h->ws = nullptr;
-    h->ws_size = 0;
-    if (cudaMalloc(&h->ws, bytes) != cudaSuccess) {
-        cudaGetLastError();
-        h->ws = nullptr;
-        return fail(h, OZ2_ENOMEM, "oz2: workspace allocation failed");
-    }
-    h->ws_size = bytes;
-    return OZ2_OK;
-}
-
-// ---------------------------------------------------------------- one emulated GEMM
-// G = 1: real; G = 3: complex 3M (groups re, im, re+im). X pointers are double* views.
-int run(oz2_context* h, char ta, char tb, int64_t m, int64_t n, int64_t k, const double* alpha, const double* A,
-        int64_t lda, const double* B, int64_t ldb, const double* beta, double* C, int64_t ldc, int G) {
-    const Plan& p = h->plan;
-    const int s = p.s;
-    const bool cplx = G == 3;
-    ModConst mc[kMaxModuli];
-    mod_constants(p, mc);
+int run_single(oz2_context* h, const Prob& p) {
+    const int s = p.plan->s;
     Layout L;
-    int st = choose_layout(h, m, n, k, s, G, L);
+    int st = choose_layout(h, p.m, p.n, p.k, s, p.G, L);
     if (st) return st;
     if ((st = ensure_workspace(h, L.bytes))) return st;
     h->tiling[0] = L.mb;
@@ -241,88 +617,185 @@ int run(oz2_context* h, char ta, char tb, int64_t m, int64_t n, int64_t k, const
     h->tiling[3] = L.pn;
     h->tiling[4] = L.kchunks;
     h->tiling[5] = static_cast<int64_t>(L.bytes);
+    const Sizes z = sizes_for(p.m, p.n, p.k, s, p.G, L.mb, L.nb);
+    size_t off = 0;
+    auto carve = [&](size_t b) {
+        const size_t o = off;
+        off += align256(b);
+        return h->ws + o;
+    };
+    auto* maxA = reinterpret_cast<unsigned long long*>(carve(z.maxA));
+    auto* maxB = reinterpret_cast<unsigned long long*>(carve(z.maxB));
+    auto* planesA = reinterpret_cast<int8_t*>(carve(z.planesA));
+    auto* planesB = reinterpret_cast<int8_t*>(carve(z.planesB));
+    auto* resid = carve(z.resid);
+    unsigned char* dev_desc = carve(0);
 
-    auto* maxA = reinterpret_cast<unsigned long long*>(h->ws + L.o_maxA);
-    auto* maxB = reinterpret_cast<unsigned long long*>(h->ws + L.o_maxB);
-    auto* planesA = reinterpret_cast<int8_t*>(h->ws + L.o_A);
-    auto* planesB = reinterpret_cast<int8_t*>(h->ws + L.o_B);
-    auto* resid = h->ws + L.o_R;
-    const int w = cplx ? 2 : 1;
-    const int64_t kb_total = ceil_div(k, kTileK);
+    const std::vector<const Prob*> probs{&p};
+    const GemmConfig cfg = config_for(h, probs);
+    h->last_cfg = cfg;
+    Program prog;
+    Op mk;
+    mk.kind = Op::Mark;
+    mk.stage = kBegin;
+    prog.ops.push_back(mk);
+    Op ms;
+    ms.kind = Op::Memset;
+    ms.ptr = maxA;
+    ms.bytes = reinterpret_cast<unsigned char*>(planesA) - reinterpret_cast<unsigned char*>(maxA);
+    prog.ops.push_back(ms);
+    std::vector<ScaleItem> sc{scale_item(p, true, maxA), scale_item(p, false, maxB)};
+    plan_scale(h, prog, sc);
     const int64_t ldr = round_up(L.mb, 32);
-    if (kb_total > 65535 * 4 || (kb_total > 65535 && (is_n(ta) || !is_n(tb))))
-        return fail(h, OZ2_EINVAL, "oz2: k too large for one call of this implementation");
-
-    mark(h, kBegin);
-    OZ2_CUDA(h, cudaMemsetAsync(maxA, 0, static_cast<size_t>(m) * 8, h->stream));
-    OZ2_CUDA(h, cudaMemsetAsync(maxB, 0, static_cast<size_t>(n) * 8, h->stream));
-    // A side: plane rows are rows i of op(A); B side: plane rows are columns j of op(B)
-    SideDesc sa{A, lda, m, k, is_n(ta), cplx, cplx && is_c(ta)};
-    SideDesc sb{B, ldb, n, k, !is_n(tb), cplx, cplx && is_c(tb)};
-    launch_scale(sa, maxA, h->num_sms, h->stream);
-    launch_scale(sb, maxB, h->num_sms, h->stream);
-    mark(h, kScale);
-
-    for (int64_t j0 = 0; j0 < n; j0 += L.nb) {
-        const int64_t nbj = std::min(L.nb, n - j0);
-        const PlaneGeom gb = plane_geom(nbj, k, kGemmJ);
-        SideDesc tb_side = sb;
-        tb_side.X = B + w * (sb.row_contig ? j0 : j0 * ldb);
-        tb_side.rows = nbj;
-        launch_split(tb_side, maxB + j0, p.tk, mc, s, planesB, gb, h->stream);
-        mark(h, kSplit);
-        for (int64_t i0 = 0; i0 < m; i0 += L.mb) {
-            const int64_t mbi = std::min(L.mb, m - i0);
-            const PlaneGeom ga = plane_geom(mbi, k, kGemmI);
-            if (L.pm > 1 || j0 == 0) {
-                SideDesc ta_side = sa;
-                ta_side.X = A + w * (sa.row_contig ? i0 : i0 * lda);
-                ta_side.rows = mbi;
-                launch_split(ta_side, maxA + i0, p.tk, mc, s, planesA, ga, h->stream);
-                mark(h, kSplit);
-            }
-            for (int64_t c = 0; c < L.kchunks; ++c) {
-                GemmArgs g{};
-                g.planes_i = planesA;
-                g.planes_j = planesB;
-                g.resid = resid;
-                g.pstride_i = ga.plane_bytes;
-                g.pstride_j = gb.plane_bytes;
-                g.rstride = L.nb * ldr;
-                g.ldr = ldr;
-                g.m = mbi;
-                g.n = nbj;
-                g.kb_total = kb_total;
-                g.kb0 = c * kChunkKB;
-                g.kb1 = std::min(kb_total, g.kb0 + kChunkKB);
-                g.s = s;
-                g.groups = G;
-                g.accumulate = c > 0;
-                g.mc = mc;
-                g.err = h->d_err;
-                launch_gemm(g, h->num_sms, h->stream);
-            }
-            mark(h, kGemm);
-            CrtArgs ca{};
-            ca.resid = resid;
-            ca.rstride = L.nb * ldr;
-            ca.ldr = ldr;
-            ca.m = mbi;
-            ca.n = nbj;
-            ca.maxA = maxA + i0;
-            ca.maxB = maxB + j0;
-            ca.tk = p.tk;
-            ca.cplx = cplx;
-            ca.alpha[0] = alpha[0];
-            ca.alpha[1] = cplx ? alpha[1] : 0.0;
-            ca.beta[0] = beta[0];
-            ca.beta[1] = cplx ? beta[1] : 0.0;
-            ca.C = C + w * (i0 + j0 * ldc);
-            ca.ldc = ldc;
-            ca.plan = &p;
-            launch_crt(ca, h->stream);
-            mark(h, kCrt);
+    for (int64_t j0 = 0; j0 < p.n; j0 += L.nb) {
+        for (int64_t i0 = 0; i0 < p.m; i0 += L.mb) {
+            Task t{&p, i0, j0, std::min(L.mb, p.m - i0), std::min(L.nb, p.n - j0), L.pm > 1 || j0 == 0, i0 == 0,
+                   maxA, maxB, planesA, planesB, resid, ldr};
+            plan_tasks(prog, {t}, cfg);
         }
+    }
+    if (prog.blob.size() > align256(desc_bytes_single(L.pm, L.pn)))
+        return fail(h, OZ2_EINTERNAL, "oz2: descriptor region too small");
+    if ((st = check_grid(h, prog))) return st;
+    if ((st = upload(h, prog, dev_desc))) return st;
+    issue(h, prog, dev_desc);
+    return OZ2_OK;
+}
+
+// ---------------------------------------------------------------- grouped
+int run_grouped(oz2_context* h, std::vector<Prob>& probs) {
+    // every problem untiled; batches of problems whose workspace fits the budget
+    const size_t limit = budget(h);
+    std::vector<std::vector<size_t>> batches;
+    std::vector<size_t> cur;
+    size_t cur_bytes = 4096;
+    std::vector<size_t> need(probs.size());
+    for (size_t i = 0; i < probs.size(); ++i) {
+        const Prob& p = probs[i];
+        need[i] = sizes_for(p.m, p.n, p.k, p.plan->s, p.G, p.m, p.n).total() + 4 * sizeof(SplitItem) + 2048;
+        if (need[i] + 4096 > limit) {  // alone too large: the tiled single path
+            h->capture_ok = false;
+            int st = run_single(h, p);
+            if (st) return st;
+            continue;
+        }
+        if (cur_bytes + need[i] > limit && !cur.empty()) {
+            batches.push_back(cur);
+            cur.clear();
+            cur_bytes = 4096;
+        }
+        cur.push_back(i);
+        cur_bytes += need[i];
+    }
+    if (!cur.empty()) batches.push_back(cur);
+
+    size_t max_bytes = 0;
+    for (auto& b : batches) {
+        size_t sum = 4096;
+        for (size_t i : b) sum += need[i];
+        max_bytes = std::max(max_bytes, sum);
+    }
+    int st = ensure_workspace(h, max_bytes);
+    if (st) return st;
+
+    for (auto& b : batches) {
+        std::vector<const Prob*> bp;
+        for (size_t i : b) bp.push_back(&probs[i]);
+        const GemmConfig cfg = config_for(h, bp);
+        h->last_cfg = cfg;
+        // carve: maxima of all problems first (one memset), then planes and residues
+        size_t off = 0;
+        auto carve = [&](size_t bytes) {
+            const size_t o = off;
+            off += align256(bytes);
+            return h->ws + o;
+        };
+        std::vector<Task> tasks;
+        std::vector<ScaleItem> sc;
+        std::vector<std::pair<unsigned long long*, unsigned long long*>> mx;
+        for (const Prob* p : bp)
+            mx.emplace_back(reinterpret_cast<unsigned long long*>(carve(p->m * 8)),
+                            reinterpret_cast<unsigned long long*>(carve(p->n * 8)));
+        const size_t max_end = off;
+        for (size_t q = 0; q < bp.size(); ++q) {
+            const Prob& p = *bp[q];
+            const Sizes z = sizes_for(p.m, p.n, p.k, p.plan->s, p.G, p.m, p.n);
+            auto* pa = reinterpret_cast<int8_t*>(carve(z.planesA));
+            auto* pb = reinterpret_cast<int8_t*>(carve(z.planesB));
+            auto* rs = carve(z.resid);
+            tasks.push_back(Task{&p, 0, 0, p.m, p.n, true, true, mx[q].first, mx[q].second, pa, pb, rs,
+                                 round_up(p.m, 32)});
+            sc.push_back(scale_item(p, true, mx[q].first));
+            sc.push_back(scale_item(p, false, mx[q].second));
+        }
+        unsigned char* dev_desc = carve(0);
+        Program prog;
+        Op mk;
+        mk.kind = Op::Mark;
+        mk.stage = kBegin;
+        prog.ops.push_back(mk);
+        Op ms;
+        ms.kind = Op::Memset;
+        ms.ptr = h->ws;
+        ms.bytes = max_end;
+        prog.ops.push_back(ms);
+        plan_scale(h, prog, sc);
+        plan_tasks(prog, tasks, cfg);
+        if (static_cast<size_t>(dev_desc - h->ws) + prog.blob.size() > h->ws_size)
+            return fail(h, OZ2_EINTERNAL, "oz2: descriptor region too small");
+        if ((st = check_grid(h, prog))) return st;
+
+        if (h->capturing) {
+            void* dev_blob = nullptr;
+            OZ2_CUDA(h, cudaMalloc(&dev_blob, std::max<size_t>(prog.blob.size(), 256)));
+            h->capturing->dev_blobs.push_back(dev_blob);
+            OZ2_CUDA(h, cudaMemcpy(dev_blob, prog.blob.data(), prog.blob.size(), cudaMemcpyHostToDevice));
+            cudaGraph_t g;
+            if (!h->cap_stream) OZ2_CUDA(h, cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking));
+            const bool prof = h->profiling;
+            cudaStream_t user = h->stream;
+            h->profiling = false;  // no event records inside a graph
+            h->stream = h->cap_stream;
+            cudaError_t ce = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
+            if (ce == cudaSuccess) {
+                issue(h, prog, static_cast<unsigned char*>(dev_blob));
+                ce = cudaStreamEndCapture(h->stream, &g);
+            }
+            h->stream = user;
+            h->profiling = prof;
+            if (ce != cudaSuccess) return cuda_fail(h, ce, "cudaStreamEndCapture");
+            cudaGraphExec_t exec = nullptr;
+            const cudaError_t ie = cudaGraphInstantiate(&exec, g, 0);
+            cudaGraphDestroy(g);
+            if (ie != cudaSuccess) return cuda_fail(h, ie, "cudaGraphInstantiate");
+            h->capturing->execs.push_back(exec);
+            OZ2_CUDA(h, cudaGraphLaunch(exec, h->stream));
+        } else {
+            if ((st = upload(h, prog, dev_desc))) return st;
+            issue(h, prog, dev_desc);
+        }
+    }
+    h->tiling[0] = h->tiling[1] = h->tiling[2] = h->tiling[3] = h->tiling[4] = 0;
+    h->tiling[5] = static_cast<int64_t>(max_bytes);
+    return OZ2_OK;
+}
+
+int validate_grouped(oz2_handle h, int count, const oz2_dgemm_problem* pr, std::vector<Prob>& out) {
+    out.clear();
+    out.reserve(count);
+    for (int i = 0; i < count; ++i) {
+        const oz2_dgemm_problem& q = pr[i];
+        int st = check_args(h, q.ta, q.tb, q.m, q.n, q.k, q.lda, q.ldb, q.ldc);
+        if (st) return fail(h, st, "oz2: problem " + std::to_string(i) + ": " + h->err);
+    }
+    for (int i = 0; i < count; ++i) {
+        const oz2_dgemm_problem& q = pr[i];
+        if (q.m == 0 || q.n == 0 || q.k == 0 || q.alpha == 0.0) continue;
+        const Plan* plan;
+        int st = get_plan(h, q.num_moduli, q.k, &plan);
+        if (st) return fail(h, st, "oz2: problem " + std::to_string(i) + ": " + h->err);
+        out.push_back(Prob{q.ta, q.tb, q.m, q.n, q.k, {q.alpha, 0.0}, {q.beta, 0.0}, q.A, q.lda, q.B, q.ldb, q.C, q.ldc, 1,
+                           plan});
     }
     return OZ2_OK;
 }
@@ -344,6 +817,7 @@ int oz2_create(void* stream, oz2_handle* out) {
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
     if (e == cudaSuccess) e = cudaMalloc(&h->d_err, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(h->d_err, 0, sizeof(int));
+    if (e == cudaSuccess) e = prepare_gemm_kernels();
     if (e != cudaSuccess) {
         const int st = cuda_fail(nullptr, e, "oz2_create");
         if (h->d_err) cudaFree(h->d_err);
@@ -358,9 +832,15 @@ int oz2_create(void* stream, oz2_handle* out) {
 int oz2_destroy(oz2_handle h) {
     if (!h) return OZ2_OK;
     cudaStreamSynchronize(h->stream);
+    drop_graphs(h);
     if (h->ws) cudaFree(h->ws);
     if (h->d_err) cudaFree(h->d_err);
     for (cudaEvent_t e : h->pool) cudaEventDestroy(e);
+    for (int i = 0; i < kRing; ++i) {
+        if (h->ring_host[i]) cudaFreeHost(h->ring_host[i]);
+        if (h->ring_ev[i]) cudaEventDestroy(h->ring_ev[i]);
+    }
+    if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
     delete h;
     return OZ2_OK;
 }
@@ -368,6 +848,7 @@ int oz2_destroy(oz2_handle h) {
 int oz2_set_stream(oz2_handle h, void* stream) {
     if (!h) return fail(nullptr, OZ2_EINVAL, "oz2: null handle");
     h->stream = static_cast<cudaStream_t>(stream);
+    drop_graphs(h);
     return OZ2_OK;
 }
 
@@ -377,17 +858,20 @@ int oz2_dgemm(oz2_handle h, char ta, char tb, int64_t m, int64_t n, int64_t k, d
               void* const* deps, int ndeps, void* done) {
     if (!h) return fail(nullptr, OZ2_EINVAL, "oz2: null handle");
     h->marks.clear();
+    if (h->plans.size() > 1024) h->plans.clear();  // between calls only: plans are borrowed during one
     int st = check_args(h, ta, tb, m, n, k, lda, ldb, ldc);
     if (st) return st;
     if ((st = begin_call(h, deps, ndeps))) return st;
     if (m == 0 || n == 0) return end_call(h, done);
-    const double al[2] = {alpha, 0.0}, be[2] = {beta, 0.0};
+    const double be[2] = {beta, 0.0};
     if (k == 0 || alpha == 0.0) {
         launch_scale_c(C, ldc, m, n, be, false, h->stream);
         return end_call(h, done);
     }
-    if ((st = ensure_plan(h, num_moduli, k))) return st;
-    if ((st = run(h, ta, tb, m, n, k, al, A, lda, B, ldb, be, C, ldc, 1))) return st;
+    const Plan* plan;
+    if ((st = get_plan(h, num_moduli, k, &plan))) return st;
+    const Prob p{ta, tb, m, n, k, {alpha, 0.0}, {beta, 0.0}, A, lda, B, ldb, C, ldc, 1, plan};
+    if ((st = run_single(h, p))) return st;
     return end_call(h, done);
 }
 
@@ -398,6 +882,7 @@ int oz2_zgemm(oz2_handle h, char ta, char tb, int64_t m, int64_t n, int64_t k, c
     if (!h) return fail(nullptr, OZ2_EINVAL, "oz2: null handle");
     if (!alpha || !beta) return fail(h, OZ2_EINVAL, "oz2: null alpha or beta");
     h->marks.clear();
+    if (h->plans.size() > 1024) h->plans.clear();
     int st = check_args(h, ta, tb, m, n, k, lda, ldb, ldc);
     if (st) return st;
     if ((st = begin_call(h, deps, ndeps))) return st;
@@ -407,9 +892,147 @@ int oz2_zgemm(oz2_handle h, char ta, char tb, int64_t m, int64_t n, int64_t k, c
         return end_call(h, done);
     }
     if (k > std::numeric_limits<int64_t>::max() / 2) return fail(h, OZ2_EINVAL, "oz2: k too large");
-    if ((st = ensure_plan(h, num_moduli, 2 * k))) return st;
-    if ((st = run(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, 3))) return st;
+    const Plan* plan;
+    if ((st = get_plan(h, num_moduli, 2 * k, &plan))) return st;
+    const Prob p{ta, tb, m, n, k, {alpha[0], alpha[1]}, {beta[0], beta[1]}, A, lda, B, ldb, C, ldc, 3, plan};
+    if ((st = run_single(h, p))) return st;
     return end_call(h, done);
+}
+
+int oz2_dgemm_grouped(oz2_handle h, int count, const oz2_dgemm_problem* problems, void* const* deps, int ndeps,
+                      void* done) {
+    if (!h) return fail(nullptr, OZ2_EINVAL, "oz2: null handle");
+    if (count < 0 || (count > 0 && !problems)) return fail(h, OZ2_EINVAL, "oz2: bad problem list");
+    h->marks.clear();
+    if (h->plans.size() > 1024) h->plans.clear();
+    std::vector<Prob> probs;
+    int st = validate_grouped(h, count, problems, probs);
+    if (st) return st;
+    if ((st = begin_call(h, deps, ndeps))) return st;
+    for (int i = 0; i < count; ++i) {  // k == 0 or alpha == 0: C = beta C
+        const oz2_dgemm_problem& q = problems[i];
+        if (q.m > 0 && q.n > 0 && (q.k == 0 || q.alpha == 0.0)) {
+            const double be[2] = {q.beta, 0.0};
+            launch_scale_c(q.C, q.ldc, q.m, q.n, be, false, h->stream);
+        }
+    }
+    if (probs.empty()) return end_call(h, done);
+    if (!h->graph_mode) {
+        if ((st = run_grouped(h, probs))) return st;
+        return end_call(h, done);
+    }
+    // graph mode: the same problem list (shapes, pointers, scalars) replays its graphs
+    const unsigned char* raw = reinterpret_cast<const unsigned char*>(problems);
+    const size_t raw_bytes = static_cast<size_t>(count) * sizeof(oz2_dgemm_problem);
+    uint64_t key = 1469598103934665603ull;  // FNV-1a
+    for (size_t i = 0; i < raw_bytes; ++i) key = (key ^ raw[i]) * 1099511628211ull;
+    auto it = h->graphs.find(key);
+    if (it != h->graphs.end() && it->second.problems.size() == raw_bytes &&
+        std::memcmp(it->second.problems.data(), raw, raw_bytes) == 0) {
+        mark(h, kBegin);
+        for (auto e : it->second.execs) OZ2_CUDA(h, cudaGraphLaunch(e, h->stream));
+        mark(h, kCrt);
+        return end_call(h, done);
+    }
+    if (h->graphs.size() >= 64) drop_graphs(h);
+    GraphEntry fresh;
+    fresh.problems.assign(raw, raw + raw_bytes);
+    GraphEntry& ge = h->graphs[key];
+    for (auto e : ge.execs) cudaGraphExecDestroy(e);
+    for (auto b : ge.dev_blobs) cudaFree(b);
+    ge = std::move(fresh);
+    h->capturing = &ge;
+    h->capture_ok = true;
+    st = run_grouped(h, probs);
+    const bool keep = h->capturing != nullptr && h->capture_ok;
+    h->capturing = nullptr;
+    if (st || !keep) drop_graphs(h);
+    if (st) return st;
+    return end_call(h, done);
+}
+
+int oz2_set_graph_mode(oz2_handle h, int enable) {
+    if (!h) return fail(nullptr, OZ2_EINVAL, "oz2: null handle");
+    h->graph_mode = enable != 0;
+    if (!h->graph_mode) drop_graphs(h);
+    return OZ2_OK;
+}
+
+int oz2_set_gemm_config(oz2_handle h, int bn, int group_j, int ctas) {
+    if (!h) return fail(nullptr, OZ2_EINVAL, "oz2: null handle");
+    if (bn == 0) {
+        h->has_forced = false;
+        drop_graphs(h);
+        return OZ2_OK;
+    }
+    if ((bn != 128 && bn != 256) || group_j < 1 || ctas < 0)
+        return fail(h, OZ2_EINVAL, "oz2: gemm config: bn must be 128 or 256, group_j >= 1, ctas >= 0");
+    h->forced = GemmConfig{bn, group_j, ctas};
+    h->has_forced = true;
+    drop_graphs(h);
+    return OZ2_OK;
+}
+
+int oz2_get_gemm_config(oz2_handle h, int* out3) {
+    if (!h || !out3) return fail(h, OZ2_EINVAL, "oz2: null argument");
+    out3[0] = h->last_cfg.bn;
+    out3[1] = h->last_cfg.group_j;
+    out3[2] = h->last_cfg.ctas;
+    return OZ2_OK;
+}
+
+// Times the grouped call's GEMM phase under each candidate configuration (tile width along i,
+// raster group, CTA count) on the caller's problems and keeps the fastest for problem sets of
+// the same shapes. Runs the problems (C is written) once per candidate plus once to warm up.
+int oz2_autotune_grouped(oz2_handle h, int count, const oz2_dgemm_problem* problems, int* out3) {
+    if (!h) return fail(nullptr, OZ2_EINVAL, "oz2: null handle");
+    std::vector<Prob> probs;
+    int st = validate_grouped(h, count, problems, probs);
+    if (st) return st;
+    if (probs.empty()) return fail(h, OZ2_EINVAL, "oz2: nothing to tune");
+    std::vector<const Prob*> bp;
+    for (auto& p : probs) bp.push_back(&p);
+    const bool had_forced = h->has_forced, had_graph = h->graph_mode, had_prof = h->profiling;
+    const GemmConfig saved = h->forced;
+    h->graph_mode = false;
+    h->profiling = true;
+    std::vector<GemmConfig> cands;
+    for (int bn : {256, 128})
+        for (int gj : {4, 8, 16, 32}) cands.push_back(GemmConfig{bn, gj, 0});
+    GemmConfig best = heuristic_config(bp);
+    double best_ms = std::numeric_limits<double>::infinity();
+    h->forced = best;
+    h->has_forced = true;
+    if ((st = run_grouped(h, probs))) goto done;  // warm-up
+    for (const GemmConfig& c : cands) {
+        h->forced = c;
+        double total = 0;
+        for (int rep = 0; rep < 2; ++rep) {
+            h->marks.clear();
+            h->pool_used = 0;
+            if ((st = run_grouped(h, probs))) goto done;
+            double v[4];
+            if ((st = oz2_stage_times(h, v))) goto done;
+            total += v[2];
+        }
+        if (total < best_ms) {
+            best_ms = total;
+            best = c;
+        }
+    }
+    h->tuned[shape_signature(bp)] = best;
+    drop_graphs(h);
+    if (out3) {
+        out3[0] = best.bn;
+        out3[1] = best.group_j;
+        out3[2] = best.ctas;
+    }
+done:
+    h->has_forced = had_forced;
+    h->forced = saved;
+    h->graph_mode = had_graph;
+    h->profiling = had_prof;
+    return st;
 }
 
 int oz2_precision_bits(int64_t k, int num_moduli, int* out) {
@@ -456,9 +1079,11 @@ int oz2_release_workspace(oz2_handle h) {
     if (!h) return fail(nullptr, OZ2_EINVAL, "oz2: null handle");
     if (!h->ws) return OZ2_OK;
     OZ2_CUDA(h, cudaStreamSynchronize(h->stream));
+    drop_graphs(h);
     cudaFree(h->ws);
     h->ws = nullptr;
     h->ws_size = 0;
+    ++h->ws_gen;
     return OZ2_OK;
 }
 

@@ -7,6 +7,7 @@
 // Bandwidth-bound: s bytes of residues per entry in (3s for complex), 8 (16) bytes of C out,
 // plus 8 (16) in when beta != 0. Each thread handles 4 consecutive rows of one column.
 #include <algorithm>
+#include <cstring>
 
 #include "oz2_kernels.cuh"
 
@@ -14,13 +15,8 @@ namespace oz2 {
 namespace {
 
 struct CrtParams {
-    const uint8_t* resid;
-    int64_t rstride, gstride, ldr, m, n, ldc;
-    const unsigned long long* maxA;
-    const unsigned long long* maxB;
-    int tk;
-    double ar, ai, br, bi;
-    double* C;
+    const CrtItem* items;
+    int count;
     CrtConst cc;
     uint32_t mod_m[kMaxModuli];
 };
@@ -113,30 +109,45 @@ __device__ __forceinline__ uint32_t sub_mod(uint32_t a, uint32_t b, uint32_t m) 
 template <int S, bool CPLX>
 __global__ void __launch_bounds__(256) crt_kernel(const __grid_constant__ CrtParams P) {
     constexpr int NL = limbs_for(S);
-    const int64_t i0 = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) * 4;
-    if (i0 >= P.m) return;
-    for (int64_t j = blockIdx.y; j < P.n; j += gridDim.y) {
-        const int Ej = exponent_of(P.maxB[j], P.tk);
-        const uint8_t* base = P.resid + j * P.ldr + i0;
+    int lo = 0, hi = P.count - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (P.items[mid].block0 <= static_cast<int64_t>(blockIdx.x)) lo = mid;
+        else hi = mid - 1;
+    }
+    const CrtItem* __restrict__ I = P.items + lo;
+    const int64_t local = static_cast<int64_t>(blockIdx.x) - I->block0;
+    const int64_t jblk = local / I->iblocks, ib = local - jblk * I->iblocks;
+    const int tq = I->tq;
+    const int64_t j = jblk * I->jb + threadIdx.x / tq;
+    const int64_t i0 = (ib * tq + threadIdx.x % tq) * 4;
+    const int64_t m = I->m;
+    if (i0 >= m || j >= I->n) return;
+    const int tk = I->tk;
+    const double ar = I->ar, ai = I->ai, br = I->br, bi = I->bi;
+    const int64_t rstride = I->rstride, gstride = I->gstride;
+    {
+        const int Ej = exponent_of(I->maxB[j], tk);
+        const uint8_t* base = I->resid + j * I->ldr + i0;
         // one 32-bit word per plane = the residues of the 4 entries i0..i0+3
         uint32_t w0[S], w1[CPLX ? S : 1], w2[CPLX ? S : 1];
 #pragma unroll
         for (int t = 0; t < S; ++t) {
-            w0[t] = __ldg(reinterpret_cast<const uint32_t*>(base + t * P.rstride));
+            w0[t] = __ldg(reinterpret_cast<const uint32_t*>(base + t * rstride));
             if (CPLX) {
-                w1[t] = __ldg(reinterpret_cast<const uint32_t*>(base + P.gstride + t * P.rstride));
-                w2[t] = __ldg(reinterpret_cast<const uint32_t*>(base + 2 * P.gstride + t * P.rstride));
+                w1[t] = __ldg(reinterpret_cast<const uint32_t*>(base + gstride + t * rstride));
+                w2[t] = __ldg(reinterpret_cast<const uint32_t*>(base + 2 * gstride + t * rstride));
             }
         }
 #pragma unroll 1
         for (int e = 0; e < 4; ++e) {
             const int64_t i = i0 + e;
-            if (i >= P.m) break;
-            const int De = exponent_of(P.maxA[i], P.tk);
+            if (i >= m) break;
+            const int De = exponent_of(I->maxA[i], tk);
             const bool nonfinite = De == kNonFinite || Ej == kNonFinite;
             const int shift = nonfinite ? 0 : De + Ej;
             const uint32_t sel = 0x4440 + e;  // byte e of a word, zero-extended
-            double* cp = P.C + (CPLX ? 2 : 1) * (i + j * P.ldc);
+            double* cp = I->C + (CPLX ? 2 : 1) * (i + j * I->ldc);
             if (!CPLX) {
                 uint32_t r[S];
 #pragma unroll
@@ -144,8 +155,8 @@ __global__ void __launch_bounds__(256) crt_kernel(const __grid_constant__ CrtPar
                 double v = crt_value<S, NL>(r, P.cc, shift);
                 if (nonfinite) v = __longlong_as_double(0x7FF8000000000000ll);
                 // the reference's unfused alpha*v + beta*c, one rounding per operation
-                const double av = __dmul_rn(P.ar, v);
-                cp[0] = P.br == 0.0 ? av : __dadd_rn(av, __dmul_rn(P.br, cp[0]));
+                const double av = __dmul_rn(ar, v);
+                cp[0] = br == 0.0 ? av : __dadd_rn(av, __dmul_rn(br, cp[0]));
             } else {
                 uint32_t rr[S], ri[S];
 #pragma unroll
@@ -159,12 +170,12 @@ __global__ void __launch_bounds__(256) crt_kernel(const __grid_constant__ CrtPar
                 double vr = crt_value<S, NL>(rr, P.cc, shift);
                 double vi = crt_value<S, NL>(ri, P.cc, shift);
                 if (nonfinite) vr = vi = __longlong_as_double(0x7FF8000000000000ll);
-                double orr = __dsub_rn(__dmul_rn(P.ar, vr), __dmul_rn(P.ai, vi));
-                double oi = __dadd_rn(__dmul_rn(P.ar, vi), __dmul_rn(P.ai, vr));
-                if (P.br != 0.0 || P.bi != 0.0) {
+                double orr = __dsub_rn(__dmul_rn(ar, vr), __dmul_rn(ai, vi));
+                double oi = __dadd_rn(__dmul_rn(ar, vi), __dmul_rn(ai, vr));
+                if (br != 0.0 || bi != 0.0) {
                     const double cr = cp[0], ci = cp[1];
-                    orr = __dadd_rn(orr, __dsub_rn(__dmul_rn(P.br, cr), __dmul_rn(P.bi, ci)));
-                    oi = __dadd_rn(oi, __dadd_rn(__dmul_rn(P.br, ci), __dmul_rn(P.bi, cr)));
+                    orr = __dadd_rn(orr, __dsub_rn(__dmul_rn(br, cr), __dmul_rn(bi, ci)));
+                    oi = __dadd_rn(oi, __dadd_rn(__dmul_rn(br, ci), __dmul_rn(bi, cr)));
                 }
                 cp[0] = orr;
                 cp[1] = oi;
@@ -174,19 +185,26 @@ __global__ void __launch_bounds__(256) crt_kernel(const __grid_constant__ CrtPar
 }
 
 template <int S>
-void crt_launch_s(const CrtParams& P, bool cplx, cudaStream_t st) {
-    const int64_t quads = ceil_div(P.m, 4);
-    dim3 grid(static_cast<unsigned>(ceil_div(quads, 256)), static_cast<unsigned>(std::min<int64_t>(P.n, 65535)));
-    if (cplx) crt_kernel<S, true><<<grid, 256, 0, st>>>(P);
-    else crt_kernel<S, false><<<grid, 256, 0, st>>>(P);
+void crt_launch_s(const CrtParams& P, int64_t blocks, bool cplx, cudaStream_t st) {
+    if (cplx) crt_kernel<S, true><<<static_cast<unsigned>(blocks), 256, 0, st>>>(P);
+    else crt_kernel<S, false><<<static_cast<unsigned>(blocks), 256, 0, st>>>(P);
 }
 
 template <int S>
-void crt_dispatch(int s, const CrtParams& P, bool cplx, cudaStream_t st) {
+void crt_dispatch(int s, const CrtParams& P, int64_t blocks, bool cplx, cudaStream_t st) {
     if constexpr (S <= kMaxModuli) {
-        if (s == S) return crt_launch_s<S>(P, cplx, st);
-        crt_dispatch<S + 1>(s, P, cplx, st);
+        if (s == S) return crt_launch_s<S>(P, blocks, cplx, st);
+        crt_dispatch<S + 1>(s, P, blocks, cplx, st);
     }
+}
+
+struct alignas(16) BlobParam {
+    unsigned char data[kParamBlobBytes];
+    uint32_t bytes;
+};
+__global__ void write_blob_kernel(const __grid_constant__ BlobParam b, unsigned char* dst) {
+    for (uint32_t i = threadIdx.x * 16; i < b.bytes; i += blockDim.x * 16)
+        *reinterpret_cast<uint4*>(dst + i) = *reinterpret_cast<const uint4*>(b.data + i);
 }
 
 __global__ void scale_c_kernel(double* C, int64_t ldc, int64_t m, int64_t n, double br, double bi, int cplx) {
@@ -212,27 +230,36 @@ __global__ void scale_c_kernel(double* C, int64_t ldc, int64_t m, int64_t n, dou
 
 }  // namespace
 
-void launch_crt(const CrtArgs& a, cudaStream_t st) {
-    if (a.m <= 0 || a.n <= 0) return;
+int64_t crt_item_blocks(CrtItem& it, int64_t block0) {
+    it.block0 = block0;
+    const int64_t quads = ceil_div(it.m, 4);
+    int tq = 1;
+    while (tq < 256 && tq < quads) tq *= 2;  // short columns share a block
+    it.tq = tq;
+    it.jb = 256 / tq;
+    it.iblocks = ceil_div(quads, tq);
+    return it.m > 0 ? ceil_div(it.n, it.jb) * it.iblocks : 0;
+}
+
+void launch_crt(const CrtItem* d_items, int count, int64_t blocks, const Plan& plan, bool cplx, cudaStream_t st) {
+    if (count <= 0 || blocks <= 0) return;
     CrtParams P{};
-    P.resid = a.resid;
-    P.rstride = a.rstride;
-    P.gstride = a.rstride * a.plan->s;
-    P.ldr = a.ldr;
-    P.m = a.m;
-    P.n = a.n;
-    P.ldc = a.ldc;
-    P.maxA = a.maxA;
-    P.maxB = a.maxB;
-    P.tk = a.tk;
-    P.ar = a.alpha[0];
-    P.ai = a.alpha[1];
-    P.br = a.beta[0];
-    P.bi = a.beta[1];
-    P.C = a.C;
-    crt_constants(*a.plan, P.cc);
-    for (int t = 0; t < a.plan->s; ++t) P.mod_m[t] = a.plan->m[t];
-    crt_dispatch<2>(a.plan->s, P, a.cplx, st);
+    P.items = d_items;
+    P.count = count;
+    crt_constants(plan, P.cc);
+    for (int t = 0; t < plan.s; ++t) P.mod_m[t] = plan.m[t];
+    crt_dispatch<2>(plan.s, P, blocks, cplx, st);
+}
+
+void launch_write_blob(const void* src, size_t bytes, void* dst, cudaStream_t st) {
+    static thread_local BlobParam bp;
+    const unsigned char* p = static_cast<const unsigned char*>(src);
+    for (size_t off = 0; off < bytes; off += kParamBlobBytes) {
+        const size_t n = std::min(kParamBlobBytes, bytes - off);
+        std::memcpy(bp.data, p + off, n);
+        bp.bytes = static_cast<uint32_t>((n + 15) & ~size_t{15});
+        write_blob_kernel<<<1, 256, 0, st>>>(bp, static_cast<unsigned char*>(dst) + off);
+    }
 }
 
 void launch_scale_c(double* C, int64_t ldc, int64_t m, int64_t n, const double* beta, bool cplx, cudaStream_t st) {

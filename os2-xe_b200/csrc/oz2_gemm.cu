@@ -6,10 +6,13 @@
 // instead of s int32 planes (4 bytes per entry) the kernel writes one uint8 residue c mod m_t
 // per entry, so the CRT phase reads 1 byte per entry and modulus.
 //
-// Persistent kernel, one CTA per SM, 6 warps:
+// Persistent kernel over a table of problems (one emulated GEMM, or a group of them), one CTA
+// per SM, 6 warps:
 //   warp 0   producer: 1-D bulk copies of pre-tiled 16 KiB plane tiles into a 4-stage ring
-//   warp 1   MMA issuer: tcgen05.mma kind::i8, M=128 (columns j of C), N=256 (rows i of C),
-//            K=32 per instruction, int32 accumulators in TMEM (2 x 256 columns, double buffer)
+//   warp 1   MMA issuer: tcgen05.mma kind::i8, M=128 (columns j of C), N=BN (rows i of C,
+//            BN = 256 or 128), K=32 per instruction, int32 accumulators in TMEM (2 x BN
+//            columns, double buffer); k beyond 130944 runs as chunks inside one job, each chunk
+//            adding its residues to the previous ones mod m
 //   warps 2-5 epilogue: tcgen05.ld 32 lanes x 32 columns, c mod m_t, 32 residue bytes per
 //            thread and chunk stored to residue plane row j (i contiguous)
 // Every mbarrier wait is time-bounded; on expiry the kernel records an error code, drains its
@@ -23,61 +26,76 @@
 namespace oz2 {
 namespace {
 
-constexpr int kStages = 4;
-constexpr int kStageJ = kGemmJ * kTileK;              // 16 KiB
-constexpr int kStageI = kGemmI * kTileK;              // 32 KiB
-constexpr int kStageBytes = kStageJ + kStageI;       // 48 KiB
-constexpr int kGroupJ = 16;                          // raster: 16 column tiles share the row panels
-constexpr uint32_t kTmemCols = 512;
-constexpr uint32_t kIdesc = dev::idesc_i8(kGemmJ, kGemmI);
-constexpr int kBarBytes = 256;
-constexpr int kSmemBytes = 1024 + kStages * kStageBytes + kBarBytes;
+constexpr uint32_t kBarBytes = 256;
+
+template <int BN>
+struct Cfg {
+    static constexpr int kStageJ = kGemmJ * kTileK;       // 16 KiB
+    static constexpr int kStageI = BN * kTileK;           // 32 KiB (BN 256) / 16 KiB (BN 128)
+    static constexpr int kStageBytes = kStageJ + kStageI;
+    static constexpr int kStages = BN == 256 ? 4 : 6;
+    static constexpr uint32_t kTmemCols = 2 * BN;         // two accumulators
+    static constexpr uint32_t kIdesc = dev::idesc_i8(kGemmJ, BN);
+    static constexpr int kSmemBytes = 1024 + kStages * kStageBytes + kBarBytes;
+};
 
 struct GemmParams {
-    const int8_t* planes_i;
-    const int8_t* planes_j;
-    uint8_t* resid;
-    int64_t pstride_i, pstride_j, rstride, ldr, m, n, kb_total, kb0, kb1;
-    int64_t tiles, jobs;
-    int tiles_i, tiles_j, s, accumulate;
+    const GemmItem* items;
+    int count;
+    int group_j;
+    int64_t jobs;
     int* err;
-    uint32_t mod_m[kMaxModuli], mod_mu[kMaxModuli], mod_kneg[kMaxModuli];
 };
 
 struct Job {
+    const GemmItem* I;
     int gt;  // group * s + modulus
     int ti, tj;
+    int64_t nch;  // k chunks
 };
 __device__ __forceinline__ Job decode(const GemmParams& P, int64_t job) {
+    int lo = 0, hi = P.count - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (P.items[mid].job0 <= job) lo = mid;
+        else hi = mid - 1;
+    }
     Job J;
-    J.gt = static_cast<int>(job / P.tiles);
-    const int64_t tile = job - static_cast<int64_t>(J.gt) * P.tiles;
-    const int64_t per_grp = static_cast<int64_t>(kGroupJ) * P.tiles_i;
+    J.I = P.items + lo;
+    const int64_t local = job - J.I->job0;
+    const int64_t tiles = J.I->tiles;
+    J.gt = static_cast<int>(local / tiles);
+    const int64_t tile = local - static_cast<int64_t>(J.gt) * tiles;
+    const int tiles_i = J.I->tiles_i, tiles_j = J.I->tiles_j;
+    const int64_t per_grp = static_cast<int64_t>(P.group_j) * tiles_i;
     const int64_t grp = tile / per_grp, rem = tile - grp * per_grp;
-    const int first_j = static_cast<int>(grp) * kGroupJ;
-    const int gj = min(kGroupJ, P.tiles_j - first_j);
+    const int first_j = static_cast<int>(grp) * P.group_j;
+    const int gj = min(P.group_j, tiles_j - first_j);
     J.tj = first_j + static_cast<int>(rem % gj);
     J.ti = static_cast<int>(rem / gj);
+    J.nch = (J.I->kb_total + kChunkKB - 1) / kChunkKB;
     return J;
 }
 
+template <int BN>
 __global__ void __launch_bounds__(192, 1) gemm_i8_modm_kernel(const __grid_constant__ GemmParams P) {
+    using C = Cfg<BN>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t{1023});
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + C::kStages * C::kStageBytes);
     // barriers: full[kStages] empty[kStages] acc_full[2] acc_empty[2] drain
     const uint32_t bar0 = dev::smem_addr(bars);
     auto full = [&](int i) { return bar0 + 8u * i; };
-    auto empty = [&](int i) { return bar0 + 8u * (kStages + i); };
-    auto acc_full = [&](int a) { return bar0 + 8u * (2 * kStages + a); };
-    auto acc_empty = [&](int a) { return bar0 + 8u * (2 * kStages + 2 + a); };
-    const uint32_t drain = bar0 + 8u * (2 * kStages + 4);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 5);
+    auto empty = [&](int i) { return bar0 + 8u * (C::kStages + i); };
+    auto acc_full = [&](int a) { return bar0 + 8u * (2 * C::kStages + a); };
+    auto acc_empty = [&](int a) { return bar0 + 8u * (2 * C::kStages + 2 + a); };
+    const uint32_t drain = bar0 + 8u * (2 * C::kStages + 4);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * C::kStages + 5);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
-        for (int i = 0; i < kStages; ++i) {
+        for (int i = 0; i < C::kStages; ++i) {
             dev::mbar_init(full(i), 1);
             dev::mbar_init(empty(i), 1);
         }
@@ -90,7 +108,7 @@ __global__ void __launch_bounds__(192, 1) gemm_i8_modm_kernel(const __grid_const
         dev::fence_barrier_init();
     }
     if (warp == 1) {
-        dev::tmem_alloc(dev::smem_addr(tmem_slot), kTmemCols);
+        dev::tmem_alloc(dev::smem_addr(tmem_slot), C::kTmemCols);
         dev::tmem_relinquish();
     }
     dev::tc_fence_before();
@@ -98,7 +116,6 @@ __global__ void __launch_bounds__(192, 1) gemm_i8_modm_kernel(const __grid_const
     dev::tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
     const int64_t nprog = gridDim.x;
-    const int64_t row_block = P.kb_total * kTileBytes;
 
     if (warp == 0) {
         if (lane == 0) {
@@ -108,29 +125,30 @@ __global__ void __launch_bounds__(192, 1) gemm_i8_modm_kernel(const __grid_const
             bool ok = true;
             for (int64_t job = blockIdx.x; ok && job < P.jobs; job += nprog) {
                 const Job J = decode(P, job);
-                const int8_t* srcJ = P.planes_j + J.gt * P.pstride_j + J.tj * row_block;
-                const int8_t* srcI = P.planes_i + J.gt * P.pstride_i + (2 * static_cast<int64_t>(J.ti)) * row_block;
-                for (int64_t kb = P.kb0; kb < P.kb1; ++kb) {
+                const int64_t kb_total = J.I->kb_total, row_block = kb_total * kTileBytes;
+                const int8_t* srcJ = J.I->planes_j + J.gt * J.I->pstride_j + J.tj * row_block;
+                const int8_t* srcI = J.I->planes_i + J.gt * J.I->pstride_i + (static_cast<int64_t>(J.ti) * (BN / 128)) * row_block;
+                for (int64_t kb = 0; ok && kb < kb_total; ++kb) {
                     if (!dev::mbar_wait(empty(stage), phase ^ 1u, abort_flag, P.err, dev::kErrTimeoutEmpty)) {
                         ok = false;
                         break;
                     }
-                    const uint32_t sJ = dev::smem_addr(smem + stage * kStageBytes);
-                    const uint32_t sI = sJ + kStageJ;
-                    dev::mbar_arrive_expect_tx(full(stage), kStageBytes);
+                    const uint32_t sJ = dev::smem_addr(smem + stage * C::kStageBytes);
+                    const uint32_t sI = sJ + C::kStageJ;
+                    dev::mbar_arrive_expect_tx(full(stage), C::kStageBytes);
                     dev::bulk_load(sJ, srcJ + kb * kTileBytes, kTileBytes, full(stage));
                     dev::bulk_load(sI, srcI + kb * kTileBytes, kTileBytes, full(stage));
-                    dev::bulk_load(sI + kTileBytes, srcI + row_block + kb * kTileBytes, kTileBytes, full(stage));
+                    if (BN == 256) dev::bulk_load(sI + kTileBytes, srcI + row_block + kb * kTileBytes, kTileBytes, full(stage));
                     issued_mask |= 1u << stage;
                     issued_phase = (issued_phase & ~(1u << stage)) | (phase << stage);
-                    if (++stage == kStages) {
+                    if (++stage == C::kStages) {
                         stage = 0;
                         phase ^= 1u;
                     }
                 }
             }
             if (!ok) {  // let every copy that was issued land before the CTA exits
-                for (int i = 0; i < kStages; ++i)
+                for (int i = 0; i < C::kStages; ++i)
                     if (issued_mask & (1u << i)) dev::mbar_wait_drain(full(i), (issued_phase >> i) & 1u);
             }
         }
@@ -139,38 +157,43 @@ __global__ void __launch_bounds__(192, 1) gemm_i8_modm_kernel(const __grid_const
             int stage = 0;
             uint32_t phase = 0;
             bool ok = true, issued = false;
-            int local = 0;
-            for (int64_t job = blockIdx.x; ok && job < P.jobs; job += nprog, ++local) {
-                const int acc = local & 1;
-                const uint32_t use = static_cast<uint32_t>(local >> 1);
-                if (!dev::mbar_wait(acc_empty(acc), (use & 1u) ^ 1u, abort_flag, P.err, dev::kErrTimeoutAccEmpty)) {
-                    ok = false;
-                    break;
-                }
-                dev::tc_fence_after();
-                const uint32_t d_tmem = tmem_base + static_cast<uint32_t>(acc) * kGemmI;
-                for (int64_t kb = P.kb0; kb < P.kb1; ++kb) {
-                    if (!dev::mbar_wait(full(stage), phase, abort_flag, P.err, dev::kErrTimeoutFull)) {
+            int local = 0;  // (job, chunk) pairs processed: selects the accumulator
+            for (int64_t job = blockIdx.x; ok && job < P.jobs; job += nprog) {
+                const Job J = decode(P, job);
+                const int64_t kb_total = J.I->kb_total;
+                for (int64_t c = 0; ok && c < J.nch; ++c, ++local) {
+                    const int acc = local & 1;
+                    const uint32_t use = static_cast<uint32_t>(local >> 1);
+                    if (!dev::mbar_wait(acc_empty(acc), (use & 1u) ^ 1u, abort_flag, P.err, dev::kErrTimeoutAccEmpty)) {
                         ok = false;
                         break;
                     }
                     dev::tc_fence_after();
-                    const uint32_t sJ = dev::smem_addr(smem + stage * kStageBytes);
-                    const uint32_t sI = sJ + kStageJ;
+                    const uint32_t d_tmem = tmem_base + static_cast<uint32_t>(acc) * BN;
+                    const int64_t kb0 = c * kChunkKB, kb1 = min(kb_total, kb0 + kChunkKB);
+                    for (int64_t kb = kb0; kb < kb1; ++kb) {
+                        if (!dev::mbar_wait(full(stage), phase, abort_flag, P.err, dev::kErrTimeoutFull)) {
+                            ok = false;
+                            break;
+                        }
+                        dev::tc_fence_after();
+                        const uint32_t sJ = dev::smem_addr(smem + stage * C::kStageBytes);
+                        const uint32_t sI = sJ + C::kStageJ;
 #pragma unroll
-                    for (int kk = 0; kk < kTileK / 32; ++kk) {
-                        dev::mma_i8(d_tmem, dev::sw128_kmajor_desc(sJ + kk * 32), dev::sw128_kmajor_desc(sI + kk * 32),
-                                    kIdesc, (kb > P.kb0 || kk > 0) ? 1u : 0u);
+                        for (int kk = 0; kk < kTileK / 32; ++kk) {
+                            dev::mma_i8(d_tmem, dev::sw128_kmajor_desc(sJ + kk * 32), dev::sw128_kmajor_desc(sI + kk * 32),
+                                        C::kIdesc, (kb > kb0 || kk > 0) ? 1u : 0u);
+                        }
+                        issued = true;
+                        dev::tc_commit(empty(stage));
+                        if (++stage == C::kStages) {
+                            stage = 0;
+                            phase ^= 1u;
+                        }
                     }
-                    issued = true;
-                    dev::tc_commit(empty(stage));
-                    if (++stage == kStages) {
-                        stage = 0;
-                        phase ^= 1u;
-                    }
+                    if (!ok) break;
+                    dev::tc_commit(acc_full(acc));
                 }
-                if (!ok) break;
-                dev::tc_commit(acc_full(acc));
             }
             if (!ok && issued) {  // wait until every MMA issued so far has completed
                 dev::tc_commit(drain);
@@ -180,61 +203,69 @@ __global__ void __launch_bounds__(192, 1) gemm_i8_modm_kernel(const __grid_const
     } else {
         const int quarter = warp & 3;  // TMEM lanes this warp may access
         int local = 0;
-        for (int64_t job = blockIdx.x; job < P.jobs; job += nprog, ++local) {
-            const int acc = local & 1;
-            const uint32_t use = static_cast<uint32_t>(local >> 1);
-            int ok = 1;
-            if (lane == 0) ok = dev::mbar_wait(acc_full(acc), use & 1u, abort_flag, P.err, dev::kErrTimeoutAccFull);
-            ok = __shfl_sync(0xFFFFFFFFu, ok, 0);
-            if (!ok) break;
-            dev::tc_fence_after();
+        bool ok = true;
+        for (int64_t job = blockIdx.x; ok && job < P.jobs; job += nprog) {
             const Job J = decode(P, job);
-            const int t = J.gt % P.s;
-            const uint32_t m = P.mod_m[t], mu = P.mod_mu[t], kneg = P.mod_kneg[t];
+            const int t = J.gt % J.I->s;
+            const uint32_t m = J.I->mod_m[t], mu = J.I->mod_mu[t], kneg = J.I->mod_kneg[t];
             const int64_t j = static_cast<int64_t>(J.tj) * kGemmJ + quarter * 32 + lane;
-            uint8_t* row = P.resid + J.gt * P.rstride + j * P.ldr;
-            const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) +
-                                   static_cast<uint32_t>(acc) * kGemmI;
-#pragma unroll 1
-            for (int c = 0; c < kGemmI / 32; ++c) {
-                uint32_t v[32];
-                dev::tmem_load_32x32(taddr + c * 32, v);
-                dev::tmem_load_wait();
-                const int64_t i0 = static_cast<int64_t>(J.ti) * kGemmI + c * 32;
-                if (j < P.n && i0 < P.m) {
-                    uint32_t w[8];
-                    uint4 old0 = make_uint4(0, 0, 0, 0), old1 = old0;
-                    if (P.accumulate) {
-                        old0 = *reinterpret_cast<const uint4*>(row + i0);
-                        old1 = *reinterpret_cast<const uint4*>(row + i0 + 16);
-                    }
-                    const uint32_t ow[8] = {old0.x, old0.y, old0.z, old0.w, old1.x, old1.y, old1.z, old1.w};
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) {
-                        uint32_t word = 0;
-#pragma unroll
-                        for (int b = 0; b < 4; ++b) {
-                            const uint32_t u = v[4 * q + b] + 0x80000000u;  // int32 c + 2^31
-                            const uint32_t qq = __umulhi(u, mu);
-                            uint32_t r = u - qq * m;
-                            r = min(r, r - m);    // (c + 2^31) mod m
-                            r += kneg;
-                            r = min(r, r - m);    // c mod m
-                            if (P.accumulate) {
-                                r += (ow[q] >> (8 * b)) & 0xFFu;
-                                r = min(r, r - m);
-                            }
-                            word |= r << (8 * b);
-                        }
-                        w[q] = word;
-                    }
-                    *reinterpret_cast<uint4*>(row + i0) = make_uint4(w[0], w[1], w[2], w[3]);
-                    *reinterpret_cast<uint4*>(row + i0 + 16) = make_uint4(w[4], w[5], w[6], w[7]);
+            const int64_t mm = J.I->m, nn = J.I->n;
+            uint8_t* row = J.I->resid + J.gt * J.I->rstride + j * J.I->ldr;
+            for (int64_t c = 0; c < J.nch; ++c, ++local) {
+                const int acc = local & 1;
+                const uint32_t use = static_cast<uint32_t>(local >> 1);
+                int w_ok = 1;
+                if (lane == 0) w_ok = dev::mbar_wait(acc_full(acc), use & 1u, abort_flag, P.err, dev::kErrTimeoutAccFull);
+                w_ok = __shfl_sync(0xFFFFFFFFu, w_ok, 0);
+                if (!w_ok) {
+                    ok = false;
+                    break;
                 }
+                dev::tc_fence_after();
+                const bool accumulate = c > 0;
+                const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) +
+                                       static_cast<uint32_t>(acc) * BN;
+#pragma unroll 1
+                for (int cc = 0; cc < BN / 32; ++cc) {
+                    uint32_t v[32];
+                    dev::tmem_load_32x32(taddr + cc * 32, v);
+                    dev::tmem_load_wait();
+                    const int64_t i0 = static_cast<int64_t>(J.ti) * BN + cc * 32;
+                    if (j < nn && i0 < mm) {
+                        uint32_t w[8];
+                        uint4 old0 = make_uint4(0, 0, 0, 0), old1 = old0;
+                        if (accumulate) {
+                            old0 = *reinterpret_cast<const uint4*>(row + i0);
+                            old1 = *reinterpret_cast<const uint4*>(row + i0 + 16);
+                        }
+                        const uint32_t ow[8] = {old0.x, old0.y, old0.z, old0.w, old1.x, old1.y, old1.z, old1.w};
+#pragma unroll
+                        for (int q = 0; q < 8; ++q) {
+                            uint32_t word = 0;
+#pragma unroll
+                            for (int b = 0; b < 4; ++b) {
+                                const uint32_t u = v[4 * q + b] + 0x80000000u;  // int32 c + 2^31
+                                const uint32_t qq = __umulhi(u, mu);
+                                uint32_t r = u - qq * m;
+                                r = min(r, r - m);  // (c + 2^31) mod m
+                                r += kneg;
+                                r = min(r, r - m);  // c mod m
+                                if (accumulate) {
+                                    r += (ow[q] >> (8 * b)) & 0xFFu;
+                                    r = min(r, r - m);
+                                }
+                                word |= r << (8 * b);
+                            }
+                            w[q] = word;
+                        }
+                        *reinterpret_cast<uint4*>(row + i0) = make_uint4(w[0], w[1], w[2], w[3]);
+                        *reinterpret_cast<uint4*>(row + i0 + 16) = make_uint4(w[4], w[5], w[6], w[7]);
+                    }
+                }
+                dev::tc_fence_before();
+                __syncwarp();
+                if (lane == 0) dev::mbar_arrive(acc_empty(acc));
             }
-            dev::tc_fence_before();
-            __syncwarp();
-            if (lane == 0) dev::mbar_arrive(acc_empty(acc));
         }
     }
     __syncwarp();
@@ -242,46 +273,36 @@ __global__ void __launch_bounds__(192, 1) gemm_i8_modm_kernel(const __grid_const
     __syncthreads();
     if (warp == 1) {
         dev::tc_fence_after();
-        dev::tmem_dealloc(tmem_base, kTmemCols);
+        dev::tmem_dealloc(tmem_base, C::kTmemCols);
     }
+}
+
+template <int BN>
+void launch_bn(const GemmParams& P, int grid, cudaStream_t st) {
+    gemm_i8_modm_kernel<BN><<<grid, 192, Cfg<BN>::kSmemBytes, st>>>(P);
 }
 
 }  // namespace
 
-void launch_gemm(const GemmArgs& a, int num_sms, cudaStream_t st) {
-    GemmParams P{};
-    P.planes_i = a.planes_i;
-    P.planes_j = a.planes_j;
-    P.resid = a.resid;
-    P.pstride_i = a.pstride_i;
-    P.pstride_j = a.pstride_j;
-    P.rstride = a.rstride;
-    P.ldr = a.ldr;
-    P.m = a.m;
-    P.n = a.n;
-    P.kb_total = a.kb_total;
-    P.kb0 = a.kb0;
-    P.kb1 = a.kb1;
-    P.tiles_i = static_cast<int>(ceil_div(a.m, kGemmI));
-    P.tiles_j = static_cast<int>(ceil_div(a.n, kGemmJ));
-    P.tiles = static_cast<int64_t>(P.tiles_i) * P.tiles_j;
-    P.jobs = P.tiles * a.groups * a.s;
-    P.s = a.s;
-    P.accumulate = a.accumulate;
-    P.err = a.err;
-    for (int t = 0; t < a.s; ++t) {
-        P.mod_m[t] = a.mc[t].m;
-        P.mod_mu[t] = a.mc[t].mu;
-        P.mod_kneg[t] = a.mc[t].kneg;
-    }
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(gemm_i8_modm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
-        attr_set = true;
-    }
-    const int64_t grid = std::min<int64_t>(num_sms, P.jobs);
-    if (grid <= 0) return;
-    gemm_i8_modm_kernel<<<static_cast<unsigned>(grid), 192, kSmemBytes, st>>>(P);
+cudaError_t prepare_gemm_kernels() {
+    cudaError_t e = cudaFuncSetAttribute(gemm_i8_modm_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         Cfg<256>::kSmemBytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(gemm_i8_modm_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 Cfg<128>::kSmemBytes);
+    return e;
+}
+
+int64_t gemm_tiles_i(int64_t m, int bn) { return ceil_div(m, bn); }
+
+void launch_gemm(const GemmItem* d_items, int count, int64_t jobs, const GemmConfig& cfg, int num_sms, int* err,
+                 cudaStream_t st) {
+    if (count <= 0 || jobs <= 0) return;
+    GemmParams P{d_items, count, cfg.group_j > 0 ? cfg.group_j : 16, jobs, err};
+    const int ctas = cfg.ctas > 0 ? std::min(cfg.ctas, num_sms) : num_sms;
+    const int grid = static_cast<int>(std::min<int64_t>(ctas, jobs));
+    if (cfg.bn == 128) launch_bn<128>(P, grid, st);
+    else launch_bn<256>(P, grid, st);
 }
 
 }  // namespace oz2

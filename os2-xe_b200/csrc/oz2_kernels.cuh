@@ -1,10 +1,13 @@
-// oz2_kernels.cuh - parameter blocks and launchers of the Ozaki-II device phases:
+// oz2_kernels.cuh - descriptor tables and launchers of the Ozaki-II device phases:
 //   scale : row / column max |x| of op(A), op(B) as raw FP64 bits       (oz2_split.cu)
 //   split : exact power-of-two scaling + symmetric INT8 residues, written
 //           as pre-tiled 128x128-byte swizzled planes                   (oz2_split.cu)
 //   gemm  : tcgen05 kind::i8 products with the mod-m reduction fused
 //           into the epilogue, uint8 residue planes out                  (oz2_gemm.cu)
 //   crt   : CRT reconstruction + unscaling + alpha/beta update           (oz2_crt.cu)
+// Every phase works on a table of items in device memory, so that one launch serves one
+// problem or a whole group of independent problems; blocks (or persistent jobs) are mapped to
+// items through per-item prefix offsets.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -23,9 +26,10 @@ namespace oz2 {
 constexpr int kTileRows = 128;
 constexpr int kTileK = 128;
 constexpr int kTileBytes = kTileRows * kTileK;
-// GEMM tile: 128 columns j of C (MMA M, TMEM lanes) x 256 rows i of C (MMA N, TMEM columns)
+// GEMM tile: 128 columns j of C (MMA M, TMEM lanes) x BN rows i of C (MMA N, TMEM columns),
+// BN in {128, 256}. I-side planes are padded to 256 rows so both widths can read them.
 constexpr int kGemmJ = 128;
-constexpr int kGemmI = 256;
+constexpr int kGemmIPad = 256;
 // k blocks per exact int32 accumulation: 1023 * 128 = 130944 <= 131071, so that
 // k_chunk * 128^2 < 2^31 (ref src/ozaki2_gpu.hpp:32)
 constexpr int kChunkKB = 1023;
@@ -33,23 +37,11 @@ constexpr int kChunkKB = 1023;
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 inline int64_t round_up(int64_t a, int64_t b) { return ceil_div(a, b) * b; }
 
-// One operand side of the scale and split phases, in terms of the plane rows r (rows of op(A)
-// for A, columns of op(B) for B) and the inner index p < k.
-struct SideDesc {
-    const double* X;   // first element of row 0 (already offset for tiles)
-    int64_t ldx;       // leading dimension in elements (complex: in complex elements)
-    int64_t rows;      // valid plane rows
-    int64_t k;
-    bool row_contig;   // element (r, p) at X[r + p*ldx]; else at X[p + r*ldx]
-    bool cplx;         // interleaved (re, im)
-    bool conj;         // use conj(x) (complex only)
-};
-
 // plane geometry of one side
 struct PlaneGeom {
-    int64_t rows_pad;    // rows padded to the tile multiple this side needs (128 for j, 256 for i)
-    int64_t kb_total;    // k blocks per row block
-    int64_t plane_bytes; // bytes of one plane
+    int64_t rows_pad;     // rows padded to the tile multiple this side needs
+    int64_t kb_total;     // k blocks per row block
+    int64_t plane_bytes;  // bytes of one plane
 };
 inline PlaneGeom plane_geom(int64_t rows, int64_t k, int row_multiple) {
     PlaneGeom g;
@@ -59,43 +51,85 @@ inline PlaneGeom plane_geom(int64_t rows, int64_t k, int row_multiple) {
     return g;
 }
 
-void launch_scale(const SideDesc& sd, unsigned long long* maxbits, int num_sms, cudaStream_t st);
-
-// planes: s planes (3s for complex: groups re | im | re+im, group stride s * plane_bytes)
-void launch_split(const SideDesc& sd, const unsigned long long* maxbits, int tk, const ModConst* mc, int s,
-                  int8_t* planes, const PlaneGeom& g, cudaStream_t st);
-
-struct GemmArgs {
-    const int8_t* planes_i;   // I side (op(A) rows), plane rows padded to 256
-    const int8_t* planes_j;   // J side (op(B) columns), plane rows padded to 128
-    uint8_t* resid;           // residue planes: [g][t][j * ldr + i]
-    int64_t pstride_i, pstride_j;  // bytes per plane
-    int64_t rstride;               // bytes per residue plane
-    int64_t ldr;                   // residue plane leading dimension, multiple of 32
-    int64_t m, n;                  // valid i rows, j rows
-    int64_t kb_total;              // k blocks per row block (same on both sides)
-    int64_t kb0, kb1;              // k-block range of this launch
-    int s, groups;
-    int accumulate;                // add to the residues already in resid (k chunks after the first)
-    const ModConst* mc;            // host array of s constants (copied into the kernel parameters)
-    int* err;                      // device error word
+// ---- scale: one item per operand side of a problem. Plane rows r are rows of op(A) (A side)
+// or columns of op(B) (B side); p < k is the inner index.
+struct ScaleItem {
+    const double* X;
+    int64_t ldx, rows, k;
+    int row_contig;  // element (r, p) at X[r + p*ldx]; else at X[p + r*ldx] (complex: pairs)
+    int cplx;
+    unsigned long long* out;  // rows entries, zeroed before the launch
+    int64_t kchunk;           // inner indices per block
+    int64_t block0;           // first block of this item in the launch
+    int64_t rblocks;          // row blocks (blocks = rblocks * k chunks)
 };
-void launch_gemm(const GemmArgs& a, int num_sms, cudaStream_t st);
 
-struct CrtArgs {
+// ---- split: one item per operand panel
+struct SplitItem {
+    const double* X;
+    int64_t ldx, rows, k;
+    int row_contig, cplx, conj;
+    int tk, s;
+    const unsigned long long* maxbits;  // of the panel's rows
+    int8_t* planes;                     // s planes (complex: 3 groups of s)
+    int64_t plane_bytes, kb_total, rows_pad;
+    int64_t block0, rblocks, kblocks;   // blocks = rblocks * kblocks
+    ModConst mc[kMaxModuli];
+};
+
+// ---- gemm: one item per problem; jobs = groups * s * tiles, each job runs all k chunks
+struct GemmItem {
+    const int8_t* planes_i;  // I side (op(A) rows), plane rows padded to 256
+    const int8_t* planes_j;  // J side (op(B) columns), plane rows padded to 128
+    uint8_t* resid;          // residue planes [g][t][j * ldr + i]
+    int64_t pstride_i, pstride_j, rstride, ldr, m, n, kb_total;
+    int64_t tiles, job0;
+    int tiles_i, tiles_j, s, groups;
+    uint32_t mod_m[kMaxModuli], mod_mu[kMaxModuli], mod_kneg[kMaxModuli];
+};
+
+// ---- crt: one item per problem; all items of a launch share s
+struct CrtItem {
     const uint8_t* resid;
-    int64_t rstride, ldr;
-    int64_t m, n;                  // tile dims
-    const unsigned long long* maxA;  // row max bits of op(A) for the tile rows
-    const unsigned long long* maxB;  // column max bits of op(B) for the tile columns
+    int64_t rstride, gstride, ldr, m, n, ldc;
+    const unsigned long long* maxA;  // row max bits of op(A) for the problem rows
+    const unsigned long long* maxB;  // column max bits of op(B) for the problem columns
     int tk;
-    bool cplx;
-    double alpha[2], beta[2];
-    double* C;                     // tile origin (complex: interleaved)
-    int64_t ldc;
-    const Plan* plan;
+    double ar, ai, br, bi;
+    double* C;
+    int64_t block0, iblocks;  // blocks = ceil(n / jb) * iblocks
+    int tq, jb;               // a block: tq threads (4 rows each) along i x jb columns, tq * jb = 256
 };
-void launch_crt(const CrtArgs& a, cudaStream_t st);
+
+// host-side helpers filling the launch-geometry fields; they return the blocks of the item
+int64_t scale_item_blocks(ScaleItem& it, int num_sms, int64_t block0);
+int64_t split_item_blocks(SplitItem& it, int64_t block0);
+int64_t crt_item_blocks(CrtItem& it, int64_t block0);
+
+// launches over device tables (d_items) whose host copies (h_items) give the geometry
+void launch_scale(const ScaleItem* d_items, const ScaleItem* h_items, int count, int64_t blocks, cudaStream_t st);
+// all items of one split launch share row_contig, cplx and the narrow/wide limb path
+void launch_split(const SplitItem* d_items, const SplitItem* h_items, int count, int64_t blocks, cudaStream_t st);
+
+struct GemmConfig {
+    int bn = 256;        // tile width along i (MMA N): 256 or 128
+    int group_j = 16;    // raster: column tiles that share a row panel in flight
+    int ctas = 0;        // persistent CTAs (0 = one per SM)
+};
+void launch_gemm(const GemmItem* d_items, int count, int64_t jobs, const GemmConfig& cfg, int num_sms, int* err,
+                 cudaStream_t st);
+int64_t gemm_tiles_i(int64_t m, int bn);
+
+// all items of one CRT launch share s (the CRT table is a kernel parameter)
+void launch_crt(const CrtItem* d_items, int count, int64_t blocks, const Plan& plan, bool cplx, cudaStream_t st);
+
+// sets the GEMM kernels' shared-memory attribute (once per device, before any graph capture)
+cudaError_t prepare_gemm_kernels();
+
+// Copies up to kParamBlobBytes of host data to device memory by passing them as the parameter
+// of a one-block kernel: no staging buffer, no memcpy, capturable in a graph.
+constexpr size_t kParamBlobBytes = 30 * 1024;
+void launch_write_blob(const void* src, size_t bytes, void* dst, cudaStream_t st);
 
 // C = beta * C (beta == 0 writes zeros), the k == 0 / alpha == 0 path
 void launch_scale_c(double* C, int64_t ldc, int64_t m, int64_t n, const double* beta, bool cplx, cudaStream_t st);

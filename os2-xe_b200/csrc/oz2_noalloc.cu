@@ -102,11 +102,9 @@ extern "C" int oz2_dgemm_noalloc(void* stream, char ta, char tb, int64_t m, int6
         return reject(ps == 1 ? OZ2_EINVAL : OZ2_EINTERNAL, plan_error_text(num_moduli, k, ps, buf, sizeof buf));
     }
     const int s = p.s;
-    const PlaneGeom ga = plane_geom(m, k, kGemmI), gb = plane_geom(n, k, kGemmJ);
+    const PlaneGeom ga = plane_geom(m, k, kGemmIPad), gb = plane_geom(n, k, kGemmJ);
     const int64_t ldr = round_up(m, 32);
     const int64_t kb_total = ga.kb_total;
-    if (kb_total > 65535 * 4 || (kb_total > 65535 && (is_n(ta) || !is_n(tb))))
-        return reject(OZ2_EINVAL, "oz2: k too large for one call of this implementation");
     // scratch layout: error word | maxA | maxB | planes A | planes B | residues
     const size_t o_err = 0;
     const size_t o_maxA = 256;
@@ -121,6 +119,16 @@ extern "C" int oz2_dgemm_noalloc(void* stream, char ta, char tb, int64_t m, int6
                       "oz2_dgemm_noalloc: this problem needs %zu bytes of scratch; the static scratch holds %zu "
                       "bytes (64 MiB): use oz2_dgemm",
                       need, kScratchBytes);
+        return reject(OZ2_EINVAL, buf);
+    }
+    const size_t o_D = need;  // item tables after the buffers
+    const size_t desc_need = o_D + 8 * 1024;
+    if (desc_need > kScratchBytes) {
+        char buf[200];
+        std::snprintf(buf, sizeof buf,
+                      "oz2_dgemm_noalloc: this problem needs %zu bytes of scratch; the static scratch holds %zu "
+                      "bytes (64 MiB): use oz2_dgemm",
+                      desc_need, kScratchBytes);
         return reject(OZ2_EINVAL, buf);
     }
     unsigned char* scratch = nullptr;
@@ -139,52 +147,93 @@ extern "C" int oz2_dgemm_noalloc(void* stream, char ta, char tb, int64_t m, int6
     cudaError_t e = cudaMemsetAsync(scratch, 0, o_A, st);
     if (e != cudaSuccess) return reject(OZ2_ECUDA, std::string("oz2_dgemm_noalloc: ") + cudaGetErrorString(e));
 
+    // item tables (one problem), written into the scratch by a kernel that takes them as its
+    // parameter: host memory only, no staging buffer
     ModConst mc[kMaxModuli];
     mod_constants(p, mc);
-    SideDesc sa{A, lda, m, k, is_n(ta), false, false};
-    SideDesc sb{B, ldb, n, k, !is_n(tb), false, false};
-    launch_scale(sa, maxA, num_sms, st);
-    launch_scale(sb, maxB, num_sms, st);
-    launch_split(sb, maxB, p.tk, mc, s, planesB, gb, st);
-    launch_split(sa, maxA, p.tk, mc, s, planesA, ga, st);
-    const int64_t chunks = ceil_div(kb_total, kChunkKB);
-    for (int64_t c = 0; c < chunks; ++c) {
-        GemmArgs g{};
-        g.planes_i = planesA;
-        g.planes_j = planesB;
-        g.resid = resid;
-        g.pstride_i = ga.plane_bytes;
-        g.pstride_j = gb.plane_bytes;
-        g.rstride = n * ldr;
-        g.ldr = ldr;
-        g.m = m;
-        g.n = n;
-        g.kb_total = kb_total;
-        g.kb0 = c * kChunkKB;
-        g.kb1 = std::min(kb_total, g.kb0 + kChunkKB);
-        g.s = s;
-        g.groups = 1;
-        g.accumulate = c > 0;
-        g.mc = mc;
-        g.err = err;
-        launch_gemm(g, num_sms, st);
+    struct Tables {
+        ScaleItem sc[2];
+        SplitItem sp[2];
+        GemmItem g;
+        CrtItem c;
+    };
+    static thread_local Tables T;
+    T = Tables{};
+    for (int side = 0; side < 2; ++side) {
+        ScaleItem& si = T.sc[side];
+        si.X = side ? B : A;
+        si.ldx = side ? ldb : lda;
+        si.rows = side ? n : m;
+        si.k = k;
+        si.row_contig = side ? !is_n(tb) : is_n(ta);
+        si.out = side ? maxB : maxA;
+        scale_item_blocks(si, num_sms, 0);
+        SplitItem& sp = T.sp[side];
+        sp.X = si.X;
+        sp.ldx = si.ldx;
+        sp.rows = si.rows;
+        sp.k = k;
+        sp.row_contig = si.row_contig;
+        sp.tk = p.tk;
+        sp.s = s;
+        sp.maxbits = si.out;
+        sp.planes = side ? planesB : planesA;
+        const PlaneGeom& gg = side ? gb : ga;
+        sp.plane_bytes = gg.plane_bytes;
+        sp.kb_total = gg.kb_total;
+        sp.rows_pad = gg.rows_pad;
+        for (int t = 0; t < s; ++t) sp.mc[t] = mc[t];
+        split_item_blocks(sp, 0);
     }
-    CrtArgs ca{};
-    ca.resid = resid;
-    ca.rstride = n * ldr;
-    ca.ldr = ldr;
-    ca.m = m;
-    ca.n = n;
-    ca.maxA = maxA;
-    ca.maxB = maxB;
-    ca.tk = p.tk;
-    ca.cplx = false;
-    ca.alpha[0] = alpha;
-    ca.beta[0] = beta;
-    ca.C = C;
-    ca.ldc = ldc;
-    ca.plan = &p;
-    launch_crt(ca, st);
+    GemmConfig cfg;
+    cfg.bn = m <= 384 ? 128 : 256;
+    GemmItem& g = T.g;
+    g.planes_i = planesA;
+    g.planes_j = planesB;
+    g.resid = resid;
+    g.pstride_i = ga.plane_bytes;
+    g.pstride_j = gb.plane_bytes;
+    g.rstride = n * ldr;
+    g.ldr = ldr;
+    g.m = m;
+    g.n = n;
+    g.kb_total = kb_total;
+    g.tiles_i = static_cast<int>(gemm_tiles_i(m, cfg.bn));
+    g.tiles_j = static_cast<int>(ceil_div(n, kGemmJ));
+    g.tiles = static_cast<int64_t>(g.tiles_i) * g.tiles_j;
+    g.s = s;
+    g.groups = 1;
+    g.job0 = 0;
+    for (int t = 0; t < s; ++t) {
+        g.mod_m[t] = mc[t].m;
+        g.mod_mu[t] = mc[t].mu;
+        g.mod_kneg[t] = mc[t].kneg;
+    }
+    CrtItem& c = T.c;
+    c.resid = resid;
+    c.rstride = n * ldr;
+    c.gstride = c.rstride * s;
+    c.ldr = ldr;
+    c.m = m;
+    c.n = n;
+    c.ldc = ldc;
+    c.maxA = maxA;
+    c.maxB = maxB;
+    c.tk = p.tk;
+    c.ar = alpha;
+    c.br = beta;
+    c.C = C;
+    const int64_t crt_blocks = crt_item_blocks(c, 0);
+    static_assert(sizeof(Tables) <= 8 * 1024, "item tables exceed their scratch region");
+    unsigned char* dtab = scratch + o_D;
+    launch_write_blob(&T, sizeof(Tables), dtab, st);
+    const Tables* D = reinterpret_cast<const Tables*>(dtab);
+    for (int side = 0; side < 2; ++side)
+        launch_scale(&D->sc[side], &T.sc[side], 1, T.sc[side].rblocks * ceil_div(k, T.sc[side].kchunk), st);
+    for (int side = 1; side >= 0; --side)
+        launch_split(&D->sp[side], &T.sp[side], 1, T.sp[side].rblocks * T.sp[side].kblocks, st);
+    launch_gemm(&D->g, 1, g.tiles * s, cfg, num_sms, err, st);
+    launch_crt(&D->c, 1, crt_blocks, p, false, st);
     e = cudaGetLastError();
     return e == cudaSuccess ? OZ2_OK : reject(OZ2_ECUDA, std::string("oz2_dgemm_noalloc: ") + cudaGetErrorString(e));
 }

@@ -127,6 +127,7 @@ int make_plan(int s, int64_t k, Plan& p) {
         p.y[t] = static_cast<uint32_t>(y);
     }
     std::memcpy(p.M, M.w, sizeof M.w);
+    mod_constants(p, p.mc);
     return 0;
 }
 

@@ -26,22 +26,6 @@ OZ2_HD constexpr int limbs_for(int s) {
     return t[s];
 }
 
-struct Plan {
-    int s = 0;
-    int nl = 0;
-    int tk = 0;
-    double log2M = 0;
-    uint32_t m[kMaxModuli] = {};
-    uint32_t y[kMaxModuli] = {};             // (M/m_t)^-1 mod m_t
-    uint32_t W[kMaxModuli][kBigWords] = {};  // CRT weights (M/m_t) y_t
-    uint32_t M[kBigWords] = {};
-};
-
-// Returns 0, or 1 (invalid: s out of [2, 24], k < 1, s too small for k), or 5 (overflow).
-// ref src/ozaki2_gpu.hpp:159-200
-int make_plan(int s, int64_t k, Plan& p);
-const char* plan_error_text(int s, int64_t k, int status, char* buf, int len);
-
 // Constants of one modulus as the kernels use them.
 struct ModConst {
     uint32_t m;      // modulus
@@ -52,6 +36,23 @@ struct ModConst {
     uint32_t koff5;  // (h - 2^104 mod m) mod m: wide limb offset
     uint32_t kneg;   // (m - 2^31 mod m) mod m: undoes the +2^31 bias of a signed int32
 };
+
+struct Plan {
+    int s = 0;
+    int nl = 0;
+    int tk = 0;
+    double log2M = 0;
+    uint32_t m[kMaxModuli] = {};
+    uint32_t y[kMaxModuli] = {};             // (M/m_t)^-1 mod m_t
+    uint32_t W[kMaxModuli][kBigWords] = {};  // CRT weights (M/m_t) y_t
+    uint32_t M[kBigWords] = {};
+    ModConst mc[kMaxModuli] = {};            // per-modulus kernel constants (mod_constants)
+};
+
+// Returns 0, or 1 (invalid: s out of [2, 24], k < 1, s too small for k), or 5 (overflow).
+// ref src/ozaki2_gpu.hpp:159-200
+int make_plan(int s, int64_t k, Plan& p);
+const char* plan_error_text(int s, int64_t k, int status, char* buf, int len);
 
 void mod_constants(const Plan& p, ModConst* out);
 

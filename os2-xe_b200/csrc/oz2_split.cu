@@ -7,6 +7,8 @@
 //        e_r = tk - frexp_exp(max_r) (ref :360-377, :251-289) and its symmetric residue
 //        modulo each m_t in [-h_t, m_t-1-h_t] (ref :407-455, complex 3M form :457-520),
 //        stored as int8 in the pre-tiled plane layout of oz2_kernels.cuh.
+#include <algorithm>
+
 #include "oz2_kernels.cuh"
 
 namespace oz2 {
@@ -23,125 +25,101 @@ __device__ __forceinline__ int exponent_of(unsigned long long b, int tk) {
     return tk - e2;
 }
 
-// ------------------------------------------------------------------ scale
-struct ScaleParams {
-    const double* X;
-    int64_t ldx, rows, k, kchunk;
-    unsigned long long* out;
-};
-
-// plane rows contiguous in memory: one thread per row, a k range per grid row
-template <bool CPLX>
-__global__ void __launch_bounds__(256) scale_rowc_kernel(const __grid_constant__ ScaleParams P) {
-    const int64_t r = static_cast<int64_t>(blockIdx.x) * 256 + threadIdx.x;
-    if (r >= P.rows) return;
-    const int64_t p0 = static_cast<int64_t>(blockIdx.y) * P.kchunk;
-    const int64_t p1 = min(P.k, p0 + P.kchunk);
-    unsigned long long best = 0;
-    const unsigned long long* X = reinterpret_cast<const unsigned long long*>(P.X);
-    for (int64_t p = p0; p < p1; ++p) {
-        const int64_t idx = r + p * P.ldx;
-        if (CPLX) {
-            best = max(best, X[2 * idx] & kAbsMask);
-            best = max(best, X[2 * idx + 1] & kAbsMask);
-        } else {
-            best = max(best, __ldg(X + idx) & kAbsMask);
-        }
+// ------------------------------------------------------------------ item lookup
+// index of the item whose [block0, next block0) range holds `b` (items sorted by block0)
+template <class Item>
+__device__ __forceinline__ int find_item(const Item* items, int count, int64_t b) {
+    int lo = 0, hi = count - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (items[mid].block0 <= b) lo = mid;
+        else hi = mid - 1;
     }
-    if (best) atomicMax(P.out + r, best);
+    return lo;
 }
 
-// inner index contiguous: one warp per row, a k range per grid row
-template <bool CPLX>
-__global__ void __launch_bounds__(256) scale_kc_kernel(const __grid_constant__ ScaleParams P) {
-    const int64_t r = static_cast<int64_t>(blockIdx.x) * 8 + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
-    if (r >= P.rows) return;
-    const int w = CPLX ? 2 : 1;
-    const int64_t p0 = static_cast<int64_t>(blockIdx.y) * P.kchunk * w;
-    const int64_t p1 = min(P.k * w, p0 + P.kchunk * w);
-    const unsigned long long* X = reinterpret_cast<const unsigned long long*>(P.X) + r * P.ldx * w;
-    unsigned long long best = 0;
-    for (int64_t p = p0 + lane; p < p1; p += 32) best = max(best, __ldg(X + p) & kAbsMask);
+// ------------------------------------------------------------------ scale
+// ROWC: plane rows contiguous in memory, one thread per row and a k range per block.
+// Otherwise: inner index contiguous, one warp per row and a k range per block.
+template <bool CPLX, bool ROWC>
+__global__ void __launch_bounds__(256) scale_kernel(const ScaleItem* __restrict__ items, int count) {
+    const ScaleItem* I = items + find_item(items, count, blockIdx.x);
+    const int64_t local = static_cast<int64_t>(blockIdx.x) - I->block0;
+    const int64_t rb = local % I->rblocks, kc = local / I->rblocks;
+    const unsigned long long* X = reinterpret_cast<const unsigned long long*>(I->X);
+    const int64_t rows = I->rows, k = I->k, ldx = I->ldx, kchunk = I->kchunk;
+    if (ROWC) {
+        // 32 consecutive rows per block (one per lane); the 8 warps interleave the k range
+        const int64_t r = rb * 32 + (threadIdx.x & 31);
+        if (r >= rows) return;
+        const int64_t p0 = kc * kchunk, p1 = min(k, p0 + kchunk);
+        unsigned long long best = 0;
+        for (int64_t p = p0 + (threadIdx.x >> 5); p < p1; p += 8) {
+            const int64_t idx = r + p * ldx;
+            if (CPLX) {
+                best = max(best, __ldg(X + 2 * idx) & kAbsMask);
+                best = max(best, __ldg(X + 2 * idx + 1) & kAbsMask);
+            } else {
+                best = max(best, __ldg(X + idx) & kAbsMask);
+            }
+        }
+        if (best) atomicMax(I->out + r, best);
+    } else {
+        const int64_t r = rb * 8 + (threadIdx.x >> 5);
+        const int lane = threadIdx.x & 31;
+        if (r >= rows) return;
+        const int w = CPLX ? 2 : 1;
+        const int64_t p0 = kc * kchunk * w, p1 = min(k * w, p0 + kchunk * w);
+        const unsigned long long* row = X + r * ldx * w;
+        unsigned long long best = 0;
+        for (int64_t p = p0 + lane; p < p1; p += 32) best = max(best, __ldg(row + p) & kAbsMask);
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) best = max(best, __shfl_xor_sync(0xFFFFFFFFu, best, o));
-    if (lane == 0 && best) atomicMax(P.out + r, best);
+        for (int o = 16; o > 0; o >>= 1) best = max(best, __shfl_xor_sync(0xFFFFFFFFu, best, o));
+        if (lane == 0 && best) atomicMax(I->out + r, best);
+    }
 }
 
 // ------------------------------------------------------------------ split
-struct SplitParams {
-    const double* X;
-    int64_t ldx, rows, k;
-    const unsigned long long* maxbits;
-    int tk, s, conj;
-    int8_t* planes;
-    int64_t plane_bytes, kb_total, rows_pad;
-    ModConst mc[kMaxModuli];
-};
-
-// 21-bit limbs of 2^OFF + RNE(v 2^e) (OFF = 62 for NLIMB = 3, 104 for NLIMB = 5)
-template <int NLIMB>
-__device__ __forceinline__ void offset_limbs(double v, int e, uint32_t (&L)[NLIMB]) {
-    const uint64_t bits = static_cast<uint64_t>(__double_as_longlong(v));
-    const bool neg = (bits >> 63) != 0;
-    const int be = static_cast<int>((bits >> 52) & 0x7FF);
-    uint64_t mant = bits & 0xFFFFFFFFFFFFFull;
-    if (be) mant |= 0x10000000000000ull;
-    const int sh = (be ? be : 1) - 1075 + e;
-    uint64_t lo = 0, hi = 0;
-    if (mant) {
-        if (sh >= 0) {
-            if (NLIMB == 3) {
-                lo = mant << sh;
-            } else {
-                lo = sh < 64 ? mant << sh : 0;
-                hi = sh == 0 ? 0 : (sh < 64 ? mant >> (64 - sh) : mant << (sh - 64));
-            }
-        } else if (sh >= -54) {
-            const int rs = -sh;
-            const uint64_t q = mant >> rs;
-            const uint64_t rem = mant & ((1ull << rs) - 1);
-            const uint64_t half = 1ull << (rs - 1);
-            lo = q + ((rem > half || (rem == half && (q & 1))) ? 1 : 0);
-        }
-    }
-    if (NLIMB == 3) {
-        const uint64_t xo = neg ? (1ull << 62) - lo : (1ull << 62) + lo;
-        L[0] = static_cast<uint32_t>(xo) & kMask21;
-        L[1] = static_cast<uint32_t>(xo >> 21) & kMask21;
-        L[2] = static_cast<uint32_t>(xo >> 42) & kMask21;
-    } else {
-        uint64_t ol, oh;
-        if (neg) {
-            ol = 0 - lo;
-            oh = (1ull << 40) - hi - (lo != 0 ? 1 : 0);
-        } else {
-            ol = lo;
-            oh = (1ull << 40) + hi;
-        }
-        L[0] = static_cast<uint32_t>(ol) & kMask21;
-        L[1] = static_cast<uint32_t>(ol >> 21) & kMask21;
-        L[2] = static_cast<uint32_t>(ol >> 42) & kMask21;
-        L[NLIMB > 3 ? 3 : 0] = static_cast<uint32_t>((ol >> 63) | (oh << 1)) & kMask21;
-        L[NLIMB > 4 ? 4 : 0] = static_cast<uint32_t>(oh >> 20) & kMask21;
-    }
-}
-
 // 2^k as a double for k in [-1022, 1023]
 __device__ __forceinline__ double pow2(int k) {
     return __longlong_as_double(static_cast<long long>(k + 1023) << 52);
 }
 
-// Narrow path (tk <= 62) in floating point: y = v 2^e as two exact power-of-two products
-// (e = e1 + e2 keeps both factors normal for every e this path produces; a product that
-// underflows means |y| < 2^-1022, which rounds to 0 like the exact value), then one
-// round-to-nearest-even conversion to int64: the same integer as the bit-level RNE above.
+// x = RNE(v 2^e) as the reference derives it from the double's bits (src/ozaki2_gpu.hpp:251-289),
+// computed in floating point: y = v 2^e as two exact power-of-two products (e = e1 + e2 keeps
+// both factors normal for every e the split sees; a product that underflows means
+// |y| < 2^-1022, which rounds to 0 like the exact value), then one round-to-nearest-even
+// conversion. Narrow path (tk <= 62): x fits int64, limbs of 2^62 + x.
 __device__ __forceinline__ void offset_limbs_fp(double v, double s1, double s2, uint32_t (&L)[3]) {
     const long long x = __double2ll_rn((v * s1) * s2);
     const uint64_t xo = static_cast<uint64_t>(x + (1ll << 62));
     L[0] = static_cast<uint32_t>(xo) & kMask21;
     L[1] = static_cast<uint32_t>(xo >> 21) & kMask21;
     L[2] = static_cast<uint32_t>(xo >> 42) & kMask21;
+}
+
+// Wide path (62 < tk <= 100) in floating point: y = v 2^e as above, a = |rint(y)| < 2^101 split
+// exactly into hi = trunc(a 2^-64) and lo = a - hi 2^64 (both exact: power-of-two scaling, and
+// lo keeps a subset of a's 53 significant bits), then 2^104 +- (hi:lo) in 21-bit limbs.
+__device__ __forceinline__ void offset_limbs_fp_wide(double v, double s1, double s2, uint32_t (&L)[5]) {
+    const double y = rint((v * s1) * s2);
+    const double a = fabs(y);
+    const double hd = trunc(a * 5.421010862427522e-20);  // 2^-64
+    const double ld = fma(hd, -18446744073709551616.0, a);  // a - hd 2^64, exact
+    const uint64_t hi = __double2ull_rz(hd), lo = __double2ull_rz(ld);
+    uint64_t ol, oh;
+    if (y < 0.0) {
+        ol = 0 - lo;
+        oh = (1ull << 40) - hi - (lo != 0 ? 1 : 0);
+    } else {
+        ol = lo;
+        oh = (1ull << 40) + hi;
+    }
+    L[0] = static_cast<uint32_t>(ol) & kMask21;
+    L[1] = static_cast<uint32_t>(ol >> 21) & kMask21;
+    L[2] = static_cast<uint32_t>(ol >> 42) & kMask21;
+    L[3] = static_cast<uint32_t>((ol >> 63) | (oh << 1)) & kMask21;
+    L[4] = static_cast<uint32_t>(oh >> 20) & kMask21;
 }
 
 // symmetric residue of the value whose offset limbs are L, as an int in [-h, m-1-h]
@@ -166,18 +144,42 @@ __device__ __forceinline__ uint32_t pack_bytes(uint32_t a, uint32_t b, uint32_t 
 // warps of a block are the 8 chunks of one 128-wide k block. Otherwise a warp is one row and
 // 32 consecutive chunks (512 inner indices), the 8 warps are 8 rows.
 template <int NLIMB, bool CPLX, bool ROWC>
-__global__ void __launch_bounds__(256) split_kernel(const __grid_constant__ SplitParams P) {
+__global__ void __launch_bounds__(256) split_kernel(const SplitItem* __restrict__ items, int count) {
+    const SplitItem* __restrict__ I = items + find_item(items, count, blockIdx.x);
+    const int64_t local = static_cast<int64_t>(blockIdx.x) - I->block0;
+    const int64_t bx = local % I->rblocks, by = local / I->rblocks;
     int64_t r, k0;
     if (ROWC) {
-        r = static_cast<int64_t>(blockIdx.x) * 32 + (threadIdx.x & 31);
-        k0 = static_cast<int64_t>(blockIdx.y) * kTileK + (threadIdx.x >> 5) * 16;
+        r = bx * 32 + (threadIdx.x & 31);
+        k0 = by * kTileK + (threadIdx.x >> 5) * 16;
     } else {
-        r = static_cast<int64_t>(blockIdx.x) * 8 + (threadIdx.x >> 5);
-        k0 = static_cast<int64_t>(blockIdx.y) * (4 * kTileK) + (threadIdx.x & 31) * 16;
+        r = bx * 8 + (threadIdx.x >> 5);
+        k0 = by * (4 * kTileK) + (threadIdx.x & 31) * 16;
     }
-    if (r >= P.rows_pad || k0 >= P.kb_total * kTileK) return;
-    const int e = r < P.rows ? exponent_of(P.maxbits[r], P.tk) : 0;
-    const bool live = r < P.rows && e != kNonFinite;
+    const int64_t kb_total = I->kb_total, plane_bytes = I->plane_bytes, ldx = I->ldx, k = I->k;
+    const int64_t rows = I->rows;
+    if (r >= I->rows_pad || k0 >= kb_total * kTileK) return;
+    const double* X = I->X;
+    const int conj = I->conj, nmod = I->s;
+    const int64_t rb = r >> 7;
+    const int rr = static_cast<int>(r & 127);
+    const int64_t kb = k0 >> 7;
+    const int c = static_cast<int>((k0 >> 4) & 7);
+    int8_t* out = I->planes + (rb * kb_total + kb) * kTileBytes + rr * kTileK + ((c ^ (rr & 7)) << 4);
+    const int64_t gstride = static_cast<int64_t>(nmod) * plane_bytes;
+    if (r >= rows || k0 >= k) {  // padding: residues of zero are zero
+        const uint4 z = make_uint4(0, 0, 0, 0);
+        for (int t = 0; t < nmod; ++t) {
+            *reinterpret_cast<uint4*>(out + t * plane_bytes) = z;
+            if (CPLX) {
+                *reinterpret_cast<uint4*>(out + gstride + t * plane_bytes) = z;
+                *reinterpret_cast<uint4*>(out + 2 * gstride + t * plane_bytes) = z;
+            }
+        }
+        return;
+    }
+    const int e = exponent_of(I->maxbits[r], I->tk);
+    const bool live = e != kNonFinite;
 
     constexpr int NG = CPLX ? 2 : 1;
     uint32_t L[NG][16][NLIMB];
@@ -187,34 +189,27 @@ __global__ void __launch_bounds__(256) split_kernel(const __grid_constant__ Spli
     for (int q = 0; q < 16; ++q) {
         const int64_t p = k0 + q;
         double v0 = 0.0, v1 = 0.0;
-        if (live && p < P.k) {
-            const int64_t idx = ROWC ? r + p * P.ldx : p + r * P.ldx;
+        if (live && p < k) {
+            const int64_t idx = ROWC ? r + p * ldx : p + r * ldx;
             if (CPLX) {
-                v0 = __ldg(P.X + 2 * idx);
-                v1 = __ldg(P.X + 2 * idx + 1);
-                if (P.conj) v1 = -v1;  // residues of -y are the negated residues of y
+                v0 = __ldg(X + 2 * idx);
+                v1 = __ldg(X + 2 * idx + 1);
+                if (conj) v1 = -v1;  // residues of -y are the negated residues of y
             } else {
-                v0 = __ldg(P.X + idx);
+                v0 = __ldg(X + idx);
             }
         }
         if constexpr (NLIMB == 3) {
             offset_limbs_fp(v0, s1, s2, L[0][q]);
             if (CPLX) offset_limbs_fp(v1, s1, s2, L[NG - 1][q]);
         } else {
-            offset_limbs<NLIMB>(v0, e, L[0][q]);
-            if (CPLX) offset_limbs<NLIMB>(v1, e, L[NG - 1][q]);
+            offset_limbs_fp_wide(v0, s1, s2, L[0][q]);
+            if (CPLX) offset_limbs_fp_wide(v1, s1, s2, L[NG - 1][q]);
         }
     }
 
-    const int64_t rb = r >> 7;
-    const int rr = static_cast<int>(r & 127);
-    const int64_t kb = k0 >> 7;
-    const int c = static_cast<int>((k0 >> 4) & 7);
-    int8_t* out = P.planes + (rb * P.kb_total + kb) * kTileBytes + rr * kTileK + ((c ^ (rr & 7)) << 4);
-    const int64_t gstride = static_cast<int64_t>(P.s) * P.plane_bytes;
-
-    for (int t = 0; t < P.s; ++t) {
-        const ModConst mc = P.mc[t];
+    for (int t = 0; t < nmod; ++t) {
+        const ModConst mc = I->mc[t];
         uint32_t b0[16], b1[16], b2[16];  // residue bytes in the low 8 bits
         if (mc.m == 256) {
             // 2^21 j = 0 mod 256 and 2^62 = 0 mod 256: the residue byte is the low byte of 2^62 + x
@@ -251,74 +246,78 @@ __global__ void __launch_bounds__(256) split_kernel(const __grid_constant__ Spli
                 w2[q] = pack_bytes(b2[4 * q], b2[4 * q + 1], b2[4 * q + 2], b2[4 * q + 3]);
             }
         }
-        *reinterpret_cast<uint4*>(out + t * P.plane_bytes) = make_uint4(w0[0], w0[1], w0[2], w0[3]);
+        *reinterpret_cast<uint4*>(out + t * plane_bytes) = make_uint4(w0[0], w0[1], w0[2], w0[3]);
         if (CPLX) {
-            *reinterpret_cast<uint4*>(out + gstride + t * P.plane_bytes) = make_uint4(w1[0], w1[1], w1[2], w1[3]);
-            *reinterpret_cast<uint4*>(out + 2 * gstride + t * P.plane_bytes) =
-                make_uint4(w2[0], w2[1], w2[2], w2[3]);
+            *reinterpret_cast<uint4*>(out + gstride + t * plane_bytes) = make_uint4(w1[0], w1[1], w1[2], w1[3]);
+            *reinterpret_cast<uint4*>(out + 2 * gstride + t * plane_bytes) = make_uint4(w2[0], w2[1], w2[2], w2[3]);
         }
     }
 }
 
 template <int NLIMB, bool CPLX>
-void split_dispatch(const SplitParams& P, bool rowc, cudaStream_t st) {
-    if (rowc) {
-        dim3 grid(static_cast<unsigned>(ceil_div(P.rows_pad, 32)), static_cast<unsigned>(P.kb_total));
-        split_kernel<NLIMB, CPLX, true><<<grid, 256, 0, st>>>(P);
-    } else {
-        dim3 grid(static_cast<unsigned>(ceil_div(P.rows_pad, 8)), static_cast<unsigned>(ceil_div(P.kb_total, 4)));
-        split_kernel<NLIMB, CPLX, false><<<grid, 256, 0, st>>>(P);
-    }
+void split_dispatch(const SplitItem* d, int count, int64_t blocks, bool rowc, cudaStream_t st) {
+    if (rowc) split_kernel<NLIMB, CPLX, true><<<static_cast<unsigned>(blocks), 256, 0, st>>>(d, count);
+    else split_kernel<NLIMB, CPLX, false><<<static_cast<unsigned>(blocks), 256, 0, st>>>(d, count);
 }
 
 }  // namespace
 
-void launch_scale(const SideDesc& sd, unsigned long long* maxbits, int num_sms, cudaStream_t st) {
-    if (sd.rows <= 0 || sd.k <= 0) return;
-    ScaleParams P{sd.X, sd.ldx, sd.rows, sd.k, 0, maxbits};
+int64_t scale_item_blocks(ScaleItem& it, int num_sms, int64_t block0) {
+    it.block0 = block0;
+    if (it.rows <= 0 || it.k <= 0) {
+        it.rblocks = 1;
+        it.kchunk = 1;
+        return 0;
+    }
     const int64_t target = static_cast<int64_t>(num_sms) * 2048 * 2;  // threads in flight
-    if (sd.row_contig) {
-        const int64_t rthreads = round_up(sd.rows, 256);
-        int64_t chunks = std::max<int64_t>(1, std::min<int64_t>(sd.k, target / rthreads));
-        chunks = std::min<int64_t>(chunks, 65535);
-        P.kchunk = ceil_div(sd.k, chunks);
-        dim3 grid(static_cast<unsigned>(rthreads / 256), static_cast<unsigned>(ceil_div(sd.k, P.kchunk)));
-        if (sd.cplx) scale_rowc_kernel<true><<<grid, 256, 0, st>>>(P);
-        else scale_rowc_kernel<false><<<grid, 256, 0, st>>>(P);
+    if (it.row_contig) {
+        it.rblocks = ceil_div(it.rows, 32);
+        // at least 64 inner indices per block (8 per warp)
+        const int64_t chunks =
+            std::max<int64_t>(1, std::min<int64_t>(ceil_div(it.k, 64), target / (it.rblocks * 256)));
+        it.kchunk = ceil_div(it.k, chunks);
     } else {
-        const int64_t rthreads = sd.rows * 32;
-        int64_t chunks = std::max<int64_t>(1, std::min<int64_t>(ceil_div(sd.k, 256), target / rthreads));
-        chunks = std::min<int64_t>(chunks, 65535);
-        P.kchunk = ceil_div(sd.k, chunks);
-        dim3 grid(static_cast<unsigned>(ceil_div(sd.rows, 8)), static_cast<unsigned>(ceil_div(sd.k, P.kchunk)));
-        if (sd.cplx) scale_kc_kernel<true><<<grid, 256, 0, st>>>(P);
-        else scale_kc_kernel<false><<<grid, 256, 0, st>>>(P);
+        it.rblocks = ceil_div(it.rows, 8);
+        const int64_t chunks = std::max<int64_t>(1, std::min<int64_t>(ceil_div(it.k, 256), target / (it.rows * 32)));
+        it.kchunk = ceil_div(it.k, chunks);
+    }
+    return it.rblocks * ceil_div(it.k, it.kchunk);
+}
+
+int64_t split_item_blocks(SplitItem& it, int64_t block0) {
+    it.block0 = block0;
+    if (it.row_contig) {
+        it.rblocks = ceil_div(it.rows_pad, 32);
+        it.kblocks = it.kb_total;
+    } else {
+        it.rblocks = ceil_div(it.rows_pad, 8);
+        it.kblocks = ceil_div(it.kb_total, 4);
+    }
+    return it.rblocks * it.kblocks;
+}
+
+void launch_scale(const ScaleItem* d, const ScaleItem* h, int count, int64_t blocks, cudaStream_t st) {
+    if (count <= 0 || blocks <= 0) return;
+    const bool rowc = h[0].row_contig != 0, cplx = h[0].cplx != 0;
+    const unsigned g = static_cast<unsigned>(blocks);
+    if (rowc) {
+        if (cplx) scale_kernel<true, true><<<g, 256, 0, st>>>(d, count);
+        else scale_kernel<false, true><<<g, 256, 0, st>>>(d, count);
+    } else {
+        if (cplx) scale_kernel<true, false><<<g, 256, 0, st>>>(d, count);
+        else scale_kernel<false, false><<<g, 256, 0, st>>>(d, count);
     }
 }
 
-void launch_split(const SideDesc& sd, const unsigned long long* maxbits, int tk, const ModConst* mc, int s,
-                  int8_t* planes, const PlaneGeom& g, cudaStream_t st) {
-    SplitParams P{};
-    P.X = sd.X;
-    P.ldx = sd.ldx;
-    P.rows = sd.rows;
-    P.k = sd.k;
-    P.maxbits = maxbits;
-    P.tk = tk;
-    P.s = s;
-    P.conj = sd.conj ? 1 : 0;
-    P.planes = planes;
-    P.plane_bytes = g.plane_bytes;
-    P.kb_total = g.kb_total;
-    P.rows_pad = g.rows_pad;
-    for (int t = 0; t < s; ++t) P.mc[t] = mc[t];
-    const bool wide = tk > kNarrowScaleBits;
-    if (sd.cplx) {
-        if (wide) split_dispatch<5, true>(P, sd.row_contig, st);
-        else split_dispatch<3, true>(P, sd.row_contig, st);
+void launch_split(const SplitItem* d, const SplitItem* h, int count, int64_t blocks, cudaStream_t st) {
+    if (count <= 0 || blocks <= 0) return;
+    const bool wide = h[0].tk > kNarrowScaleBits, rowc = h[0].row_contig != 0;
+    if (h[0].cplx) {
+        if (wide) split_dispatch<5, true>(d, count, blocks, rowc, st);
+        else split_dispatch<3, true>(d, count, blocks, rowc, st);
     } else {
-        if (wide) split_dispatch<5, false>(P, sd.row_contig, st);
-        else split_dispatch<3, false>(P, sd.row_contig, st);
+        if (wide) split_dispatch<5, false>(d, count, blocks, rowc, st);
+        else split_dispatch<3, false>(d, count, blocks, rowc, st);
     }
 }
 

@@ -42,6 +42,20 @@ _lib.oz2_stage_times.argtypes = [_vp, C.POINTER(_dbl)]
 _lib.oz2_last_tiling.argtypes = [_vp, C.POINTER(_i64)]
 _lib.oz2_set_tuning.argtypes = [_vp, _i32, _i32, _i32]
 _lib.oz2_check_device_error.argtypes = [_vp]
+
+
+class DgemmProblem(C.Structure):
+    """oz2_dgemm_problem of include/oz2/oz2.h"""
+    _fields_ = [("ta", _chr), ("tb", _chr), ("num_moduli", _i32), ("m", _i64), ("n", _i64), ("k", _i64),
+                ("alpha", _dbl), ("beta", _dbl), ("A", _vp), ("lda", _i64), ("B", _vp), ("ldb", _i64), ("C", _vp),
+                ("ldc", _i64)]
+
+
+_lib.oz2_dgemm_grouped.argtypes = [_vp, _i32, C.POINTER(DgemmProblem), _vp, _i32, _vp]
+_lib.oz2_set_graph_mode.argtypes = [_vp, _i32]
+_lib.oz2_set_gemm_config.argtypes = [_vp, _i32, _i32, _i32]
+_lib.oz2_get_gemm_config.argtypes = [_vp, C.POINTER(_i32)]
+_lib.oz2_autotune_grouped.argtypes = [_vp, _i32, C.POINTER(DgemmProblem), C.POINTER(_i32)]
 _lib.oz2_last_error.argtypes = [_vp]
 _lib.oz2_last_error.restype = C.c_char_p
 _lib.oz2_status_string.argtypes = [_i32]
@@ -213,6 +227,40 @@ class Ozaki2:
 
     def check_device_error(self):
         _raise(_lib.oz2_check_device_error(self._h), self._h)
+
+    # ---- grouped calls (no counterpart in the reference)
+    @staticmethod
+    def _problems(problems):
+        arr = (DgemmProblem * len(problems))()
+        for i, p in enumerate(problems):
+            ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C_, ldc, s = p
+            arr[i] = DgemmProblem(_op(ta), _op(tb), s, m, n, k, float(alpha), float(beta), _addr(A), lda, _addr(B),
+                                  ldb, _addr(C_), ldc)
+        return arr
+
+    def gemm_grouped(self, problems, deps=None, done=None):
+        """problems: sequence of (ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, num_moduli),
+        the arguments of gemm() per problem; all run in one set of launches"""
+        arr = self._problems(problems)
+        ev, nev = self._events(deps)
+        d = done.cuda_event if hasattr(done, "cuda_event") else done
+        _raise(_lib.oz2_dgemm_grouped(self._h, len(problems), arr, ev, nev, d), self._h)
+
+    def set_graph_mode(self, on):
+        _raise(_lib.oz2_set_graph_mode(self._h, int(bool(on))), self._h)
+
+    def set_gemm_config(self, bn=0, group_j=16, ctas=0):
+        _raise(_lib.oz2_set_gemm_config(self._h, bn, group_j, ctas), self._h)
+
+    def gemm_config(self):
+        out = (_i32 * 3)()
+        _raise(_lib.oz2_get_gemm_config(self._h, out), self._h)
+        return {"bn": out[0], "group_j": out[1], "ctas": out[2]}
+
+    def autotune_grouped(self, problems):
+        out = (_i32 * 3)()
+        _raise(_lib.oz2_autotune_grouped(self._h, len(problems), self._problems(problems), out), self._h)
+        return {"bn": out[0], "group_j": out[1], "ctas": out[2]}
 
     # ---- the products (ref :739-786)
     @staticmethod
