@@ -1,20 +1,30 @@
 #!/usr/bin/env python
 """Benchmark: emulated FP64 DGEMM (Ozaki Scheme II on the INT8 tensor cores) on B200.
 
-Workload (one step): C = 1.5 A B - 0.5 C with m = n = k = 8192, op = N,N, ldc = m + 16,
-A and B i.i.d. U[-1,1) FP64 (seeded, generated on the device), s = 16 moduli.
-Metric: FP64-equivalent TFLOP/s = 2 m n k / t. Inputs are 512 MiB each, larger than the
-126 MB L2, so no flush is needed between steps.
+Headline workload (one step = one batched call over one batch of the stream): the adaptive-s
+stream, DGEMMs with m = n = k log-uniform in [256, 4096], inputs (u - 0.5) exp(phi g) with
+u ~ U[0,1), g ~ N(0,1), phi per problem uniform in [0, 8], the rows of A and the columns of B
+scaled by 2^e, e uniform in [-40, 40]; alpha = 1, beta = 0, target DGEMM-level error
+(|C - AB| <= k 2^-53 (|A||B|)_ij). The MLP picks s per 512 x 512 tile, tiles below their analytic
+s are probed and rerun at it on failure. Seeded synthetic inputs generated on the device; each
+batch (several GB) is larger than the 126 MB L2, so no flush is needed between steps.
+Metric: FP64-equivalent TFLOP/s = sum 2 m n k / t. Beside it, the fixed-s forms of the same
+stream (per-problem analytic s batched and as plain calls, s = 24, the reference's
+moduli_for_bits(k, 53)), each output of each form checked against a double-double product.
+Extras: the m = n = k = 8192 DGEMM at s = 16 (alpha 1.5, beta -0.5, ldc = m + 16) against cuBLAS
+DGEMM, and the grouped launch of 512 uneven DGEMMs.
 
   python bench.py [--gpus N --steps K --warmup W]            this implementation
   python bench.py --impl reference [--steps K --warmup W]    the reference's CPU path
 
-Under torchrun every rank runs its own full problem (weak scaling, no collective on the data
-path); value = all ranks' work / max over ranks of the device-timed region.
+Under torchrun every rank runs its own stream (weak scaling, no collective on the data path);
+value = all ranks' work / max over ranks of the device-timed region.
 """
 import argparse
 import json
+import math
 import os
+import random
 import statistics
 import subprocess
 import sys
@@ -26,25 +36,65 @@ sys.path.insert(0, os.path.join(ROOT, "os2-xe_b200"))
 
 METRIC = "FP64-equiv TFLOP/s at DGEMM-level error: adaptive-s batched vs fixed-s, 1 B200"
 UNIT = "TFLOP/s"
+TARGET_BITS = 53
+STREAM_BYTES = 48 << 30  # device bytes of distinct stream problems kept resident
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="oz2", choices=["oz2", "reference"])
-    ap.add_argument("--size", type=int, default=8192)
-    ap.add_argument("--s", type=int, default=16)
-    ap.add_argument("--no-extras", action="store_true", help="skip the e2e, cuBLAS and CPU legs")
+    ap.add_argument("--batch", type=int, default=64, help="problems per step of the adaptive-s stream")
+    ap.add_argument("--seed", type=int, default=2025)
+    ap.add_argument("--size", type=int, default=8192, help="m = n = k of the DGEMM extra")
+    ap.add_argument("--s", type=int, default=16, help="moduli of the DGEMM extra")
+    ap.add_argument("--no-extras", action="store_true", help="skip the DGEMM, grouped and CPU legs")
     return ap.parse_args()
 
 
 def workload(a):
-    n = a.size
-    return {"workload": f"dgemm {n}x{n}x{n} op=NN s={a.s} alpha=1.5 beta=-0.5 ldc=m+16 U[-1,1)",
-            "m": n, "n": n, "k": n, "s": a.s, "alpha": 1.5, "beta": -0.5, "ldc": n + 16,
-            "l2": "inputs (8 n^2 bytes each) larger than the 126 MB L2; no flush"}
+    return {"workload": f"adaptive-s stream: batches of {a.batch} dgemm, m=n=k log-uniform [256,4096], "
+                        "(u-0.5)exp(phi g), phi~U[0,8] per problem, rows of A / columns of B scaled by "
+                        "2^U[-40,40], alpha=1 beta=0, target 53 bits, MLP s per 512x512 tile + probe",
+            "batch": a.batch, "tile": 512, "target_bits": TARGET_BITS, "seed": a.seed,
+            "l2": "each batch holds several GB, larger than the 126 MB L2; no flush"}
+
+
+def stream_specs(seed, count):
+    """(n, phi, seed) of the first `count` problems of the stream"""
+    rnd = random.Random(seed)
+    out = []
+    for i in range(count):
+        n = int(math.exp(rnd.uniform(math.log(256), math.log(4096))))
+        phi = rnd.uniform(0.0, 8.0)
+        out.append((n, phi, seed * 1000003 + i))
+    return out
+
+
+def make_problem(torch, dev, n, phi, seed):
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+
+    def mat(row_scaled):
+        x = torch.rand((n, n), dtype=torch.float64, device=dev, generator=g) - 0.5  # [col][row]
+        x *= torch.exp(phi * torch.randn((n, n), dtype=torch.float64, device=dev, generator=g))
+        e = torch.randint(-40, 41, (1, n) if row_scaled else (n, 1), device=dev, generator=g).double()
+        return (x * torch.exp2(e)).view(-1)
+    A = mat(True)    # column-major n x n, rows scaled
+    B = mat(False)   # column-major n x n, columns scaled
+    C = torch.zeros(n * n, dtype=torch.float64, device=dev)
+    return {"n": n, "phi": phi, "A": A, "B": B, "C": C}
+
+
+def as_args(p, s=16, C_=None):
+    n = p["n"]
+    return ("N", "N", n, n, n, 1.0, p["A"], n, p["B"], n, 0.0, p["C"] if C_ is None else C_, n, s)
+
+
+def flops_of(batch):
+    return sum(2.0 * p["n"] ** 3 for p in batch)
 
 
 # ------------------------------------------------------------------ clocks during the timed region
@@ -96,50 +146,78 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ CPU legs (reference / oracle)
-def cpu_sample(a, steps, warmup):
-    """The reference's own CPU path (oracle/_ref: src/ozaki2_gpu.hpp compiled for the host) on a
-    512 x 512 x k slice of the workload, all host threads; the C oracle when it was not built."""
+CPU_MAX_N = 1024  # problems of the stream the CPU sample takes (larger ones take minutes each)
+
+
+def cpu_stream(a, budget_s, start=0):
+    """The reference's own CPU path (oracle/_ref: src/ozaki2_gpu.hpp compiled for the host, all
+    host threads; the C oracle where it was not built) over the stream's problems with n <= 1024,
+    in stream order from `start`, until `budget_s` seconds of DGEMM time; each problem at its
+    per-problem analytic s (the fixed s that meets the target). Returns (flops, seconds, problems,
+    next start, kind)."""
     import numpy as np
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import adaptive_oracle
     from pyoracle import Oracle, Ref, ref_available
     threads = os.cpu_count() or 1
-    m = n = min(512, a.size)
-    k = a.size
-    rng = np.random.default_rng(7)
-    A = np.asfortranarray(rng.uniform(-1, 1, (m, k)))
-    B = np.asfortranarray(rng.uniform(-1, 1, (k, n)))
-    C = np.asfortranarray(rng.uniform(-1, 1, (m, n)))
-    if ref_available():
-        lib, kind = Ref(), "reference"
-        run = lambda: lib.dgemm("N", "N", m, n, k, 1.5, A, m, B, k, -0.5, C, m, a.s)
-    else:
-        lib, kind = Oracle(), "port"
-        run = lambda: lib.dgemm("N", "N", m, n, k, 1.5, A, m, B, k, -0.5, C, m, a.s)
+    lib, kind = (Ref(), "reference") if ref_available() else (Oracle(), "port")
     lib.set_threads(threads)
-    for _ in range(warmup):
-        run()
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        run()
-    t = (time.perf_counter() - t0) / max(steps, 1)
-    return {"value": 2.0 * m * n * k / t / 1e12, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": f"dgemm {m}x{n}x{k} op=NN s={a.s} (a {m}x{n} block of C at full k), "
-                      f"{'src/ozaki2_gpu.hpp built for the host' if kind == 'reference' else 'C oracle'}",
-            "seconds_per_step": t}
+    plan_oracle = Oracle()
+    flops = secs = 0.0
+    done = 0
+    i = start
+    specs = stream_specs(a.seed, 100000)
+    while secs < budget_s and i < len(specs):
+        n, phi, seed = specs[i]
+        i += 1
+        if n > CPU_MAX_N:
+            continue
+        rng = np.random.default_rng(seed)
+        A = (rng.random((n, n)) - 0.5) * np.exp(phi * rng.standard_normal((n, n)))
+        A = np.asfortranarray(A * np.ldexp(1.0, rng.integers(-40, 41, (n, 1))))
+        B = (rng.random((n, n)) - 0.5) * np.exp(phi * rng.standard_normal((n, n)))
+        B = np.asfortranarray(B * np.ldexp(1.0, rng.integers(-40, 41, (1, n))))
+        C = np.zeros((n, n), order="F")
+        sv = adaptive_oracle.problem_analytic_s(plan_oracle, "N", "N", n, n, n, A, B, TARGET_BITS)
+        t0 = time.perf_counter()
+        lib.dgemm("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n, sv)
+        secs += time.perf_counter() - t0
+        flops += 2.0 * n ** 3
+        done += 1
+    return flops, secs, done, i, kind, threads
+
+
+def cpu_sample(a, budget_s=12.0):
+    flops, secs, done, _, kind, threads = cpu_stream(a, budget_s)
+    return {"value": flops / secs / 1e12, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"the first {done} problems of the same stream with n <= {CPU_MAX_N} (numpy-generated, same "
+                      f"distribution), each at its per-problem analytic s, "
+                      f"{'src/ozaki2_gpu.hpp built for the host' if kind == 'reference' else 'C oracle'}, "
+                      f"{secs:.1f} s of DGEMM time"}
 
 
 def run_reference_arm(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    warm = min(a.warmup, 1)
-    cb = cpu_sample(a, max(1, min(a.steps, 3)), warm)
-    line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "impl": "reference", "n_gpus": a.gpus,
-            "steps": a.steps, "warmup": a.warmup, "ms_per_step": cb["seconds_per_step"] * 1e3,
+    pos = 0
+    for _ in range(a.warmup):
+        _, _, _, pos, _, _ = cpu_stream(a, 1.0, pos)
+    flops = secs = 0.0
+    total = 0
+    for _ in range(a.steps):
+        f, t, d, pos, kind, threads = cpu_stream(a, 4.0, pos)
+        flops, secs, total = flops + f, secs + t, total + d
+    value = flops / secs / 1e12
+    sample = (f"{total} problems of the same stream with n <= {CPU_MAX_N} (numpy-generated, same distribution; "
+              f"about 4 s of DGEMM per step), each at its per-problem analytic s, all host threads, "
+              f"{'src/ozaki2_gpu.hpp built for the host' if kind == 'reference' else 'C oracle'}")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": secs / a.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 (int8 residues)",
             "data": "synthetic", "config": workload(a),
-            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
-            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
@@ -151,12 +229,44 @@ def launches_per_call(t):
     return 2 + t.pn + (tiles if t.pm > 1 else 1) + tiles * t.k_chunks + tiles
 
 
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        return {}
+
+
+def int8_peak():
+    bf16 = peaks().get("bf16_tflops")
+    if bf16:
+        return 2.0 * bf16, ("2 x measured dense bf16 (MEASURED_PEAKS.json bf16_tflops): B200 int8 dense rate is "
+                            "twice bf16")
+    return 2.0 * 1590.0, "2 x fallback bf16 1.59 PF"
+
+
+class Timer:
+    """CUDA events on the launching stream around a region"""
+
+    def __init__(self, torch, stream):
+        self.torch, self.stream = torch, stream
+        self.e0 = torch.cuda.Event(enable_timing=True)
+        self.e1 = torch.cuda.Event(enable_timing=True)
+
+    def __enter__(self):
+        self.torch.cuda.synchronize()
+        self.e0.record(self.stream)
+        return self
+
+    def __exit__(self, *exc):
+        self.e1.record(self.stream)
+        self.torch.cuda.synchronize()
+        self.ms = self.e0.elapsed_time(self.e1)
+
+
 def grouped_leg(oz2, torch, dev, stream, reps=5):
     """512 DGEMMs, m, n, k log-uniform in [32, 2048], ops uniform over NN/NT/TN/TT, s uniform in
     14..20, U[-1,1): one grouped call (autotuned GEMM configuration, replayed from a CUDA graph)
     against 512 sequential calls of the same problems. FP64-equivalent TFLOP/s = sum 2 m n k / t."""
-    import math
-    import random
     rnd = random.Random(2024)
     g = torch.Generator(device=dev)
     g.manual_seed(77)
@@ -175,37 +285,150 @@ def grouped_leg(oz2, torch, dev, stream, reps=5):
     cfg = oz.autotune_grouped(probs)
     oz.set_graph_mode(True)
     oz.gemm_grouped(probs)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(reps):
-        oz.gemm_grouped(probs)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    t_grouped = e0.elapsed_time(e1) / reps
+    with Timer(torch, stream) as tg:
+        for _ in range(reps):
+            oz.gemm_grouped(probs)
     for p in probs:
         oz.gemm(*p)
-    torch.cuda.synchronize()
-    e0.record(stream)
-    for _ in range(reps):
-        for p in probs:
-            oz.gemm(*p)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    t_seq = e0.elapsed_time(e1) / reps
+    with Timer(torch, stream) as ts:
+        for _ in range(reps):
+            for p in probs:
+                oz.gemm(*p)
     oz.check_device_error()
     oz.close()
+    t_grouped, t_seq = tg.ms / reps, ts.ms / reps
     return {"workload": "512 dgemm, m,n,k log-uniform [32,2048], ops uniform NN/NT/TN/TT, s uniform 14..20, "
                         "U[-1,1)", "grouped_tflops": flops / (t_grouped * 1e-3) / 1e12, "grouped_ms": t_grouped,
             "sequential_tflops": flops / (t_seq * 1e-3) / 1e12, "sequential_ms": t_seq,
             "speedup": t_seq / t_grouped, "gemm_config": cfg, "graph": True}
 
 
-def peaks():
+def dgemm_leg(a, oz2, torch, dev, stream, rank):
+    """m = n = k = 8192 DGEMM at s = 16, alpha 1.5, beta -0.5, ldc = m + 16, U[-1,1): device time,
+    stage times, the GEMM kernel against the int8 roofline, end to end with host buffers, and
+    native cuBLAS DGEMM / cuBLASLt int8 at the same shape."""
+    n = a.size
+    m = k = n
+    ldc = m + 16
+    g = torch.Generator(device=dev)
+    g.manual_seed(1234 + rank)
+    A = torch.rand(m * k, dtype=torch.float64, device=dev, generator=g) * 2 - 1
+    B = torch.rand(k * n, dtype=torch.float64, device=dev, generator=g) * 2 - 1
+    C0 = torch.rand(ldc * n, dtype=torch.float64, device=dev, generator=g) * 2 - 1
+    C = C0.clone()
+    oz = oz2.Ozaki2(stream)
+    steps = 20
+
+    def step():
+        oz.gemm("N", "N", m, n, k, 1.5, A, m, B, k, -0.5, C, ldc, a.s)
+
+    for _ in range(3):
+        step()
+    with Timer(torch, stream) as t:
+        for _ in range(steps):
+            step()
+    ms = t.ms / steps
+    flops = 2.0 * m * n * k
+    oz.set_profiling(True)
+    st_sum = [0.0] * 4
+    for _ in range(steps):
+        step()
+        st = oz.stage_times()
+        for i, v in enumerate((st.scale_ms, st.split_ms, st.gemm_ms, st.crt_ms)):
+            st_sum[i] += v / steps
+    oz.set_profiling(False)
+    tiling = oz.last_tiling()
+    peak, note = int8_peak()
+    achieved = 2.0 * a.s * m * n * k / (st_sum[2] * 1e-3) / 1e12
+    out = {"workload": f"dgemm {n}x{n}x{n} op=NN s={a.s} alpha=1.5 beta=-0.5 ldc=m+16 U[-1,1)",
+           "tflops": flops / (ms * 1e-3) / 1e12, "ms": ms, "steps": steps,
+           "stage_ms": {"scale": st_sum[0], "split": st_sum[1], "gemm": st_sum[2], "crt": st_sum[3]},
+           "gpu_launches_per_call": launches_per_call(tiling),
+           "roofline": {"bound": "tensor", "kernel": "gemm_i8_modm_kernel", "achieved": achieved, "peak": peak,
+                        "unit": "TOPS (int8)", "frac": achieved / peak, "peak_note": note,
+                        "algorithmic": "2 s m n k int8 ops per call"}}
+    # end to end with host buffers: H2D of A, B, C and D2H of C every step
+    hA = torch.empty(m * k, dtype=torch.float64, pin_memory=True)
+    hB = torch.empty(k * n, dtype=torch.float64, pin_memory=True)
+    hC = torch.empty(ldc * n, dtype=torch.float64, pin_memory=True)
+    hA.copy_(A)
+    hB.copy_(B)
+    hC.copy_(C0)
+    res = torch.empty(ldc * n, dtype=torch.float64, pin_memory=True)
+
+    def e2e_step():
+        A.copy_(hA, non_blocking=True)
+        B.copy_(hB, non_blocking=True)
+        C.copy_(hC, non_blocking=True)
+        oz.gemm("N", "N", m, n, k, 1.5, A, m, B, k, -0.5, C, ldc, a.s)
+        res.copy_(C, non_blocking=True)
+
+    e2e_step()
+    with Timer(torch, stream) as t:
+        for _ in range(5):
+            e2e_step()
+    out["e2e_tflops"] = flops / (t.ms / 5 * 1e-3) / 1e12
+    # native cuBLAS FP64 DGEMM on the same device, same shape (reference point, not the product)
+    X = A.view(k, m).t()
+    Y = B.view(n, k).t()
+    torch.mm(X, Y)
+    with Timer(torch, stream) as t:
+        for _ in range(3):
+            torch.mm(X, Y)
+    out["cublas_dgemm_tflops"] = flops / (t.ms / 3 * 1e-3) / 1e12
+    out["vs_cublas_dgemm"] = out["tflops"] / out["cublas_dgemm_tflops"]
     try:
-        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except (OSError, ValueError):
-        return {}
+        Xi = torch.randint(-128, 127, (m, k), dtype=torch.int8, device=dev)
+        Yi = torch.randint(-128, 127, (k, n), dtype=torch.int8, device=dev).t().contiguous().t()
+        torch._int_mm(Xi, Yi)
+        with Timer(torch, stream) as t:
+            for _ in range(5):
+                torch._int_mm(Xi, Yi)
+        out["cublaslt_int8_tops"] = 2.0 * m * n * k / (t.ms / 5 * 1e-3) / 1e12
+    except Exception as e:  # noqa: BLE001
+        out["cublaslt_int8_tops"] = f"unavailable: {type(e).__name__}"
+    oz.check_device_error()
+    oz.close()
+    return out
+
+
+# ------------------------------------------------------------------ the adaptive-s stream
+def stream_batches(a, torch, dev, rank):
+    """distinct batches of the stream kept on the device (up to STREAM_BYTES); the timed steps
+    cycle through them"""
+    specs = stream_specs(a.seed + 7919 * rank, a.steps * a.batch)
+    batches, used = [], 0
+    for b in range(a.steps):
+        part = specs[b * a.batch:(b + 1) * a.batch]
+        need = sum(24 * n * n for n, _, _ in part)
+        if batches and used + need > STREAM_BYTES:
+            break
+        batches.append([make_problem(torch, dev, n, phi, sd) for n, phi, sd in part])
+        used += need
+    return batches, used
+
+
+def problem_analytic_s(oz, batch):
+    """per-problem analytic s: the largest tile analytic s of each problem"""
+    out = []
+    for p in batch:
+        _, sa = oz.tile_features([as_args(p)], TARGET_BITS)
+        out.append(int(sa.max()))
+    return out
+
+
+def verify(oz, torch, batch, run, refs):
+    """runs `run` over the batch and measures every output against its double-double product:
+    (problems over the bound, largest ratio)"""
+    run()
+    torch.cuda.synchronize()
+    bad, worst = 0, 0.0
+    for p, (hi, lo, ab) in zip(batch, refs):
+        n = p["n"]
+        r = oz.error_ratio(n, n, n, p["C"], n, hi, lo, ab, TARGET_BITS)
+        worst = max(worst, r)
+        bad += r > 1.0
+    return bad, worst
 
 
 def main():
@@ -222,148 +445,199 @@ def main():
     torch.cuda.set_device(local)
     if world > 1:
         from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
-    n = a.size
-    m = k = n
-    ldc = m + 16
-    g = torch.Generator(device=dev)
-    g.manual_seed(1234 + rank)
-    A = torch.rand(m * k, dtype=torch.float64, device=dev, generator=g) * 2 - 1
-    B = torch.rand(k * n, dtype=torch.float64, device=dev, generator=g) * 2 - 1
-    C0 = torch.rand(ldc * n, dtype=torch.float64, device=dev, generator=g) * 2 - 1
-    C = C0.clone()
     stream = torch.cuda.current_stream()
     oz = oz2.Ozaki2(stream)
+    model = oz.load_model()
+    ref_rule = oz2.Ozaki2.moduli_for_bits
 
-    def step():
-        oz.gemm("N", "N", m, n, k, 1.5, A, m, B, k, -0.5, C, ldc, a.s)
+    batches, resident = stream_batches(a, torch, dev, rank)
+    nb = len(batches)
+    s_an = [problem_analytic_s(oz, b) for b in batches]
 
-    for _ in range(a.warmup):
-        step()
-    torch.cuda.synchronize()
+    # forms of the stream, each one call (or one call per problem) over a batch
+    def adaptive(b):
+        return oz.gemm_adaptive([as_args(p) for p in batches[b]], TARGET_BITS, oz.ADAPTIVE_MLP)
+
+    def analytic_batched(b):
+        return oz.gemm_adaptive([as_args(p) for p in batches[b]], TARGET_BITS, oz.ADAPTIVE_ANALYTIC_PROBLEM)
+
+    def analytic_plain(b):
+        for p, sv in zip(batches[b], s_an[b]):
+            oz.gemm(*as_args(p, sv))
+
+    def s24_grouped(b):
+        oz.gemm_grouped([as_args(p, 24) for p in batches[b]])
+
+    def refrule_grouped(b):
+        oz.gemm_grouped([as_args(p, max(2, ref_rule(p["n"], TARGET_BITS))) for p in batches[b]])
+
+    forms = {"adaptive_mlp_batched": adaptive, "analytic_per_problem_batched": analytic_batched,
+             "analytic_per_problem_plain_calls": analytic_plain, "s24_grouped": s24_grouped,
+             "reference_rule_grouped": refrule_grouped}
+
+    # every output of every form against the double-double product (untimed; also sizes the
+    # workspaces before the timed steps)
+    checks = {f: {"problems": 0, "over_bound": 0, "max_ratio": 0.0} for f in forms}
+    adaptive_stats = {}
+    for b in range(nb):
+        refs = []
+        for p in batches[b]:
+            n = p["n"]
+            hi = torch.empty(n * n, dtype=torch.float64, device=dev)
+            lo, ab = torch.empty_like(hi), torch.empty_like(hi)
+            oz.dd_reference(n, n, n, p["A"], n, p["B"], n, hi, lo, ab)
+            refs.append((hi, lo, ab))
+        for name, fn in forms.items():
+            holder = {}
+            bad, worst = verify(oz, torch, batches[b], lambda: holder.update(st=fn(b)), refs)
+            c = checks[name]
+            c["problems"] += len(batches[b])
+            c["over_bound"] += int(bad)
+            c["max_ratio"] = max(c["max_ratio"], worst)
+            if name == "adaptive_mlp_batched":
+                for key, v in holder["st"].items():
+                    adaptive_stats[key] = adaptive_stats.get(key, 0) + v
+        del refs
+    torch.cuda.empty_cache()
     oz.check_device_error()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        ev0.record(stream)
-        for _ in range(a.steps):
-            step()
-        ev1.record(stream)
-        torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    ms = ev0.elapsed_time(ev1) / a.steps
-    oz.check_device_error()
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    flops = 2.0 * m * n * k
-    value = world * flops / (ms * 1e-3) / 1e12
 
-    # per-phase device times (CUDA events between phases, on the launching stream)
-    oz.set_profiling(True)
-    st_sum = [0.0, 0.0, 0.0, 0.0]
-    for _ in range(a.steps):
-        step()
-        st = oz.stage_times()
-        for i, v in enumerate((st.scale_ms, st.split_ms, st.gemm_ms, st.crt_ms)):
-            st_sum[i] += v / a.steps
-    oz.set_profiling(False)
-    tiling = oz.last_tiling()
-    gemm_ms = st_sum[2]
-    pk = peaks()
-    int8_ops = 2.0 * a.s * m * n * k
-    achieved = int8_ops / (gemm_ms * 1e-3) / 1e12
-    bf16 = pk.get("bf16_tflops")
-    peak = 2.0 * bf16 if bf16 else 2.0 * 1590.0
-    extras = {}
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
-            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64 (int8 residues, int32 accumulate)", "data": "synthetic", "config": workload(a),
-            "clocks": clk.summary(), "gpu_launches": launches_per_call(tiling) * a.steps,
-            "stage_ms": {"scale": st_sum[0], "split": st_sum[1], "gemm": st_sum[2], "crt": st_sum[3]},
-            "tiling": {"mb": tiling.mb, "nb": tiling.nb, "pm": tiling.pm, "pn": tiling.pn,
-                       "k_chunks": tiling.k_chunks, "workspace_bytes": tiling.workspace_bytes},
-            "roofline": {"bound": "tensor", "kernel": "gemm_i8_modm_kernel", "achieved": achieved, "peak": peak,
-                         "unit": "TOPS (int8)", "frac": achieved / peak,
-                         "peak_note": ("2 x measured dense bf16 (MEASURED_PEAKS.json bf16_tflops): B200 int8 "
-                                       "dense rate is twice bf16" if bf16 else "2 x fallback bf16 1.59 PF"),
-                         "algorithmic": "2 s m n k int8 ops per call", "traffic": None}}
-
-    if not a.no_extras:
-        # e2e through the public API with host buffers: H2D of A, B, C and D2H of C every step
-        hA = torch.empty(m * k, dtype=torch.float64, pin_memory=True)
-        hB = torch.empty(k * n, dtype=torch.float64, pin_memory=True)
-        hC = torch.empty(ldc * n, dtype=torch.float64, pin_memory=True)
-        hA.copy_(A)
-        hB.copy_(B)
-        hC.copy_(C0)
-        dA, dB, dC = torch.empty_like(A), torch.empty_like(B), torch.empty_like(C0)
-        out = torch.empty(ldc * n, dtype=torch.float64, pin_memory=True)
-
-        def e2e_step():
-            dA.copy_(hA, non_blocking=True)
-            dB.copy_(hB, non_blocking=True)
-            dC.copy_(hC, non_blocking=True)
-            oz.gemm("N", "N", m, n, k, 1.5, dA, m, dB, k, -0.5, dC, ldc, a.s)
-            out.copy_(dC, non_blocking=True)
-
-        for _ in range(min(a.warmup, 2)):
-            e2e_step()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(a.steps):
-            e2e_step()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        e2e_ms = e0.elapsed_time(e1) / a.steps
+    def timed(fn, steps, warmup):
+        for i in range(warmup):
+            fn(i % nb)
         if world > 1:
-            t = torch.tensor([e2e_ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_ms = float(t.item())
-        line["e2e"] = {"value": world * flops / (e2e_ms * 1e-3) / 1e12, "unit": UNIT,
-                       "h2d_bytes_per_step": 8 * (m * k + k * n + ldc * n), "d2h_bytes_per_step": 8 * ldc * n,
-                       "ms_per_step": e2e_ms}
-        del dA, dB, dC
-        # native cuBLAS FP64 DGEMM on the same device, same shape (reference point, not the product)
-        X = A.view(k, m).t()
-        Y = B.view(n, k).t()
-        torch.mm(X, Y)
-        torch.cuda.synchronize()
-        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        c0.record(stream)
-        for _ in range(3):
-            torch.mm(X, Y)
-        c1.record(stream)
-        torch.cuda.synchronize()
-        extras["cublas_dgemm_tflops"] = flops / (c0.elapsed_time(c1) / 3 * 1e-3) / 1e12
-        # cuBLASLt int8 GEMM at the same shape, for context on the tensor-pipe peak
-        try:
-            Xi = torch.randint(-128, 127, (m, k), dtype=torch.int8, device=dev)
-            Yi = torch.randint(-128, 127, (k, n), dtype=torch.int8, device=dev).t().contiguous().t()
-            torch._int_mm(Xi, Yi)
-            torch.cuda.synchronize()
-            c0.record(stream)
-            for _ in range(5):
-                torch._int_mm(Xi, Yi)
-            c1.record(stream)
-            torch.cuda.synchronize()
-            extras["cublaslt_int8_tops"] = 2.0 * m * n * k / (c0.elapsed_time(c1) / 5 * 1e-3) / 1e12
-        except Exception as e:  # noqa: BLE001
-            extras["cublaslt_int8_tops"] = f"unavailable: {type(e).__name__}"
-        line["vs_cublas_dgemm"] = value / world / extras["cublas_dgemm_tflops"]
+            dist.barrier()
+        flops = 0.0
+        with Timer(torch, stream) as t:
+            for i in range(steps):
+                fn(i % nb)
+                flops += flops_of(batches[i % nb])
+        ms = t.ms
+        if world > 1:
+            x = torch.tensor([ms, flops], dtype=torch.float64, device=dev)
+            mx = x.clone()
+            dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+            dist.all_reduce(x, op=dist.ReduceOp.SUM)
+            ms, flops = float(mx[0]), float(x[1])
+        return flops / (ms * 1e-3) / 1e12, ms / steps
+
+    # headline: the adaptive form
+    for i in range(a.warmup):
+        adaptive(i % nb)
+    if world > 1:
+        dist.barrier()
+    launches0 = oz.kernel_launches()
+    flops = 0.0
+    with ClockSampler(local) as clk:
+        with Timer(torch, stream) as t:
+            for i in range(a.steps):
+                adaptive(i % nb)
+                flops += flops_of(batches[i % nb])
+    launches = oz.kernel_launches() - launches0
+    ms = t.ms
+    if world > 1:
+        x = torch.tensor([ms, flops], dtype=torch.float64, device=dev)
+        mx = x.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(x, op=dist.ReduceOp.SUM)
+        ms, flops = float(mx[0]), float(x[1])
+    value = flops / (ms * 1e-3) / 1e12
+    ms_step = ms / a.steps
+    oz.check_device_error()
+
+    # stage times and the GEMM kernel against the int8 roofline (profiling pass, untimed)
+    oz.set_profiling(True)
+    st_sum, macs = [0.0] * 4, 0
+    for i in range(a.steps):
+        st = adaptive(i % nb)
+        macs += st["int8_macs"]
+        tt = oz.stage_times()
+        for j, v in enumerate((tt.scale_ms, tt.split_ms, tt.gemm_ms, tt.crt_ms)):
+            st_sum[j] += v
+    oz.set_profiling(False)
+    peak, note = int8_peak()
+    achieved = 2.0 * macs / (st_sum[2] * 1e-3) / 1e12
+
+    fixed = {}
+    for name, fn in forms.items():
+        if name == "adaptive_mlp_batched":
+            continue
+        tf, msf = timed(fn, a.steps, min(a.warmup, 1))
+        fixed[name] = {"tflops": tf, "ms_per_step": msf, "adaptive_speedup": value / tf}
+
+    tiles = max(adaptive_stats.get("tiles", 0), 1)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 (int8 residues, int32 accumulate)", "data": "synthetic",
+            "config": dict(workload(a), problems_timed=a.steps * a.batch,
+                           distinct_problems=sum(len(b) for b in batches), resident_gb=resident / 2 ** 30,
+                           model_threshold=model.get("threshold")),
+            "clocks": clk.summary(), "gpu_launches": launches,
+            "stage_ms_per_step": {"scale_stats_mlp": st_sum[0] / a.steps, "split": st_sum[1] / a.steps,
+                                  "gemm": st_sum[2] / a.steps, "crt": st_sum[3] / a.steps},
+            "roofline": {"bound": "tensor", "kernel": "gemm_i8_modm_kernel", "achieved": achieved, "peak": peak,
+                         "unit": "TOPS (int8)", "frac": achieved / peak, "peak_note": note,
+                         "algorithmic": "2 s m_t n_t k int8 ops per tile (reruns included), summed over the step",
+                         "traffic": None},
+            "fixed_s": fixed,
+            "error_check": {"bound": "|C - AB| <= k 2^-53 (|A||B|)_ij against a double-double product, per entry",
+                            **checks},
+            "adaptive_tiles": {"tiles": adaptive_stats.get("tiles"),
+                               "mean_s": (adaptive_stats.get("sum_s", 0) - adaptive_stats.get("rerun_sum_s", 0)) / tiles,
+                               "mean_analytic_s": adaptive_stats.get("analytic_sum_s", 0) / tiles,
+                               "probed": adaptive_stats.get("probed"), "rerun": adaptive_stats.get("rerun")}}
+
+    # end to end through the public API: H2D of the step's A and B from pinned host memory, the
+    # batched call, D2H of every C
+    b0 = batches[0]
+    host = [(torch.empty(p["n"] ** 2, dtype=torch.float64, pin_memory=True),
+             torch.empty(p["n"] ** 2, dtype=torch.float64, pin_memory=True),
+             torch.empty(p["n"] ** 2, dtype=torch.float64, pin_memory=True)) for p in b0]
+    for (hA, hB, _), p in zip(host, b0):
+        hA.copy_(p["A"])
+        hB.copy_(p["B"])
+
+    def e2e_step():
+        for (hA, hB, _), p in zip(host, b0):
+            p["A"].copy_(hA, non_blocking=True)
+            p["B"].copy_(hB, non_blocking=True)
+        oz.gemm_adaptive([as_args(p) for p in b0], TARGET_BITS, oz.ADAPTIVE_MLP)
+        for (_, _, hC), p in zip(host, b0):
+            hC.copy_(p["C"], non_blocking=True)
+
+    e2e_step()
+    e2e_steps = max(1, min(a.steps, 5))
+    with Timer(torch, stream) as t:
+        for _ in range(e2e_steps):
+            e2e_step()
+    e2e_ms = t.ms / e2e_steps
+    e2e_flops = flops_of(b0)
+    if world > 1:
+        x = torch.tensor([e2e_ms, e2e_flops], dtype=torch.float64, device=dev)
+        mx = x.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(x, op=dist.ReduceOp.SUM)
+        e2e_ms, e2e_flops = float(mx[0]), float(x[1])
+    line["e2e"] = {"value": e2e_flops / (e2e_ms * 1e-3) / 1e12, "unit": UNIT,
+                   "h2d_bytes_per_step": sum(16 * p["n"] ** 2 for p in b0),
+                   "d2h_bytes_per_step": sum(8 * p["n"] ** 2 for p in b0), "ms_per_step": e2e_ms,
+                   "note": "the first batch of the stream every step"}
+    del host
+    oz.check_device_error()
+    oz.close()
+    del batches
+    torch.cuda.empty_cache()
+
+    extras = {}
+    if not a.no_extras:
+        extras["dgemm_8192"] = dgemm_leg(a, oz2, torch, dev, stream, rank)
         extras["grouped_c4"] = grouped_leg(oz2, torch, dev, stream)
         if rank == 0:
-            line["cpu_baseline"] = {k2: v for k2, v in cpu_sample(a, 1, 0).items() if k2 != "seconds_per_step"}
+            line["cpu_baseline"] = cpu_sample(a)
     line["extras"] = extras
     if rank == 0:
         print(json.dumps(line), flush=True)
-    oz.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

@@ -77,6 +77,9 @@ int oz2_dgemm_grouped(oz2_handle h, int count, const oz2_dgemm_problem* problems
 /* Grouped calls are captured in a CUDA graph on first use and replayed when the same problem
  * list (shapes, pointers, scalars) comes again; the workspace must not grow in between. */
 int oz2_set_graph_mode(oz2_handle h, int enable);
+/* kernels launched through this handle since oz2_create, a CUDA-graph replay counting its kernel
+ * nodes (no counterpart in the reference) */
+int oz2_kernel_launches(oz2_handle h, int64_t* out);
 /* GEMM kernel configuration: tile width along the rows of C (bn = 128 or 256), raster group of
  * column tiles (group_j), persistent CTAs (ctas, 0 = one per SM); bn = 0 returns to the
  * autotuned / heuristic choice. get returns the configuration of the last call. */
@@ -85,6 +88,51 @@ int oz2_get_gemm_config(oz2_handle h, int* out3);
 /* Times the candidate configurations on these problems (C is overwritten), remembers the
  * fastest for problem lists of the same shapes and returns it in out3 (may be NULL). */
 int oz2_autotune_grouped(oz2_handle h, int count, const oz2_dgemm_problem* problems, int* out3);
+
+/* Adaptive number of moduli per C tile (no counterpart in the reference). Target: every entry
+ * within k 2^-target_bits (|A||B|)_ij of the exact product, the classical error bound of a native
+ * FP64 GEMM for target_bits = 53 ("DGEMM-level error"). Per tile of tile x tile entries (default
+ * 512), s comes from
+ *   mode 0: the MLP (oz2_mlp_set_weights), capped by the analytic s, for problems with beta = 0
+ *           (others take the analytic s); tiles below their analytic s are probed (C x against
+ *           A (B x) in double-double) and rerun at the analytic s when the probe fails; without
+ *           weights it behaves as mode 1
+ *   mode 1: the analytic s of the tile: smallest s whose tk >= R + 2 + t - floor(log2(k - 1)),
+ *           R the largest exponent gap below the row / column maximum in the tile's panels
+ *   mode 2: the analytic s of the whole problem (the largest over its tiles)
+ *   mode 3: each problem's own num_moduli (tiled like the other modes)
+ * stats8 (may be NULL): tiles, sum of s over computed tiles (reruns included), probed tiles, rerun
+ * tiles, sum of s of the reruns, sum of analytic s, MLP used, int8 multiply-adds of the computed
+ * tiles (s m_t n_t k summed, reruns included). Synchronises the stream. With profiling on,
+ * oz2_stage_times reports scale (with the tile statistics, features and MLP), split, GEMM and CRT
+ * summed over the tile batches; the probe is in none of them. */
+int oz2_dgemm_adaptive(oz2_handle h, int count, const oz2_dgemm_problem* problems, int target_bits, int mode,
+                       int64_t* stats8);
+/* tile edge (multiple of 128) and the MLP decision threshold: s is the smallest class whose
+ * cumulative predicted probability reaches it */
+int oz2_set_adaptive_options(oz2_handle h, int tile, float threshold);
+/* out4 = {parameters, features, classes (s = 2..24), hidden width} of the MLP */
+int oz2_mlp_info(int* out4);
+/* loads the MLP parameters (host floats); NULL unloads */
+int oz2_mlp_set_weights(oz2_handle h, const float* params, int nparams);
+/* trains in place (host params) on device features [count][features] and labels (s values);
+ * loss (host, epochs floats, may be NULL) receives the mean loss per epoch */
+int oz2_mlp_train(oz2_handle h, int count, const float* d_features, const int* d_labels, int epochs, float lr,
+                  unsigned int seed, float* params, float* loss);
+/* s per sample (device) and class probabilities (device, may be NULL) for host params */
+int oz2_mlp_infer(oz2_handle h, const float* params, int count, const float* d_features, float threshold, int* d_s,
+                  float* d_probs);
+/* features [tiles][features] and analytic s per tile (device outputs, tiles in problem order,
+ * column tiles outer, row tiles inner); ntiles receives the count */
+int oz2_tile_features(oz2_handle h, int count, const oz2_dgemm_problem* problems, int target_bits,
+                      float* d_features, int* d_s_analytic, int64_t* ntiles);
+/* double-double product hi + lo ~= A B and |A| |B| (m x n, leading dimension m) of column-major
+ * A (m x k) and B (k x n) on the device: the reference the labels are measured against */
+int oz2_dd_reference(oz2_handle h, int64_t m, int64_t n, int64_t k, const double* A, int64_t lda, const double* B,
+                     int64_t ldb, double* hi, double* lo, double* absab);
+/* out = max over entries of |C - (hi + lo)| / (k 2^-target_bits |A||B|); synchronises */
+int oz2_error_ratio(oz2_handle h, int64_t m, int64_t n, int64_t k, const double* C, int64_t ldc, const double* hi,
+                    const double* lo, const double* absab, int target_bits, float* out);
 
 /* Ozaki2::precision_bits / precision_bits_complex / moduli_for_bits: src/ozaki2_gpu.hpp:689-700, :762 */
 int oz2_precision_bits(int64_t k, int num_moduli, int* out);

@@ -1,0 +1,359 @@
+// oz2_adaptive.cu - device side of the adaptive choice of the number of moduli s per C tile
+// (no counterpart in the reference):
+//   stats    : per panel of 512 rows of op(A) (columns of op(B)), a histogram of exponent gaps
+//              g = e(row max) - e(|x|) over the nonzero elements, and the count of zeros
+//   features : per tile, quantiles of both panels' gaps, zero fractions, the spread of row
+//              (column) maxima, log2 k and the target bits, plus the analytic s: the smallest s
+//              whose bits per element tk reach R + 2 + t - floor(log2(k - 1)), R the largest
+//              gap. Every product term then carries a relative error <= 3 * 2^(R - tk), so
+//              |C - AB| <= k 2^-t |A||B| holds entry by entry (the DGEMM-level target).
+//   probe    : Freivalds-style check of a computed tile: C x against A (B x) in double-double
+//              for sparse random x with four +-1 entries, tolerance sum_j |x_j| k 2^-t (|A||B|)_ij
+//              plus the rounding of C itself, so a tile meeting the target always passes.
+//   dd_ref / error ratio : double-double products and max_ij |C - AB| / (k 2^-t (|A||B|)_ij),
+//              used to label training tiles (the smallest s that meets the target).
+#include <cstdint>
+
+#include "oz2_adaptive.cuh"
+
+namespace oz2 {
+namespace {
+
+__device__ __forceinline__ int frexp_exp_bits(unsigned long long b) {  // frexp exponent of |x| from bits
+    const int be = static_cast<int>((b >> 52) & 0x7FF);
+    return be ? be - 1022 : -1010 - __clzll(static_cast<long long>(b));
+}
+
+template <class Item>
+__device__ __forceinline__ int find_block_item(const Item* items, int count, int64_t b) {
+    int lo = 0, hi = count - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (items[mid].block0 <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// ---------------------------------------------------------------- panel statistics
+template <bool ROWC>
+__global__ void __launch_bounds__(256) panel_stats_kernel(const StatItem* __restrict__ items, int count) {
+    __shared__ unsigned int hist[kGapBins + 1];
+    for (int i = threadIdx.x; i <= kGapBins; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    const StatItem* I = items + find_block_item(items, count, blockIdx.x);
+    const int64_t local = static_cast<int64_t>(blockIdx.x) - I->block0;
+    const int64_t rb = local % I->rblocks, kc = local / I->rblocks;
+    const unsigned long long* X = reinterpret_cast<const unsigned long long*>(I->X);
+    const int64_t rows = I->rows, k = I->k, ldx = I->ldx;
+    const int64_t p0 = kc * I->kchunk, p1 = min(k, p0 + I->kchunk);
+    auto add = [&](unsigned long long bits, int erow) {
+        bits &= 0x7FFFFFFFFFFFFFFFull;
+        if (bits == 0) {
+            atomicAdd(&hist[kGapBins], 1u);
+        } else if (bits < 0x7FF0000000000000ull) {
+            const int g = min(max(erow - frexp_exp_bits(bits), 0), kGapBins - 1);
+            atomicAdd(&hist[g], 1u);
+        }
+    };
+    if (ROWC) {  // 32 rows per block, warps interleave k
+        const int64_t r = rb * 32 + (threadIdx.x & 31);
+        if (r < rows) {
+            const unsigned long long mb = I->maxbits[r];
+            if (mb != 0 && mb < 0x7FF0000000000000ull) {
+                const int erow = frexp_exp_bits(mb);
+                for (int64_t p = p0 + (threadIdx.x >> 5); p < p1; p += 8) add(__ldg(X + r + p * ldx), erow);
+            }
+        }
+    } else {  // 8 rows per block, lanes over k
+        const int64_t r = rb * 8 + (threadIdx.x >> 5);
+        if (r < rows) {
+            const unsigned long long mb = I->maxbits[r];
+            if (mb != 0 && mb < 0x7FF0000000000000ull) {
+                const int erow = frexp_exp_bits(mb);
+                for (int64_t p = p0 + (threadIdx.x & 31); p < p1; p += 32) add(__ldg(X + p + r * ldx), erow);
+            }
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i <= kGapBins; i += blockDim.x)
+        if (hist[i]) atomicAdd(I->hist + i, hist[i]);
+}
+
+// ---------------------------------------------------------------- features + analytic s
+__device__ float gap_quantile(const unsigned int* h, unsigned long long nonzero, float q) {
+    if (nonzero == 0) return 0.0f;
+    const unsigned long long want = static_cast<unsigned long long>(q * static_cast<double>(nonzero - 1)) + 1;
+    unsigned long long c = 0;
+    for (int g = 0; g < kGapBins; ++g) {
+        c += h[g];
+        if (c >= want) return static_cast<float>(g);
+    }
+    return static_cast<float>(kGapBins - 1);
+}
+__device__ int gap_max(const unsigned int* h) {
+    for (int g = kGapBins - 1; g >= 0; --g)
+        if (h[g]) return g;
+    return 0;
+}
+
+// e(max) - e(min) over the finite nonzero row maxima of a panel
+__device__ float exponent_spread(const unsigned long long* maxbits, int64_t rows) {
+    int lo = 1 << 30, hi = -(1 << 30);
+    for (int64_t r = 0; r < rows; ++r) {
+        const unsigned long long b = maxbits[r];
+        if (b == 0 || b >= 0x7FF0000000000000ull) continue;
+        const int e = frexp_exp_bits(b);
+        lo = min(lo, e);
+        hi = max(hi, e);
+    }
+    return hi >= lo ? static_cast<float>(hi - lo) : 0.0f;
+}
+
+__global__ void tile_features_kernel(const FeatureItem* __restrict__ items, int count, float* __restrict__ feat,
+                                     int* __restrict__ s_analytic) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const FeatureItem& I = items[t];
+    const unsigned int* ha = I.hist_a;
+    const unsigned int* hb = I.hist_b;
+    unsigned long long na = 0, nb = 0;
+    for (int g = 0; g < kGapBins; ++g) {
+        na += ha[g];
+        nb += hb[g];
+    }
+    const double ta = static_cast<double>(na + ha[kGapBins]), tb = static_cast<double>(nb + hb[kGapBins]);
+    float* f = feat + static_cast<int64_t>(t) * kFeatures;
+    f[0] = log2f(static_cast<float>(I.k)) / 16.0f;
+    f[1] = static_cast<float>(I.target_bits) / 64.0f;
+    const float qs[4] = {0.5f, 0.75f, 0.9f, 0.99f};
+    for (int q = 0; q < 4; ++q) {
+        f[2 + q] = gap_quantile(ha, na, qs[q]) / 64.0f;
+        f[8 + q] = gap_quantile(hb, nb, qs[q]) / 64.0f;
+    }
+    const int ra = gap_max(ha), rb = gap_max(hb);
+    f[6] = ra / 64.0f;
+    f[12] = rb / 64.0f;
+    f[7] = ta > 0 ? static_cast<float>(ha[kGapBins] / ta) : 0.0f;
+    f[13] = tb > 0 ? static_cast<float>(hb[kGapBins] / tb) : 0.0f;
+    f[14] = exponent_spread(I.maxbits_a, I.rows_a) / 64.0f;
+    f[15] = exponent_spread(I.maxbits_b, I.rows_b) / 64.0f;
+    // analytic s: tk >= R + 2 + t - floor(log2(k - 1))
+    const int R = max(ra, rb);
+    int lg = 0;
+    for (int64_t v = I.k - 1; v > 1; v >>= 1) ++lg;
+    const int need = R + 2 + I.target_bits - lg;
+    int s = kMaxModuli;
+    for (int c = 2; c <= kMaxModuli; ++c)
+        if (I.tk[c] >= need) {
+            s = c;
+            break;
+        }
+    s_analytic[t] = s;
+}
+
+// ---------------------------------------------------------------- double-double helpers
+struct dd {
+    double hi, lo;
+};
+__device__ __forceinline__ dd two_sum(double a, double b) {
+    const double s = a + b;
+    const double bb = s - a;
+    return {s, (a - (s - bb)) + (b - bb)};
+}
+__device__ __forceinline__ dd dd_add(dd a, dd b) {
+    dd s = two_sum(a.hi, b.hi);
+    s.lo += a.lo + b.lo;
+    return two_sum(s.hi, s.lo);
+}
+__device__ __forceinline__ dd dd_add_prod(dd acc, double a, double b) {  // acc + a*b
+    const double ph = a * b;
+    const double pl = fma(a, b, -ph);
+    dd s = two_sum(acc.hi, ph);
+    s.lo += acc.lo + pl;
+    return two_sum(s.hi, s.lo);
+}
+
+// ---------------------------------------------------------------- probe
+// One block per (tile, probe vector, 256 rows of the tile). Random columns j_c and signs from a
+// hash of (problem seed, tile, probe, c).
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+__global__ void __launch_bounds__(256) probe_kernel(const ProbeItem* __restrict__ items, int count,
+                                                    int* __restrict__ fail) {
+    const ProbeItem* I = items + find_block_item(items, count, blockIdx.x);
+    const int64_t local = static_cast<int64_t>(blockIdx.x) - I->block0;
+    const int pr = static_cast<int>(local % kProbes);
+    const int64_t rblk = local / kProbes;
+    const int64_t mt = I->mt, nt = I->nt, k = I->k;
+    __shared__ int64_t cols[kProbeCols];
+    __shared__ double sign[kProbeCols];
+    __shared__ double uh[kProbeChunk], ul[kProbeChunk], ub[kProbeChunk];
+    if (threadIdx.x < kProbeCols) {
+        const uint64_t h = mix64(I->seed ^ (static_cast<uint64_t>(pr) << 40) ^ static_cast<uint64_t>(threadIdx.x));
+        cols[threadIdx.x] = static_cast<int64_t>(h % static_cast<uint64_t>(nt));
+        sign[threadIdx.x] = (h >> 63) ? -1.0 : 1.0;
+    }
+    __syncthreads();
+    const int64_t i = rblk * 256 + threadIdx.x;
+    const bool live = i < mt;
+    dd z{0.0, 0.0};
+    double za = 0.0;
+    for (int64_t p0 = 0; p0 < k; p0 += kProbeChunk) {
+        const int64_t pn = min(static_cast<int64_t>(kProbeChunk), k - p0);
+        // u = B x and |B| |x| for this chunk of the inner index
+        for (int64_t q = threadIdx.x; q < pn; q += blockDim.x) {
+            const int64_t p = p0 + q;
+            dd u{0.0, 0.0};
+            double a = 0.0;
+            for (int c = 0; c < kProbeCols; ++c) {
+                const int64_t j = cols[c];
+                const double b = I->b_rowc ? I->B[j + p * I->ldb] : I->B[p + j * I->ldb];
+                u = dd_add(u, dd{sign[c] * b, 0.0});
+                a += fabs(b);
+            }
+            uh[q] = u.hi;
+            ul[q] = u.lo;
+            ub[q] = a;
+        }
+        __syncthreads();
+        if (live) {
+            for (int64_t q = 0; q < pn; ++q) {
+                const int64_t p = p0 + q;
+                const double av = I->a_rowc ? I->A[i + p * I->lda] : I->A[p + i * I->lda];
+                z = dd_add_prod(z, av, uh[q]);
+                z = dd_add_prod(z, av, ul[q]);
+                za = fma(fabs(av), ub[q], za);
+            }
+        }
+        __syncthreads();
+    }
+    if (!live) return;
+    dd y{0.0, 0.0};
+    double ya = 0.0;
+    for (int c = 0; c < kProbeCols; ++c) {
+        const double cv = I->C[i + cols[c] * I->ldc];
+        y = dd_add(y, dd{sign[c] * cv, 0.0});
+        ya += fabs(cv);
+    }
+    // y - alpha z in double-double
+    const dd az{I->alpha * z.hi, fma(I->alpha, z.hi, -I->alpha * z.hi) + I->alpha * z.lo};
+    const dd diff = dd_add(y, dd{-az.hi, -az.lo});
+    const double err = fabs(diff.hi + diff.lo);
+    // za carries a relative rounding error below k 2^-53: widen by k 2^-50
+    const double tol = fabs(I->alpha) * I->tol_scale * za * (1.0 + static_cast<double>(k) * 0x1p-50) +
+                       0x1p-52 * ya + 1e-300;
+    if (!(err <= tol)) atomicOr(fail + I->tile, 1);
+}
+
+// ---------------------------------------------------------------- double-double reference
+// C_hi + C_lo ~= op(A) op(B) and |op(A)| |op(B)| for an m x n block, N/N column-major inputs.
+__global__ void __launch_bounds__(256) dd_gemm_nn_kernel(int64_t m, int64_t n, int64_t k, const double* __restrict__ A,
+                                                         int64_t lda, const double* __restrict__ B, int64_t ldb,
+                                                         double* __restrict__ hi, double* __restrict__ lo,
+                                                         double* __restrict__ absab) {
+    __shared__ double As[32][33];
+    __shared__ double Bs[32][33];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;  // 16 x 16 threads, 2 x 2 outputs each
+    const int64_t i0 = static_cast<int64_t>(blockIdx.x) * 32, j0 = static_cast<int64_t>(blockIdx.y) * 32;
+    dd acc[2][2] = {{{0, 0}, {0, 0}}, {{0, 0}, {0, 0}}};
+    double ab[2][2] = {{0, 0}, {0, 0}};
+    for (int64_t p0 = 0; p0 < k; p0 += 32) {
+        for (int e = threadIdx.x; e < 32 * 32; e += 256) {
+            const int r = e & 31, c = e >> 5;
+            As[r][c] = (i0 + r < m && p0 + c < k) ? A[(i0 + r) + (p0 + c) * lda] : 0.0;
+            Bs[r][c] = (p0 + r < k && j0 + c < n) ? B[(p0 + r) + (j0 + c) * ldb] : 0.0;
+        }
+        __syncthreads();
+        for (int q = 0; q < 32; ++q)
+            for (int a = 0; a < 2; ++a)
+                for (int b = 0; b < 2; ++b) {
+                    const double x = As[ty + 16 * a][q], y = Bs[q][tx + 16 * b];
+                    acc[a][b] = dd_add_prod(acc[a][b], x, y);
+                    ab[a][b] = fma(fabs(x), fabs(y), ab[a][b]);
+                }
+        __syncthreads();
+    }
+    for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b) {
+            const int64_t i = i0 + ty + 16 * a, j = j0 + tx + 16 * b;
+            if (i < m && j < n) {
+                hi[i + j * m] = acc[a][b].hi;
+                lo[i + j * m] = acc[a][b].lo;
+                absab[i + j * m] = ab[a][b];
+            }
+        }
+}
+
+// max over entries of |(C - hi) - lo| / (scale * absab), as float bits for atomicMax
+__global__ void error_ratio_kernel(int64_t m, int64_t n, const double* __restrict__ C, int64_t ldc,
+                                   const double* __restrict__ hi, const double* __restrict__ lo,
+                                   const double* __restrict__ absab, double scale, unsigned int* __restrict__ out) {
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= m * n) return;
+    const int64_t i = e % m, j = e / m;
+    const double err = fabs((C[i + j * ldc] - hi[e]) - lo[e]);
+    const double t = scale * absab[e];
+    float r;
+    if (err == 0.0) r = 0.0f;
+    else if (!(t > 0.0)) r = __int_as_float(0x7F800000);  // error where none is allowed
+    else r = static_cast<float>(err / t);
+    if (!(r == r)) r = __int_as_float(0x7F800000);
+    atomicMax(out, __float_as_uint(r));  // non-negative floats order like their bits
+}
+
+}  // namespace
+
+int64_t stat_item_blocks(StatItem& it, int64_t block0) {
+    it.block0 = block0;
+    if (it.rows <= 0 || it.k <= 0) {
+        it.rblocks = 1;
+        it.kchunk = 1;
+        return 0;
+    }
+    it.rblocks = it.row_contig ? (it.rows + 31) / 32 : (it.rows + 7) / 8;
+    const int64_t chunks = (it.k + 2047) / 2048;
+    it.kchunk = (it.k + chunks - 1) / chunks;
+    return it.rblocks * chunks;
+}
+
+void launch_panel_stats(const StatItem* d, const StatItem* h, int count, int64_t blocks, cudaStream_t st) {
+    if (count <= 0 || blocks <= 0) return;
+    if (h[0].row_contig) panel_stats_kernel<true><<<static_cast<unsigned>(blocks), 256, 0, st>>>(d, count);
+    else panel_stats_kernel<false><<<static_cast<unsigned>(blocks), 256, 0, st>>>(d, count);
+}
+
+void launch_tile_features(const FeatureItem* d, int count, float* feat, int* s_analytic, cudaStream_t st) {
+    if (count <= 0) return;
+    tile_features_kernel<<<(count + 127) / 128, 128, 0, st>>>(d, count, feat, s_analytic);
+}
+
+int64_t probe_item_blocks(ProbeItem& it, int64_t block0) {
+    it.block0 = block0;
+    return ((it.mt + 255) / 256) * kProbes;
+}
+
+void launch_probe(const ProbeItem* d, int count, int64_t blocks, int* fail, cudaStream_t st) {
+    if (count <= 0 || blocks <= 0) return;
+    probe_kernel<<<static_cast<unsigned>(blocks), 256, 0, st>>>(d, count, fail);
+}
+
+void launch_dd_gemm_nn(int64_t m, int64_t n, int64_t k, const double* A, int64_t lda, const double* B, int64_t ldb,
+                       double* hi, double* lo, double* absab, cudaStream_t st) {
+    dim3 grid(static_cast<unsigned>((m + 31) / 32), static_cast<unsigned>((n + 31) / 32));
+    dd_gemm_nn_kernel<<<grid, 256, 0, st>>>(m, n, k, A, lda, B, ldb, hi, lo, absab);
+}
+
+void launch_error_ratio(int64_t m, int64_t n, const double* C, int64_t ldc, const double* hi, const double* lo,
+                        const double* absab, double scale, unsigned int* out, cudaStream_t st) {
+    const int64_t total = m * n;
+    error_ratio_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, st>>>(m, n, C, ldc, hi, lo, absab, scale,
+                                                                                 out);
+}
+
+}  // namespace oz2

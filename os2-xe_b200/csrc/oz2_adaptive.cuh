@@ -1,0 +1,79 @@
+// oz2_adaptive.cuh - item tables and launchers of the adaptive-s subsystem (tile statistics,
+// features, analytic s, the Freivalds-style probe, the double-double reference used to label
+// training tiles) and of the small MLP that predicts s per tile. No counterpart in the
+// reference, whose number of moduli is fixed per call.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "oz2_plan.hpp"
+
+namespace oz2 {
+
+constexpr int kGapBins = 64;     // exponent gaps 0..63 (63 = "63 or more"), plus a zero counter
+constexpr int kFeatures = 16;
+constexpr int kHidden = 32;
+constexpr int kClasses = kMaxModuli - 1;  // s = 2..24
+constexpr int kMlpParams = kHidden * kFeatures + kHidden + kHidden * kHidden + kHidden + kClasses * kHidden + kClasses;
+constexpr int kProbes = 2;       // probe vectors per tile
+constexpr int kProbeCols = 4;    // +-1 entries per probe vector
+constexpr int kProbeChunk = 1024;
+
+// histogram of exponent gaps for the rows [0, rows) of one panel (rows of op(A) or columns of
+// op(B)), all k; layout like ScaleItem
+struct StatItem {
+    const double* X;
+    int64_t ldx, rows, k;
+    int row_contig;
+    const unsigned long long* maxbits;  // row maxima of the panel rows
+    unsigned int* hist;                 // kGapBins + 1 counters, zeroed before the launch
+    int64_t kchunk, block0, rblocks;
+};
+
+// one C tile: its two panels' histograms and maxima, k, target, tk per s for this k
+struct FeatureItem {
+    const unsigned int* hist_a;
+    const unsigned int* hist_b;
+    const unsigned long long* maxbits_a;
+    const unsigned long long* maxbits_b;
+    int64_t rows_a, rows_b, k;
+    int target_bits;
+    int tk[kMaxModuli + 1];  // tk[s] for s = 2..24 (0 where s is too small for k)
+};
+
+// probe of one computed tile (pointers at the tile's first row / column)
+struct ProbeItem {
+    const double* A;  // op(A) rows of the tile
+    const double* B;  // op(B) columns of the tile
+    const double* C;
+    int64_t lda, ldb, ldc, mt, nt, k;
+    int a_rowc;       // op(A)(i, p) at A[i + p lda] (else A[p + i lda])
+    int b_rowc;       // op(B)(p, j) at B[j + p ldb] (else B[p + j ldb])
+    double alpha, tol_scale;  // tol_scale = k 2^-t
+    uint64_t seed;
+    int tile;         // index into the failure flags
+    int64_t block0;
+};
+
+int64_t stat_item_blocks(StatItem& it, int64_t block0);
+void launch_panel_stats(const StatItem* d, const StatItem* h, int count, int64_t blocks, cudaStream_t st);
+void launch_tile_features(const FeatureItem* d, int count, float* feat, int* s_analytic, cudaStream_t st);
+int64_t probe_item_blocks(ProbeItem& it, int64_t block0);
+void launch_probe(const ProbeItem* d, int count, int64_t blocks, int* fail, cudaStream_t st);
+void launch_dd_gemm_nn(int64_t m, int64_t n, int64_t k, const double* A, int64_t lda, const double* B, int64_t ldb,
+                       double* hi, double* lo, double* absab, cudaStream_t st);
+void launch_error_ratio(int64_t m, int64_t n, const double* C, int64_t ldc, const double* hi, const double* lo,
+                        const double* absab, double scale, unsigned int* out, cudaStream_t st);
+
+// MLP: kFeatures -> kHidden (ReLU) -> kHidden (ReLU) -> kClasses, parameters packed as
+// W1[kHidden][kFeatures] b1 W2[kHidden][kHidden] b2 W3[kClasses][kHidden] b3.
+// s = 2 + the smallest class whose cumulative softmax probability reaches `threshold`.
+void launch_mlp_infer(const float* params, int count, const float* feat, float threshold, int* s_out,
+                      float* probs_out, cudaStream_t st);
+// mini-batch Adam with cross-entropy, one block; loss_out[epoch] = mean training loss
+void launch_mlp_train(float* params, int count, const float* feat, const int* label, int epochs, float lr,
+                      unsigned int seed, float* loss_out, cudaStream_t st);
+
+}  // namespace oz2

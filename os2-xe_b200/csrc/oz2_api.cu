@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "../../include/oz2/oz2.h"
+#include "oz2_adaptive.cuh"
 #include "oz2_kernels.cuh"
 #include "oz2_plan.hpp"
 
@@ -71,6 +72,7 @@ struct GraphEntry {
     std::vector<cudaGraphExec_t> execs;
     std::vector<void*> dev_blobs;
     std::vector<unsigned char> problems;
+    int64_t kernels = 0;  // kernel launches one replay makes
 };
 
 }  // namespace
@@ -108,6 +110,15 @@ struct oz2_context {
     cudaStream_t cap_stream = nullptr;
     std::map<uint64_t, GraphEntry> graphs;
     GraphEntry* capturing = nullptr;  // entry being filled by the current grouped call
+    // adaptive s: MLP parameters on the device, second workspace for the per-tile phase
+    float* d_mlp = nullptr;
+    bool mlp_loaded = false;
+    float mlp_threshold = 0.9f;
+    int adaptive_tile = 512;
+    uint8_t* ws2 = nullptr;
+    size_t ws2_size = 0;
+    int64_t astats[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int64_t launches = 0;  // kernels launched through this handle (graph replays included)
     bool capture_ok = true;           // false when part of the call ran outside the graphs
     std::string err;
 };
@@ -464,11 +475,13 @@ int check_grid(oz2_context* h, const Program& prog) {
 }
 
 // ---------------------------------------------------------------- issuing a program
-int upload(oz2_context* h, const Program& prog, unsigned char* dev) {
-    const size_t bytes = prog.blob.size();
+// copies host bytes to device memory on the stream: small blobs through a kernel parameter,
+// large ones through the pinned staging ring
+int put_blob(oz2_context* h, const void* data, size_t bytes, unsigned char* dev) {
     if (bytes == 0) return OZ2_OK;
-    if (bytes <= kParamBlobBytes) {  // written by a kernel that takes the bytes as its parameter
-        launch_write_blob(prog.blob.data(), bytes, dev, h->stream);
+    if (bytes <= kParamBlobBytes) {
+        launch_write_blob(data, bytes, dev, h->stream);
+        ++h->launches;
         return OZ2_OK;
     }
     const int slot = h->ring_next;
@@ -482,16 +495,21 @@ int upload(oz2_context* h, const Program& prog, unsigned char* dev) {
         OZ2_CUDA(h, cudaHostAlloc(&h->ring_host[slot], cap, cudaHostAllocDefault));
         h->ring_cap[slot] = cap;
     }
-    std::memcpy(h->ring_host[slot], prog.blob.data(), bytes);
+    std::memcpy(h->ring_host[slot], data, bytes);
     OZ2_CUDA(h, cudaMemcpyAsync(dev, h->ring_host[slot], bytes, cudaMemcpyHostToDevice, h->stream));
     OZ2_CUDA(h, cudaEventRecord(h->ring_ev[slot], h->stream));
     h->ring_used[slot] = true;
     return OZ2_OK;
 }
 
+int upload(oz2_context* h, const Program& prog, unsigned char* dev) {
+    return put_blob(h, prog.blob.data(), prog.blob.size(), dev);
+}
+
 void issue(oz2_context* h, const Program& prog, const unsigned char* dev) {
     const unsigned char* hb = prog.blob.data();
     for (const Op& op : prog.ops) {
+        if (op.kind != Op::Memset && op.kind != Op::Mark) ++h->launches;
         switch (op.kind) {
             case Op::Memset: cudaMemsetAsync(op.ptr, 0, op.bytes, h->stream); break;
             case Op::Scale:
@@ -758,7 +776,9 @@ int run_grouped(oz2_context* h, std::vector<Prob>& probs) {
             h->stream = h->cap_stream;
             cudaError_t ce = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
             if (ce == cudaSuccess) {
+                const int64_t before = h->launches;
                 issue(h, prog, static_cast<unsigned char*>(dev_blob));
+                h->capturing->kernels += h->launches - before;
                 ce = cudaStreamEndCapture(h->stream, &g);
             }
             h->stream = user;
@@ -777,6 +797,376 @@ int run_grouped(oz2_context* h, std::vector<Prob>& probs) {
     }
     h->tiling[0] = h->tiling[1] = h->tiling[2] = h->tiling[3] = h->tiling[4] = 0;
     h->tiling[5] = static_cast<int64_t>(max_bytes);
+    return OZ2_OK;
+}
+
+
+// ---------------------------------------------------------------- adaptive s per tile
+int ensure_ws2(oz2_context* h, size_t bytes) {
+    if (h->ws2_size >= bytes) return OZ2_OK;
+    OZ2_CUDA(h, cudaStreamSynchronize(h->stream));
+    drop_graphs(h);
+    if (h->ws2) cudaFree(h->ws2);
+    h->ws2 = nullptr;
+    h->ws2_size = 0;
+    if (cudaMalloc(&h->ws2, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(h, OZ2_ENOMEM, "oz2: workspace allocation failed");
+    }
+    h->ws2_size = bytes;
+    return OZ2_OK;
+}
+
+// tk[s] for one k (0 where s is too small)
+void tk_table(oz2_context* h, int64_t k, int* tk) {
+    for (int s = 0; s <= kMaxModuli; ++s) tk[s] = 0;
+    for (int s = 2; s <= kMaxModuli; ++s) {
+        const Plan* p;
+        if (get_plan(h, s, k, &p) == OZ2_OK) tk[s] = p->tk;
+    }
+}
+
+struct TileRef {
+    int prob;      // index into the problem list
+    int64_t i0, j0, mb, nb;
+    int ia, jb;    // panel indices
+};
+
+// mode: 0 MLP per tile (analytic cap, probe, rerun at analytic s), 1 analytic per tile,
+// 2 analytic per problem (the largest of its tiles), 3 the problems' own num_moduli
+int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>& fixed_s, int target_bits,
+                 int mode, float* feat_out = nullptr, int* sa_out = nullptr, int64_t* ntiles_out = nullptr) {
+    const int64_t T = h->adaptive_tile;
+    for (int q = 0; q < 8; ++q) h->astats[q] = 0;
+    // ---- phase 1: maxima, panel statistics, tile features, analytic s, MLP
+    std::vector<TileRef> tiles;
+    std::vector<int64_t> pa0(base.size()), pb0(base.size());
+    int64_t npanels = 0;
+    for (size_t q = 0; q < base.size(); ++q) {
+        const Prob& p = base[q];
+        const int64_t na = ceil_div(p.m, T), nbp = ceil_div(p.n, T);
+        pa0[q] = npanels;
+        npanels += na;
+        pb0[q] = npanels;
+        npanels += nbp;
+        for (int64_t J = 0; J < nbp; ++J)
+            for (int64_t I = 0; I < na; ++I)
+                tiles.push_back(TileRef{static_cast<int>(q), I * T, J * T, std::min(T, p.m - I * T),
+                                        std::min(T, p.n - J * T), static_cast<int>(pa0[q] + I),
+                                        static_cast<int>(pb0[q] + J)});
+    }
+    const int64_t ntiles = static_cast<int64_t>(tiles.size());
+    size_t off = 0;
+    auto carve1 = [&](size_t bytes) {
+        const size_t o = off;
+        off += align256(bytes);
+        return o;
+    };
+    std::vector<size_t> omaxA(base.size()), omaxB(base.size());
+    for (size_t q = 0; q < base.size(); ++q) {
+        omaxA[q] = carve1(base[q].m * 8);
+        omaxB[q] = carve1(base[q].n * 8);
+    }
+    const size_t ohist = carve1(static_cast<size_t>(npanels) * (kGapBins + 1) * 4);
+    const size_t ofail = carve1(static_cast<size_t>(ntiles) * 4);
+    const size_t zero_end = off;
+    const size_t ofeat = carve1(static_cast<size_t>(ntiles) * kFeatures * 4);
+    const size_t osa = carve1(static_cast<size_t>(ntiles) * 4);
+    const size_t osm = carve1(static_cast<size_t>(ntiles) * 4);
+    const size_t desc_bytes = 1024 + base.size() * 2 * sizeof(ScaleItem) + npanels * sizeof(StatItem) +
+                              ntiles * (sizeof(FeatureItem) + sizeof(ProbeItem)) + 16 * 256;
+    const size_t odesc = carve1(desc_bytes);
+    int st = ensure_workspace(h, off);
+    if (st) return st;
+    auto* ws = h->ws;
+    auto maxA = [&](int q) { return reinterpret_cast<unsigned long long*>(ws + omaxA[q]); };
+    auto maxB = [&](int q) { return reinterpret_cast<unsigned long long*>(ws + omaxB[q]); };
+    auto hist = [&](int64_t panel) { return reinterpret_cast<unsigned int*>(ws + ohist) + panel * (kGapBins + 1); };
+    int* d_fail = reinterpret_cast<int*>(ws + ofail);
+    float* d_feat = reinterpret_cast<float*>(ws + ofeat);
+    int* d_sa = reinterpret_cast<int*>(ws + osa);
+    int* d_sm = reinterpret_cast<int*>(ws + osm);
+    OZ2_CUDA(h, cudaMemsetAsync(ws, 0, zero_end, h->stream));
+
+    Program ph1;
+    std::vector<ScaleItem> sc;
+    for (size_t q = 0; q < base.size(); ++q) {
+        sc.push_back(scale_item(base[q], true, maxA(static_cast<int>(q))));
+        sc.push_back(scale_item(base[q], false, maxB(static_cast<int>(q))));
+    }
+    plan_scale(h, ph1, sc);
+    // panel statistics, grouped by layout
+    std::map<int, std::vector<StatItem>> stat_groups;
+    for (size_t q = 0; q < base.size(); ++q) {
+        const Prob& p = base[q];
+        for (int side = 0; side < 2; ++side) {
+            const int64_t rows = side ? p.n : p.m;
+            const bool rowc = side ? !is_n(p.tb) : is_n(p.ta);
+            const double* X = side ? p.B : p.A;
+            const int64_t ldx = side ? p.ldb : p.lda;
+            for (int64_t r0 = 0, pi = 0; r0 < rows; r0 += T, ++pi) {
+                StatItem it{};
+                it.X = X + (rowc ? r0 : r0 * ldx);
+                it.ldx = ldx;
+                it.rows = std::min(T, rows - r0);
+                it.k = p.k;
+                it.row_contig = rowc;
+                it.maxbits = (side ? maxB(static_cast<int>(q)) : maxA(static_cast<int>(q))) + r0;
+                it.hist = hist((side ? pb0[q] : pa0[q]) + pi);
+                stat_groups[rowc].push_back(it);
+            }
+        }
+    }
+    struct StatOp {
+        size_t off;
+        int count;
+        int64_t blocks;
+    };
+    std::vector<StatOp> stat_ops;
+    for (auto& kv : stat_groups) {
+        int64_t blocks = 0;
+        for (auto& it : kv.second) blocks += stat_item_blocks(it, blocks);
+        stat_ops.push_back({ph1.add(kv.second.data(), kv.second.size() * sizeof(StatItem)),
+                            static_cast<int>(kv.second.size()), blocks});
+    }
+    std::vector<FeatureItem> fi(ntiles);
+    std::map<int64_t, std::vector<int>> tk_cache;
+    for (int64_t t = 0; t < ntiles; ++t) {
+        const TileRef& r = tiles[t];
+        const Prob& p = base[r.prob];
+        FeatureItem& f = fi[t];
+        f.hist_a = hist(r.ia);
+        f.hist_b = hist(r.jb);
+        f.maxbits_a = maxA(r.prob) + r.i0;
+        f.maxbits_b = maxB(r.prob) + r.j0;
+        f.rows_a = r.mb;
+        f.rows_b = r.nb;
+        f.k = p.k;
+        f.target_bits = target_bits;
+        auto it = tk_cache.find(p.k);
+        if (it == tk_cache.end()) {
+            std::vector<int> tk(kMaxModuli + 1);
+            tk_table(h, p.k, tk.data());
+            it = tk_cache.emplace(p.k, tk).first;
+        }
+        for (int s = 0; s <= kMaxModuli; ++s) f.tk[s] = it->second[s];
+    }
+    const size_t ofi = ph1.add(fi.data(), fi.size() * sizeof(FeatureItem));
+    if (ph1.blob.size() > desc_bytes) return fail(h, OZ2_EINTERNAL, "oz2: descriptor region too small");
+    unsigned char* dd = ws + odesc;
+    if ((st = put_blob(h, ph1.blob.data(), ph1.blob.size(), dd))) return st;
+    mark(h, kBegin);
+    issue(h, ph1, dd);  // scale (its mark closes the scale stage)
+    for (const StatOp& so : stat_ops) {
+        launch_panel_stats(reinterpret_cast<const StatItem*>(dd + so.off),
+                           reinterpret_cast<const StatItem*>(ph1.blob.data() + so.off), so.count, so.blocks,
+                           h->stream);
+        ++h->launches;
+    }
+    launch_tile_features(reinterpret_cast<const FeatureItem*>(dd + ofi), static_cast<int>(ntiles), d_feat, d_sa,
+                         h->stream);
+    const bool use_mlp = mode == 0 && h->mlp_loaded;
+    ++h->launches;
+    if (use_mlp) {
+        launch_mlp_infer(h->d_mlp, static_cast<int>(ntiles), d_feat, h->mlp_threshold, d_sm, nullptr, h->stream);
+        ++h->launches;
+    }
+    mark(h, kScale);  // statistics, features and the MLP count with the scale stage
+    std::vector<int> s_an(ntiles), s_ml(ntiles, kMaxModuli);
+    OZ2_CUDA(h, cudaMemcpyAsync(s_an.data(), d_sa, ntiles * 4, cudaMemcpyDeviceToHost, h->stream));
+    if (use_mlp) OZ2_CUDA(h, cudaMemcpyAsync(s_ml.data(), d_sm, ntiles * 4, cudaMemcpyDeviceToHost, h->stream));
+    OZ2_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (mode < 0) {  // features only
+        if (feat_out)
+            OZ2_CUDA(h, cudaMemcpyAsync(feat_out, d_feat, ntiles * kFeatures * 4, cudaMemcpyDeviceToDevice, h->stream));
+        if (sa_out) OZ2_CUDA(h, cudaMemcpyAsync(sa_out, d_sa, ntiles * 4, cudaMemcpyDeviceToDevice, h->stream));
+        if (ntiles_out) *ntiles_out = ntiles;
+        return OZ2_OK;
+    }
+
+    // ---- per-tile s
+    std::vector<int> s_tile(ntiles);
+    std::vector<int> prob_max(base.size(), 2);
+    for (int64_t t = 0; t < ntiles; ++t) prob_max[tiles[t].prob] = std::max(prob_max[tiles[t].prob], s_an[t]);
+    for (int64_t t = 0; t < ntiles; ++t) {
+        const int q = tiles[t].prob;
+        int sv;
+        switch (mode) {
+            // the probe and the rerun need C's old values gone (beta = 0): other problems keep
+            // the analytic s
+            case 0: sv = use_mlp && base[q].beta[0] == 0.0 ? std::min(s_ml[t], s_an[t]) : s_an[t]; break;
+            case 1: sv = s_an[t]; break;
+            case 2: sv = prob_max[q]; break;
+            default: sv = fixed_s[q]; break;
+        }
+        // never below the smallest s that k admits
+        const std::vector<int>& tk = tk_cache[base[q].k];
+        while (sv < kMaxModuli && tk[sv] == 0) ++sv;
+        s_tile[t] = std::max(2, std::min(kMaxModuli, sv));
+    }
+
+    // ---- phase 2: tiles with their s, panels split once per (panel, s); batches by budget
+    auto run_tiles = [&](const std::vector<int64_t>& which, const std::vector<int>& svals) -> int {
+        std::vector<std::unique_ptr<Prob>> probs;  // one per (problem, s)
+        std::map<std::pair<int, int>, Prob*> prob_for;
+        auto get_prob = [&](int q, int sv) -> Prob* {
+            auto key = std::make_pair(q, sv);
+            auto it = prob_for.find(key);
+            if (it != prob_for.end()) return it->second;
+            auto np = std::make_unique<Prob>(base[q]);
+            const Plan* plan;
+            if (get_plan(h, sv, base[q].k, &plan)) return nullptr;
+            np->plan = plan;
+            Prob* raw = np.get();
+            probs.push_back(std::move(np));
+            prob_for[key] = raw;
+            return raw;
+        };
+        // the first workspace holds phase-1 data; the second may use what is left
+        size_t limit = h->ws_limit;
+        if (!limit) {
+            size_t free_b = 0, total = 0;
+            if (cudaMemGetInfo(&free_b, &total) != cudaSuccess) return fail(h, OZ2_ECUDA, "oz2: cudaMemGetInfo");
+            free_b += h->ws2_size;
+            const size_t reserve = (size_t{512} << 20) + total / 32;
+            limit = free_b > reserve ? free_b - reserve : 0;
+        }
+        size_t i = 0;
+        while (i < which.size()) {
+            // one batch: tiles until the budget is reached
+            std::map<std::tuple<int, int, int>, std::pair<size_t, bool>> panels;  // (panel, side, s) -> offset
+            size_t off2 = 0;
+            auto carve2 = [&](size_t bytes) {
+                const size_t o = off2;
+                off2 += align256(bytes);
+                return o;
+            };
+            std::vector<std::tuple<int64_t, size_t, size_t, size_t>> batch;  // tile, A planes, B planes, resid
+            size_t start = i;
+            for (; i < which.size(); ++i) {
+                const int64_t t = which[i];
+                const TileRef& r = tiles[t];
+                const int sv = svals[i];
+                const Prob& p = base[r.prob];
+                const size_t pa = static_cast<size_t>(sv) * plane_geom(r.mb, p.k, kGemmIPad).plane_bytes;
+                const size_t pb = static_cast<size_t>(sv) * plane_geom(r.nb, p.k, kGemmJ).plane_bytes;
+                const size_t rs = static_cast<size_t>(sv) * r.nb * round_up(r.mb, 32);
+                const bool newa = !panels.count({r.ia, 0, sv}), newb = !panels.count({r.jb, 1, sv});
+                const size_t add = (newa ? align256(pa) : 0) + (newb ? align256(pb) : 0) + align256(rs) +
+                                   2 * sizeof(SplitItem) + sizeof(GemmItem) + sizeof(CrtItem) + 2048;
+                if (i > start && off2 + add + (1 << 20) > limit) break;
+                if (newa) panels[{r.ia, 0, sv}] = {carve2(pa), true};
+                if (newb) panels[{r.jb, 1, sv}] = {carve2(pb), true};
+                batch.emplace_back(t, panels[{r.ia, 0, sv}].first, panels[{r.jb, 1, sv}].first, carve2(rs));
+            }
+            const size_t obase_desc = off2;
+            const size_t need = off2 + align256(batch.size() * (2 * sizeof(SplitItem) + sizeof(GemmItem) +
+                                                                sizeof(CrtItem) + 1024) + 8192);
+            int st2 = ensure_ws2(h, need);
+            if (st2) return st2;
+            std::vector<Task> tasks;
+            std::map<std::tuple<int, int, int>, bool> split_done;
+            for (size_t b = 0; b < batch.size(); ++b) {
+                const int64_t t = std::get<0>(batch[b]);
+                const TileRef& r = tiles[t];
+                const int sv = svals[start + b];
+                Prob* p = get_prob(r.prob, sv);
+                if (!p) return fail(h, OZ2_EINTERNAL, "oz2: no plan for adaptive tile");
+                Task tk{};
+                tk.p = p;
+                tk.i0 = r.i0;
+                tk.j0 = r.j0;
+                tk.mb = r.mb;
+                tk.nb = r.nb;
+                tk.split_a = !split_done[{r.ia, 0, sv}];
+                tk.split_b = !split_done[{r.jb, 1, sv}];
+                split_done[{r.ia, 0, sv}] = true;
+                split_done[{r.jb, 1, sv}] = true;
+                tk.maxA = maxA(r.prob);
+                tk.maxB = maxB(r.prob);
+                tk.planesA = reinterpret_cast<int8_t*>(h->ws2 + std::get<1>(batch[b]));
+                tk.planesB = reinterpret_cast<int8_t*>(h->ws2 + std::get<2>(batch[b]));
+                tk.resid = h->ws2 + std::get<3>(batch[b]);
+                tk.ldr = round_up(r.mb, 32);
+                tasks.push_back(tk);
+                h->astats[1] += sv;
+                h->astats[7] += static_cast<int64_t>(sv) * r.mb * r.nb * base[r.prob].k;
+            }
+            std::vector<const Prob*> bp;
+            for (auto& up : probs) bp.push_back(up.get());
+            const GemmConfig cfg = config_for(h, bp);
+            h->last_cfg = cfg;
+            Program prog;
+            plan_tasks(prog, tasks, cfg);
+            if (obase_desc + prog.blob.size() > h->ws2_size)
+                return fail(h, OZ2_EINTERNAL, "oz2: descriptor region too small");
+            if ((st2 = check_grid(h, prog))) return st2;
+            if ((st2 = upload(h, prog, h->ws2 + obase_desc))) return st2;
+            mark(h, kBegin);
+            issue(h, prog, h->ws2 + obase_desc);
+        }
+        return OZ2_OK;
+    };
+    std::vector<int64_t> all(ntiles);
+    for (int64_t t = 0; t < ntiles; ++t) all[t] = t;
+    h->astats[0] = ntiles;
+    if ((st = run_tiles(all, s_tile))) return st;
+
+    // ---- probe (MLP mode, problems with beta = 0) and rerun at the analytic s
+    if (mode == 0) {
+        std::vector<ProbeItem> pi;
+        int64_t blocks = 0;
+        for (int64_t t = 0; t < ntiles; ++t) {
+            const TileRef& r = tiles[t];
+            const Prob& p = base[r.prob];
+            if (p.beta[0] != 0.0 || s_tile[t] >= s_an[t]) continue;  // analytic s needs no probe
+            ProbeItem it{};
+            it.a_rowc = is_n(p.ta);
+            it.b_rowc = !is_n(p.tb);
+            it.A = p.A + (it.a_rowc ? r.i0 : r.i0 * p.lda);
+            it.B = p.B + (it.b_rowc ? r.j0 : r.j0 * p.ldb);
+            it.C = p.C + r.i0 + r.j0 * p.ldc;
+            it.lda = p.lda;
+            it.ldb = p.ldb;
+            it.ldc = p.ldc;
+            it.mt = r.mb;
+            it.nt = r.nb;
+            it.k = p.k;
+            it.alpha = p.alpha[0];
+            it.tol_scale = static_cast<double>(p.k) * std::ldexp(1.0, -target_bits);
+            it.seed = 0x5DEECE66Dull * static_cast<uint64_t>(t + 1) + static_cast<uint64_t>(r.prob);
+            it.tile = static_cast<int>(t);
+            blocks += probe_item_blocks(it, blocks);
+            pi.push_back(it);
+        }
+        if (!pi.empty()) {
+            unsigned char* pd = ws + odesc;  // phase-1 descriptors are consumed by now (stream order)
+            if ((st = put_blob(h, pi.data(), pi.size() * sizeof(ProbeItem), pd))) return st;
+            launch_probe(reinterpret_cast<const ProbeItem*>(pd), static_cast<int>(pi.size()), blocks, d_fail, h->stream);
+            ++h->launches;
+            std::vector<int> failed(ntiles);
+            OZ2_CUDA(h, cudaMemcpyAsync(failed.data(), d_fail, ntiles * 4, cudaMemcpyDeviceToHost, h->stream));
+            OZ2_CUDA(h, cudaStreamSynchronize(h->stream));
+            h->astats[2] = static_cast<int64_t>(pi.size());
+            std::vector<int64_t> redo;
+            std::vector<int> redo_s;
+            for (int64_t t = 0; t < ntiles; ++t)
+                if (failed[t]) {
+                    redo.push_back(t);
+                    redo_s.push_back(s_an[t]);
+                }
+            h->astats[3] = static_cast<int64_t>(redo.size());
+            if (!redo.empty()) {
+                // beta = 0 for every probed tile, so recomputing C overwrites the failed values
+                int64_t extra = 0;
+                for (size_t q = 0; q < redo.size(); ++q) extra += redo_s[q];
+                h->astats[4] = extra;
+                if ((st = run_tiles(redo, redo_s))) return st;
+            }
+        }
+    }
+    for (int64_t t = 0; t < ntiles; ++t) h->astats[5] += s_an[t];
+    h->astats[6] = use_mlp ? 1 : 0;
     return OZ2_OK;
 }
 
@@ -800,6 +1190,30 @@ int validate_grouped(oz2_handle h, int count, const oz2_dgemm_problem* pr, std::
     return OZ2_OK;
 }
 
+
+int validate_adaptive(oz2_handle h, int count, const oz2_dgemm_problem* pr, std::vector<Prob>& out,
+                      std::vector<int>& fixed_s, bool need_fixed) {
+    out.clear();
+    fixed_s.clear();
+    for (int i = 0; i < count; ++i) {
+        const oz2_dgemm_problem& q = pr[i];
+        int st = check_args(h, q.ta, q.tb, q.m, q.n, q.k, q.lda, q.ldb, q.ldc);
+        if (st) return fail(h, st, "oz2: problem " + std::to_string(i) + ": " + h->err);
+    }
+    for (int i = 0; i < count; ++i) {
+        const oz2_dgemm_problem& q = pr[i];
+        if (q.m == 0 || q.n == 0 || q.k == 0 || q.alpha == 0.0) continue;
+        if (need_fixed) {
+            const Plan* plan;
+            int st = get_plan(h, q.num_moduli, q.k, &plan);
+            if (st) return fail(h, st, "oz2: problem " + std::to_string(i) + ": " + h->err);
+        }
+        out.push_back(Prob{q.ta, q.tb, q.m, q.n, q.k, {q.alpha, 0.0}, {q.beta, 0.0}, q.A, q.lda, q.B, q.ldb, q.C, q.ldc, 1,
+                           nullptr});
+        fixed_s.push_back(q.num_moduli);
+    }
+    return OZ2_OK;
+}
 }  // namespace
 
 namespace oz2 {
@@ -815,8 +1229,8 @@ int oz2_create(void* stream, oz2_handle* out) {
     h->stream = static_cast<cudaStream_t>(stream);
     cudaError_t e = cudaGetDevice(&h->device);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
-    if (e == cudaSuccess) e = cudaMalloc(&h->d_err, sizeof(int));
-    if (e == cudaSuccess) e = cudaMemset(h->d_err, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&h->d_err, 4 * sizeof(int));  // error word + scratch words
+    if (e == cudaSuccess) e = cudaMemset(h->d_err, 0, 4 * sizeof(int));
     if (e == cudaSuccess) e = prepare_gemm_kernels();
     if (e != cudaSuccess) {
         const int st = cuda_fail(nullptr, e, "oz2_create");
@@ -841,6 +1255,8 @@ int oz2_destroy(oz2_handle h) {
         if (h->ring_ev[i]) cudaEventDestroy(h->ring_ev[i]);
     }
     if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
+    if (h->d_mlp) cudaFree(h->d_mlp);
+    if (h->ws2) cudaFree(h->ws2);
     delete h;
     return OZ2_OK;
 }
@@ -866,6 +1282,7 @@ int oz2_dgemm(oz2_handle h, char ta, char tb, int64_t m, int64_t n, int64_t k, d
     const double be[2] = {beta, 0.0};
     if (k == 0 || alpha == 0.0) {
         launch_scale_c(C, ldc, m, n, be, false, h->stream);
+        ++h->launches;
         return end_call(h, done);
     }
     const Plan* plan;
@@ -889,6 +1306,7 @@ int oz2_zgemm(oz2_handle h, char ta, char tb, int64_t m, int64_t n, int64_t k, c
     if (m == 0 || n == 0) return end_call(h, done);
     if (k == 0 || (alpha[0] == 0.0 && alpha[1] == 0.0)) {
         launch_scale_c(C, ldc, m, n, beta, true, h->stream);
+        ++h->launches;
         return end_call(h, done);
     }
     if (k > std::numeric_limits<int64_t>::max() / 2) return fail(h, OZ2_EINVAL, "oz2: k too large");
@@ -914,6 +1332,7 @@ int oz2_dgemm_grouped(oz2_handle h, int count, const oz2_dgemm_problem* problems
         if (q.m > 0 && q.n > 0 && (q.k == 0 || q.alpha == 0.0)) {
             const double be[2] = {q.beta, 0.0};
             launch_scale_c(q.C, q.ldc, q.m, q.n, be, false, h->stream);
+            ++h->launches;
         }
     }
     if (probs.empty()) return end_call(h, done);
@@ -931,6 +1350,7 @@ int oz2_dgemm_grouped(oz2_handle h, int count, const oz2_dgemm_problem* problems
         std::memcmp(it->second.problems.data(), raw, raw_bytes) == 0) {
         mark(h, kBegin);
         for (auto e : it->second.execs) OZ2_CUDA(h, cudaGraphLaunch(e, h->stream));
+        h->launches += it->second.kernels;
         mark(h, kCrt);
         return end_call(h, done);
     }
@@ -949,6 +1369,149 @@ int oz2_dgemm_grouped(oz2_handle h, int count, const oz2_dgemm_problem* problems
     if (st || !keep) drop_graphs(h);
     if (st) return st;
     return end_call(h, done);
+}
+
+
+int oz2_dgemm_adaptive(oz2_handle h, int count, const oz2_dgemm_problem* problems, int target_bits, int mode,
+                       int64_t* stats8) {
+    if (!h) return fail(nullptr, OZ2_EINVAL, "oz2: null handle");
+    if (count < 0 || (count > 0 && !problems)) return fail(h, OZ2_EINVAL, "oz2: bad problem list");
+    if (target_bits < 1 || target_bits > 120) return fail(h, OZ2_EINVAL, "oz2: target_bits must be in [1, 120]");
+    if (mode < 0 || mode > 3) return fail(h, OZ2_EINVAL, "oz2: mode must be 0..3");
+    h->marks.clear();
+    if (h->plans.size() > 1024) h->plans.clear();
+    std::vector<Prob> probs;
+    std::vector<int> fixed_s;
+    int st = validate_adaptive(h, count, problems, probs, fixed_s, mode == 3);
+    if (st) return st;
+    if ((st = begin_call(h, nullptr, 0))) return st;
+    for (int i = 0; i < count; ++i) {
+        const oz2_dgemm_problem& q = problems[i];
+        if (q.m > 0 && q.n > 0 && (q.k == 0 || q.alpha == 0.0)) {
+            const double be[2] = {q.beta, 0.0};
+            launch_scale_c(q.C, q.ldc, q.m, q.n, be, false, h->stream);
+            ++h->launches;
+        }
+    }
+    for (int q = 0; q < 8; ++q) h->astats[q] = 0;
+    if (!probs.empty() && (st = run_adaptive(h, probs, fixed_s, target_bits, mode))) return st;
+    if (stats8)
+        for (int q = 0; q < 8; ++q) stats8[q] = h->astats[q];
+    return end_call(h, nullptr);
+}
+
+int oz2_tile_features(oz2_handle h, int count, const oz2_dgemm_problem* problems, int target_bits,
+                      float* d_features, int* d_s_analytic, int64_t* ntiles) {
+    if (!h) return fail(nullptr, OZ2_EINVAL, "oz2: null handle");
+    std::vector<Prob> probs;
+    std::vector<int> fixed_s;
+    int st = validate_adaptive(h, count, problems, probs, fixed_s, false);
+    if (st) return st;
+    int64_t nt = 0;
+    if (!probs.empty() && (st = run_adaptive(h, probs, fixed_s, target_bits, -1, d_features, d_s_analytic, &nt)))
+        return st;
+    if (ntiles) *ntiles = nt;
+    return end_call(h, nullptr);
+}
+
+int oz2_set_adaptive_options(oz2_handle h, int tile, float threshold) {
+    if (!h) return fail(nullptr, OZ2_EINVAL, "oz2: null handle");
+    if (tile < 128 || tile % 128 || !(threshold > 0.0f && threshold <= 1.0f))
+        return fail(h, OZ2_EINVAL, "oz2: tile must be a positive multiple of 128, threshold in (0, 1]");
+    h->adaptive_tile = tile;
+    h->mlp_threshold = threshold;
+    return OZ2_OK;
+}
+
+int oz2_mlp_info(int* out4) {
+    if (!out4) return fail(nullptr, OZ2_EINVAL, "oz2: null argument");
+    out4[0] = kMlpParams;
+    out4[1] = kFeatures;
+    out4[2] = kClasses;
+    out4[3] = kHidden;
+    return OZ2_OK;
+}
+
+int oz2_mlp_set_weights(oz2_handle h, const float* params, int nparams) {
+    if (!h) return fail(nullptr, OZ2_EINVAL, "oz2: null handle");
+    if (!params) {
+        h->mlp_loaded = false;
+        return OZ2_OK;
+    }
+    if (nparams != kMlpParams) return fail(h, OZ2_EINVAL, "oz2: wrong number of MLP parameters");
+    if (!h->d_mlp) OZ2_CUDA(h, cudaMalloc(&h->d_mlp, kMlpParams * sizeof(float)));
+    OZ2_CUDA(h, cudaMemcpyAsync(h->d_mlp, params, kMlpParams * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    OZ2_CUDA(h, cudaStreamSynchronize(h->stream));
+    h->mlp_loaded = true;
+    return OZ2_OK;
+}
+
+int oz2_mlp_train(oz2_handle h, int count, const float* d_features, const int* d_labels, int epochs, float lr,
+                  unsigned int seed, float* params, float* loss) {
+    if (!h || !params || count <= 0 || epochs <= 0) return fail(h, OZ2_EINVAL, "oz2: bad training arguments");
+    float* dp = nullptr;
+    float* dl = nullptr;
+    OZ2_CUDA(h, cudaMalloc(&dp, kMlpParams * sizeof(float)));
+    cudaError_t e = cudaMalloc(&dl, static_cast<size_t>(epochs) * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dp, params, kMlpParams * sizeof(float), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) {
+        launch_mlp_train(dp, count, d_features, d_labels, epochs, lr, seed, dl, h->stream);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(params, dp, kMlpParams * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess && loss)
+        e = cudaMemcpyAsync(loss, dl, static_cast<size_t>(epochs) * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(dp);
+    if (dl) cudaFree(dl);
+    if (e != cudaSuccess) return cuda_fail(h, e, "oz2_mlp_train");
+    return OZ2_OK;
+}
+
+int oz2_mlp_infer(oz2_handle h, const float* params, int count, const float* d_features, float threshold, int* d_s,
+                  float* d_probs) {
+    if (!h || !params || count < 0) return fail(h, OZ2_EINVAL, "oz2: bad inference arguments");
+    float* dp = nullptr;
+    OZ2_CUDA(h, cudaMalloc(&dp, kMlpParams * sizeof(float)));
+    cudaError_t e = cudaMemcpyAsync(dp, params, kMlpParams * sizeof(float), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) {
+        launch_mlp_infer(dp, count, d_features, threshold, d_s, d_probs, h->stream);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(dp);
+    if (e != cudaSuccess) return cuda_fail(h, e, "oz2_mlp_infer");
+    return OZ2_OK;
+}
+
+int oz2_dd_reference(oz2_handle h, int64_t m, int64_t n, int64_t k, const double* A, int64_t lda, const double* B,
+                     int64_t ldb, double* hi, double* lo, double* absab) {
+    if (!h) return fail(nullptr, OZ2_EINVAL, "oz2: null handle");
+    if (m < 0 || n < 0 || k < 0 || lda < std::max<int64_t>(1, m) || ldb < std::max<int64_t>(1, k))
+        return fail(h, OZ2_EINVAL, "oz2: bad dimensions");
+    if (m == 0 || n == 0) return OZ2_OK;
+    launch_dd_gemm_nn(m, n, k, A, lda, B, ldb, hi, lo, absab, h->stream);
+    return end_call(h, nullptr);
+}
+
+int oz2_error_ratio(oz2_handle h, int64_t m, int64_t n, int64_t k, const double* C, int64_t ldc, const double* hi,
+                    const double* lo, const double* absab, int target_bits, float* out) {
+    if (!h || !out) return fail(h, OZ2_EINVAL, "oz2: null argument");
+    if (m <= 0 || n <= 0 || ldc < m) return fail(h, OZ2_EINVAL, "oz2: bad dimensions");
+    OZ2_CUDA(h, cudaMemsetAsync(h->d_err + 1, 0, sizeof(unsigned int), h->stream));
+    launch_error_ratio(m, n, C, ldc, hi, lo, absab, static_cast<double>(k) * std::ldexp(1.0, -target_bits),
+                       reinterpret_cast<unsigned int*>(h->d_err + 1), h->stream);
+    unsigned int bits = 0;
+    OZ2_CUDA(h, cudaMemcpyAsync(&bits, h->d_err + 1, sizeof bits, cudaMemcpyDeviceToHost, h->stream));
+    OZ2_CUDA(h, cudaStreamSynchronize(h->stream));
+    std::memcpy(out, &bits, sizeof bits);
+    return OZ2_OK;
+}
+
+int oz2_kernel_launches(oz2_handle h, int64_t* out) {
+    if (!h || !out) return fail(h, OZ2_EINVAL, "oz2: null argument");
+    *out = h->launches;
+    return OZ2_OK;
 }
 
 int oz2_set_graph_mode(oz2_handle h, int enable) {

@@ -53,9 +53,19 @@ class DgemmProblem(C.Structure):
 
 _lib.oz2_dgemm_grouped.argtypes = [_vp, _i32, C.POINTER(DgemmProblem), _vp, _i32, _vp]
 _lib.oz2_set_graph_mode.argtypes = [_vp, _i32]
+_lib.oz2_kernel_launches.argtypes = [_vp, C.POINTER(_i64)]
 _lib.oz2_set_gemm_config.argtypes = [_vp, _i32, _i32, _i32]
 _lib.oz2_get_gemm_config.argtypes = [_vp, C.POINTER(_i32)]
 _lib.oz2_autotune_grouped.argtypes = [_vp, _i32, C.POINTER(DgemmProblem), C.POINTER(_i32)]
+_lib.oz2_dgemm_adaptive.argtypes = [_vp, _i32, C.POINTER(DgemmProblem), _i32, _i32, C.POINTER(_i64)]
+_lib.oz2_set_adaptive_options.argtypes = [_vp, _i32, C.c_float]
+_lib.oz2_mlp_info.argtypes = [C.POINTER(_i32)]
+_lib.oz2_mlp_set_weights.argtypes = [_vp, _vp, _i32]
+_lib.oz2_mlp_train.argtypes = [_vp, _i32, _vp, _vp, _i32, C.c_float, C.c_uint, _vp, _vp]
+_lib.oz2_mlp_infer.argtypes = [_vp, _vp, _i32, _vp, C.c_float, _vp, _vp]
+_lib.oz2_tile_features.argtypes = [_vp, _i32, C.POINTER(DgemmProblem), _i32, _vp, _vp, C.POINTER(_i64)]
+_lib.oz2_dd_reference.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _vp, _vp]
+_lib.oz2_error_ratio.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _vp, _vp, _i32, C.POINTER(C.c_float)]
 _lib.oz2_last_error.argtypes = [_vp]
 _lib.oz2_last_error.restype = C.c_char_p
 _lib.oz2_status_string.argtypes = [_i32]
@@ -65,6 +75,12 @@ _lib.oz2_status_string.restype = C.c_char_p
 def lib():
     """The loaded ctypes library (for callers that bind further entry points)."""
     return _lib
+
+
+def mlp_info():
+    out = (_i32 * 4)()
+    _raise(_lib.oz2_mlp_info(out))
+    return {"params": out[0], "features": out[1], "classes": out[2], "hidden": out[3]}
 
 
 def _raise(status, handle=None):
@@ -246,6 +262,12 @@ class Ozaki2:
         d = done.cuda_event if hasattr(done, "cuda_event") else done
         _raise(_lib.oz2_dgemm_grouped(self._h, len(problems), arr, ev, nev, d), self._h)
 
+    def kernel_launches(self):
+        """kernels launched through this handle so far (graph replays count their kernel nodes)"""
+        out = _i64()
+        _raise(_lib.oz2_kernel_launches(self._h, C.byref(out)), self._h)
+        return out.value
+
     def set_graph_mode(self, on):
         _raise(_lib.oz2_set_graph_mode(self._h, int(bool(on))), self._h)
 
@@ -261,6 +283,82 @@ class Ozaki2:
         out = (_i32 * 3)()
         _raise(_lib.oz2_autotune_grouped(self._h, len(problems), self._problems(problems), out), self._h)
         return {"bn": out[0], "group_j": out[1], "ctas": out[2]}
+
+    # ---- adaptive number of moduli per tile (no counterpart in the reference)
+    ADAPTIVE_MLP, ADAPTIVE_ANALYTIC_TILE, ADAPTIVE_ANALYTIC_PROBLEM, ADAPTIVE_FIXED = 0, 1, 2, 3
+
+    def gemm_adaptive(self, problems, target_bits=53, mode=0):
+        """problems as for gemm_grouped (num_moduli is used by mode 3 only). Returns the stats
+        dict: tiles, sum_s (reruns included), probed, rerun, rerun_sum_s, analytic_sum_s, mlp,
+        int8_macs (sum of s m_t n_t k over computed tiles)."""
+        arr = self._problems(problems)
+        st = (_i64 * 8)()
+        _raise(_lib.oz2_dgemm_adaptive(self._h, len(problems), arr, target_bits, mode, st), self._h)
+        keys = ["tiles", "sum_s", "probed", "rerun", "rerun_sum_s", "analytic_sum_s", "mlp", "int8_macs"]
+        return dict(zip(keys, list(st)))
+
+    def set_adaptive_options(self, tile=512, threshold=0.9):
+        _raise(_lib.oz2_set_adaptive_options(self._h, tile, threshold), self._h)
+        self._tile = tile
+
+    def set_mlp_weights(self, params):
+        """params: sequence of floats (oz2_mlp_info()[0] of them), or None to unload"""
+        if params is None:
+            _raise(_lib.oz2_mlp_set_weights(self._h, None, 0), self._h)
+            return
+        buf = (C.c_float * len(params))(*params)
+        _raise(_lib.oz2_mlp_set_weights(self._h, buf, len(params)), self._h)
+
+    def load_model(self, path=None):
+        """loads an MLP saved by oz2.adaptive.save_model (default: the model shipped with the package)"""
+        from . import adaptive
+        model = adaptive.load_model(path)
+        self.set_mlp_weights(model["params"])
+        self.set_adaptive_options(model.get("tile", 512), model.get("threshold", 0.9))
+        return model
+
+    def tile_features(self, problems, target_bits=53):
+        """features (torch float32 [tiles, F]) and analytic s (torch int32 [tiles]) on the device"""
+        import torch
+        arr = self._problems(problems)
+        T = getattr(self, "_tile", 512)
+        ntiles = sum(((p[2] + T - 1) // T) * ((p[3] + T - 1) // T) for p in problems)
+        F = mlp_info()["features"]
+        feat = torch.zeros((max(ntiles, 1), F), dtype=torch.float32, device="cuda")
+        sa = torch.zeros(max(ntiles, 1), dtype=torch.int32, device="cuda")
+        n = _i64()
+        _raise(_lib.oz2_tile_features(self._h, len(problems), arr, target_bits, feat.data_ptr(), sa.data_ptr(),
+                                      C.byref(n)), self._h)
+        return feat[: n.value], sa[: n.value]
+
+    def dd_reference(self, m, n, k, A, lda, B, ldb, hi, lo, absab):
+        _raise(_lib.oz2_dd_reference(self._h, m, n, k, _addr(A), lda, _addr(B), ldb, _addr(hi), _addr(lo),
+                                     _addr(absab)), self._h)
+
+    def error_ratio(self, m, n, k, C_, ldc, hi, lo, absab, target_bits=53):
+        out = C.c_float()
+        _raise(_lib.oz2_error_ratio(self._h, m, n, k, _addr(C_), ldc, _addr(hi), _addr(lo), _addr(absab),
+                                    target_bits, C.byref(out)), self._h)
+        return out.value
+
+    def mlp_train(self, features, labels, params, epochs=300, lr=3e-3, seed=1):
+        """trains in place: features torch float32 [N, F] and labels int32 [N] on the device,
+        params a list of floats; returns (params, per-epoch losses)"""
+        p = (C.c_float * len(params))(*params)
+        loss = (C.c_float * epochs)()
+        _raise(_lib.oz2_mlp_train(self._h, features.shape[0], features.data_ptr(), labels.data_ptr(), epochs, lr,
+                                  seed, p, loss), self._h)
+        return list(p), list(loss)
+
+    def mlp_infer(self, params, features, threshold=0.9, probs=False):
+        import torch
+        p = (C.c_float * len(params))(*params)
+        n = features.shape[0]
+        s = torch.zeros(n, dtype=torch.int32, device="cuda")
+        pr = torch.zeros((n, mlp_info()["classes"]), dtype=torch.float32, device="cuda") if probs else None
+        _raise(_lib.oz2_mlp_infer(self._h, p, n, features.data_ptr(), threshold, s.data_ptr(),
+                                  pr.data_ptr() if probs else None), self._h)
+        return (s, pr) if probs else s
 
     # ---- the products (ref :739-786)
     @staticmethod

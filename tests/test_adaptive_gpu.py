@@ -1,0 +1,326 @@
+"""Adaptive number of moduli per C tile: the MLP kernels against a torch fp32 restatement, the
+tile features and analytic s against a numpy restatement of their definition, the probe (it
+catches tiles run at too few moduli and passes tiles that meet the target), and the modes'
+results: fixed s equals the plain product bit for bit, analytic s meets the DGEMM-level target
+k 2^-53 (|A||B|)_ij against the double-double reference."""
+import math
+
+import numpy as np
+import pytest
+
+import adaptive_oracle
+from common import bits, from_dev, make_mat, op_shape, to_dev
+
+pytestmark = pytest.mark.gpu
+
+TILE = 512
+
+
+@pytest.fixture(scope="module")
+def az():
+    """a handle of its own: these tests load MLP weights and change the adaptive options"""
+    import torch
+    import oz2
+    h = oz2.Ozaki2(torch.cuda.current_stream())
+    yield h
+    h.close()
+
+
+def info():
+    import oz2
+    return oz2.mlp_info()
+
+
+def wide_rows(seed, rows, cols, phi, offsets):
+    """(u - 0.5) exp(phi g) with per-row power-of-two offsets in [-offsets, offsets], column-major"""
+    rng = np.random.default_rng(seed)
+    X = (rng.random((rows, cols)) - 0.5) * np.exp(phi * rng.standard_normal((rows, cols)))
+    if offsets:
+        X = X * np.ldexp(1.0, rng.integers(-offsets, offsets + 1, (rows, 1)))
+    return np.asfortranarray(X)
+
+
+def const_class_params(cls):
+    """an MLP whose softmax puts (nearly) all mass on one class: s = cls + 2 at any threshold"""
+    i = info()
+    P = [0.0] * i["params"]
+    P[i["params"] - i["classes"] + cls] = 60.0
+    return P
+
+
+def torch_forward(params, feat):
+    import torch
+    i = info()
+    F, H, Cn = i["features"], i["hidden"], i["classes"]
+    P = torch.tensor(params, dtype=torch.float32, device=feat.device)
+    o = 0
+    W1 = P[o:o + H * F].view(H, F); o += H * F
+    b1 = P[o:o + H]; o += H
+    W2 = P[o:o + H * H].view(H, H); o += H * H
+    b2 = P[o:o + H]; o += H
+    W3 = P[o:o + Cn * H].view(Cn, H); o += Cn * H
+    b3 = P[o:o + Cn]
+    h1 = torch.relu(feat @ W1.T + b1)
+    h2 = torch.relu(h1 @ W2.T + b2)
+    return torch.softmax(h2 @ W3.T + b3, dim=1)
+
+
+def test_mlp_inference_matches_torch_fp32(az):
+    import torch
+    from oz2 import adaptive
+    g = torch.Generator(device="cuda")
+    g.manual_seed(3)
+    feat = torch.rand((1000, info()["features"]), generator=g, device="cuda")
+    params = adaptive.init_params(seed=11)
+    # larger biases so the decision is not always the first class
+    params = [p * 3.0 for p in params]
+    s, probs = az.mlp_infer(params, feat, 0.9, probs=True)
+    want = torch_forward(params, feat)
+    assert torch.allclose(probs, want, atol=2e-5, rtol=1e-4)
+    cum = torch.cumsum(want, dim=1)
+    ref_s = 2 + torch.clamp((cum < 0.9).sum(dim=1), max=info()["classes"] - 1)
+    margin = (cum - 0.9).abs().min(dim=1).values
+    clear = margin > 1e-4
+    assert clear.float().mean() > 0.9
+    assert torch.equal(s[clear].long(), ref_s[clear].long())
+    assert int(s.min()) >= 2 and int(s.max()) <= 24
+
+
+def test_mlp_training_fits_a_learnable_rule(az):
+    import torch
+    from oz2 import adaptive
+    g = torch.Generator(device="cuda")
+    g.manual_seed(5)
+    feat = torch.rand((2048, info()["features"]), generator=g, device="cuda")
+    labels = (2 + torch.floor(feat[:, 2] * 8) + torch.floor(feat[:, 0] * 8)).to(torch.int32)
+    params, losses = az.mlp_train(feat, labels, adaptive.init_params(seed=1), epochs=150, lr=3e-3, seed=2)
+    assert all(math.isfinite(x) for x in losses)
+    assert losses[-1] < 0.5 * losses[0]
+    s = az.mlp_infer(params, feat, 0.5)
+    assert (s - labels).abs().le(1).float().mean().item() > 0.9
+
+
+def test_tile_features_and_analytic_s_match_host_restatement(oracle, az):
+    import torch
+    rng = np.random.default_rng(9)
+    probs, dev = [], []
+    for q, (ta, tb, m, n, k, phi, offs) in enumerate([("N", "N", 700, 600, 300, 1.0, 10),
+                                                      ("T", "N", 513, 1030, 999, 4.0, 40),
+                                                      ("N", "T", 128, 200, 5000, 0.0, 0),
+                                                      ("T", "T", 600, 520, 64, 8.0, 20)]):
+        Ar, Ac = op_shape(ta, m, k)
+        Br, Bc = op_shape(tb, k, n)
+        A = wide_rows(100 + q, Ar, Ac, phi, offs)
+        B = wide_rows(200 + q, Br, Bc, phi, offs)
+        A[rng.random(A.shape) < 0.05] = 0.0  # zeros are counted apart
+        if q == 0:
+            A[3, :] = 0.0  # an all-zero row contributes nothing
+        probs.append((ta, tb, m, n, k, A, B))
+        C = torch.zeros(m * n, dtype=torch.float64, device="cuda")
+        dev.append((ta, tb, m, n, k, 1.0, to_dev(A), Ar, to_dev(B), Br, 0.0, C, m, 16))
+    az.set_adaptive_options(TILE, 0.9)
+    feat, s_an = az.tile_features(dev)
+    want_f, want_s = adaptive_oracle.tile_features(oracle, probs)
+    got_f = feat.cpu().numpy()
+    assert got_f.shape == want_f.shape
+    np.testing.assert_allclose(got_f[:, 0], want_f[:, 0], rtol=1e-6)
+    assert np.array_equal(got_f[:, 1:], want_f[:, 1:])
+    assert np.array_equal(s_an.cpu().numpy(), want_s)
+
+
+def nn_problem(seed, m, n, k, phi, offsets):
+    A = wide_rows(seed, m, k, phi, offsets)
+    B = np.asfortranarray(wide_rows(seed + 1, n, k, phi, offsets).T)
+    return A, B
+
+
+def dd_check(az, m, n, k, dA, dB, dC, target_bits=53):
+    import torch
+    hi = torch.empty(m * n, dtype=torch.float64, device="cuda")
+    lo, ab = torch.empty_like(hi), torch.empty_like(hi)
+    az.dd_reference(m, n, k, dA, m, dB, k, hi, lo, ab)
+    return az.error_ratio(m, n, k, dC, m, hi, lo, ab, target_bits)
+
+
+def test_mode3_equals_plain_products(az):
+    import torch
+    probs, want = [], []
+    for q, (ta, tb, m, n, k, s) in enumerate([("N", "T", 700, 530, 260, 14), ("T", "N", 300, 1100, 777, 18),
+                                              ("T", "T", 1030, 90, 4100, 20)]):
+        Ar, Ac = op_shape(ta, m, k)
+        Br, Bc = op_shape(tb, k, n)
+        A = make_mat(30 + q, Ar, Ac, Ar + 3, "wide", 8)
+        B = make_mat(40 + q, Br, Bc, Br + 1, "wide", 8)
+        C0 = make_mat(50 + q, m, n, m + 5, "u")
+        p = (ta, tb, m, n, k, 1.25, to_dev(A), Ar + 3, to_dev(B), Br + 1, -0.5, to_dev(C0), m + 5, s)
+        probs.append((p, C0))
+        dC = to_dev(C0)
+        az.gemm(*p[:11], dC, m + 5, s)
+        want.append(from_dev(dC, C0))
+    stats = az.gemm_adaptive([p for p, _ in probs], 53, az.ADAPTIVE_FIXED)
+    torch.cuda.synchronize()
+    for (p, C0), w in zip(probs, want):
+        assert np.array_equal(bits(from_dev(p[11], C0)), bits(w))
+    assert stats["tiles"] == sum(math.ceil(p[2] / TILE) * math.ceil(p[3] / TILE) for p, _ in probs)
+    assert stats["sum_s"] == sum(p[13] * math.ceil(p[2] / TILE) * math.ceil(p[3] / TILE) for p, _ in probs)
+
+
+@pytest.mark.parametrize("phi,offsets", [(0.0, 0), (1.0, 40), (4.0, 40), (8.0, 40)])
+def test_analytic_modes_meet_the_target(az, phi, offsets):
+    import torch
+    m, n, k = 1100, 700, 1500
+    A, B = nn_problem(int(phi * 10) + 7, m, n, k, phi, offsets)
+    dA, dB = to_dev(A), to_dev(B)
+    results = {}
+    for mode in (az.ADAPTIVE_ANALYTIC_TILE, az.ADAPTIVE_ANALYTIC_PROBLEM):
+        dC = torch.full((m * n,), 7.0, dtype=torch.float64, device="cuda")
+        st = az.gemm_adaptive([("N", "N", m, n, k, 1.0, dA, m, dB, k, 0.0, dC, m, 16)], 53, mode)
+        ratio = dd_check(az, m, n, k, dA, dB, dC)
+        results[mode] = (st, ratio)
+        # s = 24 is the largest set: wide inputs may need more than it gives
+        if st["sum_s"] < 24 * st["tiles"]:
+            assert ratio <= 1.0, (mode, st, ratio)
+    st1, st2 = results[az.ADAPTIVE_ANALYTIC_TILE][0], results[az.ADAPTIVE_ANALYTIC_PROBLEM][0]
+    assert st1["sum_s"] == st1["analytic_sum_s"]
+    assert st2["sum_s"] >= st1["sum_s"]
+
+
+def test_probe_reruns_tiles_run_at_too_few_moduli(az):
+    """an MLP that always answers s = 2: every tile is probed, fails and is rerun at its analytic
+    s, so the result equals the analytic mode's bit for bit"""
+    import torch
+    m, n, k = 1030, 600, 700
+    A, B = nn_problem(71, m, n, k, 2.0, 20)
+    dA, dB = to_dev(A), to_dev(B)
+    dC1 = torch.zeros(m * n, dtype=torch.float64, device="cuda")
+    az.set_mlp_weights(None)
+    ref = az.gemm_adaptive([("N", "N", m, n, k, 1.5, dA, m, dB, k, 0.0, dC1, m, 16)], 53, az.ADAPTIVE_ANALYTIC_TILE)
+    az.set_mlp_weights(const_class_params(0))
+    try:
+        dC0 = torch.zeros(m * n, dtype=torch.float64, device="cuda")
+        st = az.gemm_adaptive([("N", "N", m, n, k, 1.5, dA, m, dB, k, 0.0, dC0, m, 16)], 53, az.ADAPTIVE_MLP)
+    finally:
+        az.set_mlp_weights(None)
+    assert st["mlp"] == 1
+    assert st["probed"] == st["tiles"] and st["rerun"] == st["tiles"]
+    assert st["rerun_sum_s"] == ref["sum_s"]
+    assert torch.equal(dC0.view(torch.int64), dC1.view(torch.int64))
+
+
+def smallest_s(az, dA, dB, m, n, k):
+    import torch
+    hi = torch.empty(m * n, dtype=torch.float64, device="cuda")
+    lo, ab = torch.empty_like(hi), torch.empty_like(hi)
+    az.dd_reference(m, n, k, dA, m, dB, k, hi, lo, ab)
+    C = torch.empty(m * n, dtype=torch.float64, device="cuda")
+    for s in range(2, 25):
+        try:
+            az.gemm("N", "N", m, n, k, 1.0, dA, m, dB, k, 0.0, C, m, s)
+        except ValueError:
+            continue
+        if az.error_ratio(m, n, k, C, m, hi, lo, ab) <= 1.0:
+            return s
+    return 25
+
+
+def test_probe_passes_tiles_that_meet_the_target(az):
+    """an MLP that answers the smallest sufficient s of the tile: the tile is probed (below its
+    analytic s) and passes, with no rerun"""
+    import torch
+    m, n, k = TILE, TILE, 1024
+    A, B = nn_problem(81, m, n, k, 0.0, 0)
+    dA, dB = to_dev(A), to_dev(B)
+    s_min = smallest_s(az, dA, dB, m, n, k)
+    _, s_an = az.tile_features([("N", "N", m, n, k, 1.0, dA, m, dB, k, 0.0, torch.empty(1, device="cuda"), m, 16)])
+    assert s_min < int(s_an[0]), "the analytic s is an upper bound with slack for uniform inputs"
+    az.set_mlp_weights(const_class_params(s_min - 2))
+    try:
+        dC = torch.zeros(m * n, dtype=torch.float64, device="cuda")
+        st = az.gemm_adaptive([("N", "N", m, n, k, 1.0, dA, m, dB, k, 0.0, dC, m, 16)], 53, az.ADAPTIVE_MLP)
+    finally:
+        az.set_mlp_weights(None)
+    assert st["probed"] == 1 and st["rerun"] == 0 and st["sum_s"] == s_min
+    assert dd_check(az, m, n, k, dA, dB, dC) <= 1.0
+
+
+def test_mode0_without_weights_is_the_tile_analytic_mode(az):
+    import torch
+    m, n, k = 800, 900, 333
+    A, B = nn_problem(91, m, n, k, 3.0, 10)
+    dA, dB = to_dev(A), to_dev(B)
+    az.set_mlp_weights(None)
+    out = []
+    for mode in (az.ADAPTIVE_MLP, az.ADAPTIVE_ANALYTIC_TILE):
+        dC = torch.zeros(m * n, dtype=torch.float64, device="cuda")
+        st = az.gemm_adaptive([("N", "N", m, n, k, 1.0, dA, m, dB, k, 0.0, dC, m, 16)], 53, mode)
+        out.append((st, dC))
+    assert out[0][0]["mlp"] == 0 and out[0][0]["probed"] == 0
+    assert out[0][0]["sum_s"] == out[1][0]["sum_s"]
+    assert torch.equal(out[0][1].view(torch.int64), out[1][1].view(torch.int64))
+
+
+def test_mlp_keeps_analytic_s_when_beta_is_nonzero(az):
+    import torch
+    m, n, k = 600, 600, 500
+    A, B = nn_problem(95, m, n, k, 0.0, 0)
+    dA, dB = to_dev(A), to_dev(B)
+    az.set_mlp_weights(const_class_params(0))
+    try:
+        C0 = torch.ones(m * n, dtype=torch.float64, device="cuda")
+        dC = C0.clone()
+        st = az.gemm_adaptive([("N", "N", m, n, k, 1.0, dA, m, dB, k, 0.5, dC, m, 16)], 53, az.ADAPTIVE_MLP)
+    finally:
+        az.set_mlp_weights(None)
+    assert st["probed"] == 0 and st["sum_s"] == st["analytic_sum_s"]
+    dC1 = C0.clone()
+    az.gemm_adaptive([("N", "N", m, n, k, 1.0, dA, m, dB, k, 0.5, dC1, m, 16)], 53, az.ADAPTIVE_ANALYTIC_TILE)
+    assert torch.equal(dC.view(torch.int64), dC1.view(torch.int64))
+
+
+def test_adaptive_early_returns_and_rejections(az):
+    import torch
+    C0 = torch.full((64 * 64,), 2.0, dtype=torch.float64, device="cuda")
+    A = torch.ones(64 * 64, dtype=torch.float64, device="cuda")
+    dC = C0.clone()
+    az.gemm_adaptive([("N", "N", 64, 64, 64, 0.0, A, 64, A, 64, -0.5, dC, 64, 16),
+                      ("N", "N", 0, 64, 64, 1.0, A, 64, A, 64, 0.0, dC, 64, 16)], 53, az.ADAPTIVE_ANALYTIC_TILE)
+    torch.cuda.synchronize()
+    assert torch.all(dC == -1.0)
+    with pytest.raises(ValueError, match="problem 0"):
+        az.gemm_adaptive([("N", "N", 64, 64, 64, 1.0, A, 0, A, 64, 0.0, dC, 64, 16)], 53, 1)
+    with pytest.raises(ValueError):
+        az.gemm_adaptive([("N", "N", 64, 64, 64, 1.0, A, 64, A, 64, 0.0, dC, 64, 16)], 53, 7)
+    with pytest.raises(ValueError):
+        az.set_adaptive_options(100, 0.9)
+
+
+def test_default_model_loads_and_meets_the_target(az):
+    """the shipped MLP: on fresh problems of the training distribution every output meets the
+    target (probe and rerun included) with fewer moduli than the analytic rule"""
+    import os
+    import torch
+    from oz2 import adaptive
+    if not os.path.exists(adaptive.DEFAULT_MODEL):
+        pytest.fail("the package ships no default MLP model")
+    model = az.load_model()
+    try:
+        rng = np.random.default_rng(2024)
+        total_s = total_an = 0
+        for q in range(6):
+            k = int(np.exp(rng.uniform(np.log(256), np.log(2048))))
+            phi = float(rng.uniform(0, 8))
+            m = n = k
+            A, B = nn_problem(500 + q, m, n, k, phi, 40)
+            dA, dB = to_dev(A), to_dev(B)
+            dC = torch.zeros(m * n, dtype=torch.float64, device="cuda")
+            st = az.gemm_adaptive([("N", "N", m, n, k, 1.0, dA, m, dB, k, 0.0, dC, m, 16)], 53, az.ADAPTIVE_MLP)
+            assert st["mlp"] == 1
+            total_s += st["sum_s"] - st["rerun_sum_s"]
+            total_an += st["analytic_sum_s"]
+            if st["analytic_sum_s"] < 24 * st["tiles"]:
+                assert dd_check(az, m, n, k, dA, dB, dC) <= 1.0, (q, k, phi, st)
+        assert total_s <= total_an
+        assert model["threshold"] > 0
+    finally:
+        az.set_mlp_weights(None)
+        az.set_adaptive_options(TILE, 0.9)
