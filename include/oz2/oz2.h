@@ -93,25 +93,32 @@ int oz2_autotune_grouped(oz2_handle h, int count, const oz2_dgemm_problem* probl
  * within k 2^-target_bits (|A||B|)_ij of the exact product, the classical error bound of a native
  * FP64 GEMM for target_bits = 53 ("DGEMM-level error"). Per tile of tile x tile entries (default
  * 512), s comes from
- *   mode 0: the MLP (oz2_mlp_set_weights), capped by the analytic s, for problems with beta = 0
- *           (others take the analytic s); tiles below their analytic s are probed (C x against
- *           A (B x) in double-double) and rerun at the analytic s when the probe fails; without
- *           weights it behaves as mode 1
+ *   mode 0: the MLP (oz2_mlp_set_weights; a tile takes the largest class over itself and its
+ *           up to 8 neighbours in the problem), capped by the analytic s, for problems with
+ *           beta = 0 (others take the analytic s); tiles below their analytic s are probed (C x
+ *           against A (B x) with x = e_j for 8 columns j, each entry checked) and rerun at the
+ *           analytic s when the probe fails; without weights it behaves as mode 1
  *   mode 1: the analytic s of the tile: smallest s whose tk >= R + 2 + t - floor(log2(k - 1)),
  *           R the largest exponent gap below the row / column maximum in the tile's panels
  *   mode 2: the analytic s of the whole problem (the largest over its tiles)
  *   mode 3: each problem's own num_moduli (tiled like the other modes)
- * stats8 (may be NULL): tiles, sum of s over computed tiles (reruns included), probed tiles, rerun
- * tiles, sum of s of the reruns, sum of analytic s, MLP used, int8 multiply-adds of the computed
- * tiles (s m_t n_t k summed, reruns included). Synchronises the stream. With profiling on,
+ * In modes 0-2 a tile that no s <= 24 brings to the target (analytic s or MLP class 25) runs as a
+ * native FP64 GEMM (cuBLAS DGEMM), the whole problem in one call when all its tiles do.
+ * stats (may be NULL, 10 entries): tiles, sum of s over emulated tiles (reruns included), probed
+ * tiles, rerun tiles, sum of s of the reruns (25 for native), sum of analytic s (25 for native),
+ * MLP used, int8 multiply-adds of the emulated tiles (s m_t n_t k summed, reruns included),
+ * native tiles, native FP64 multiply-adds. Synchronises the stream. With profiling on,
  * oz2_stage_times reports scale (with the tile statistics, features and MLP), split, GEMM and CRT
- * summed over the tile batches; the probe is in none of them. */
+ * summed over the tile batches; the probe and native tiles are in none of them. */
 int oz2_dgemm_adaptive(oz2_handle h, int count, const oz2_dgemm_problem* problems, int target_bits, int mode,
-                       int64_t* stats8);
+                       int64_t* stats);
 /* tile edge (multiple of 128) and the MLP decision threshold: s is the smallest class whose
  * cumulative predicted probability reaches it */
 int oz2_set_adaptive_options(oz2_handle h, int tile, float threshold);
-/* out4 = {parameters, features, classes (s = 2..24), hidden width} of the MLP */
+/* with profiling on: device time of the last oz2_dgemm_adaptive's probe and of its native FP64
+ * tiles (out2 = {probe_ms, native_ms}) */
+int oz2_adaptive_stage_times(oz2_handle h, double* out2);
+/* out4 = {parameters, features, classes (s = 2..24, 25 = native FP64), hidden width} of the MLP */
 int oz2_mlp_info(int* out4);
 /* loads the MLP parameters (host floats); NULL unloads */
 int oz2_mlp_set_weights(oz2_handle h, const float* params, int nparams);

@@ -10,7 +10,7 @@ Definitions (no counterpart in the reference, whose number of moduli is fixed pe
   counted apart.
   analytic s = the smallest s in 2..24 whose bits per element tk (the plan of the reference's
   Ozaki2::gemm for this k) reach R + 2 + t - floor(log2(k - 1)), R the largest gap of the tile's
-  two panels, t the target bits; 24 when none does.
+  two panels, t the target bits; 25 (the tile runs as a native FP64 GEMM) when none does.
 """
 import numpy as np
 
@@ -67,12 +67,12 @@ def tk_table(oracle, k):
 
 def analytic_s(tk, R, k, target_bits=53):
     need = R + 2 + target_bits - floor_log2_km1(k)
-    return next((s for s in range(2, 25) if tk[s] >= need), 24)
+    return next((s for s in range(2, 25) if tk[s] >= need), 25)
 
 
 def tile_features(oracle, problems, target_bits=53, tile=TILE):
     """problems: (ta, tb, m, n, k, A, B) with column-major numpy A, B (stored shapes). Returns the
-    features (float32 [tiles, 16]) and analytic s ([tiles]), column tiles outer, row tiles inner."""
+    features (float32 [tiles, 18]) and analytic s ([tiles]), column tiles outer, row tiles inner."""
     out_f, out_s = [], []
     for (ta, tb, m, n, k, A, B) in problems:
         opA = A[:m, :k] if ta == "N" else A[:k, :m].T
@@ -82,7 +82,7 @@ def tile_features(oracle, problems, target_bits=53, tile=TILE):
             hb, sb = panel_stats(opB[:, J:J + tile].T)
             for I in range(0, m, tile):
                 ha, sa = panel_stats(opA[I:I + tile, :])
-                f = np.zeros(16, dtype=np.float32)
+                f = np.zeros(18, dtype=np.float32)
                 f[0] = np.float32(np.log2(np.float32(k))) / 16
                 f[1] = np.float32(target_bits) / 64
                 for q, qq in enumerate(QUANTILES):
@@ -94,9 +94,11 @@ def tile_features(oracle, problems, target_bits=53, tile=TILE):
                 f[7] = np.float32(ha[64] / float(ha.sum())) if ha.sum() else 0
                 f[13] = np.float32(hb[64] / float(hb.sum())) if hb.sum() else 0
                 f[14], f[15] = sa / 64, sb / 64
+                f[16] = np.float32(min(tile, m - I)) / np.float32(512)
+                f[17] = np.float32(min(tile, n - J)) / np.float32(512)
                 out_f.append(f)
                 out_s.append(analytic_s(tk, max(ra, rb), k, target_bits))
-    return np.array(out_f).reshape(-1, 16), np.array(out_s, dtype=np.int64)
+    return np.array(out_f).reshape(-1, 18), np.array(out_s, dtype=np.int64)
 
 
 def problem_analytic_s(oracle, ta, tb, m, n, k, A, B, target_bits=53, tile=TILE):

@@ -3,13 +3,16 @@
 //   stats    : per panel of 512 rows of op(A) (columns of op(B)), a histogram of exponent gaps
 //              g = e(row max) - e(|x|) over the nonzero elements, and the count of zeros
 //   features : per tile, quantiles of both panels' gaps, zero fractions, the spread of row
-//              (column) maxima, log2 k and the target bits, plus the analytic s: the smallest s
+//              (column) maxima, the tile's rows and columns, log2 k and the target bits, plus the
+//              analytic s: the smallest s
 //              whose bits per element tk reach R + 2 + t - floor(log2(k - 1)), R the largest
 //              gap. Every product term then carries a relative error <= 3 * 2^(R - tk), so
-//              |C - AB| <= k 2^-t |A||B| holds entry by entry (the DGEMM-level target).
-//   probe    : Freivalds-style check of a computed tile: C x against A (B x) in double-double
-//              for sparse random x with four +-1 entries, tolerance sum_j |x_j| k 2^-t (|A||B|)_ij
-//              plus the rounding of C itself, so a tile meeting the target always passes.
+//              |C - AB| <= k 2^-t |A||B| holds entry by entry (the DGEMM-level target); 25 (native
+//              FP64) where even 24 moduli do not reach it.
+//   probe    : Freivalds-style check of a computed tile, C x against A (B x) in double-double
+//              with x = e_j for kProbeCols stratified random columns j: each entry (i, j) of those
+//              columns against its own tolerance k 2^-t (|A||B|)_ij plus the rounding of C, so a
+//              tile meeting the target always passes.
 //   dd_ref / error ratio : double-double products and max_ij |C - AB| / (k 2^-t (|A||B|)_ij),
 //              used to label training tiles (the smallest s that meets the target).
 #include <cstdint>
@@ -138,12 +141,15 @@ __global__ void tile_features_kernel(const FeatureItem* __restrict__ items, int 
     f[13] = tb > 0 ? static_cast<float>(hb[kGapBins] / tb) : 0.0f;
     f[14] = exponent_spread(I.maxbits_a, I.rows_a) / 64.0f;
     f[15] = exponent_spread(I.maxbits_b, I.rows_b) / 64.0f;
+    // edge tiles hold fewer rows / columns: fewer entries, other statistics
+    f[16] = static_cast<float>(I.rows_a) / 512.0f;
+    f[17] = static_cast<float>(I.rows_b) / 512.0f;
     // analytic s: tk >= R + 2 + t - floor(log2(k - 1))
     const int R = max(ra, rb);
     int lg = 0;
     for (int64_t v = I.k - 1; v > 1; v >>= 1) ++lg;
     const int need = R + 2 + I.target_bits - lg;
-    int s = kMaxModuli;
+    int s = kNativeS;  // no moduli set suffices: native FP64
     for (int c = 2; c <= kMaxModuli; ++c)
         if (I.tk[c] >= need) {
             s = c;
@@ -175,8 +181,14 @@ __device__ __forceinline__ dd dd_add_prod(dd acc, double a, double b) {  // acc 
 }
 
 // ---------------------------------------------------------------- probe
-// One block per (tile, probe vector, 256 rows of the tile). Random columns j_c and signs from a
-// hash of (problem seed, tile, probe, c).
+// One block per (tile, 256 rows of the tile). The probe takes kProbeCols columns j_c of the tile
+// (stratified: one random column in each of kProbeCols equal ranges) and checks every entry
+// (i, j_c) of its rows on its own: C_ij against alpha (A B)_ij, so the check is entry by entry,
+// with no cancellation between columns. (A B)_ij is summed in FP64 in blocks of 32 terms (FMA),
+// the block sums added into a second accumulator: its error is at most
+// (gamma_32 + gamma_(k/32 + 1) (1 + gamma_32)) (|A||B|)_ij < (34 + k/32) 2^-52 (|A||B|)_ij, far
+// below the k 2^-53 (|A||B|)_ij tolerance, and that error is added to the tolerance. A is read
+// once per tile.
 __device__ __forceinline__ uint64_t mix64(uint64_t z) {
     z += 0x9E3779B97F4A7C15ull;
     z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
@@ -187,68 +199,81 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
 __global__ void __launch_bounds__(256) probe_kernel(const ProbeItem* __restrict__ items, int count,
                                                     int* __restrict__ fail) {
     const ProbeItem* I = items + find_block_item(items, count, blockIdx.x);
-    const int64_t local = static_cast<int64_t>(blockIdx.x) - I->block0;
-    const int pr = static_cast<int>(local % kProbes);
-    const int64_t rblk = local / kProbes;
+    const int64_t rblk = static_cast<int64_t>(blockIdx.x) - I->block0;
     const int64_t mt = I->mt, nt = I->nt, k = I->k;
+    const int ncol = static_cast<int>(min(static_cast<int64_t>(kProbeCols), nt));
     __shared__ int64_t cols[kProbeCols];
-    __shared__ double sign[kProbeCols];
-    __shared__ double uh[kProbeChunk], ul[kProbeChunk], ub[kProbeChunk];
-    if (threadIdx.x < kProbeCols) {
-        const uint64_t h = mix64(I->seed ^ (static_cast<uint64_t>(pr) << 40) ^ static_cast<uint64_t>(threadIdx.x));
-        cols[threadIdx.x] = static_cast<int64_t>(h % static_cast<uint64_t>(nt));
-        sign[threadIdx.x] = (h >> 63) ? -1.0 : 1.0;
+    __shared__ double bs[kProbeCols][kProbeChunk];
+    if (threadIdx.x < ncol) {
+        const int c = threadIdx.x;
+        if (nt >= kProbeCols) {
+            const int64_t span = nt / kProbeCols;
+            const uint64_t h = mix64(I->seed ^ static_cast<uint64_t>(c));
+            cols[c] = c * span + static_cast<int64_t>(h % static_cast<uint64_t>(span));
+        } else {
+            cols[c] = c;
+        }
     }
     __syncthreads();
     const int64_t i = rblk * 256 + threadIdx.x;
     const bool live = i < mt;
-    dd z{0.0, 0.0};
-    double za = 0.0;
+    double z[kProbeCols], zp[kProbeCols], za[kProbeCols];
+#pragma unroll
+    for (int c = 0; c < kProbeCols; ++c) z[c] = zp[c] = za[c] = 0.0;
     for (int64_t p0 = 0; p0 < k; p0 += kProbeChunk) {
-        const int64_t pn = min(static_cast<int64_t>(kProbeChunk), k - p0);
-        // u = B x and |B| |x| for this chunk of the inner index
-        for (int64_t q = threadIdx.x; q < pn; q += blockDim.x) {
-            const int64_t p = p0 + q;
-            dd u{0.0, 0.0};
-            double a = 0.0;
-            for (int c = 0; c < kProbeCols; ++c) {
-                const int64_t j = cols[c];
-                const double b = I->b_rowc ? I->B[j + p * I->ldb] : I->B[p + j * I->ldb];
-                u = dd_add(u, dd{sign[c] * b, 0.0});
-                a += fabs(b);
-            }
-            uh[q] = u.hi;
-            ul[q] = u.lo;
-            ub[q] = a;
+        const int pn = static_cast<int>(min(static_cast<int64_t>(kProbeChunk), k - p0));
+        for (int e = threadIdx.x; e < ncol * pn; e += blockDim.x) {
+            const int c = e / pn, q = e - c * pn;
+            const int64_t j = cols[c], p = p0 + q;
+            bs[c][q] = I->b_rowc ? I->B[j + p * I->ldb] : I->B[p + j * I->ldb];
+        }
+        for (int e = ncol * pn + threadIdx.x; e < kProbeCols * pn; e += blockDim.x) {
+            const int c = e / pn, q = e - c * pn;
+            bs[c][q] = 0.0;  // columns beyond nt: never checked
         }
         __syncthreads();
         if (live) {
-            for (int64_t q = 0; q < pn; ++q) {
-                const int64_t p = p0 + q;
-                const double av = I->a_rowc ? I->A[i + p * I->lda] : I->A[p + i * I->lda];
-                z = dd_add_prod(z, av, uh[q]);
-                z = dd_add_prod(z, av, ul[q]);
-                za = fma(fabs(av), ub[q], za);
+            for (int q0 = 0; q0 < pn; q0 += 32) {  // kProbeChunk is a multiple of 32
+                const int qn = min(32, pn - q0);
+                for (int q = q0; q < q0 + qn; ++q) {
+                    const int64_t p = p0 + q;
+                    const double av = I->a_rowc ? I->A[i + p * I->lda] : I->A[p + i * I->lda];
+#pragma unroll
+                    for (int c = 0; c < kProbeCols; ++c) {
+                        const double b = bs[c][q];
+                        zp[c] = fma(av, b, zp[c]);
+                        za[c] = fma(fabs(av), fabs(b), za[c]);
+                    }
+                }
+#pragma unroll
+                for (int c = 0; c < kProbeCols; ++c) {
+                    z[c] += zp[c];
+                    zp[c] = 0.0;
+                }
             }
         }
         __syncthreads();
     }
     if (!live) return;
-    dd y{0.0, 0.0};
-    double ya = 0.0;
+    bool bad = false;
+    const double kd = static_cast<double>(k);
+#pragma unroll
     for (int c = 0; c < kProbeCols; ++c) {
-        const double cv = I->C[i + cols[c] * I->ldc];
-        y = dd_add(y, dd{sign[c] * cv, 0.0});
-        ya += fabs(cv);
+        if (c < ncol) {
+            const double cv = I->C[i + cols[c] * I->ldc];
+            // C - alpha z in double-double (alpha z exact as a two-product)
+            const dd az{I->alpha * z[c], fma(I->alpha, z[c], -I->alpha * z[c])};
+            const dd diff = dd_add(dd{cv, 0.0}, dd{-az.hi, -az.lo});
+            const double err = fabs(diff.hi + diff.lo);
+            // target k 2^-t |A||B| (za's own rounding widened by k 2^-50), plus the summation
+            // error of z, plus the rounding of C itself (2^-52 |C|)
+            const double tol = fabs(I->alpha) * za[c] *
+                                   (I->tol_scale * (1.0 + kd * 0x1p-50) + (34.0 + kd / 32.0) * 0x1p-52) +
+                               0x1p-52 * fabs(cv) + 1e-300;
+            bad |= !(err <= tol);
+        }
     }
-    // y - alpha z in double-double
-    const dd az{I->alpha * z.hi, fma(I->alpha, z.hi, -I->alpha * z.hi) + I->alpha * z.lo};
-    const dd diff = dd_add(y, dd{-az.hi, -az.lo});
-    const double err = fabs(diff.hi + diff.lo);
-    // za carries a relative rounding error below k 2^-53: widen by k 2^-50
-    const double tol = fabs(I->alpha) * I->tol_scale * za * (1.0 + static_cast<double>(k) * 0x1p-50) +
-                       0x1p-52 * ya + 1e-300;
-    if (!(err <= tol)) atomicOr(fail + I->tile, 1);
+    if (bad) atomicOr(fail + I->tile, 1);
 }
 
 // ---------------------------------------------------------------- double-double reference
@@ -335,7 +360,7 @@ void launch_tile_features(const FeatureItem* d, int count, float* feat, int* s_a
 
 int64_t probe_item_blocks(ProbeItem& it, int64_t block0) {
     it.block0 = block0;
-    return ((it.mt + 255) / 256) * kProbes;
+    return (it.mt + 255) / 256;
 }
 
 void launch_probe(const ProbeItem* d, int count, int64_t blocks, int* fail, cudaStream_t st) {

@@ -13,13 +13,17 @@
 namespace oz2 {
 
 constexpr int kGapBins = 64;     // exponent gaps 0..63 (63 = "63 or more"), plus a zero counter
-constexpr int kFeatures = 16;
+constexpr int kFeatures = 18;
 constexpr int kHidden = 32;
-constexpr int kClasses = kMaxModuli - 1;  // s = 2..24
+// s = 2..24 run emulated; kNativeS marks a tile that no s <= 24 brings to the target, run as a
+// native FP64 GEMM
+constexpr int kNativeS = kMaxModuli + 1;
+constexpr int kClasses = kNativeS - 1;  // s = 2..25
+// per-call statistics of oz2_dgemm_adaptive
+constexpr int kAdaptiveStats = 10;
 constexpr int kMlpParams = kHidden * kFeatures + kHidden + kHidden * kHidden + kHidden + kClasses * kHidden + kClasses;
-constexpr int kProbes = 2;       // probe vectors per tile
-constexpr int kProbeCols = 4;    // +-1 entries per probe vector
-constexpr int kProbeChunk = 1024;
+constexpr int kProbeCols = 8;    // columns per probed tile, each entry checked on its own
+constexpr int kProbeChunk = 512;  // inner-index chunk of the probe's B columns in shared memory
 
 // histogram of exponent gaps for the rows [0, rows) of one panel (rows of op(A) or columns of
 // op(B)), all k; layout like ScaleItem

@@ -4,6 +4,7 @@
 // Mirrors the reference's class oz2::Ozaki2 (src/ozaki2_gpu.hpp:678-1188) for single calls and
 // adds a grouped call (many independent DGEMMs in one set of launches, optionally replayed
 // from a CUDA graph) with a GEMM-configuration autotuner; the reference has neither.
+#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -27,7 +28,7 @@
 using namespace oz2;
 
 namespace {
-enum Stage { kBegin = 0, kScale = 1, kSplit = 2, kGemm = 3, kCrt = 4 };
+enum Stage { kBegin = 0, kScale = 1, kSplit = 2, kGemm = 3, kCrt = 4, kProbe = 5, kNative = 6 };
 thread_local std::string g_error;  // errors of calls without a usable handle
 constexpr int kRing = 4;
 
@@ -117,7 +118,8 @@ struct oz2_context {
     int adaptive_tile = 512;
     uint8_t* ws2 = nullptr;
     size_t ws2_size = 0;
-    int64_t astats[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int64_t astats[kAdaptiveStats] = {};
+    cublasHandle_t cublas = nullptr;  // native FP64 GEMM of tiles no moduli set brings to the target
     int64_t launches = 0;  // kernels launched through this handle (graph replays included)
     bool capture_ok = true;           // false when part of the call ran outside the graphs
     std::string err;
@@ -489,9 +491,11 @@ int put_blob(oz2_context* h, const void* data, size_t bytes, unsigned char* dev)
     if (h->ring_used[slot]) OZ2_CUDA(h, cudaEventSynchronize(h->ring_ev[slot]));
     if (!h->ring_ev[slot]) OZ2_CUDA(h, cudaEventCreateWithFlags(&h->ring_ev[slot], cudaEventDisableTiming));
     if (h->ring_cap[slot] < bytes) {
+        // pinned allocations are slow and synchronise: grow in powers of two from 1 MiB
         if (h->ring_host[slot]) cudaFreeHost(h->ring_host[slot]);
         h->ring_host[slot] = nullptr;
-        const size_t cap = std::max(bytes, h->ring_cap[slot] * 2);
+        size_t cap = std::max(h->ring_cap[slot] * 2, size_t{1} << 20);
+        while (cap < bytes) cap *= 2;
         OZ2_CUDA(h, cudaHostAlloc(&h->ring_host[slot], cap, cudaHostAllocDefault));
         h->ring_cap[slot] = cap;
     }
@@ -593,7 +597,10 @@ size_t desc_bytes_single(int64_t pm, int64_t pn) {
 // Largest column tile that fits for each row-tile candidate, scored by an analytic time model
 // of this implementation (tensor work on padded tiles, HBM traffic of split and CRT, launches).
 int choose_layout(oz2_context* h, int64_t m, int64_t n, int64_t k, int s, int G, Layout& out) {
-    const size_t limit = budget(h);
+    // a problem whose untiled layout fits the current workspace needs no free-memory query
+    const size_t untiled = sizes_for(m, n, k, s, G, m, n).total() + align256(desc_bytes_single(1, 1));
+    const size_t limit =
+        untiled <= h->ws_size && (!h->ws_limit || untiled <= h->ws_limit) ? untiled : budget(h);
     double best = std::numeric_limits<double>::infinity();
     const bool pow2 = h->tuning[2] != 0;
     const auto nbs = tile_candidates(n, kGemmJ, pow2);
@@ -809,6 +816,13 @@ int ensure_ws2(oz2_context* h, size_t bytes) {
     if (h->ws2) cudaFree(h->ws2);
     h->ws2 = nullptr;
     h->ws2_size = 0;
+    // tile batches vary from call to call: a quarter of headroom saves most regrowths
+    const size_t grown = bytes + bytes / 4;
+    if (cudaMalloc(&h->ws2, grown) == cudaSuccess) {
+        h->ws2_size = grown;
+        return OZ2_OK;
+    }
+    cudaGetLastError();
     if (cudaMalloc(&h->ws2, bytes) != cudaSuccess) {
         cudaGetLastError();
         return fail(h, OZ2_ENOMEM, "oz2: workspace allocation failed");
@@ -817,13 +831,34 @@ int ensure_ws2(oz2_context* h, size_t bytes) {
     return OZ2_OK;
 }
 
+// C[i0:i0+mb, j0:j0+nb] = alpha op(A) op(B) + beta C in native FP64 (cuBLAS DGEMM, default math:
+// no emulation), for tiles whose inputs span more exponent range than 24 moduli cover
+int native_gemm(oz2_context* h, const Prob& p, int64_t i0, int64_t j0, int64_t mb, int64_t nb) {
+    if (!h->cublas) {
+        if (cublasCreate(&h->cublas) != CUBLAS_STATUS_SUCCESS) {
+            h->cublas = nullptr;
+            return fail(h, OZ2_ECUDA, "oz2: cublasCreate failed");
+        }
+        cublasSetMathMode(h->cublas, CUBLAS_DEFAULT_MATH);
+    }
+    if (cublasSetStream(h->cublas, h->stream) != CUBLAS_STATUS_SUCCESS)
+        return fail(h, OZ2_ECUDA, "oz2: cublasSetStream failed");
+    const double* A = p.A + (is_n(p.ta) ? i0 : i0 * p.lda);
+    const double* B = p.B + (is_n(p.tb) ? j0 * p.ldb : j0);
+    double* C = p.C + i0 + j0 * p.ldc;
+    const double al = p.alpha[0], be = p.beta[0];
+    const cublasStatus_t cs = cublasDgemm_64(h->cublas, is_n(p.ta) ? CUBLAS_OP_N : CUBLAS_OP_T,
+                                             is_n(p.tb) ? CUBLAS_OP_N : CUBLAS_OP_T, mb, nb, p.k, &al, A, p.lda, B,
+                                             p.ldb, &be, C, p.ldc);
+    if (cs != CUBLAS_STATUS_SUCCESS) return fail(h, OZ2_ECUDA, "oz2: native FP64 GEMM failed");
+    ++h->launches;
+    return OZ2_OK;
+}
+
 // tk[s] for one k (0 where s is too small)
 void tk_table(oz2_context* h, int64_t k, int* tk) {
-    for (int s = 0; s <= kMaxModuli; ++s) tk[s] = 0;
-    for (int s = 2; s <= kMaxModuli; ++s) {
-        const Plan* p;
-        if (get_plan(h, s, k, &p) == OZ2_OK) tk[s] = p->tk;
-    }
+    (void)h;
+    for (int s = 0; s <= kMaxModuli; ++s) tk[s] = s >= 2 ? plan_tk(s, k) : 0;
 }
 
 struct TileRef {
@@ -837,7 +872,7 @@ struct TileRef {
 int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>& fixed_s, int target_bits,
                  int mode, float* feat_out = nullptr, int* sa_out = nullptr, int64_t* ntiles_out = nullptr) {
     const int64_t T = h->adaptive_tile;
-    for (int q = 0; q < 8; ++q) h->astats[q] = 0;
+    for (int q = 0; q < kAdaptiveStats; ++q) h->astats[q] = 0;
     // ---- phase 1: maxima, panel statistics, tile features, analytic s, MLP
     std::vector<TileRef> tiles;
     std::vector<int64_t> pa0(base.size()), pb0(base.size());
@@ -985,6 +1020,28 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
     }
 
     // ---- per-tile s
+    if (use_mlp) {
+        // the MLP's s of a tile is the largest over the tile and its neighbours in the same
+        // problem: one tile's statistics are noisy, its neighbours' see most of the same rows
+        // and columns
+        std::vector<int> pooled(ntiles);
+        int64_t t0 = 0;
+        for (size_t q = 0; q < base.size(); ++q) {
+            const int64_t na = ceil_div(base[q].m, T), nbp = ceil_div(base[q].n, T);
+            for (int64_t J = 0; J < nbp; ++J)
+                for (int64_t I = 0; I < na; ++I) {
+                    int v = 0;
+                    for (int64_t dJ = -1; dJ <= 1; ++dJ)
+                        for (int64_t dI = -1; dI <= 1; ++dI) {
+                            const int64_t I2 = I + dI, J2 = J + dJ;
+                            if (I2 >= 0 && I2 < na && J2 >= 0 && J2 < nbp) v = std::max(v, s_ml[t0 + J2 * na + I2]);
+                        }
+                    pooled[t0 + J * na + I] = v;
+                }
+            t0 += na * nbp;
+        }
+        s_ml.swap(pooled);
+    }
     std::vector<int> s_tile(ntiles);
     std::vector<int> prob_max(base.size(), 2);
     for (int64_t t = 0; t < ntiles; ++t) prob_max[tiles[t].prob] = std::max(prob_max[tiles[t].prob], s_an[t]);
@@ -999,6 +1056,10 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
             case 2: sv = prob_max[q]; break;
             default: sv = fixed_s[q]; break;
         }
+        if (sv >= kNativeS) {
+            s_tile[t] = kNativeS;
+            continue;
+        }
         // never below the smallest s that k admits
         const std::vector<int>& tk = tk_cache[base[q].k];
         while (sv < kMaxModuli && tk[sv] == 0) ++sv;
@@ -1006,7 +1067,43 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
     }
 
     // ---- phase 2: tiles with their s, panels split once per (panel, s); batches by budget
-    auto run_tiles = [&](const std::vector<int64_t>& which, const std::vector<int>& svals) -> int {
+    std::vector<int64_t> prob_tiles(base.size(), 0), native_count(base.size(), 0);
+    for (const TileRef& r : tiles) ++prob_tiles[r.prob];
+    auto run_tiles = [&](const std::vector<int64_t>& which_all, const std::vector<int>& svals_all) -> int {
+        // tiles that no moduli set brings to the target: native FP64 GEMM, one call per problem
+        // when all its tiles go this way
+        std::vector<int64_t> which, native;
+        std::vector<int> svals;
+        for (size_t i = 0; i < which_all.size(); ++i) {
+            if (svals_all[i] >= kNativeS) {
+                native.push_back(which_all[i]);
+            } else {
+                which.push_back(which_all[i]);
+                svals.push_back(svals_all[i]);
+            }
+        }
+        if (!native.empty()) {
+            mark(h, kBegin);
+            std::fill(native_count.begin(), native_count.end(), 0);
+            for (int64_t t : native) ++native_count[tiles[t].prob];
+            std::vector<bool> whole_done(base.size(), false);
+            for (int64_t t : native) {
+                const TileRef& r = tiles[t];
+                const Prob& p = base[r.prob];
+                h->astats[8] += 1;
+                h->astats[9] += r.mb * r.nb * p.k;
+                int st2;
+                if (native_count[r.prob] == prob_tiles[r.prob]) {
+                    if (whole_done[r.prob]) continue;
+                    whole_done[r.prob] = true;
+                    st2 = native_gemm(h, p, 0, 0, p.m, p.n);
+                } else {
+                    st2 = native_gemm(h, p, r.i0, r.j0, r.mb, r.nb);
+                }
+                if (st2) return st2;
+            }
+            mark(h, kNative);
+        }
         std::vector<std::unique_ptr<Prob>> probs;  // one per (problem, s)
         std::map<std::pair<int, int>, Prob*> prob_for;
         auto get_prob = [&](int q, int sv) -> Prob* {
@@ -1142,8 +1239,10 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
         if (!pi.empty()) {
             unsigned char* pd = ws + odesc;  // phase-1 descriptors are consumed by now (stream order)
             if ((st = put_blob(h, pi.data(), pi.size() * sizeof(ProbeItem), pd))) return st;
+            mark(h, kBegin);
             launch_probe(reinterpret_cast<const ProbeItem*>(pd), static_cast<int>(pi.size()), blocks, d_fail, h->stream);
             ++h->launches;
+            mark(h, kProbe);
             std::vector<int> failed(ntiles);
             OZ2_CUDA(h, cudaMemcpyAsync(failed.data(), d_fail, ntiles * 4, cudaMemcpyDeviceToHost, h->stream));
             OZ2_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -1257,6 +1356,7 @@ int oz2_destroy(oz2_handle h) {
     if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
     if (h->d_mlp) cudaFree(h->d_mlp);
     if (h->ws2) cudaFree(h->ws2);
+    if (h->cublas) cublasDestroy(h->cublas);
     delete h;
     return OZ2_OK;
 }
@@ -1274,7 +1374,7 @@ int oz2_dgemm(oz2_handle h, char ta, char tb, int64_t m, int64_t n, int64_t k, d
               void* const* deps, int ndeps, void* done) {
     if (!h) return fail(nullptr, OZ2_EINVAL, "oz2: null handle");
     h->marks.clear();
-    if (h->plans.size() > 1024) h->plans.clear();  // between calls only: plans are borrowed during one
+    if (h->plans.size() > 8192) h->plans.clear();  // between calls only: plans are borrowed during one
     int st = check_args(h, ta, tb, m, n, k, lda, ldb, ldc);
     if (st) return st;
     if ((st = begin_call(h, deps, ndeps))) return st;
@@ -1299,7 +1399,7 @@ int oz2_zgemm(oz2_handle h, char ta, char tb, int64_t m, int64_t n, int64_t k, c
     if (!h) return fail(nullptr, OZ2_EINVAL, "oz2: null handle");
     if (!alpha || !beta) return fail(h, OZ2_EINVAL, "oz2: null alpha or beta");
     h->marks.clear();
-    if (h->plans.size() > 1024) h->plans.clear();
+    if (h->plans.size() > 8192) h->plans.clear();
     int st = check_args(h, ta, tb, m, n, k, lda, ldb, ldc);
     if (st) return st;
     if ((st = begin_call(h, deps, ndeps))) return st;
@@ -1322,7 +1422,7 @@ int oz2_dgemm_grouped(oz2_handle h, int count, const oz2_dgemm_problem* problems
     if (!h) return fail(nullptr, OZ2_EINVAL, "oz2: null handle");
     if (count < 0 || (count > 0 && !problems)) return fail(h, OZ2_EINVAL, "oz2: bad problem list");
     h->marks.clear();
-    if (h->plans.size() > 1024) h->plans.clear();
+    if (h->plans.size() > 8192) h->plans.clear();
     std::vector<Prob> probs;
     int st = validate_grouped(h, count, problems, probs);
     if (st) return st;
@@ -1373,13 +1473,13 @@ int oz2_dgemm_grouped(oz2_handle h, int count, const oz2_dgemm_problem* problems
 
 
 int oz2_dgemm_adaptive(oz2_handle h, int count, const oz2_dgemm_problem* problems, int target_bits, int mode,
-                       int64_t* stats8) {
+                       int64_t* stats) {
     if (!h) return fail(nullptr, OZ2_EINVAL, "oz2: null handle");
     if (count < 0 || (count > 0 && !problems)) return fail(h, OZ2_EINVAL, "oz2: bad problem list");
     if (target_bits < 1 || target_bits > 120) return fail(h, OZ2_EINVAL, "oz2: target_bits must be in [1, 120]");
     if (mode < 0 || mode > 3) return fail(h, OZ2_EINVAL, "oz2: mode must be 0..3");
     h->marks.clear();
-    if (h->plans.size() > 1024) h->plans.clear();
+    if (h->plans.size() > 8192) h->plans.clear();
     std::vector<Prob> probs;
     std::vector<int> fixed_s;
     int st = validate_adaptive(h, count, problems, probs, fixed_s, mode == 3);
@@ -1393,10 +1493,10 @@ int oz2_dgemm_adaptive(oz2_handle h, int count, const oz2_dgemm_problem* problem
             ++h->launches;
         }
     }
-    for (int q = 0; q < 8; ++q) h->astats[q] = 0;
+    for (int q = 0; q < kAdaptiveStats; ++q) h->astats[q] = 0;
     if (!probs.empty() && (st = run_adaptive(h, probs, fixed_s, target_bits, mode))) return st;
-    if (stats8)
-        for (int q = 0; q < 8; ++q) stats8[q] = h->astats[q];
+    if (stats)
+        for (int q = 0; q < kAdaptiveStats; ++q) stats[q] = h->astats[q];
     return end_call(h, nullptr);
 }
 
@@ -1667,6 +1767,21 @@ int oz2_stage_times(oz2_handle h, double* out4) {
         OZ2_CUDA(h, cudaEventElapsedTime(&ms, h->marks[i - 1].second, h->marks[i].second));
         const int stg = h->marks[i].first;
         if (stg >= kScale && stg <= kCrt) out4[stg - 1] += ms;
+    }
+    return OZ2_OK;
+}
+
+int oz2_adaptive_stage_times(oz2_handle h, double* out2) {
+    if (!h || !out2) return fail(h, OZ2_EINVAL, "oz2: null argument");
+    out2[0] = out2[1] = 0.0;
+    if (!h->profiling || h->marks.empty()) return OZ2_OK;
+    OZ2_CUDA(h, cudaEventSynchronize(h->marks.back().second));
+    for (size_t i = 1; i < h->marks.size(); ++i) {
+        const int stg = h->marks[i].first;
+        if (stg != kProbe && stg != kNative) continue;
+        float ms = 0.0f;
+        OZ2_CUDA(h, cudaEventElapsedTime(&ms, h->marks[i - 1].second, h->marks[i].second));
+        out2[stg - kProbe] += ms;
     }
     return OZ2_OK;
 }

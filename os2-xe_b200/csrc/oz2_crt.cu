@@ -198,13 +198,23 @@ void crt_dispatch(int s, const CrtParams& P, int64_t blocks, bool cplx, cudaStre
     }
 }
 
+// the parameter block is copied with every launch: size classes keep small blobs cheap
+template <int N>
 struct alignas(16) BlobParam {
-    unsigned char data[kParamBlobBytes];
+    unsigned char data[N];
     uint32_t bytes;
 };
-__global__ void write_blob_kernel(const __grid_constant__ BlobParam b, unsigned char* dst) {
+template <int N>
+__global__ void write_blob_kernel(const __grid_constant__ BlobParam<N> b, unsigned char* dst) {
     for (uint32_t i = threadIdx.x * 16; i < b.bytes; i += blockDim.x * 16)
         *reinterpret_cast<uint4*>(dst + i) = *reinterpret_cast<const uint4*>(b.data + i);
+}
+template <int N>
+void write_blob_n(const unsigned char* src, size_t n, unsigned char* dst, cudaStream_t st) {
+    static thread_local BlobParam<N> bp;
+    std::memcpy(bp.data, src, n);
+    bp.bytes = static_cast<uint32_t>((n + 15) & ~size_t{15});
+    write_blob_kernel<N><<<1, 256, 0, st>>>(bp, dst);
 }
 
 __global__ void scale_c_kernel(double* C, int64_t ldc, int64_t m, int64_t n, double br, double bi, int cplx) {
@@ -252,13 +262,14 @@ void launch_crt(const CrtItem* d_items, int count, int64_t blocks, const Plan& p
 }
 
 void launch_write_blob(const void* src, size_t bytes, void* dst, cudaStream_t st) {
-    static thread_local BlobParam bp;
     const unsigned char* p = static_cast<const unsigned char*>(src);
     for (size_t off = 0; off < bytes; off += kParamBlobBytes) {
         const size_t n = std::min(kParamBlobBytes, bytes - off);
-        std::memcpy(bp.data, p + off, n);
-        bp.bytes = static_cast<uint32_t>((n + 15) & ~size_t{15});
-        write_blob_kernel<<<1, 256, 0, st>>>(bp, static_cast<unsigned char*>(dst) + off);
+        unsigned char* d = static_cast<unsigned char*>(dst) + off;
+        if (n <= 1024) write_blob_n<1024>(p + off, n, d, st);
+        else if (n <= 4096) write_blob_n<4096>(p + off, n, d, st);
+        else if (n <= 12288) write_blob_n<12288>(p + off, n, d, st);
+        else write_blob_n<kParamBlobBytes>(p + off, n, d, st);
     }
 }
 

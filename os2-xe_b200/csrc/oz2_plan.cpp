@@ -93,41 +93,73 @@ uint32_t pow2_mod(int e, uint32_t m) {
 
 }  // namespace
 
-int make_plan(int s, int64_t k, Plan& p) {
-    if (s < 2 || s > kMaxModuli || k < 1) return 1;
-    p = Plan{};
-    p.s = s;
-    const uint16_t* seq = s <= 6 ? kSeqSmall : (s <= 13 ? kSeqMid : kSeqLarge);
-    Big M = Big::of(1);
-    for (int t = 0; t < s; ++t) {
-        p.m[t] = seq[t];
-        if (!M.mul(seq[t])) return 5;
+namespace {
+// everything of a plan but tk depends on s alone: built once per s
+struct Templates {
+    Plan plan[kMaxModuli + 1];
+    int status[kMaxModuli + 1];
+    Templates() {
+        for (int s = 2; s <= kMaxModuli; ++s) status[s] = build(s, plan[s]);
     }
-    p.log2M = M.log2();
-    p.nl = static_cast<int>(std::floor(p.log2M / 32.0)) + 1;
-    if (p.nl < 2) p.nl = 2;
-    if (p.nl != limbs_for(s)) return 3;
+    static int build(int s, Plan& p) {
+        p = Plan{};
+        p.s = s;
+        const uint16_t* seq = s <= 6 ? kSeqSmall : (s <= 13 ? kSeqMid : kSeqLarge);
+        Big M = Big::of(1);
+        for (int t = 0; t < s; ++t) {
+            p.m[t] = seq[t];
+            if (!M.mul(seq[t])) return 5;
+        }
+        p.log2M = M.log2();
+        p.nl = static_cast<int>(std::floor(p.log2M / 32.0)) + 1;
+        if (p.nl < 2) p.nl = 2;
+        if (p.nl != limbs_for(s)) return 3;
+        for (int t = 0; t < s; ++t) {
+            Big Mt = M;
+            if (Mt.divmod(p.m[t]) != 0) return 3;
+            const int64_t y = inverse_mod(Mt.mod(p.m[t]), p.m[t]);
+            if (y < 0) return 3;
+            if (!Mt.mul(static_cast<uint32_t>(y))) return 5;
+            std::memcpy(p.W[t], Mt.w, sizeof Mt.w);
+            p.y[t] = static_cast<uint32_t>(y);
+        }
+        std::memcpy(p.M, M.w, sizeof M.w);
+        mod_constants(p, p.mc);
+        return 0;
+    }
+};
+const Templates& templates() {
+    static const Templates t;  // thread-safe initialisation
+    return t;
+}
+}  // namespace
+
+int plan_tk(int s, int64_t k) {
+    if (s < 2 || s > kMaxModuli || k < 1) return 0;
+    const Templates& T = templates();
+    if (T.status[s]) return 0;
+    const Plan& p = T.plan[s];
+    Big M;
+    std::memcpy(M.w, p.M, sizeof M.w);
     // largest tk <= 100 with k 2^(2 tk + 2) <= M, so that |x| <= M/4 for every result entry
     int tk = static_cast<int>(std::floor((p.log2M - 2.0 - std::log2(static_cast<double>(k))) / 2.0));
     if (tk > kMaxScaleBits) tk = kMaxScaleBits;
     for (;; --tk) {
-        if (tk < 1) return 1;
+        if (tk < 1) return 0;
         Big lhs = Big::of(static_cast<uint64_t>(k));
         if (!lhs.shl(2 * tk + 2)) continue;
-        if (lhs.cmp(M) <= 0) break;
+        if (lhs.cmp(M) <= 0) return tk;
     }
+}
+
+int make_plan(int s, int64_t k, Plan& p) {
+    if (s < 2 || s > kMaxModuli || k < 1) return 1;
+    const Templates& T = templates();
+    if (T.status[s]) return T.status[s];
+    const int tk = plan_tk(s, k);
+    if (tk < 1) return 1;
+    p = T.plan[s];
     p.tk = tk;
-    for (int t = 0; t < s; ++t) {
-        Big Mt = M;
-        if (Mt.divmod(p.m[t]) != 0) return 3;
-        const int64_t y = inverse_mod(Mt.mod(p.m[t]), p.m[t]);
-        if (y < 0) return 3;
-        if (!Mt.mul(static_cast<uint32_t>(y))) return 5;
-        std::memcpy(p.W[t], Mt.w, sizeof Mt.w);
-        p.y[t] = static_cast<uint32_t>(y);
-    }
-    std::memcpy(p.M, M.w, sizeof M.w);
-    mod_constants(p, p.mc);
     return 0;
 }
 

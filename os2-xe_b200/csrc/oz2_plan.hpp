@@ -52,6 +52,8 @@ struct Plan {
 // Returns 0, or 1 (invalid: s out of [2, 24], k < 1, s too small for k), or 5 (overflow).
 // ref src/ozaki2_gpu.hpp:159-200
 int make_plan(int s, int64_t k, Plan& p);
+// tk of make_plan(s, k), or 0 where that plan is invalid (s too small for k)
+int plan_tk(int s, int64_t k);
 const char* plan_error_text(int s, int64_t k, int status, char* buf, int len);
 
 void mod_constants(const Plan& p, ModConst* out);

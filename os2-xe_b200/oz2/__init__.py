@@ -18,6 +18,7 @@ LIB_PATH = os.path.join(HERE, "liboz2.so")
 
 OK, EINVAL, ENOMEM, EINTERNAL, ETIMEOUT, EOVERFLOW, ECUDA = range(7)
 K_MAX_MODULI = 24
+NATIVE_S = 25  # adaptive s of a tile run as a native FP64 GEMM
 
 if not os.path.exists(LIB_PATH):
     raise ImportError(f"{LIB_PATH} is not built: run python os2-xe_b200/build.py")
@@ -59,6 +60,7 @@ _lib.oz2_get_gemm_config.argtypes = [_vp, C.POINTER(_i32)]
 _lib.oz2_autotune_grouped.argtypes = [_vp, _i32, C.POINTER(DgemmProblem), C.POINTER(_i32)]
 _lib.oz2_dgemm_adaptive.argtypes = [_vp, _i32, C.POINTER(DgemmProblem), _i32, _i32, C.POINTER(_i64)]
 _lib.oz2_set_adaptive_options.argtypes = [_vp, _i32, C.c_float]
+_lib.oz2_adaptive_stage_times.argtypes = [_vp, C.POINTER(_dbl)]
 _lib.oz2_mlp_info.argtypes = [C.POINTER(_i32)]
 _lib.oz2_mlp_set_weights.argtypes = [_vp, _vp, _i32]
 _lib.oz2_mlp_train.argtypes = [_vp, _i32, _vp, _vp, _i32, C.c_float, C.c_uint, _vp, _vp]
@@ -289,13 +291,21 @@ class Ozaki2:
 
     def gemm_adaptive(self, problems, target_bits=53, mode=0):
         """problems as for gemm_grouped (num_moduli is used by mode 3 only). Returns the stats
-        dict: tiles, sum_s (reruns included), probed, rerun, rerun_sum_s, analytic_sum_s, mlp,
-        int8_macs (sum of s m_t n_t k over computed tiles)."""
+        dict: tiles, sum_s (emulated tiles, reruns included), probed, rerun, rerun_sum_s,
+        analytic_sum_s (25 counts a native tile), mlp, int8_macs (sum of s m_t n_t k over emulated
+        tiles), native_tiles, native_macs (tiles run as native FP64 GEMMs)."""
         arr = self._problems(problems)
-        st = (_i64 * 8)()
+        st = (_i64 * 10)()
         _raise(_lib.oz2_dgemm_adaptive(self._h, len(problems), arr, target_bits, mode, st), self._h)
-        keys = ["tiles", "sum_s", "probed", "rerun", "rerun_sum_s", "analytic_sum_s", "mlp", "int8_macs"]
+        keys = ["tiles", "sum_s", "probed", "rerun", "rerun_sum_s", "analytic_sum_s", "mlp", "int8_macs",
+                "native_tiles", "native_macs"]
         return dict(zip(keys, list(st)))
+
+    def adaptive_stage_times(self):
+        """with profiling on: {probe_ms, native_ms} of the last gemm_adaptive"""
+        out = (_dbl * 2)()
+        _raise(_lib.oz2_adaptive_stage_times(self._h, out), self._h)
+        return {"probe_ms": out[0], "native_ms": out[1]}
 
     def set_adaptive_options(self, tile=512, threshold=0.9):
         _raise(_lib.oz2_set_adaptive_options(self._h, tile, threshold), self._h)

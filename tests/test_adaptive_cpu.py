@@ -34,8 +34,8 @@ def test_analytic_s_rule(oracle):
     # R = 0: need tk >= 2 + 53 - 9 = 46
     s0 = ao.analytic_s(tk, 0, k)
     assert tk[s0] >= 46 and tk[s0 - 1] < 46
-    # beyond what 24 moduli give: the largest set
-    assert ao.analytic_s(tk, 63, k) == 24
+    # beyond what 24 moduli give: native FP64
+    assert ao.analytic_s(tk, 63, k) == 25
     assert ao.floor_log2_km1(1) == 0 and ao.floor_log2_km1(2) == 0 and ao.floor_log2_km1(1025) == 10
 
 
@@ -44,7 +44,9 @@ def test_tile_order_and_edges(oracle):
     A = np.asfortranarray(rng.standard_normal((700, 40)))
     B = np.asfortranarray(rng.standard_normal((40, 600)))
     f, s = ao.tile_features(oracle, [("N", "N", 700, 600, 40, A, B)])
-    assert f.shape == (4, 16) and s.shape == (4,)
+    assert f.shape == (4, 18) and s.shape == (4,)
+    # rows / columns of each tile over 512: tiles (0,0) (1,0) (0,1) (1,1)
+    assert np.allclose(f[:, 16], [1.0, 188 / 512, 1.0, 188 / 512]) and np.allclose(f[:, 17], [1, 1, 88 / 512, 88 / 512])
     assert np.all(f[:, 0] == np.float32(np.log2(np.float32(40))) / 16)
 
 
@@ -54,7 +56,7 @@ def test_shipped_model_file():
     path = os.path.join(ROOT, "os2-xe_b200", "oz2", "adaptive_mlp.json")
     with open(path) as fh:
         model = json.load(fh)
-    # parameter count of the 16 -> 32 -> 32 -> 23 MLP
-    assert len(model["params"]) == 32 * 16 + 32 + 32 * 32 + 32 + 23 * 32 + 23
+    # parameter count of the 18 -> 32 -> 32 -> 24 MLP (classes s = 2..24 and native FP64)
+    assert len(model["params"]) == 32 * 18 + 32 + 32 * 32 + 32 + 24 * 32 + 24
     assert all(np.isfinite(model["params"]))
     assert 0 < model["threshold"] <= 1 and model["tile"] % 128 == 0
