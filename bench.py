@@ -340,7 +340,19 @@ def dgemm_leg(a, oz2, torch, dev, stream, rank):
     tiling = oz.last_tiling()
     peak, note = int8_peak()
     achieved = 2.0 * a.s * m * n * k / (st_sum[2] * 1e-3) / 1e12
+    # accuracy of the product on a 1024 x 1024 block (full k) against a double-double product
+    blk = min(1024, n)
+    C2 = torch.empty(m * n, dtype=torch.float64, device=dev)
+    oz.gemm("N", "N", m, n, k, 1.0, A, m, B, k, 0.0, C2, m, a.s)
+    hi = torch.empty(blk * blk, dtype=torch.float64, device=dev)
+    lo, ab = torch.empty_like(hi), torch.empty_like(hi)
+    oz.dd_reference(blk, blk, k, A, m, B, k, hi, lo, ab)
+    ulp, cr = oz.accuracy(blk, blk, C2, m, hi, lo)
+    ratio = oz.error_ratio(blk, blk, k, C2, m, hi, lo, ab, TARGET_BITS)
+    del C2, hi, lo, ab
     out = {"workload": f"dgemm {n}x{n}x{n} op=NN s={a.s} alpha=1.5 beta=-0.5 ldc=m+16 U[-1,1)",
+           "accuracy": {"block": f"C[0:{blk}, 0:{blk}] of A B (alpha 1, beta 0) against double-double",
+                        "ulp_max": ulp, "cr_frac": cr / (blk * blk), "dgemm_level_ratio": ratio},
            "tflops": flops / (ms * 1e-3) / 1e12, "ms": ms, "steps": steps,
            "stage_ms": {"scale": st_sum[0], "split": st_sum[1], "gemm": st_sum[2], "crt": st_sum[3]},
            "gpu_launches_per_call": launches_per_call(tiling),
@@ -419,16 +431,18 @@ def problem_analytic_s(oz, batch):
 
 def verify(oz, torch, batch, run, refs):
     """runs `run` over the batch and measures every output against its double-double product:
-    (problems over the bound, largest ratio)"""
+    (problems over the bound, largest ratio, largest ulp error, correctly rounded entries)"""
     run()
     torch.cuda.synchronize()
-    bad, worst = 0, 0.0
+    bad, worst, ulp, cr = 0, 0.0, 0.0, 0
     for p, (hi, lo, ab) in zip(batch, refs):
         n = p["n"]
         r = oz.error_ratio(n, n, n, p["C"], n, hi, lo, ab, TARGET_BITS)
         worst = max(worst, r)
         bad += r > 1.0
-    return bad, worst
+        u, c = oz.accuracy(n, n, p["C"], n, hi, lo)
+        ulp, cr = max(ulp, u), cr + c
+    return bad, worst, ulp, cr
 
 
 def main():
@@ -489,7 +503,8 @@ def main():
 
     # every output of every form against the double-double product (untimed; also sizes the
     # workspaces before the timed steps)
-    checks = {f: {"problems": 0, "over_bound": 0, "max_ratio": 0.0} for f in forms}
+    checks = {f: {"problems": 0, "over_bound": 0, "max_ratio": 0.0, "ulp_max": 0.0, "cr_frac": 0.0} for f in forms}
+    entries = sum(p["n"] ** 2 for b in batches for p in b)
     adaptive_stats = {}
     for b in range(nb):
         refs = []
@@ -501,11 +516,13 @@ def main():
             refs.append((hi, lo, ab))
         for name, fn in forms.items():
             holder = {}
-            bad, worst = verify(oz, torch, batches[b], lambda: holder.update(st=fn(b)), refs)
+            bad, worst, ulp, cr = verify(oz, torch, batches[b], lambda: holder.update(st=fn(b)), refs)
             c = checks[name]
             c["problems"] += len(batches[b])
             c["over_bound"] += int(bad)
             c["max_ratio"] = max(c["max_ratio"], worst)
+            c["ulp_max"] = max(c["ulp_max"], ulp)
+            c["cr_frac"] += cr / entries
             if name == "adaptive_mlp_batched":
                 for key, v in holder["st"].items():
                     adaptive_stats[key] = adaptive_stats.get(key, 0) + v
@@ -592,7 +609,8 @@ def main():
                          "algorithmic": "2 s m_t n_t k int8 ops per tile (reruns included), summed over the step",
                          "traffic": None},
             "fixed_s": fixed,
-            "error_check": {"bound": "|C - AB| <= k 2^-53 (|A||B|)_ij against a double-double product, per entry",
+            "error_check": {"bound": "|C - AB| <= k 2^-53 (|A||B|)_ij against a double-double product, per entry; "
+                                     "ulp_max in units of the spacing above |AB|, cr_frac = entries equal to RN(AB)",
                             **checks},
             "adaptive_tiles": {"tiles": adaptive_stats.get("tiles"),
                                "native_tiles": adaptive_stats.get("native_tiles"),

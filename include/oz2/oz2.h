@@ -137,6 +137,12 @@ int oz2_tile_features(oz2_handle h, int count, const oz2_dgemm_problem* problems
  * A (m x k) and B (k x n) on the device: the reference the labels are measured against */
 int oz2_dd_reference(oz2_handle h, int64_t m, int64_t n, int64_t k, const double* A, int64_t lda, const double* B,
                      int64_t ldb, double* hi, double* lo, double* absab);
+/* max_ulp = max over entries of |C - (hi + lo)| in units of the spacing above |hi|;
+ * correctly_rounded = entries equal to RN(hi + lo) (hi, lo from oz2_dd_reference, m x n,
+ * leading dimension m); synchronises. No counterpart in the reference's API (its accuracy bench
+ * reports the same two figures, benchmarks/bench_accuracy.cpp:69-94). */
+int oz2_accuracy(oz2_handle h, int64_t m, int64_t n, const double* C, int64_t ldc, const double* hi,
+                 const double* lo, double* max_ulp, int64_t* correctly_rounded);
 /* out = max over entries of |C - (hi + lo)| / (k 2^-target_bits |A||B|); synchronises */
 int oz2_error_ratio(oz2_handle h, int64_t m, int64_t n, int64_t k, const double* C, int64_t ldc, const double* hi,
                     const double* lo, const double* absab, int target_bits, float* out);

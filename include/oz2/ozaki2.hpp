@@ -39,6 +39,34 @@ struct TileInfo {
     size_t workspace_bytes = 0;
 };
 
+// one problem of a grouped or adaptive call (no counterpart in the reference): the arguments of
+// gemm(); num_moduli is ignored by the adaptive modes other than Fixed
+struct Problem {
+    Trans ta = Trans::N, tb = Trans::N;
+    int64_t m = 0, n = 0, k = 0;
+    double alpha = 1.0;
+    const double* A = nullptr;
+    int64_t lda = 1;
+    const double* B = nullptr;
+    int64_t ldb = 1;
+    double beta = 0.0;
+    double* C = nullptr;
+    int64_t ldc = 1;
+    int num_moduli = 16;
+};
+
+struct GemmConfig {
+    int bn = 256, group_j = 16, ctas = 0;
+};
+
+// how gemm_adaptive picks s per tile (oz2_dgemm_adaptive modes)
+enum class Adaptive { Mlp = 0, AnalyticTile = 1, AnalyticProblem = 2, Fixed = 3 };
+
+struct AdaptiveStats {
+    int64_t tiles = 0, sum_s = 0, probed = 0, rerun = 0, rerun_sum_s = 0, analytic_sum_s = 0, mlp = 0,
+            int8_macs = 0, native_tiles = 0, native_macs = 0;
+};
+
 namespace detail {
 inline void check(int status, oz2_handle h = nullptr) {
     if (status == OZ2_OK) return;
@@ -50,6 +78,15 @@ inline void check(int status, oz2_handle h = nullptr) {
     }
 }
 inline char op(Trans t) { return t == Trans::N ? 'N' : (t == Trans::T ? 'T' : 'C'); }
+inline std::vector<oz2_dgemm_problem> problems(const std::vector<Problem>& ps) {
+    std::vector<oz2_dgemm_problem> out(ps.size());
+    for (size_t i = 0; i < ps.size(); ++i) {
+        const Problem& p = ps[i];
+        out[i] = oz2_dgemm_problem{op(p.ta), op(p.tb), p.num_moduli, p.m,   p.n, p.k,   p.alpha,
+                                   p.beta,   p.A,      p.lda,        p.B,   p.ldb, p.C, p.ldc};
+    }
+    return out;
+}
 }  // namespace detail
 
 class Ozaki2 {
@@ -121,6 +158,47 @@ public:
                                 lda, reinterpret_cast<const double*>(B), ldb, be, reinterpret_cast<double*>(C), ldc,
                                 num_moduli, d.data(), static_cast<int>(d.size()), done),
                       h_);
+    }
+
+    // ---- beyond the reference: many problems in one set of launches, and adaptive s per tile
+
+    // every problem as gemm() would compute it, bit for bit, in one grouped launch
+    void gemm_grouped(const std::vector<Problem>& ps, const std::vector<cudaEvent_t>& deps = {},
+                      cudaEvent_t done = nullptr) {
+        auto q = detail::problems(ps);
+        std::vector<void*> d(deps.begin(), deps.end());
+        detail::check(oz2_dgemm_grouped(h_, static_cast<int>(q.size()), q.data(), d.data(),
+                                        static_cast<int>(d.size()), done),
+                      h_);
+    }
+    void set_graph_mode(bool on) { detail::check(oz2_set_graph_mode(h_, on ? 1 : 0), h_); }
+    void set_gemm_config(const GemmConfig& c) { detail::check(oz2_set_gemm_config(h_, c.bn, c.group_j, c.ctas), h_); }
+    void clear_gemm_config() { detail::check(oz2_set_gemm_config(h_, 0, 0, 0), h_); }
+    GemmConfig autotune_grouped(const std::vector<Problem>& ps) {
+        auto q = detail::problems(ps);
+        int v[3] = {0, 0, 0};
+        detail::check(oz2_autotune_grouped(h_, static_cast<int>(q.size()), q.data(), v), h_);
+        return GemmConfig{v[0], v[1], v[2]};
+    }
+
+    // C = alpha op(A) op(B) + beta C with s chosen per tile for `target_bits` (53: DGEMM-level
+    // error); synchronises the stream
+    AdaptiveStats gemm_adaptive(const std::vector<Problem>& ps, int target_bits = 53,
+                                Adaptive mode = Adaptive::Mlp) {
+        auto q = detail::problems(ps);
+        int64_t v[10] = {};
+        detail::check(oz2_dgemm_adaptive(h_, static_cast<int>(q.size()), q.data(), target_bits,
+                                         static_cast<int>(mode), v),
+                      h_);
+        return AdaptiveStats{v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7], v[8], v[9]};
+    }
+    // MLP parameters (the "params" array of a model file written by oz2.adaptive); empty unloads
+    void set_mlp_weights(const std::vector<float>& params) {
+        detail::check(oz2_mlp_set_weights(h_, params.empty() ? nullptr : params.data(), static_cast<int>(params.size())),
+                      h_);
+    }
+    void set_adaptive_options(int tile, float threshold) {
+        detail::check(oz2_set_adaptive_options(h_, tile, threshold), h_);
     }
 
     // synchronises the stream; throws std::runtime_error if a kernel's bounded wait ran out

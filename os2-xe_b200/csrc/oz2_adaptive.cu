@@ -332,7 +332,41 @@ __global__ void error_ratio_kernel(int64_t m, int64_t n, const double* __restric
     atomicMax(out, __float_as_uint(r));  // non-negative floats order like their bits
 }
 
+// accuracy of C against the double-double product, as the reference's accuracy bench defines it
+// (benchmarks/bench_accuracy.cpp:69-94): the largest |C - (hi + lo)| in units of the spacing above
+// |hi| (the smallest subnormal where hi = 0), and how many entries equal RN(hi + lo)
+__global__ void accuracy_kernel(int64_t m, int64_t n, const double* __restrict__ C, int64_t ldc,
+                                const double* __restrict__ hi, const double* __restrict__ lo,
+                                unsigned int* __restrict__ max_ulp, unsigned long long* __restrict__ correct) {
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    float u = 0.0f;
+    bool cr = false;
+    if (e < m * n) {
+        const int64_t i = e % m, j = e / m;
+        const double c = C[i + j * ldc], h = hi[e], l = lo[e];
+        const double rn = h + l;  // hi + lo is normalised: their sum rounds the exact value once
+        cr = c == rn || (c != c && rn != rn);
+        int ex;
+        frexp(h, &ex);
+        const double ulp = h == 0.0 ? 0x1p-1074 : ldexp(1.0, max(ex - 53, -1074));
+        const double err = fabs((c - h) - l) / ulp;
+        u = err == err ? static_cast<float>(err) : __int_as_float(0x7F800000);
+    }
+    for (int o = 16; o > 0; o >>= 1) u = fmaxf(u, __shfl_xor_sync(0xFFFFFFFFu, u, o));
+    const unsigned int votes = __popc(__ballot_sync(0xFFFFFFFFu, cr));
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(max_ulp, __float_as_uint(u));
+        if (votes) atomicAdd(correct, static_cast<unsigned long long>(votes));
+    }
+}
+
 }  // namespace
+
+void launch_accuracy(int64_t m, int64_t n, const double* C, int64_t ldc, const double* hi, const double* lo,
+                     unsigned int* max_ulp, unsigned long long* correct, cudaStream_t st) {
+    const int64_t total = m * n;
+    accuracy_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, st>>>(m, n, C, ldc, hi, lo, max_ulp, correct);
+}
 
 int64_t stat_item_blocks(StatItem& it, int64_t block0) {
     it.block0 = block0;

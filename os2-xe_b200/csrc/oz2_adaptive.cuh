@@ -70,6 +70,9 @@ void launch_dd_gemm_nn(int64_t m, int64_t n, int64_t k, const double* A, int64_t
                        double* hi, double* lo, double* absab, cudaStream_t st);
 void launch_error_ratio(int64_t m, int64_t n, const double* C, int64_t ldc, const double* hi, const double* lo,
                         const double* absab, double scale, unsigned int* out, cudaStream_t st);
+// max error in ulps of RN(hi + lo) (float bits) and the count of entries equal to RN(hi + lo)
+void launch_accuracy(int64_t m, int64_t n, const double* C, int64_t ldc, const double* hi, const double* lo,
+                     unsigned int* max_ulp, unsigned long long* correct, cudaStream_t st);
 
 // MLP: kFeatures -> kHidden (ReLU) -> kHidden (ReLU) -> kClasses, parameters packed as
 // W1[kHidden][kFeatures] b1 W2[kHidden][kHidden] b2 W3[kClasses][kHidden] b3.

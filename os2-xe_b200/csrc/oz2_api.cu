@@ -120,6 +120,9 @@ struct oz2_context {
     size_t ws2_size = 0;
     int64_t astats[kAdaptiveStats] = {};
     cublasHandle_t cublas = nullptr;  // native FP64 GEMM of tiles no moduli set brings to the target
+    cudaStream_t cublas_stream = nullptr;
+    bool cublas_bound = false;        // cublas_stream is set on the handle
+    void* cublas_ws = nullptr;        // its workspace, owned here so that no call allocates
     int64_t launches = 0;  // kernels launched through this handle (graph replays included)
     bool capture_ok = true;           // false when part of the call ran outside the graphs
     std::string err;
@@ -834,15 +837,27 @@ int ensure_ws2(oz2_context* h, size_t bytes) {
 // C[i0:i0+mb, j0:j0+nb] = alpha op(A) op(B) + beta C in native FP64 (cuBLAS DGEMM, default math:
 // no emulation), for tiles whose inputs span more exponent range than 24 moduli cover
 int native_gemm(oz2_context* h, const Prob& p, int64_t i0, int64_t j0, int64_t mb, int64_t nb) {
+    constexpr size_t kCublasWs = size_t{32} << 20;
     if (!h->cublas) {
         if (cublasCreate(&h->cublas) != CUBLAS_STATUS_SUCCESS) {
             h->cublas = nullptr;
             return fail(h, OZ2_ECUDA, "oz2: cublasCreate failed");
         }
         cublasSetMathMode(h->cublas, CUBLAS_DEFAULT_MATH);
+        if (cudaMalloc(&h->cublas_ws, kCublasWs) != cudaSuccess) {
+            cudaGetLastError();
+            h->cublas_ws = nullptr;
+        }
+        h->cublas_bound = false;
     }
-    if (cublasSetStream(h->cublas, h->stream) != CUBLAS_STATUS_SUCCESS)
-        return fail(h, OZ2_ECUDA, "oz2: cublasSetStream failed");
+    // setting the stream resets the workspace: only when the stream changed
+    if (!h->cublas_bound || h->cublas_stream != h->stream) {
+        if (cublasSetStream(h->cublas, h->stream) != CUBLAS_STATUS_SUCCESS)
+            return fail(h, OZ2_ECUDA, "oz2: cublasSetStream failed");
+        if (h->cublas_ws) cublasSetWorkspace(h->cublas, h->cublas_ws, kCublasWs);
+        h->cublas_stream = h->stream;
+        h->cublas_bound = true;
+    }
     const double* A = p.A + (is_n(p.ta) ? i0 : i0 * p.lda);
     const double* B = p.B + (is_n(p.tb) ? j0 * p.ldb : j0);
     double* C = p.C + i0 + j0 * p.ldc;
@@ -1357,6 +1372,7 @@ int oz2_destroy(oz2_handle h) {
     if (h->d_mlp) cudaFree(h->d_mlp);
     if (h->ws2) cudaFree(h->ws2);
     if (h->cublas) cublasDestroy(h->cublas);
+    if (h->cublas_ws) cudaFree(h->cublas_ws);
     delete h;
     return OZ2_OK;
 }
@@ -1605,6 +1621,27 @@ int oz2_error_ratio(oz2_handle h, int64_t m, int64_t n, int64_t k, const double*
     OZ2_CUDA(h, cudaMemcpyAsync(&bits, h->d_err + 1, sizeof bits, cudaMemcpyDeviceToHost, h->stream));
     OZ2_CUDA(h, cudaStreamSynchronize(h->stream));
     std::memcpy(out, &bits, sizeof bits);
+    return OZ2_OK;
+}
+
+int oz2_accuracy(oz2_handle h, int64_t m, int64_t n, const double* C, int64_t ldc, const double* hi,
+                 const double* lo, double* max_ulp, int64_t* correctly_rounded) {
+    if (!h || !max_ulp || !correctly_rounded) return fail(h, OZ2_EINVAL, "oz2: null argument");
+    if (m <= 0 || n <= 0 || ldc < m) return fail(h, OZ2_EINVAL, "oz2: bad dimensions");
+    // d_err[2..3] hold the 64-bit count, d_err[1] the float bits of the maximum
+    OZ2_CUDA(h, cudaMemsetAsync(h->d_err + 1, 0, 3 * sizeof(int), h->stream));
+    auto* cnt = reinterpret_cast<unsigned long long*>(h->d_err + 2);
+    launch_accuracy(m, n, C, ldc, hi, lo, reinterpret_cast<unsigned int*>(h->d_err + 1), cnt, h->stream);
+    ++h->launches;
+    unsigned int out[3] = {0, 0, 0};
+    OZ2_CUDA(h, cudaMemcpyAsync(out, h->d_err + 1, sizeof out, cudaMemcpyDeviceToHost, h->stream));
+    OZ2_CUDA(h, cudaStreamSynchronize(h->stream));
+    float f;
+    std::memcpy(&f, &out[0], sizeof f);
+    unsigned long long c;
+    std::memcpy(&c, &out[1], sizeof c);
+    *max_ulp = f;
+    *correctly_rounded = static_cast<int64_t>(c);
     return OZ2_OK;
 }
 

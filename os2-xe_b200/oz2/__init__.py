@@ -55,6 +55,7 @@ class DgemmProblem(C.Structure):
 _lib.oz2_dgemm_grouped.argtypes = [_vp, _i32, C.POINTER(DgemmProblem), _vp, _i32, _vp]
 _lib.oz2_set_graph_mode.argtypes = [_vp, _i32]
 _lib.oz2_kernel_launches.argtypes = [_vp, C.POINTER(_i64)]
+_lib.oz2_accuracy.argtypes = [_vp, _i64, _i64, _vp, _i64, _vp, _vp, C.POINTER(_dbl), C.POINTER(_i64)]
 _lib.oz2_set_gemm_config.argtypes = [_vp, _i32, _i32, _i32]
 _lib.oz2_get_gemm_config.argtypes = [_vp, C.POINTER(_i32)]
 _lib.oz2_autotune_grouped.argtypes = [_vp, _i32, C.POINTER(DgemmProblem), C.POINTER(_i32)]
@@ -344,6 +345,14 @@ class Ozaki2:
     def dd_reference(self, m, n, k, A, lda, B, ldb, hi, lo, absab):
         _raise(_lib.oz2_dd_reference(self._h, m, n, k, _addr(A), lda, _addr(B), ldb, _addr(hi), _addr(lo),
                                      _addr(absab)), self._h)
+
+    def accuracy(self, m, n, C_, ldc, hi, lo):
+        """(max error in ulps of the correctly rounded value, entries correctly rounded) of C
+        against the double-double product hi + lo"""
+        u, c = _dbl(), _i64()
+        _raise(_lib.oz2_accuracy(self._h, m, n, _addr(C_), ldc, _addr(hi), _addr(lo), C.byref(u), C.byref(c)),
+               self._h)
+        return u.value, c.value
 
     def error_ratio(self, m, n, k, C_, ldc, hi, lo, absab, target_bits=53):
         out = C.c_float()

@@ -57,8 +57,13 @@ def test_null_handle_is_rejected():
 def test_cpp_header_compiles():
     """include/oz2/ozaki2.hpp (the reference's class over the C ABI) compiles and links"""
     src = os.path.join(ROOT, "include", "oz2", "ozaki2.hpp")
+    # the grouped / adaptive members are instantiated (not run: no device here)
     prog = ('#include "oz2/ozaki2.hpp"\n'
-            "int main() { return oz2::Ozaki2::moduli_for_bits(1024, 53) == 15 ? 0 : 1; }\n")
+            "void use(oz2::Ozaki2& oz) { std::vector<oz2::Problem> ps(1); oz.gemm_grouped(ps);\n"
+            "  oz2::AdaptiveStats st = oz.gemm_adaptive(ps, 53, oz2::Adaptive::Mlp); (void)st;\n"
+            "  oz.set_mlp_weights({}); oz.set_adaptive_options(512, 0.99f); oz.autotune_grouped(ps); }\n"
+            "int main(int argc, char**) { if (argc > 5) { oz2::Ozaki2 oz; use(oz); }\n"
+            "  return oz2::Ozaki2::moduli_for_bits(1024, 53) == 15 ? 0 : 1; }\n")
     exe = os.path.join(ROOT, "os2-xe_b200", "_build", "hdr_check")
     os.makedirs(os.path.dirname(exe), exist_ok=True)
     r = subprocess.run(["/usr/bin/g++", "-std=c++17", "-x", "c++", "-", "-I" + os.path.join(ROOT, "include"),

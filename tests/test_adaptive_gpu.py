@@ -324,3 +324,25 @@ def test_default_model_loads_and_meets_the_target(az):
     finally:
         az.set_mlp_weights(None)
         az.set_adaptive_options(TILE, 0.9)
+
+
+def test_accuracy_metrics_match_the_oracle(oracle, az):
+    """max ulp error and the correctly rounded count against the double-double product, on the
+    device and by the oracle's restatement of the reference's accuracy bench"""
+    import torch
+    m, n, k = 300, 200, 700
+    A, B = nn_problem(123, m, n, k, 2.0, 10)
+    dA, dB = to_dev(A), to_dev(B)
+    hi = torch.empty(m * n, dtype=torch.float64, device="cuda")
+    lo, ab = torch.empty_like(hi), torch.empty_like(hi)
+    az.dd_reference(m, n, k, dA, m, dB, k, hi, lo, ab)
+    rn = hi + lo
+    u, c = az.accuracy(m, n, rn, m, hi, lo)
+    assert c == m * n and u <= 0.5
+    for s in (10, 16):
+        dC = torch.zeros(m * n, dtype=torch.float64, device="cuda")
+        az.gemm("N", "N", m, n, k, 1.0, dA, m, dB, k, 0.0, dC, m, s)
+        u, c = az.accuracy(m, n, dC, m, hi, lo)
+        want = oracle.metrics(dC.cpu().numpy(), hi.cpu().numpy(), lo.cpu().numpy())
+        assert abs(u - want["ulp_max"]) <= 1e-6 * max(1.0, want["ulp_max"])
+        assert c == round(want["cr_frac"] * m * n)
