@@ -399,9 +399,56 @@ def dgemm_leg(a, oz2, torch, dev, stream, rank):
         out["cublaslt_int8_tops"] = 2.0 * m * n * k / (t.ms / 5 * 1e-3) / 1e12
     except Exception as e:  # noqa: BLE001
         out["cublaslt_int8_tops"] = f"unavailable: {type(e).__name__}"
+    # the other moduli counts of the same shape (alpha 1.5, beta -0.5), NN
+    sweep = {}
+    for sv in (8, 12, 16, 20, 24):
+        oz.gemm("N", "N", m, n, k, 1.5, A, m, B, k, -0.5, C, ldc, sv)
+        with Timer(torch, stream) as t:
+            for _ in range(5):
+                oz.gemm("N", "N", m, n, k, 1.5, A, m, B, k, -0.5, C, ldc, sv)
+        sweep[str(sv)] = flops / (t.ms / 5 * 1e-3) / 1e12
+    out["tflops_by_s"] = sweep
     oz.check_device_error()
     oz.close()
     return out
+
+
+def zgemm_leg(oz2, torch, dev, stream, rank):
+    """ZGEMM 4096^3, op(A) = C, op(B) = N, alpha (1, 0.5), beta (0.25, -1), ldc = m + 8, s = 16,
+    U[-1,1) real and imaginary parts: FP64-equivalent 8 m n k / t, against cuBLAS ZGEMM"""
+    m = n = k = 4096
+    ldc = m + 8
+    g = torch.Generator(device=dev)
+    g.manual_seed(4321 + rank)
+    A = torch.rand(2 * k * m, dtype=torch.float64, device=dev, generator=g) * 2 - 1
+    B = torch.rand(2 * k * n, dtype=torch.float64, device=dev, generator=g) * 2 - 1
+    C = torch.rand(2 * ldc * n, dtype=torch.float64, device=dev, generator=g) * 2 - 1
+    oz = oz2.Ozaki2(stream)
+    for _ in range(2):
+        oz.zgemm("C", "N", m, n, k, 1 + 0.5j, A, k, B, k, 0.25 - 1j, C, ldc, 16)
+    with Timer(torch, stream) as t:
+        for _ in range(5):
+            oz.zgemm("C", "N", m, n, k, 1 + 0.5j, A, k, B, k, 0.25 - 1j, C, ldc, 16)
+    ms = t.ms / 5
+    oz.set_profiling(True)
+    oz.zgemm("C", "N", m, n, k, 1 + 0.5j, A, k, B, k, 0.25 - 1j, C, ldc, 16)
+    st = oz.stage_times()
+    oz.set_profiling(False)
+    oz.check_device_error()
+    oz.close()
+    flops = 8.0 * m * n * k
+    Az = torch.view_as_complex(A.view(m, k, 2))  # row i of this view is column i of the stored A
+    Bz = torch.view_as_complex(B.view(n, k, 2))
+    # C^T = B^T conj(A) in row-major views of the column-major data
+    torch.mm(Bz, Az.conj().t())
+    with Timer(torch, stream) as t:
+        for _ in range(3):
+            torch.mm(Bz, Az.conj().t())
+    zref = flops / (t.ms / 3 * 1e-3) / 1e12
+    return {"workload": "zgemm 4096x4096x4096 op=(C,N) alpha=(1,0.5) beta=(0.25,-1) ldc=m+8 s=16 U[-1,1)",
+            "tflops": flops / (ms * 1e-3) / 1e12, "ms": ms,
+            "stage_ms": {"scale": st.scale_ms, "split": st.split_ms, "gemm": st.gemm_ms, "crt": st.crt_ms},
+            "cublas_zgemm_tflops": zref, "vs_cublas_zgemm": flops / (ms * 1e-3) / 1e12 / zref}
 
 
 # ------------------------------------------------------------------ the adaptive-s stream
@@ -418,6 +465,17 @@ def stream_batches(a, torch, dev, rank):
         batches.append([make_problem(torch, dev, n, phi, sd) for n, phi, sd in part])
         used += need
     return batches, used
+
+
+def over_ranks(dist, torch, world, dev, ms, flops):
+    """(max over ranks of the timed region, sum over ranks of the work); identity on one rank"""
+    if world <= 1:
+        return ms, flops
+    x = torch.tensor([ms, flops], dtype=torch.float64, device=dev)
+    mx = x.clone()
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    dist.all_reduce(x, op=dist.ReduceOp.SUM)
+    return float(mx[0]), float(x[1])
 
 
 def problem_analytic_s(oz, batch):
@@ -541,12 +599,7 @@ def main():
                 fn(i % nb)
                 flops += flops_of(batches[i % nb])
         ms = t.ms
-        if world > 1:
-            x = torch.tensor([ms, flops], dtype=torch.float64, device=dev)
-            mx = x.clone()
-            dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-            dist.all_reduce(x, op=dist.ReduceOp.SUM)
-            ms, flops = float(mx[0]), float(x[1])
+        ms, flops = over_ranks(dist, torch, world, dev, ms, flops)
         return flops / (ms * 1e-3) / 1e12, ms / steps
 
     # headline: the adaptive form
@@ -563,24 +616,19 @@ def main():
                 flops += flops_of(batches[i % nb])
     launches = oz.kernel_launches() - launches0
     ms = t.ms
-    if world > 1:
-        x = torch.tensor([ms, flops], dtype=torch.float64, device=dev)
-        mx = x.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        dist.all_reduce(x, op=dist.ReduceOp.SUM)
-        ms, flops = float(mx[0]), float(x[1])
+    ms, flops = over_ranks(dist, torch, world, dev, ms, flops)
     value = flops / (ms * 1e-3) / 1e12
     ms_step = ms / a.steps
     oz.check_device_error()
 
     # stage times and the GEMM kernel against the int8 roofline (profiling pass, untimed)
     oz.set_profiling(True)
-    st_sum, macs = [0.0] * 4, 0
+    st_sum, macs = [0.0] * 6, 0
     for i in range(a.steps):
         st = adaptive(i % nb)
         macs += st["int8_macs"]
-        tt = oz.stage_times()
-        for j, v in enumerate((tt.scale_ms, tt.split_ms, tt.gemm_ms, tt.crt_ms)):
+        tt, at = oz.stage_times(), oz.adaptive_stage_times()
+        for j, v in enumerate((tt.scale_ms, tt.split_ms, tt.gemm_ms, tt.crt_ms, at["probe_ms"], at["native_ms"])):
             st_sum[j] += v
     oz.set_profiling(False)
     peak, note = int8_peak()
@@ -603,7 +651,8 @@ def main():
                            model_threshold=model.get("threshold")),
             "clocks": clk.summary(), "gpu_launches": launches,
             "stage_ms_per_step": {"scale_stats_mlp": st_sum[0] / a.steps, "split": st_sum[1] / a.steps,
-                                  "gemm": st_sum[2] / a.steps, "crt": st_sum[3] / a.steps},
+                                  "gemm": st_sum[2] / a.steps, "crt": st_sum[3] / a.steps,
+                                  "probe": st_sum[4] / a.steps, "native_fp64": st_sum[5] / a.steps},
             "roofline": {"bound": "tensor", "kernel": "gemm_i8_modm_kernel", "achieved": achieved, "peak": peak,
                          "unit": "TOPS (int8)", "frac": achieved / peak, "peak_note": note,
                          "algorithmic": "2 s m_t n_t k int8 ops per tile (reruns included), summed over the step",
@@ -644,12 +693,7 @@ def main():
             e2e_step()
     e2e_ms = t.ms / e2e_steps
     e2e_flops = flops_of(b0)
-    if world > 1:
-        x = torch.tensor([e2e_ms, e2e_flops], dtype=torch.float64, device=dev)
-        mx = x.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        dist.all_reduce(x, op=dist.ReduceOp.SUM)
-        e2e_ms, e2e_flops = float(mx[0]), float(x[1])
+    e2e_ms, e2e_flops = over_ranks(dist, torch, world, dev, e2e_ms, e2e_flops)
     line["e2e"] = {"value": e2e_flops / (e2e_ms * 1e-3) / 1e12, "unit": UNIT,
                    "h2d_bytes_per_step": sum(16 * p["n"] ** 2 for p in b0),
                    "d2h_bytes_per_step": sum(8 * p["n"] ** 2 for p in b0), "ms_per_step": e2e_ms,
@@ -663,6 +707,7 @@ def main():
     extras = {}
     if not a.no_extras:
         extras["dgemm_8192"] = dgemm_leg(a, oz2, torch, dev, stream, rank)
+        extras["zgemm_4096"] = zgemm_leg(oz2, torch, dev, stream, rank)
         extras["grouped_c4"] = grouped_leg(oz2, torch, dev, stream)
         if rank == 0:
             line["cpu_baseline"] = cpu_sample(a)

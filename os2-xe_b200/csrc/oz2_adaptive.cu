@@ -196,7 +196,7 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
     return z ^ (z >> 31);
 }
 
-__global__ void __launch_bounds__(256) probe_kernel(const ProbeItem* __restrict__ items, int count,
+__global__ void __launch_bounds__(256, 3) probe_kernel(const ProbeItem* __restrict__ items, int count,
                                                     int* __restrict__ fail) {
     const ProbeItem* I = items + find_block_item(items, count, blockIdx.x);
     const int64_t rblk = static_cast<int64_t>(blockIdx.x) - I->block0;
@@ -233,16 +233,25 @@ __global__ void __launch_bounds__(256) probe_kernel(const ProbeItem* __restrict_
         }
         __syncthreads();
         if (live) {
+            const double* __restrict__ Ai = I->a_rowc ? I->A + i : I->A + i * I->lda;
+            const int64_t astep = I->a_rowc ? I->lda : 1;
             for (int q0 = 0; q0 < pn; q0 += 32) {  // kProbeChunk is a multiple of 32
                 const int qn = min(32, pn - q0);
-                for (int q = q0; q < q0 + qn; ++q) {
-                    const int64_t p = p0 + q;
-                    const double av = I->a_rowc ? I->A[i + p * I->lda] : I->A[p + i * I->lda];
+                for (int q1 = q0; q1 < q0 + qn; q1 += 8) {
+                    // eight loads of A in flight before their products
+                    double av[8];
 #pragma unroll
-                    for (int c = 0; c < kProbeCols; ++c) {
-                        const double b = bs[c][q];
-                        zp[c] = fma(av, b, zp[c]);
-                        za[c] = fma(fabs(av), fabs(b), za[c]);
+                    for (int u = 0; u < 8; ++u)
+                        av[u] = q1 + u < q0 + qn ? __ldg(Ai + (p0 + q1 + u) * astep) : 0.0;
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        const int q = min(q1 + u, pn - 1);  // av[u] = 0 past the chunk
+#pragma unroll
+                        for (int c = 0; c < kProbeCols; ++c) {
+                            const double b = bs[c][q];
+                            zp[c] = fma(av[u], b, zp[c]);
+                            za[c] = fma(fabs(av[u]), fabs(b), za[c]);
+                        }
                     }
                 }
 #pragma unroll

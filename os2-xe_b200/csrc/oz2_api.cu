@@ -122,7 +122,6 @@ struct oz2_context {
     cublasHandle_t cublas = nullptr;  // native FP64 GEMM of tiles no moduli set brings to the target
     cudaStream_t cublas_stream = nullptr;
     bool cublas_bound = false;        // cublas_stream is set on the handle
-    void* cublas_ws = nullptr;        // its workspace, owned here so that no call allocates
     int64_t launches = 0;  // kernels launched through this handle (graph replays included)
     bool capture_ok = true;           // false when part of the call ran outside the graphs
     std::string err;
@@ -837,24 +836,18 @@ int ensure_ws2(oz2_context* h, size_t bytes) {
 // C[i0:i0+mb, j0:j0+nb] = alpha op(A) op(B) + beta C in native FP64 (cuBLAS DGEMM, default math:
 // no emulation), for tiles whose inputs span more exponent range than 24 moduli cover
 int native_gemm(oz2_context* h, const Prob& p, int64_t i0, int64_t j0, int64_t mb, int64_t nb) {
-    constexpr size_t kCublasWs = size_t{32} << 20;
     if (!h->cublas) {
         if (cublasCreate(&h->cublas) != CUBLAS_STATUS_SUCCESS) {
             h->cublas = nullptr;
             return fail(h, OZ2_ECUDA, "oz2: cublasCreate failed");
         }
         cublasSetMathMode(h->cublas, CUBLAS_DEFAULT_MATH);
-        if (cudaMalloc(&h->cublas_ws, kCublasWs) != cudaSuccess) {
-            cudaGetLastError();
-            h->cublas_ws = nullptr;
-        }
         h->cublas_bound = false;
     }
-    // setting the stream resets the workspace: only when the stream changed
+    // setting the stream resets cuBLAS's workspace: only when the stream changed
     if (!h->cublas_bound || h->cublas_stream != h->stream) {
         if (cublasSetStream(h->cublas, h->stream) != CUBLAS_STATUS_SUCCESS)
             return fail(h, OZ2_ECUDA, "oz2: cublasSetStream failed");
-        if (h->cublas_ws) cublasSetWorkspace(h->cublas, h->cublas_ws, kCublasWs);
         h->cublas_stream = h->stream;
         h->cublas_bound = true;
     }
@@ -1228,7 +1221,14 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
     if (mode == 0) {
         std::vector<ProbeItem> pi;
         int64_t blocks = 0;
-        for (int64_t t = 0; t < ntiles; ++t) {
+        // tiles of one row panel next to each other: their blocks run together and share the
+        // panel's rows of A through the L2
+        std::vector<int64_t> porder(ntiles);
+        for (int64_t t = 0; t < ntiles; ++t) porder[t] = t;
+        std::stable_sort(porder.begin(), porder.end(), [&](int64_t x, int64_t y) {
+            return std::make_pair(tiles[x].prob, tiles[x].i0) < std::make_pair(tiles[y].prob, tiles[y].i0);
+        });
+        for (const int64_t t : porder) {
             const TileRef& r = tiles[t];
             const Prob& p = base[r.prob];
             if (p.beta[0] != 0.0 || s_tile[t] >= s_an[t]) continue;  // analytic s needs no probe
@@ -1372,7 +1372,6 @@ int oz2_destroy(oz2_handle h) {
     if (h->d_mlp) cudaFree(h->d_mlp);
     if (h->ws2) cudaFree(h->ws2);
     if (h->cublas) cublasDestroy(h->cublas);
-    if (h->cublas_ws) cudaFree(h->cublas_ws);
     delete h;
     return OZ2_OK;
 }

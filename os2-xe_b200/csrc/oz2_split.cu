@@ -139,22 +139,31 @@ __device__ __forceinline__ uint32_t pack_bytes(uint32_t a, uint32_t b, uint32_t 
     return __byte_perm(__byte_perm(a, b, 0x0040), __byte_perm(c, d, 0x0040), 0x5410);
 }
 
-// Each thread: one plane row r and 16 consecutive inner indices k0..k0+15, i.e. one 16-byte
-// chunk of every plane. ROWC: a warp is 32 consecutive rows (coalesced loads along r), the 8
-// warps of a block are the 8 chunks of one 128-wide k block. Otherwise a warp is one row and
-// 32 consecutive chunks (512 inner indices), the 8 warps are 8 rows.
+// elements per thread: 16 (one 16-byte chunk of every plane) on the real narrow path; 8 (half a
+// chunk) on the wide path and for complex inputs, whose limbs per element (five, or two groups)
+// would otherwise hold 128 to 200 registers
+template <int NLIMB, bool CPLX>
+__host__ __device__ constexpr int split_ept() {
+    return NLIMB == 3 && !CPLX ? 16 : 8;
+}
+
+// Each thread: one plane row r and EPT consecutive inner indices k0..k0+EPT-1 of every plane.
+// ROWC: a warp is 32 consecutive rows (coalesced loads along r), the 8 warps of a block are 8
+// consecutive EPT-wide pieces of the inner index. Otherwise a warp is one row and 32
+// consecutive pieces, the 8 warps are 8 rows.
 template <int NLIMB, bool CPLX, bool ROWC>
 __global__ void __launch_bounds__(256) split_kernel(const SplitItem* __restrict__ items, int count) {
+    constexpr int EPT = split_ept<NLIMB, CPLX>();
     const SplitItem* __restrict__ I = items + find_item(items, count, blockIdx.x);
     const int64_t local = static_cast<int64_t>(blockIdx.x) - I->block0;
     const int64_t bx = local % I->rblocks, by = local / I->rblocks;
     int64_t r, k0;
     if (ROWC) {
         r = bx * 32 + (threadIdx.x & 31);
-        k0 = by * kTileK + (threadIdx.x >> 5) * 16;
+        k0 = by * (8 * EPT) + (threadIdx.x >> 5) * EPT;
     } else {
         r = bx * 8 + (threadIdx.x >> 5);
-        k0 = by * (4 * kTileK) + (threadIdx.x & 31) * 16;
+        k0 = by * (32 * EPT) + (threadIdx.x & 31) * EPT;
     }
     const int64_t kb_total = I->kb_total, plane_bytes = I->plane_bytes, ldx = I->ldx, k = I->k;
     const int64_t rows = I->rows;
@@ -165,15 +174,20 @@ __global__ void __launch_bounds__(256) split_kernel(const SplitItem* __restrict_
     const int rr = static_cast<int>(r & 127);
     const int64_t kb = k0 >> 7;
     const int c = static_cast<int>((k0 >> 4) & 7);
-    int8_t* out = I->planes + (rb * kb_total + kb) * kTileBytes + rr * kTileK + ((c ^ (rr & 7)) << 4);
+    int8_t* out = I->planes + (rb * kb_total + kb) * kTileBytes + rr * kTileK + ((c ^ (rr & 7)) << 4) +
+                  (k0 & 15);  // the second half of a chunk on the wide path
     const int64_t gstride = static_cast<int64_t>(nmod) * plane_bytes;
+    auto store = [&](int8_t* dst, const uint32_t (&w)[EPT / 4]) {
+        if constexpr (EPT == 16) *reinterpret_cast<uint4*>(dst) = make_uint4(w[0], w[1], w[2], w[3]);
+        else *reinterpret_cast<uint2*>(dst) = make_uint2(w[0], w[1]);
+    };
     if (r >= rows || k0 >= k) {  // padding: residues of zero are zero
-        const uint4 z = make_uint4(0, 0, 0, 0);
+        const uint32_t z[EPT / 4] = {};
         for (int t = 0; t < nmod; ++t) {
-            *reinterpret_cast<uint4*>(out + t * plane_bytes) = z;
+            store(out + t * plane_bytes, z);
             if (CPLX) {
-                *reinterpret_cast<uint4*>(out + gstride + t * plane_bytes) = z;
-                *reinterpret_cast<uint4*>(out + 2 * gstride + t * plane_bytes) = z;
+                store(out + gstride + t * plane_bytes, z);
+                store(out + 2 * gstride + t * plane_bytes, z);
             }
         }
         return;
@@ -182,11 +196,11 @@ __global__ void __launch_bounds__(256) split_kernel(const SplitItem* __restrict_
     const bool live = e != kNonFinite;
 
     constexpr int NG = CPLX ? 2 : 1;
-    uint32_t L[NG][16][NLIMB];
+    uint32_t L[NG][EPT][NLIMB];
     const int e1 = e >> 1;
     const double s1 = pow2(live ? e1 : 0), s2 = pow2(live ? e - e1 : 0);
 #pragma unroll
-    for (int q = 0; q < 16; ++q) {
+    for (int q = 0; q < EPT; ++q) {
         const int64_t p = k0 + q;
         double v0 = 0.0, v1 = 0.0;
         if (live && p < k) {
@@ -210,11 +224,11 @@ __global__ void __launch_bounds__(256) split_kernel(const SplitItem* __restrict_
 
     for (int t = 0; t < nmod; ++t) {
         const ModConst mc = I->mc[t];
-        uint32_t b0[16], b1[16], b2[16];  // residue bytes in the low 8 bits
+        uint32_t b0[EPT], b1[EPT], b2[EPT];  // residue bytes in the low 8 bits
         if (mc.m == 256) {
             // 2^21 j = 0 mod 256 and 2^62 = 0 mod 256: the residue byte is the low byte of 2^62 + x
 #pragma unroll
-            for (int q = 0; q < 16; ++q) {
+            for (int q = 0; q < EPT; ++q) {
                 b0[q] = L[0][q][0];
                 if (CPLX) {
                     b1[q] = L[NG - 1][q][0];
@@ -223,7 +237,7 @@ __global__ void __launch_bounds__(256) split_kernel(const SplitItem* __restrict_
             }
         } else {
 #pragma unroll
-            for (int q = 0; q < 16; ++q) {
+            for (int q = 0; q < EPT; ++q) {
                 const int s0 = sym_residue<NLIMB>(L[0][q], mc);
                 b0[q] = static_cast<uint32_t>(s0);
                 if (CPLX) {
@@ -237,19 +251,19 @@ __global__ void __launch_bounds__(256) split_kernel(const SplitItem* __restrict_
                 }
             }
         }
-        uint32_t w0[4], w1[4], w2[4];
+        uint32_t w0[EPT / 4], w1[EPT / 4], w2[EPT / 4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < EPT / 4; ++q) {
             w0[q] = pack_bytes(b0[4 * q], b0[4 * q + 1], b0[4 * q + 2], b0[4 * q + 3]);
             if (CPLX) {
                 w1[q] = pack_bytes(b1[4 * q], b1[4 * q + 1], b1[4 * q + 2], b1[4 * q + 3]);
                 w2[q] = pack_bytes(b2[4 * q], b2[4 * q + 1], b2[4 * q + 2], b2[4 * q + 3]);
             }
         }
-        *reinterpret_cast<uint4*>(out + t * plane_bytes) = make_uint4(w0[0], w0[1], w0[2], w0[3]);
+        store(out + t * plane_bytes, w0);
         if (CPLX) {
-            *reinterpret_cast<uint4*>(out + gstride + t * plane_bytes) = make_uint4(w1[0], w1[1], w1[2], w1[3]);
-            *reinterpret_cast<uint4*>(out + 2 * gstride + t * plane_bytes) = make_uint4(w2[0], w2[1], w2[2], w2[3]);
+            store(out + gstride + t * plane_bytes, w1);
+            store(out + 2 * gstride + t * plane_bytes, w2);
         }
     }
 }
@@ -286,12 +300,14 @@ int64_t scale_item_blocks(ScaleItem& it, int num_sms, int64_t block0) {
 
 int64_t split_item_blocks(SplitItem& it, int64_t block0) {
     it.block0 = block0;
+    const int ept = it.tk > kNarrowScaleBits || it.cplx ? split_ept<5, false>() : split_ept<3, false>();
+    const int64_t kpad = it.kb_total * kTileK;  // inner indices of the plane, padding included
     if (it.row_contig) {
         it.rblocks = ceil_div(it.rows_pad, 32);
-        it.kblocks = it.kb_total;
+        it.kblocks = ceil_div(kpad, 8 * ept);
     } else {
         it.rblocks = ceil_div(it.rows_pad, 8);
-        it.kblocks = ceil_div(it.kb_total, 4);
+        it.kblocks = ceil_div(kpad, 32 * ept);
     }
     return it.rblocks * it.kblocks;
 }
