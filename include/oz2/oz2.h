@@ -95,9 +95,11 @@ int oz2_autotune_grouped(oz2_handle h, int count, const oz2_dgemm_problem* probl
  * 512), s comes from
  *   mode 0: the MLP (oz2_mlp_set_weights; a tile takes the largest class over itself and its
  *           up to 8 neighbours in the problem), capped by the analytic s, for problems with
- *           beta = 0 (others take the analytic s); tiles below their analytic s are probed (C x
- *           against A (B x) with x = e_j for 8 columns j, each entry checked) and rerun at the
- *           analytic s when the probe fails; without weights it behaves as mode 1
+ *           beta = 0 (others take the analytic s); a problem whose tiles then differ by at most
+ *           one takes the largest for all; tiles below their analytic s are probed (C x against
+ *           A (B x) with x = e_j for 8 columns j, each entry checked) and rerun at the analytic s
+ *           when the probe fails; without weights it behaves as mode 1
+ * A problem whose tiles all share one s runs as one task (as a plain call would).
  *   mode 1: the analytic s of the tile: smallest s whose tk >= R + 2 + t - floor(log2(k - 1)),
  *           R the largest exponent gap below the row / column maximum in the tile's panels
  *   mode 2: the analytic s of the whole problem (the largest over its tiles)

@@ -122,6 +122,11 @@ struct oz2_context {
     cublasHandle_t cublas = nullptr;  // native FP64 GEMM of tiles no moduli set brings to the target
     cudaStream_t cublas_stream = nullptr;
     bool cublas_bound = false;        // cublas_stream is set on the handle
+    // native tiles run on their own stream, beside the emulation of the other tiles
+    cudaStream_t nat_stream = nullptr;
+    cudaEvent_t nat_fork = nullptr, nat_join = nullptr, nat_t0 = nullptr, nat_t1 = nullptr;
+    bool nat_pending = false;         // the caller's stream must still wait for nat_join
+    double native_ms = 0.0;           // device time of the last call's native tiles (profiling)
     int64_t launches = 0;  // kernels launched through this handle (graph replays included)
     bool capture_ok = true;           // false when part of the call ran outside the graphs
     std::string err;
@@ -835,7 +840,7 @@ int ensure_ws2(oz2_context* h, size_t bytes) {
 
 // C[i0:i0+mb, j0:j0+nb] = alpha op(A) op(B) + beta C in native FP64 (cuBLAS DGEMM, default math:
 // no emulation), for tiles whose inputs span more exponent range than 24 moduli cover
-int native_gemm(oz2_context* h, const Prob& p, int64_t i0, int64_t j0, int64_t mb, int64_t nb) {
+int native_gemm(oz2_context* h, cudaStream_t st, const Prob& p, int64_t i0, int64_t j0, int64_t mb, int64_t nb) {
     if (!h->cublas) {
         if (cublasCreate(&h->cublas) != CUBLAS_STATUS_SUCCESS) {
             h->cublas = nullptr;
@@ -845,10 +850,10 @@ int native_gemm(oz2_context* h, const Prob& p, int64_t i0, int64_t j0, int64_t m
         h->cublas_bound = false;
     }
     // setting the stream resets cuBLAS's workspace: only when the stream changed
-    if (!h->cublas_bound || h->cublas_stream != h->stream) {
-        if (cublasSetStream(h->cublas, h->stream) != CUBLAS_STATUS_SUCCESS)
+    if (!h->cublas_bound || h->cublas_stream != st) {
+        if (cublasSetStream(h->cublas, st) != CUBLAS_STATUS_SUCCESS)
             return fail(h, OZ2_ECUDA, "oz2: cublasSetStream failed");
-        h->cublas_stream = h->stream;
+        h->cublas_stream = st;
         h->cublas_bound = true;
     }
     const double* A = p.A + (is_n(p.ta) ? i0 : i0 * p.lda);
@@ -860,6 +865,29 @@ int native_gemm(oz2_context* h, const Prob& p, int64_t i0, int64_t j0, int64_t m
                                              p.ldb, &be, C, p.ldc);
     if (cs != CUBLAS_STATUS_SUCCESS) return fail(h, OZ2_ECUDA, "oz2: native FP64 GEMM failed");
     ++h->launches;
+    return OZ2_OK;
+}
+
+// opens the native stream's part of a call: it starts after everything issued so far
+int native_fork(oz2_context* h) {
+    if (!h->nat_stream) {
+        OZ2_CUDA(h, cudaStreamCreateWithFlags(&h->nat_stream, cudaStreamNonBlocking));
+        OZ2_CUDA(h, cudaEventCreateWithFlags(&h->nat_fork, cudaEventDisableTiming));
+        OZ2_CUDA(h, cudaEventCreateWithFlags(&h->nat_join, cudaEventDisableTiming));
+        OZ2_CUDA(h, cudaEventCreate(&h->nat_t0));
+        OZ2_CUDA(h, cudaEventCreate(&h->nat_t1));
+    }
+    OZ2_CUDA(h, cudaEventRecord(h->nat_fork, h->stream));
+    OZ2_CUDA(h, cudaStreamWaitEvent(h->nat_stream, h->nat_fork, 0));
+    return OZ2_OK;
+}
+
+// the caller's stream waits for the native tiles
+int native_join(oz2_context* h) {
+    if (!h->nat_pending) return OZ2_OK;
+    h->nat_pending = false;
+    OZ2_CUDA(h, cudaEventRecord(h->nat_join, h->nat_stream));
+    OZ2_CUDA(h, cudaStreamWaitEvent(h->stream, h->nat_join, 0));
     return OZ2_OK;
 }
 
@@ -1073,6 +1101,19 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
         while (sv < kMaxModuli && tk[sv] == 0) ++sv;
         s_tile[t] = std::max(2, std::min(kMaxModuli, sv));
     }
+    if (use_mlp) {
+        // a problem whose tiles' s differ by at most one (none native) takes the largest for all
+        // of them: it then runs as one task, its panels split once
+        std::vector<int> lo(base.size(), kNativeS), hi(base.size(), 0);
+        for (int64_t t = 0; t < ntiles; ++t) {
+            lo[tiles[t].prob] = std::min(lo[tiles[t].prob], s_tile[t]);
+            hi[tiles[t].prob] = std::max(hi[tiles[t].prob], s_tile[t]);
+        }
+        for (int64_t t = 0; t < ntiles; ++t) {
+            const int q = tiles[t].prob;
+            if (hi[q] <= kMaxModuli && hi[q] - lo[q] <= 1) s_tile[t] = hi[q];
+        }
+    }
 
     // ---- phase 2: tiles with their s, panels split once per (panel, s); batches by budget
     std::vector<int64_t> prob_tiles(base.size(), 0), native_count(base.size(), 0);
@@ -1091,7 +1132,11 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
             }
         }
         if (!native.empty()) {
-            mark(h, kBegin);
+            // no emulated tile shares data with them: they run beside the rest of the call
+            int stf = native_fork(h);
+            if (stf) return stf;
+            h->nat_pending = true;
+            if (h->profiling) OZ2_CUDA(h, cudaEventRecord(h->nat_t0, h->nat_stream));
             std::fill(native_count.begin(), native_count.end(), 0);
             for (int64_t t : native) ++native_count[tiles[t].prob];
             std::vector<bool> whole_done(base.size(), false);
@@ -1104,13 +1149,19 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
                 if (native_count[r.prob] == prob_tiles[r.prob]) {
                     if (whole_done[r.prob]) continue;
                     whole_done[r.prob] = true;
-                    st2 = native_gemm(h, p, 0, 0, p.m, p.n);
+                    st2 = native_gemm(h, h->nat_stream, p, 0, 0, p.m, p.n);
                 } else {
-                    st2 = native_gemm(h, p, r.i0, r.j0, r.mb, r.nb);
+                    st2 = native_gemm(h, h->nat_stream, p, r.i0, r.j0, r.mb, r.nb);
                 }
                 if (st2) return st2;
             }
-            mark(h, kNative);
+            if (h->profiling) {
+                OZ2_CUDA(h, cudaEventRecord(h->nat_t1, h->nat_stream));
+                OZ2_CUDA(h, cudaEventSynchronize(h->nat_t1));
+                float ms = 0.0f;
+                OZ2_CUDA(h, cudaEventElapsedTime(&ms, h->nat_t0, h->nat_t1));
+                h->native_ms += ms;
+            }
         }
         std::vector<std::unique_ptr<Prob>> probs;  // one per (problem, s)
         std::map<std::pair<int, int>, Prob*> prob_for;
@@ -1136,9 +1187,36 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
             const size_t reserve = (size_t{512} << 20) + total / 32;
             limit = free_b > reserve ? free_b - reserve : 0;
         }
+        // a problem whose tiles all run here at one s is one task: its GEMM jobs then share the
+        // planes through the L2 across the whole problem, as in a plain call
+        struct Unit {
+            int64_t tile;  // -1: the whole problem
+            int prob, s;
+        };
+        std::vector<Unit> units;
+        {
+            std::vector<int> common(base.size(), 0);  // 0 unseen, -1 mixed, else the s
+            std::vector<int64_t> seen(base.size(), 0);
+            for (size_t u = 0; u < which.size(); ++u) {
+                const int q = tiles[which[u]].prob;
+                common[q] = seen[q] == 0 ? svals[u] : (common[q] == svals[u] ? common[q] : -1);
+                ++seen[q];
+            }
+            std::vector<bool> emitted(base.size(), false);
+            for (size_t u = 0; u < which.size(); ++u) {
+                const int q = tiles[which[u]].prob;
+                const bool whole = prob_tiles[q] > 1 && seen[q] == prob_tiles[q] && common[q] > 0;
+                if (!whole) {
+                    units.push_back(Unit{which[u], q, svals[u]});
+                } else if (!emitted[q]) {
+                    emitted[q] = true;
+                    units.push_back(Unit{-1, q, common[q]});
+                }
+            }
+        }
         size_t i = 0;
-        while (i < which.size()) {
-            // one batch: tiles until the budget is reached
+        while (i < units.size()) {
+            // one batch: units until the budget is reached
             std::map<std::tuple<int, int, int>, std::pair<size_t, bool>> panels;  // (panel, side, s) -> offset
             size_t off2 = 0;
             auto carve2 = [&](size_t bytes) {
@@ -1146,23 +1224,34 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
                 off2 += align256(bytes);
                 return o;
             };
-            std::vector<std::tuple<int64_t, size_t, size_t, size_t>> batch;  // tile, A planes, B planes, resid
+            struct Slot {
+                size_t a, b, r;  // offsets of the A planes, B planes and residues
+            };
+            std::vector<Slot> batch;
             size_t start = i;
-            for (; i < which.size(); ++i) {
-                const int64_t t = which[i];
-                const TileRef& r = tiles[t];
-                const int sv = svals[i];
-                const Prob& p = base[r.prob];
-                const size_t pa = static_cast<size_t>(sv) * plane_geom(r.mb, p.k, kGemmIPad).plane_bytes;
-                const size_t pb = static_cast<size_t>(sv) * plane_geom(r.nb, p.k, kGemmJ).plane_bytes;
-                const size_t rs = static_cast<size_t>(sv) * r.nb * round_up(r.mb, 32);
+            for (; i < units.size(); ++i) {
+                const Unit& un = units[i];
+                const int sv = un.s;
+                const Prob& p = base[un.prob];
+                const int64_t mb = un.tile < 0 ? p.m : tiles[un.tile].mb, nb = un.tile < 0 ? p.n : tiles[un.tile].nb;
+                const size_t pa = static_cast<size_t>(sv) * plane_geom(mb, p.k, kGemmIPad).plane_bytes;
+                const size_t pb = static_cast<size_t>(sv) * plane_geom(nb, p.k, kGemmJ).plane_bytes;
+                const size_t rs = static_cast<size_t>(sv) * nb * round_up(mb, 32);
+                const size_t items = 2 * sizeof(SplitItem) + sizeof(GemmItem) + sizeof(CrtItem) + 2048;
+                if (un.tile < 0) {
+                    const size_t add = align256(pa) + align256(pb) + align256(rs) + items;
+                    if (i > start && off2 + add + (1 << 20) > limit) break;
+                    const size_t oa = carve2(pa), ob = carve2(pb);
+                    batch.push_back(Slot{oa, ob, carve2(rs)});
+                    continue;
+                }
+                const TileRef& r = tiles[un.tile];
                 const bool newa = !panels.count({r.ia, 0, sv}), newb = !panels.count({r.jb, 1, sv});
-                const size_t add = (newa ? align256(pa) : 0) + (newb ? align256(pb) : 0) + align256(rs) +
-                                   2 * sizeof(SplitItem) + sizeof(GemmItem) + sizeof(CrtItem) + 2048;
+                const size_t add = (newa ? align256(pa) : 0) + (newb ? align256(pb) : 0) + align256(rs) + items;
                 if (i > start && off2 + add + (1 << 20) > limit) break;
                 if (newa) panels[{r.ia, 0, sv}] = {carve2(pa), true};
                 if (newb) panels[{r.jb, 1, sv}] = {carve2(pb), true};
-                batch.emplace_back(t, panels[{r.ia, 0, sv}].first, panels[{r.jb, 1, sv}].first, carve2(rs));
+                batch.push_back(Slot{panels[{r.ia, 0, sv}].first, panels[{r.jb, 1, sv}].first, carve2(rs)});
             }
             const size_t obase_desc = off2;
             const size_t need = off2 + align256(batch.size() * (2 * sizeof(SplitItem) + sizeof(GemmItem) +
@@ -1172,30 +1261,38 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
             std::vector<Task> tasks;
             std::map<std::tuple<int, int, int>, bool> split_done;
             for (size_t b = 0; b < batch.size(); ++b) {
-                const int64_t t = std::get<0>(batch[b]);
-                const TileRef& r = tiles[t];
-                const int sv = svals[start + b];
-                Prob* p = get_prob(r.prob, sv);
+                const Unit& un = units[start + b];
+                const int sv = un.s;
+                Prob* p = get_prob(un.prob, sv);
                 if (!p) return fail(h, OZ2_EINTERNAL, "oz2: no plan for adaptive tile");
                 Task tk{};
                 tk.p = p;
-                tk.i0 = r.i0;
-                tk.j0 = r.j0;
-                tk.mb = r.mb;
-                tk.nb = r.nb;
-                tk.split_a = !split_done[{r.ia, 0, sv}];
-                tk.split_b = !split_done[{r.jb, 1, sv}];
-                split_done[{r.ia, 0, sv}] = true;
-                split_done[{r.jb, 1, sv}] = true;
-                tk.maxA = maxA(r.prob);
-                tk.maxB = maxB(r.prob);
-                tk.planesA = reinterpret_cast<int8_t*>(h->ws2 + std::get<1>(batch[b]));
-                tk.planesB = reinterpret_cast<int8_t*>(h->ws2 + std::get<2>(batch[b]));
-                tk.resid = h->ws2 + std::get<3>(batch[b]);
-                tk.ldr = round_up(r.mb, 32);
+                if (un.tile < 0) {
+                    tk.i0 = tk.j0 = 0;
+                    tk.mb = p->m;
+                    tk.nb = p->n;
+                    tk.split_a = tk.split_b = true;
+                    h->astats[1] += static_cast<int64_t>(sv) * prob_tiles[un.prob];
+                } else {
+                    const TileRef& r = tiles[un.tile];
+                    tk.i0 = r.i0;
+                    tk.j0 = r.j0;
+                    tk.mb = r.mb;
+                    tk.nb = r.nb;
+                    tk.split_a = !split_done[{r.ia, 0, sv}];
+                    tk.split_b = !split_done[{r.jb, 1, sv}];
+                    split_done[{r.ia, 0, sv}] = true;
+                    split_done[{r.jb, 1, sv}] = true;
+                    h->astats[1] += sv;
+                }
+                tk.maxA = maxA(un.prob);
+                tk.maxB = maxB(un.prob);
+                tk.planesA = reinterpret_cast<int8_t*>(h->ws2 + batch[b].a);
+                tk.planesB = reinterpret_cast<int8_t*>(h->ws2 + batch[b].b);
+                tk.resid = h->ws2 + batch[b].r;
+                tk.ldr = round_up(tk.mb, 32);
                 tasks.push_back(tk);
-                h->astats[1] += sv;
-                h->astats[7] += static_cast<int64_t>(sv) * r.mb * r.nb * base[r.prob].k;
+                h->astats[7] += static_cast<int64_t>(sv) * tk.mb * tk.nb * base[un.prob].k;
             }
             std::vector<const Prob*> bp;
             for (auto& up : probs) bp.push_back(up.get());
@@ -1372,6 +1469,9 @@ int oz2_destroy(oz2_handle h) {
     if (h->d_mlp) cudaFree(h->d_mlp);
     if (h->ws2) cudaFree(h->ws2);
     if (h->cublas) cublasDestroy(h->cublas);
+    if (h->nat_stream) cudaStreamDestroy(h->nat_stream);
+    for (cudaEvent_t e : {h->nat_fork, h->nat_join, h->nat_t0, h->nat_t1})
+        if (e) cudaEventDestroy(e);
     delete h;
     return OZ2_OK;
 }
@@ -1509,7 +1609,11 @@ int oz2_dgemm_adaptive(oz2_handle h, int count, const oz2_dgemm_problem* problem
         }
     }
     for (int q = 0; q < kAdaptiveStats; ++q) h->astats[q] = 0;
-    if (!probs.empty() && (st = run_adaptive(h, probs, fixed_s, target_bits, mode))) return st;
+    h->native_ms = 0.0;
+    if (!probs.empty()) st = run_adaptive(h, probs, fixed_s, target_bits, mode);
+    const int sj = native_join(h);  // on every path: the stream must cover the native tiles
+    if (st) return st;
+    if (sj) return sj;
     if (stats)
         for (int q = 0; q < kAdaptiveStats; ++q) stats[q] = h->astats[q];
     return end_call(h, nullptr);
@@ -1810,7 +1914,9 @@ int oz2_stage_times(oz2_handle h, double* out4) {
 int oz2_adaptive_stage_times(oz2_handle h, double* out2) {
     if (!h || !out2) return fail(h, OZ2_EINVAL, "oz2: null argument");
     out2[0] = out2[1] = 0.0;
-    if (!h->profiling || h->marks.empty()) return OZ2_OK;
+    if (!h->profiling) return OZ2_OK;
+    out2[1] = h->native_ms;
+    if (h->marks.empty()) return OZ2_OK;
     OZ2_CUDA(h, cudaEventSynchronize(h->marks.back().second));
     for (size_t i = 1; i < h->marks.size(); ++i) {
         const int stg = h->marks[i].first;
