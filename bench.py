@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--size", type=int, default=8192, help="m = n = k of the DGEMM extra")
     ap.add_argument("--s", type=int, default=16, help="moduli of the DGEMM extra")
     ap.add_argument("--no-extras", action="store_true", help="skip the DGEMM, grouped and CPU legs")
+    ap.add_argument("--dgemm-only", action="store_true",
+                    help="time only the DGEMM of --size and --s (a profiling aid; not the headline)")
     return ap.parse_args()
 
 
@@ -520,6 +522,14 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream()
+    if a.dgemm_only:
+        out = dgemm_leg(a, oz2, torch, dev, stream, rank)
+        if rank == 0:
+            print(json.dumps({"dgemm_only": out}), flush=True)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     oz = oz2.Ozaki2(stream)
     model = oz.load_model()
     ref_rule = oz2.Ozaki2.moduli_for_bits

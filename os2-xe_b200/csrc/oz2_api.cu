@@ -409,7 +409,7 @@ void plan_tasks(Program& prog, const std::vector<Task>& tasks, const GemmConfig&
         for (int q = 0; q < g.s; ++q) {
             g.mod_m[q] = mc[q].m;
             g.mod_mu[q] = mc[q].mu;
-            g.mod_kneg[q] = mc[q].kneg;
+            g.mod_kbias[q] = mc[q].kbias;
         }
         jobs += g.tiles * p.G * g.s;
         gi.push_back(g);

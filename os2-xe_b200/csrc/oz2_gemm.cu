@@ -7,14 +7,16 @@
 // per entry, so the CRT phase reads 1 byte per entry and modulus.
 //
 // Persistent kernel over a table of problems (one emulated GEMM, or a group of them), one CTA
-// per SM, 6 warps:
+// per SM, 10 warps:
 //   warp 0   producer: 1-D bulk copies of pre-tiled 16 KiB plane tiles into a 4-stage ring
 //   warp 1   MMA issuer: tcgen05.mma kind::i8, M=128 (columns j of C), N=BN (rows i of C,
 //            BN = 256 or 128), K=32 per instruction, int32 accumulators in TMEM (2 x BN
 //            columns, double buffer); k beyond 130944 runs as chunks inside one job, each chunk
 //            adding its residues to the previous ones mod m
-//   warps 2-5 epilogue: tcgen05.ld 32 lanes x 32 columns, c mod m_t, 32 residue bytes per
-//            thread and chunk stored to residue plane row j (i contiguous)
+//   warps 2-9 epilogue, two per TMEM lane quarter, each half of the BN columns: tcgen05.ld
+//            32 lanes x 32 columns (the next load in flight during the arithmetic), c mod m_t
+//            as (c + m ceil(2^31/m)) mod m with one Barrett step, 32 residue bytes per thread
+//            and chunk stored to residue plane row j (i contiguous)
 // Every mbarrier wait is time-bounded; on expiry the kernel records an error code, drains its
 // in-flight copies and MMAs, frees TMEM and returns.
 #include <algorithm>
@@ -27,6 +29,8 @@ namespace oz2 {
 namespace {
 
 constexpr uint32_t kBarBytes = 256;
+constexpr int kEpiWarps = 8;                       // two per TMEM lane quarter
+constexpr int kGemmThreads = 64 + 32 * kEpiWarps;  // producer, MMA issuer, epilogue
 
 template <int BN>
 struct Cfg {
@@ -78,7 +82,7 @@ __device__ __forceinline__ Job decode(const GemmParams& P, int64_t job) {
 }
 
 template <int BN>
-__global__ void __launch_bounds__(192, 1) gemm_i8_modm_kernel(const __grid_constant__ GemmParams P) {
+__global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __grid_constant__ GemmParams P) {
     using C = Cfg<BN>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t{1023});
@@ -101,7 +105,7 @@ __global__ void __launch_bounds__(192, 1) gemm_i8_modm_kernel(const __grid_const
         }
         for (int a = 0; a < 2; ++a) {
             dev::mbar_init(acc_full(a), 1);
-            dev::mbar_init(acc_empty(a), 4);
+            dev::mbar_init(acc_empty(a), kEpiWarps);
         }
         dev::mbar_init(drain, 1);
         *abort_flag = 0;
@@ -201,13 +205,15 @@ __global__ void __launch_bounds__(192, 1) gemm_i8_modm_kernel(const __grid_const
             }
         }
     } else {
-        const int quarter = warp & 3;  // TMEM lanes this warp may access
+        const int quarter = warp & 3;           // TMEM lanes this warp may access
+        const int half = (warp - 2) >> 2;       // which half of the BN columns
+        constexpr int kChunks = BN / 64;        // 32-column chunks per warp
         int local = 0;
         bool ok = true;
         for (int64_t job = blockIdx.x; ok && job < P.jobs; job += nprog) {
             const Job J = decode(P, job);
             const int t = J.gt % J.I->s;
-            const uint32_t m = J.I->mod_m[t], mu = J.I->mod_mu[t], kneg = J.I->mod_kneg[t];
+            const uint32_t m = J.I->mod_m[t], mu = J.I->mod_mu[t], kbias = J.I->mod_kbias[t];
             const int64_t j = static_cast<int64_t>(J.tj) * kGemmJ + quarter * 32 + lane;
             const int64_t mm = J.I->m, nn = J.I->n;
             uint8_t* row = J.I->resid + J.gt * J.I->rstride + j * J.I->ldr;
@@ -224,43 +230,45 @@ __global__ void __launch_bounds__(192, 1) gemm_i8_modm_kernel(const __grid_const
                 dev::tc_fence_after();
                 const bool accumulate = c > 0;
                 const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) +
-                                       static_cast<uint32_t>(acc) * BN;
-#pragma unroll 1
-                for (int cc = 0; cc < BN / 32; ++cc) {
-                    uint32_t v[32];
-                    dev::tmem_load_32x32(taddr + cc * 32, v);
-                    dev::tmem_load_wait();
-                    const int64_t i0 = static_cast<int64_t>(J.ti) * BN + cc * 32;
+                                       static_cast<uint32_t>(acc) * BN + static_cast<uint32_t>(half * kChunks * 32);
+                uint32_t v[2][32];
+                dev::tmem_load_32x32(taddr, v[0]);
+                dev::tmem_load_wait();
+#pragma unroll
+                for (int cc = 0; cc < kChunks; ++cc) {
+                    uint32_t(&cur)[32] = v[cc & 1];
+                    // the next chunk's load is in flight during this chunk's arithmetic
+                    if (cc + 1 < kChunks) dev::tmem_load_32x32(taddr + (cc + 1) * 32, v[(cc + 1) & 1]);
+                    const int64_t i0 = static_cast<int64_t>(J.ti) * BN + (half * kChunks + cc) * 32;
                     if (j < nn && i0 < mm) {
-                        uint32_t w[8];
-                        uint4 old0 = make_uint4(0, 0, 0, 0), old1 = old0;
+                        uint32_t ow[8] = {0, 0, 0, 0, 0, 0, 0, 0};
                         if (accumulate) {
-                            old0 = *reinterpret_cast<const uint4*>(row + i0);
-                            old1 = *reinterpret_cast<const uint4*>(row + i0 + 16);
+                            const uint4 o0 = *reinterpret_cast<const uint4*>(row + i0);
+                            const uint4 o1 = *reinterpret_cast<const uint4*>(row + i0 + 16);
+                            ow[0] = o0.x; ow[1] = o0.y; ow[2] = o0.z; ow[3] = o0.w;
+                            ow[4] = o1.x; ow[5] = o1.y; ow[6] = o1.z; ow[7] = o1.w;
                         }
-                        const uint32_t ow[8] = {old0.x, old0.y, old0.z, old0.w, old1.x, old1.y, old1.z, old1.w};
+                        uint32_t w[8];
 #pragma unroll
                         for (int q = 0; q < 8; ++q) {
-                            uint32_t word = 0;
+                            uint32_t r4[4];
 #pragma unroll
                             for (int b = 0; b < 4; ++b) {
-                                const uint32_t u = v[4 * q + b] + 0x80000000u;  // int32 c + 2^31
-                                const uint32_t qq = __umulhi(u, mu);
-                                uint32_t r = u - qq * m;
-                                r = min(r, r - m);  // (c + 2^31) mod m
-                                r += kneg;
-                                r = min(r, r - m);  // c mod m
+                                const uint32_t u = cur[4 * q + b] + kbias;  // c + m ceil(2^31/m), in [0, 2^32)
+                                uint32_t r = u - __umulhi(u, mu) * m;      // in [0, 2m)
+                                r = min(r, r - m);
                                 if (accumulate) {
-                                    r += (ow[q] >> (8 * b)) & 0xFFu;
+                                    r += __byte_perm(ow[q], 0, 0x4440 + b);
                                     r = min(r, r - m);
                                 }
-                                word |= r << (8 * b);
+                                r4[b] = r;
                             }
-                            w[q] = word;
+                            w[q] = __byte_perm(__byte_perm(r4[0], r4[1], 0x0040), __byte_perm(r4[2], r4[3], 0x0040), 0x5410);
                         }
                         *reinterpret_cast<uint4*>(row + i0) = make_uint4(w[0], w[1], w[2], w[3]);
                         *reinterpret_cast<uint4*>(row + i0 + 16) = make_uint4(w[4], w[5], w[6], w[7]);
                     }
+                    if (cc + 1 < kChunks) dev::tmem_load_wait();
                 }
                 dev::tc_fence_before();
                 __syncwarp();
@@ -279,7 +287,7 @@ __global__ void __launch_bounds__(192, 1) gemm_i8_modm_kernel(const __grid_const
 
 template <int BN>
 void launch_bn(const GemmParams& P, int grid, cudaStream_t st) {
-    gemm_i8_modm_kernel<BN><<<grid, 192, Cfg<BN>::kSmemBytes, st>>>(P);
+    gemm_i8_modm_kernel<BN><<<grid, kGemmThreads, Cfg<BN>::kSmemBytes, st>>>(P);
 }
 
 }  // namespace

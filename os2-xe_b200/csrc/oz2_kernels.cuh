@@ -85,7 +85,7 @@ struct GemmItem {
     int64_t pstride_i, pstride_j, rstride, ldr, m, n, kb_total;
     int64_t tiles, job0;
     int tiles_i, tiles_j, s, groups;
-    uint32_t mod_m[kMaxModuli], mod_mu[kMaxModuli], mod_kneg[kMaxModuli];
+    uint32_t mod_m[kMaxModuli], mod_mu[kMaxModuli], mod_kbias[kMaxModuli];
 };
 
 // ---- crt: one item per problem; all items of a launch share s

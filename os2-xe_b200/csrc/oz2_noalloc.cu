@@ -207,7 +207,7 @@ extern "C" int oz2_dgemm_noalloc(void* stream, char ta, char tb, int64_t m, int6
     for (int t = 0; t < s; ++t) {
         g.mod_m[t] = mc[t].m;
         g.mod_mu[t] = mc[t].mu;
-        g.mod_kneg[t] = mc[t].kneg;
+        g.mod_kbias[t] = mc[t].kbias;
     }
     CrtItem& c = T.c;
     c.resid = resid;

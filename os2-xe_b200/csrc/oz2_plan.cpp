@@ -187,7 +187,7 @@ void mod_constants(const Plan& p, ModConst* out) {
         for (int j = 1; j <= 4; ++j) c.c[j - 1] = pow2_mod(21 * j, m);
         c.koff3 = (h + m - pow2_mod(62, m)) % m;
         c.koff5 = (h + m - pow2_mod(104, m)) % m;
-        c.kneg = (m - pow2_mod(31, m)) % m;
+        c.kbias = m * static_cast<uint32_t>(((uint64_t{1} << 31) + m - 1) / m);
     }
 }
 

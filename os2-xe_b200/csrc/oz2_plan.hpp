@@ -34,7 +34,8 @@ struct ModConst {
     uint32_t c[4];   // 2^(21 j) mod m, j = 1..4 (21-bit limb weights)
     uint32_t koff3;  // (h - 2^62 mod m) mod m: narrow limb offset (tk <= 62)
     uint32_t koff5;  // (h - 2^104 mod m) mod m: wide limb offset
-    uint32_t kneg;   // (m - 2^31 mod m) mod m: undoes the +2^31 bias of a signed int32
+    uint32_t kbias;  // m ceil(2^31 / m): c + kbias is in [0, 2^32) for every int32 GEMM sum c
+                     // (|c| < 2^31 - 2^21) and congruent to c modulo m
 };
 
 struct Plan {
