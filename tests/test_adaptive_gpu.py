@@ -346,3 +346,41 @@ def test_accuracy_metrics_match_the_oracle(oracle, az):
         want = oracle.metrics(dC.cpu().numpy(), hi.cpu().numpy(), lo.cpu().numpy())
         assert abs(u - want["ulp_max"]) <= 1e-6 * max(1.0, want["ulp_max"])
         assert c == round(want["cr_frac"] * m * n)
+
+
+def test_native_tiles_keep_alpha_beta(az):
+    """tiles sent to native FP64 (phi = 8, row offsets) with alpha and beta != 0: C is alpha A B +
+    beta C within the DGEMM-level bound plus the rounding of the update"""
+    import torch
+    m, n, k = 900, 700, 800
+    A, B = nn_problem(131, m, n, k, 8.0, 40)
+    dA, dB = to_dev(A), to_dev(B)
+    C0 = torch.rand(m * n, dtype=torch.float64, device="cuda") - 0.5
+    dC = C0.clone()
+    st = az.gemm_adaptive([("N", "N", m, n, k, -1.25, dA, m, dB, k, 0.75, dC, m, 16)], 53, az.ADAPTIVE_ANALYTIC_TILE)
+    assert st["native_tiles"] > 0
+    hi = torch.empty(m * n, dtype=torch.float64, device="cuda")
+    lo, ab = torch.empty_like(hi), torch.empty_like(hi)
+    az.dd_reference(m, n, k, dA, m, dB, k, hi, lo, ab)
+    want = -1.25 * hi + 0.75 * C0
+    err = (dC - want - (-1.25) * lo).abs()
+    tol = 1.25 * k * 2.0 ** -53 * ab + 2.0 ** -51 * (want.abs() + (0.75 * C0).abs()) + 1e-300
+    assert bool((err <= tol).all())
+
+
+def test_ops_do_not_change_adaptive_results(az):
+    """mode 1 with op(A) = T and op(B) = T on explicitly transposed copies equals the NN call bit
+    for bit (statistics, features and s are functions of op(A) rows and op(B) columns)"""
+    import torch
+    m, n, k = 700, 1100, 600
+    A, B = nn_problem(141, m, n, k, 3.0, 20)
+    dA, dB = to_dev(A), to_dev(B)
+    dAt, dBt = to_dev(np.asfortranarray(A.T)), to_dev(np.asfortranarray(B.T))
+    out = []
+    for ta, tb, AA, lda, BB, ldb in (("N", "N", dA, m, dB, k), ("T", "T", dAt, k, dBt, n), ("T", "N", dAt, k, dB, k)):
+        dC = torch.zeros(m * n, dtype=torch.float64, device="cuda")
+        st = az.gemm_adaptive([(ta, tb, m, n, k, 1.0, AA, lda, BB, ldb, 0.0, dC, m, 16)], 53, az.ADAPTIVE_ANALYTIC_TILE)
+        out.append((st["sum_s"], st["native_tiles"], dC))
+    for s_, nat, c in out[1:]:
+        assert s_ == out[0][0] and nat == out[0][1]
+        assert torch.equal(c.view(torch.int64), out[0][2].view(torch.int64))
