@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(256) crt_kernel(const __grid_constant__ CrtPar
     const int64_t rstride = I->rstride, gstride = I->gstride;
     {
         const int Ej = exponent_of(I->maxB[j], tk);
-        const uint8_t* base = I->resid + j * I->ldr + i0;
+        const uint8_t* base = I->resid + (i0 >> 5) * (32 * I->n) + j * 32 + (i0 & 31);
         // one 32-bit word per plane = the residues of the 4 entries i0..i0+3
         uint32_t w0[S], w1[CPLX ? S : 1], w2[CPLX ? S : 1];
 #pragma unroll
@@ -244,7 +244,7 @@ int64_t crt_item_blocks(CrtItem& it, int64_t block0) {
     it.block0 = block0;
     const int64_t quads = ceil_div(it.m, 4);
     int tq = 1;
-    while (tq < 256 && tq < quads) tq *= 2;  // short columns share a block
+    while (tq < 8 && tq < quads) tq *= 2;  // a warp reads 4 columns x 32 rows: one 128-byte line per plane
     it.tq = tq;
     it.jb = 256 / tq;
     it.iblocks = ceil_div(quads, tq);

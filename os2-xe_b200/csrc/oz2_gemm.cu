@@ -16,7 +16,8 @@
 //   warps 2-9 epilogue, two per TMEM lane quarter, each half of the BN columns: tcgen05.ld
 //            32 lanes x 32 columns (the next load in flight during the arithmetic), c mod m_t
 //            as (c + m ceil(2^31/m)) mod m with one Barrett step, 32 residue bytes per thread
-//            and chunk stored to residue plane row j (i contiguous)
+//            and chunk: a warp's 32 rows j x 32 columns i form one contiguous kilobyte of the
+//            residue plane (layout in oz2_kernels.cuh)
 // Every mbarrier wait is time-bounded; on expiry the kernel records an error code, drains its
 // in-flight copies and MMAs, frees TMEM and returns.
 #include <algorithm>
@@ -29,7 +30,8 @@ namespace oz2 {
 namespace {
 
 constexpr uint32_t kBarBytes = 256;
-constexpr int kEpiWarps = 8;                       // two per TMEM lane quarter
+constexpr int kEpiWarps = 8;                       // two per TMEM lane quarter (four measured slower)
+constexpr int kEpiParts = kEpiWarps / 4;           // column ranges of the accumulator
 constexpr int kGemmThreads = 64 + 32 * kEpiWarps;  // producer, MMA issuer, epilogue
 
 template <int BN>
@@ -206,8 +208,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
         }
     } else {
         const int quarter = warp & 3;           // TMEM lanes this warp may access
-        const int half = (warp - 2) >> 2;       // which half of the BN columns
-        constexpr int kChunks = BN / 64;        // 32-column chunks per warp
+        const int half = (warp - 2) >> 2;       // which part of the BN columns
+        constexpr int kChunks = BN / 32 / kEpiParts;  // 32-column chunks per warp
         int local = 0;
         bool ok = true;
         for (int64_t job = blockIdx.x; ok && job < P.jobs; job += nprog) {
@@ -216,7 +218,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
             const uint32_t m = J.I->mod_m[t], mu = J.I->mod_mu[t], kbias = J.I->mod_kbias[t];
             const int64_t j = static_cast<int64_t>(J.tj) * kGemmJ + quarter * 32 + lane;
             const int64_t mm = J.I->m, nn = J.I->n;
-            uint8_t* row = J.I->resid + J.gt * J.I->rstride + j * J.I->ldr;
+            uint8_t* rowj = J.I->resid + J.gt * J.I->rstride + j * 32;  // + (i / 32) * 32 n
             for (int64_t c = 0; c < J.nch; ++c, ++local) {
                 const int acc = local & 1;
                 const uint32_t use = static_cast<uint32_t>(local >> 1);
@@ -240,11 +242,12 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
                     // the next chunk's load is in flight during this chunk's arithmetic
                     if (cc + 1 < kChunks) dev::tmem_load_32x32(taddr + (cc + 1) * 32, v[(cc + 1) & 1]);
                     const int64_t i0 = static_cast<int64_t>(J.ti) * BN + (half * kChunks + cc) * 32;
+                    uint8_t* blk = rowj + (i0 >> 5) * (32 * nn);  // this chunk's 32 bytes of row j
                     if (j < nn && i0 < mm) {
                         uint32_t ow[8] = {0, 0, 0, 0, 0, 0, 0, 0};
                         if (accumulate) {
-                            const uint4 o0 = *reinterpret_cast<const uint4*>(row + i0);
-                            const uint4 o1 = *reinterpret_cast<const uint4*>(row + i0 + 16);
+                            const uint4 o0 = *reinterpret_cast<const uint4*>(blk);
+                            const uint4 o1 = *reinterpret_cast<const uint4*>(blk + 16);
                             ow[0] = o0.x; ow[1] = o0.y; ow[2] = o0.z; ow[3] = o0.w;
                             ow[4] = o1.x; ow[5] = o1.y; ow[6] = o1.z; ow[7] = o1.w;
                         }
@@ -265,8 +268,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
                             }
                             w[q] = __byte_perm(__byte_perm(r4[0], r4[1], 0x0040), __byte_perm(r4[2], r4[3], 0x0040), 0x5410);
                         }
-                        *reinterpret_cast<uint4*>(row + i0) = make_uint4(w[0], w[1], w[2], w[3]);
-                        *reinterpret_cast<uint4*>(row + i0 + 16) = make_uint4(w[4], w[5], w[6], w[7]);
+                        *reinterpret_cast<uint4*>(blk) = make_uint4(w[0], w[1], w[2], w[3]);
+                        *reinterpret_cast<uint4*>(blk + 16) = make_uint4(w[4], w[5], w[6], w[7]);
                     }
                     if (cc + 1 < kChunks) dev::tmem_load_wait();
                 }

@@ -81,7 +81,7 @@ struct SplitItem {
 struct GemmItem {
     const int8_t* planes_i;  // I side (op(A) rows), plane rows padded to 256
     const int8_t* planes_j;  // J side (op(B) columns), plane rows padded to 128
-    uint8_t* resid;          // residue planes [g][t][j * ldr + i]
+    uint8_t* resid;          // residue planes [g][t]; entry (i, j) at (i / 32) * 32 n + j * 32 + i % 32
     int64_t pstride_i, pstride_j, rstride, ldr, m, n, kb_total;
     int64_t tiles, job0;
     int tiles_i, tiles_j, s, groups;
