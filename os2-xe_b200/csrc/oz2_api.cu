@@ -60,11 +60,6 @@ struct Program {
         std::memcpy(blob.data() + off, p, bytes);
         return off;
     }
-    size_t reserve(size_t bytes) {
-        const size_t off = (blob.size() + 255) & ~size_t{255};
-        blob.resize(off + bytes);
-        return off;
-    }
 };
 
 // one grouped call captured for replay: an executable graph per batch of problems, the device
@@ -892,8 +887,7 @@ int native_join(oz2_context* h) {
 }
 
 // tk[s] for one k (0 where s is too small)
-void tk_table(oz2_context* h, int64_t k, int* tk) {
-    (void)h;
+void tk_table(int64_t k, int* tk) {
     for (int s = 0; s <= kMaxModuli; ++s) tk[s] = s >= 2 ? plan_tk(s, k) : 0;
 }
 
@@ -1017,7 +1011,7 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
         auto it = tk_cache.find(p.k);
         if (it == tk_cache.end()) {
             std::vector<int> tk(kMaxModuli + 1);
-            tk_table(h, p.k, tk.data());
+            tk_table(p.k, tk.data());
             it = tk_cache.emplace(p.k, tk).first;
         }
         for (int s = 0; s <= kMaxModuli; ++s) f.tk[s] = it->second[s];
@@ -1205,7 +1199,14 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
             std::vector<bool> emitted(base.size(), false);
             for (size_t u = 0; u < which.size(); ++u) {
                 const int q = tiles[which[u]].prob;
-                const bool whole = prob_tiles[q] > 1 && seen[q] == prob_tiles[q] && common[q] > 0;
+                bool whole = prob_tiles[q] > 1 && seen[q] == prob_tiles[q] && common[q] > 0;
+                if (whole) {  // and only while the whole problem fits well inside the budget
+                    const Prob& p = base[q];
+                    const size_t bytes = static_cast<size_t>(common[q]) *
+                                         (plane_geom(p.m, p.k, kGemmIPad).plane_bytes +
+                                          plane_geom(p.n, p.k, kGemmJ).plane_bytes + p.n * round_up(p.m, 32));
+                    whole = bytes <= limit / 2;
+                }
                 if (!whole) {
                     units.push_back(Unit{which[u], q, svals[u]});
                 } else if (!emitted[q]) {

@@ -384,3 +384,29 @@ def test_ops_do_not_change_adaptive_results(az):
     for s_, nat, c in out[1:]:
         assert s_ == out[0][0] and nat == out[0][1]
         assert torch.equal(c.view(torch.int64), out[0][2].view(torch.int64))
+
+
+def test_whole_problem_and_tile_tasks_agree(az):
+    """a problem whose tiles share one s runs as one task unless the workspace limit forbids it;
+    both ways give the same bits"""
+    import torch
+    import oz2
+    m = n = 2048
+    k = 1024
+    A, B = nn_problem(151, m, n, k, 1.0, 10)
+    dA, dB = to_dev(A), to_dev(B)
+    out = []
+    for limit in (0, 200 << 20):
+        h = oz2.Ozaki2(torch.cuda.current_stream())
+        try:
+            h.set_workspace_limit(limit)
+            dC = torch.zeros(m * n, dtype=torch.float64, device="cuda")
+            h.gemm_adaptive([("N", "N", m, n, k, 1.0, dA, m, dB, k, 0.0, dC, m, 16)], 53, az.ADAPTIVE_FIXED)
+            torch.cuda.synchronize()
+            out.append(dC)
+        finally:
+            h.close()
+    assert torch.equal(out[0].view(torch.int64), out[1].view(torch.int64))
+    dC = torch.zeros(m * n, dtype=torch.float64, device="cuda")
+    az.gemm("N", "N", m, n, k, 1.0, dA, m, dB, k, 0.0, dC, m, 16)
+    assert torch.equal(out[0].view(torch.int64), dC.view(torch.int64))
