@@ -181,7 +181,7 @@ __device__ __forceinline__ dd dd_add_prod(dd acc, double a, double b) {  // acc 
 }
 
 // ---------------------------------------------------------------- probe
-// One block per (tile, 256 rows of the tile). The probe takes kProbeCols columns j_c of the tile
+// One block per (tile, kProbeRows rows of the tile). The probe takes kProbeCols columns j_c of the tile
 // (stratified: one random column in each of kProbeCols equal ranges) and checks every entry
 // (i, j_c) of its rows on its own: C_ij against alpha (A B)_ij, so the check is entry by entry,
 // with no cancellation between columns. (A B)_ij is summed in FP64 in blocks of 32 terms (FMA),
@@ -196,7 +196,7 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
     return z ^ (z >> 31);
 }
 
-__global__ void __launch_bounds__(256, 3) probe_kernel(const ProbeItem* __restrict__ items, int count,
+__global__ void __launch_bounds__(kProbeRows, 6) probe_kernel(const ProbeItem* __restrict__ items, int count,
                                                     int* __restrict__ fail) {
     const ProbeItem* I = items + find_block_item(items, count, blockIdx.x);
     const int64_t rblk = static_cast<int64_t>(blockIdx.x) - I->block0;
@@ -215,7 +215,7 @@ __global__ void __launch_bounds__(256, 3) probe_kernel(const ProbeItem* __restri
         }
     }
     __syncthreads();
-    const int64_t i = rblk * 256 + threadIdx.x;
+    const int64_t i = rblk * kProbeRows + threadIdx.x;
     const bool live = i < mt;
     double z[kProbeCols], zp[kProbeCols], za[kProbeCols];
 #pragma unroll
@@ -403,12 +403,12 @@ void launch_tile_features(const FeatureItem* d, int count, float* feat, int* s_a
 
 int64_t probe_item_blocks(ProbeItem& it, int64_t block0) {
     it.block0 = block0;
-    return (it.mt + 255) / 256;
+    return (it.mt + kProbeRows - 1) / kProbeRows;
 }
 
 void launch_probe(const ProbeItem* d, int count, int64_t blocks, int* fail, cudaStream_t st) {
     if (count <= 0 || blocks <= 0) return;
-    probe_kernel<<<static_cast<unsigned>(blocks), 256, 0, st>>>(d, count, fail);
+    probe_kernel<<<static_cast<unsigned>(blocks), kProbeRows, 0, st>>>(d, count, fail);
 }
 
 void launch_dd_gemm_nn(int64_t m, int64_t n, int64_t k, const double* A, int64_t lda, const double* B, int64_t ldb,

@@ -1319,11 +1319,13 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
     if (mode == 0) {
         std::vector<ProbeItem> pi;
         int64_t blocks = 0;
-        // tiles of one row panel next to each other: their blocks run together and share the
-        // panel's rows of A through the L2
+        // the longest tiles (largest k) first, so that the short ones fill the last wave; within
+        // a problem, tiles of one row panel next to each other share its rows of A in the L2
         std::vector<int64_t> porder(ntiles);
         for (int64_t t = 0; t < ntiles; ++t) porder[t] = t;
         std::stable_sort(porder.begin(), porder.end(), [&](int64_t x, int64_t y) {
+            const int64_t kx = base[tiles[x].prob].k, ky = base[tiles[y].prob].k;
+            if (kx != ky) return kx > ky;
             return std::make_pair(tiles[x].prob, tiles[x].i0) < std::make_pair(tiles[y].prob, tiles[y].i0);
         });
         for (const int64_t t : porder) {
