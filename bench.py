@@ -719,7 +719,7 @@ def main():
         extras["dgemm_8192"] = dgemm_leg(a, oz2, torch, dev, stream, rank)
         extras["zgemm_4096"] = zgemm_leg(oz2, torch, dev, stream, rank)
         extras["grouped_c4"] = grouped_leg(oz2, torch, dev, stream)
-        if rank == 0:
+        if world == 1:  # the host-core baseline is quoted at one GPU only
             line["cpu_baseline"] = cpu_sample(a)
     line["extras"] = extras
     if rank == 0:

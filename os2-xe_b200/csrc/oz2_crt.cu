@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(256) crt_kernel(const __grid_constant__ CrtPar
                 w2[t] = __ldg(reinterpret_cast<const uint32_t*>(base + 2 * gstride + t * rstride));
             }
         }
-#pragma unroll 1
+#pragma unroll
         for (int e = 0; e < 4; ++e) {
             const int64_t i = i0 + e;
             if (i >= m) break;
