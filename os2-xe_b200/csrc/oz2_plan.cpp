@@ -188,6 +188,11 @@ void mod_constants(const Plan& p, ModConst* out) {
         c.koff3 = (h + m - pow2_mod(62, m)) % m;
         c.koff5 = (h + m - pow2_mod(104, m)) % m;
         c.kbias = m * static_cast<uint32_t>(((uint64_t{1} << 31) + m - 1) / m);
+        // division by a constant with an exact multiply-high (Granlund and Montgomery, 1994):
+        // with M = ceil(2^(N + 8) / m) and m <= 2^8, floor(v M / 2^(N + 8)) = floor(v / m) for
+        // every v < 2^N; M < 2^32 for the moduli here (m >= 157)
+        c.mx30 = static_cast<uint32_t>(((uint64_t{1} << 38) + m - 1) / m);
+        c.mx31 = static_cast<uint32_t>(((uint64_t{1} << 39) + m - 1) / m);
     }
 }
 

@@ -36,6 +36,8 @@ struct ModConst {
     uint32_t koff5;  // (h - 2^104 mod m) mod m: wide limb offset
     uint32_t kbias;  // m ceil(2^31 / m): c + kbias is in [0, 2^32) for every int32 GEMM sum c
                      // (|c| < 2^31 - 2^21) and congruent to c modulo m
+    uint32_t mx30;   // ceil(2^38 / m): floor(v / m) = umulhi(v, mx30) >> 6 exactly for v < 2^30
+    uint32_t mx31;   // ceil(2^39 / m): floor(v / m) = umulhi(v, mx31) >> 7 exactly for v < 2^31
 };
 
 struct Plan {

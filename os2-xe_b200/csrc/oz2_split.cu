@@ -122,16 +122,16 @@ __device__ __forceinline__ void offset_limbs_fp_wide(double v, double s1, double
     L[4] = static_cast<uint32_t>(oh >> 20) & kMask21;
 }
 
-// symmetric residue of the value whose offset limbs are L, as an int in [-h, m-1-h]
+// (x + h) mod m in [0, m) for the value x whose offset limbs are L; the symmetric residue is this
+// minus h. The limb sum v stays below 2^30 (three limbs) or 2^31 (five limbs), where the
+// multiply-high quotient of the plan's mx30 / mx31 is exact, so no correction step follows.
 template <int NLIMB>
-__device__ __forceinline__ int sym_residue(const uint32_t (&L)[NLIMB], const ModConst& c) {
+__device__ __forceinline__ uint32_t shifted_residue(const uint32_t (&L)[NLIMB], const ModConst& c) {
     uint32_t v = L[0] + (NLIMB == 3 ? c.koff3 : c.koff5);
 #pragma unroll
     for (int j = 1; j < NLIMB; ++j) v += L[j] * c.c[j - 1];
-    const uint32_t q = __umulhi(v, c.mu);
-    uint32_t r = v - q * c.m;
-    r = min(r, r - c.m);
-    return static_cast<int>(r) - static_cast<int>(c.h);
+    const uint32_t q = NLIMB == 3 ? __umulhi(v, c.mx30) >> 6 : __umulhi(v, c.mx31) >> 7;
+    return v - q * c.m;
 }
 
 // low bytes of a, b, c, d as one little-endian word
@@ -238,26 +238,28 @@ __global__ void __launch_bounds__(256) split_kernel(const SplitItem* __restrict_
         } else {
 #pragma unroll
             for (int q = 0; q < EPT; ++q) {
-                const int s0 = sym_residue<NLIMB>(L[0][q], mc);
-                b0[q] = static_cast<uint32_t>(s0);
+                const uint32_t r0 = shifted_residue<NLIMB>(L[0][q], mc);
+                b0[q] = r0;
                 if (CPLX) {
-                    const int s1 = sym_residue<NLIMB>(L[NG - 1][q], mc);
-                    const int m = static_cast<int>(mc.m), h = static_cast<int>(mc.h);
-                    int ss = s0 + s1;
-                    ss = ss > m - 1 - h ? ss - m : ss;
-                    ss = ss < -h ? ss + m : ss;
-                    b1[q] = static_cast<uint32_t>(s1);
-                    b2[q] = static_cast<uint32_t>(ss);
+                    const uint32_t r1 = shifted_residue<NLIMB>(L[NG - 1][q], mc);
+                    // (x0 + x1 + h) mod m from the two shifted residues
+                    uint32_t r2 = r0 + r1 + (mc.m - mc.h);
+                    r2 = min(r2, r2 - mc.m);
+                    r2 = min(r2, r2 - mc.m);
+                    b1[q] = r1;
+                    b2[q] = r2;
                 }
             }
         }
+        // bytes r - h modulo 256, four per word (m = 256 stores x mod 256 directly)
+        const uint32_t h4 = mc.m == 256 ? 0u : mc.h * 0x01010101u;
         uint32_t w0[EPT / 4], w1[EPT / 4], w2[EPT / 4];
 #pragma unroll
         for (int q = 0; q < EPT / 4; ++q) {
-            w0[q] = pack_bytes(b0[4 * q], b0[4 * q + 1], b0[4 * q + 2], b0[4 * q + 3]);
+            w0[q] = __vsub4(pack_bytes(b0[4 * q], b0[4 * q + 1], b0[4 * q + 2], b0[4 * q + 3]), h4);
             if (CPLX) {
-                w1[q] = pack_bytes(b1[4 * q], b1[4 * q + 1], b1[4 * q + 2], b1[4 * q + 3]);
-                w2[q] = pack_bytes(b2[4 * q], b2[4 * q + 1], b2[4 * q + 2], b2[4 * q + 3]);
+                w1[q] = __vsub4(pack_bytes(b1[4 * q], b1[4 * q + 1], b1[4 * q + 2], b1[4 * q + 3]), h4);
+                w2[q] = __vsub4(pack_bytes(b2[4 * q], b2[4 * q + 1], b2[4 * q + 2], b2[4 * q + 3]), h4);
             }
         }
         store(out + t * plane_bytes, w0);
