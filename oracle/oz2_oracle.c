@@ -700,3 +700,73 @@ void oz2o_set_threads(int n) {
     (void)n;
 #endif
 }
+
+/* ---- Ozaki Scheme I, the reference's comparison baseline (benchmarks/ozaki1_gpu.hpp:10-155).
+ * tk = 7L - 2 bits per element with the Ozaki-II exponent rule and RNE scaling (:116-131); each
+ * scaled integer as L balanced base-128 digits, most significant first (:31-40); the digit
+ * products of the first L anti-diagonals summed exactly (:139-143); Horner over the diagonals in
+ * double-double, then one ldexp by 7(L - 1) - D_i - E_j, NaN for non-finite rows / columns
+ * (:50-75). C = A B for column-major A (m x k), B (k x n). */
+int oz1o_precision_bits(int L) { return 7 * L - 2; }
+
+int oz1o_dgemm(int64_t m, int64_t n, int64_t k, const double* A, int64_t lda, const double* B, int64_t ldb,
+               double* C, int64_t ldc, int L) {
+    if (L < 2 || L > 9) return OZ2O_EINVAL;
+    if (k * 4096 >= ((int64_t)1 << 31)) return OZ2O_EINVAL;
+    if (m <= 0 || n <= 0) return OZ2O_OK;
+    const int tk = oz1o_precision_bits(L);
+    const size_t kk = (size_t)(k > 0 ? k : 1);
+    int* D = (int*)malloc(sizeof(int) * (size_t)m);
+    int* E = (int*)malloc(sizeof(int) * (size_t)n);
+    int8_t* Ad = (int8_t*)malloc((size_t)L * (size_t)m * kk);  /* [digit][i][p] */
+    int8_t* Bd = (int8_t*)malloc((size_t)L * (size_t)n * kk);  /* [digit][j][p] */
+    if (!D || !E || !Ad || !Bd) {
+        free(D); free(E); free(Ad); free(Bd);
+        return OZ2O_EINTERNAL;
+    }
+    oz2o_exponents('N', 'N', m, n, k, A, lda, B, ldb, tk, 0, D, E);
+    for (int side = 0; side < 2; ++side) {
+        const int64_t rows = side ? n : m;
+        int8_t* dst = side ? Bd : Ad;
+        for (int64_t r = 0; r < rows; ++r) {
+            const int ee = side ? E[r] : D[r];
+            for (int64_t p = 0; p < k; ++p) {
+                const double v = ee == OZ2O_NON_FINITE ? 0.0 : (side ? B[p + r * ldb] : A[r + p * lda]);
+                int neg;
+                uint64_t lo, hi;
+                oz2o_scaled_int(v, ee, &neg, &lo, &hi);
+                int64_t x = neg ? -(int64_t)lo : (int64_t)lo;
+                for (int i = L - 1; i >= 0; --i) {
+                    const int64_t dgt = ((x + 64) & 127) - 64;
+                    x = (x - dgt) >> 7;
+                    dst[((size_t)i * (size_t)rows + (size_t)r) * kk + (size_t)p] = (int8_t)dgt;
+                }
+            }
+        }
+    }
+#pragma omp parallel for schedule(dynamic)
+    for (int64_t j = 0; j < n; ++j)
+        for (int64_t i = 0; i < m; ++i) {
+            double hi = 0.0, lo = 0.0;
+            for (int d = 0; d < L; ++d) {
+                int64_t S = 0;
+                for (int a = 0; a <= d; ++a)
+                    S += dot_i8(Ad + ((size_t)a * (size_t)m + (size_t)i) * kk,
+                                Bd + ((size_t)(d - a) * (size_t)n + (size_t)j) * kk, k);
+                if (d > 0) {
+                    hi *= 128.0;
+                    lo *= 128.0;
+                }
+                const double sd = (double)S;
+                const double s = hi + sd, bb = s - hi;
+                const double err = (hi - (s - bb)) + (sd - bb) + lo;
+                hi = s + err;
+                lo = err - (hi - s);
+            }
+            double v = ldexp(hi + lo, 7 * (L - 1) - D[i] - E[j]);
+            if (D[i] == OZ2O_NON_FINITE || E[j] == OZ2O_NON_FINITE) v = nan_value();
+            C[i + j * ldc] = v;
+        }
+    free(D); free(E); free(Ad); free(Bd);
+    return OZ2O_OK;
+}

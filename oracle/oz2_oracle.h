@@ -50,6 +50,7 @@ typedef struct {
 /* status codes shared with the product's C ABI */
 #define OZ2O_OK 0
 #define OZ2O_EINVAL 1
+#define OZ2O_EINTERNAL 3
 #define OZ2O_EOVERFLOW 5
 
 int oz2o_moduli(int s, uint32_t* out);
@@ -104,6 +105,13 @@ double oz2o_zbound_ratio(char ta, char tb, int64_t m, int64_t n, int64_t k, int 
  * out = {ulp_max, ulp_mean, cr_frac, ab_max, fro_rel}; absAB may be NULL. */
 void oz2o_metrics(int64_t count, const double* C, const double* hi, const double* lo, const double* absAB,
                   double* out);
+
+/* Ozaki Scheme I, the reference's comparison baseline (benchmarks/ozaki1_gpu.hpp): C = A B (N, N)
+ * with L digits of 7 bits, tk = 7L - 2; returns OZ2O_EINVAL for L outside [2, 9] or k * 4096 >= 2^31,
+ * OZ2O_EINTERNAL when memory runs out */
+int oz1o_precision_bits(int L);
+int oz1o_dgemm(int64_t m, int64_t n, int64_t k, const double* A, int64_t lda, const double* B, int64_t ldb,
+               double* C, int64_t ldc, int L);
 
 /* threads used by the oracle's parallel loops (1 = serial) */
 void oz2o_set_threads(int n);

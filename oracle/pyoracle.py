@@ -70,9 +70,14 @@ class Oracle:
         L.oz2o_zbound_ratio.restype = _dbl
         L.oz2o_metrics.argtypes = [_i64, _vp, _vp, _vp, _vp, _vp]
         L.oz2o_set_threads.argtypes = [_i32]
+        L.oz1o_dgemm.argtypes = [_i64, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i32]
 
     def set_threads(self, n):
         self.lib.oz2o_set_threads(n)
+
+    def ozaki1(self, m, n, k, A, lda, B, ldb, C_, ldc, L):
+        """Ozaki-I restatement: C = A B (N, N), column-major; returns the status"""
+        return self.lib.oz1o_dgemm(m, n, k, _ptr(A), lda, _ptr(B), ldb, _ptr(C_), ldc, L)
 
     def plan(self, s, k):
         p = Plan()
@@ -171,9 +176,14 @@ class Ref:
         L.ozref_dgemm.argtypes = gemm_args + [_dbl, _vp, _i64, _vp, _i64, _dbl, _vp, _i64, _i32, C.c_size_t, _vp]
         L.ozref_zgemm.argtypes = gemm_args + [_vp, _vp, _i64, _vp, _i64, _vp, _vp, _i64, _i32, C.c_size_t]
         L.ozref_set_threads.argtypes = [_i32]
+        L.ozref_ozaki1.argtypes = [_i64, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i32]
 
     def set_threads(self, n):
         self.lib.ozref_set_threads(n)
+
+    def ozaki1(self, m, n, k, A, lda, B, ldb, C_, ldc, L):
+        """the reference's oz1::Ozaki1::gemm: C = A B (N, N); returns the status"""
+        return self.lib.ozref_ozaki1(m, n, k, _ptr(A), lda, _ptr(B), ldb, _ptr(C_), ldc, L)
 
     def plan(self, s, k):
         tk, nl, l2 = _i32(), _i32(), _dbl()

@@ -6,6 +6,7 @@
 #include <stdexcept>
 
 #include "ozaki2_gpu.hpp"
+#include "ozaki1_gpu.hpp"
 
 namespace {
 sycl::queue& q() {
@@ -116,6 +117,15 @@ int ozref_zgemm(char ta, char tb, int64_t m, int64_t n, int64_t k, const double*
         oz.zgemm(tr(ta), tr(tb), m, n, k, cd(alpha[0], alpha[1]), reinterpret_cast<const cd*>(A), lda,
                  reinterpret_cast<const cd*>(B), ldb, cd(beta[0], beta[1]), reinterpret_cast<cd*>(C), ldc, s)
             .wait();
+    });
+}
+
+// the reference's Ozaki-I comparison baseline, oz1::Ozaki1::gemm (benchmarks/ozaki1_gpu.hpp:85-97)
+int ozref_ozaki1(int64_t m, int64_t n, int64_t k, const double* A, int64_t lda, const double* B, int64_t ldb,
+                 double* C, int64_t ldc, int L) {
+    return guard([&] {
+        oz1::Ozaki1 oz(q());
+        oz.gemm(m, n, k, A, lda, B, ldb, C, ldc, L).wait();
     });
 }
 
