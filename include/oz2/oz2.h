@@ -149,6 +149,13 @@ int oz2_accuracy(oz2_handle h, int64_t m, int64_t n, const double* C, int64_t ld
 int oz2_error_ratio(oz2_handle h, int64_t m, int64_t n, int64_t k, const double* C, int64_t ldc, const double* hi,
                     const double* lo, const double* absab, int target_bits, float* out);
 
+/* The reference's Ozaki Scheme I comparison baseline, oz1::Ozaki1::gemm (benchmarks/ozaki1_gpu.hpp:85-147):
+ * C = A B for column-major, untransposed A (m x k) and B (k x n) with L in [2, 9] digits of 7 bits
+ * (7L - 2 bits per element, L (L + 1) / 2 INT8 GEMMs), the same results as the reference bit for bit.
+ * k * 4096 must stay below 2^31. Asynchronous on the handle's stream. */
+int oz2_ozaki1_dgemm(oz2_handle h, int64_t m, int64_t n, int64_t k, const double* A, int64_t lda, const double* B,
+                     int64_t ldb, double* C, int64_t ldc, int L);
+
 /* Ozaki2::precision_bits / precision_bits_complex / moduli_for_bits: src/ozaki2_gpu.hpp:689-700, :762 */
 int oz2_precision_bits(int64_t k, int num_moduli, int* out);
 int oz2_precision_bits_complex(int64_t k, int num_moduli, int* out);

@@ -212,3 +212,30 @@ private:
 };
 
 }  // namespace oz2
+
+namespace oz1 {
+
+// The reference's Ozaki Scheme I comparison baseline (benchmarks/ozaki1_gpu.hpp:78-155) on this
+// library's kernels: C = A B, column-major, untransposed, L 7-bit digits per element.
+class Ozaki1 {
+public:
+    explicit Ozaki1(cudaStream_t stream = nullptr) { oz2::detail::check(oz2_create(stream, &h_)); }
+    ~Ozaki1() { oz2_destroy(h_); }
+    Ozaki1(const Ozaki1&) = delete;
+    Ozaki1& operator=(const Ozaki1&) = delete;
+
+    static int precision_bits(int L) { return 7 * L - 2; }
+    static int num_gemms(int L) { return L * (L + 1) / 2; }
+
+    // asynchronous on the stream; throws std::invalid_argument for L outside [2, 9] or k 4096 >= 2^31
+    void gemm(int64_t m, int64_t n, int64_t k, const double* A, int64_t lda, const double* B, int64_t ldb, double* C,
+              int64_t ldc, int L) {
+        oz2::detail::check(oz2_ozaki1_dgemm(h_, m, n, k, A, lda, B, ldb, C, ldc, L), h_);
+    }
+    void release() { oz2::detail::check(oz2_release_workspace(h_), h_); }
+
+private:
+    oz2_handle h_ = nullptr;
+};
+
+}  // namespace oz1

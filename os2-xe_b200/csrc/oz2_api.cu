@@ -36,7 +36,7 @@ constexpr int kRing = 4;
 // A call is planned on the host into a descriptor blob and a list of operations, then issued
 // on the stream (or captured into a CUDA graph and replayed).
 struct Op {
-    enum Kind { Memset, Scale, Split, Gemm, Crt, ScaleC, Mark } kind;
+    enum Kind { Memset, Scale, Split, Gemm, Crt, ScaleC, Mark, Slice, GemmOz1 } kind;
     size_t off = 0;    // descriptor offset in the blob
     int count = 0;     // items
     int64_t blocks = 0;
@@ -529,6 +529,14 @@ void issue(oz2_context* h, const Program& prog, const unsigned char* dev) {
             case Op::Gemm:
                 launch_gemm(reinterpret_cast<const GemmItem*>(dev + op.off), op.count, op.jobs, op.cfg, h->num_sms, h->d_err,
                             h->stream);
+                break;
+            case Op::Slice:
+                launch_slice(reinterpret_cast<const SplitItem*>(dev + op.off), reinterpret_cast<const SplitItem*>(hb + op.off),
+                             op.count, op.blocks, h->stream);
+                break;
+            case Op::GemmOz1:
+                launch_gemm_oz1(reinterpret_cast<const GemmItem*>(dev + op.off), op.count, op.jobs, op.cfg, h->num_sms,
+                                h->d_err, h->stream);
                 break;
             case Op::Crt:
                 launch_crt(reinterpret_cast<const CrtItem*>(dev + op.off), op.count, op.blocks, *op.plan, op.cplx,
@@ -1508,6 +1516,116 @@ int oz2_dgemm(oz2_handle h, char ta, char tb, int64_t m, int64_t n, int64_t k, d
     const Prob p{ta, tb, m, n, k, {alpha, 0.0}, {beta, 0.0}, A, lda, B, ldb, C, ldc, 1, plan};
     if ((st = run_single(h, p))) return st;
     return end_call(h, done);
+}
+
+// The reference's Ozaki Scheme I comparison baseline, oz1::Ozaki1::gemm
+// (benchmarks/ozaki1_gpu.hpp:85-147): C = A B, A and B column-major and not transposed.
+int oz2_ozaki1_dgemm(oz2_handle h, int64_t m, int64_t n, int64_t k, const double* A, int64_t lda, const double* B,
+                     int64_t ldb, double* C, int64_t ldc, int L) {
+    if (!h) return fail(nullptr, OZ2_EINVAL, "oz2: null handle");
+    h->marks.clear();
+    if (L < 2 || L > 9) return fail(h, OZ2_EINVAL, "oz2: L must be in [2, 9]");
+    int st = check_args(h, 'N', 'N', m, n, k, lda, ldb, ldc);
+    if (st) return st;
+    if (k * 4096 >= (int64_t{1} << 31)) return fail(h, OZ2_EINVAL, "oz2: k too large for the int32 digit products");
+    if ((st = begin_call(h, nullptr, 0))) return st;
+    if (m == 0 || n == 0) return end_call(h, nullptr);
+    if (k == 0) {  // C = A B = 0
+        const double zero[2] = {0.0, 0.0};
+        launch_scale_c(C, ldc, m, n, zero, false, h->stream);
+        ++h->launches;
+        return end_call(h, nullptr);
+    }
+    const int tk = 7 * L - 2, npairs = L * (L + 1) / 2;
+    const PlaneGeom ga = plane_geom(m, k, kGemmIPad), gb = plane_geom(n, k, kGemmJ);
+    size_t off = 0;
+    auto carve = [&](size_t bytes) {
+        const size_t o = off;
+        off += align256(bytes);
+        return o;
+    };
+    const size_t o_ma = carve(static_cast<size_t>(m) * 8), o_mb = carve(static_cast<size_t>(n) * 8);
+    const size_t o_acc = carve(static_cast<size_t>(L) * m * n * 8);
+    const size_t zero_end = off;
+    const size_t o_pa = carve(static_cast<size_t>(L) * ga.plane_bytes), o_pb = carve(static_cast<size_t>(L) * gb.plane_bytes);
+    const size_t o_desc = carve(64 << 10);
+    if ((st = ensure_workspace(h, off))) return st;
+    auto* maxA = reinterpret_cast<unsigned long long*>(h->ws + o_ma);
+    auto* maxB = reinterpret_cast<unsigned long long*>(h->ws + o_mb);
+    auto* acc = reinterpret_cast<int64_t*>(h->ws + o_acc);
+    auto* planesA = reinterpret_cast<int8_t*>(h->ws + o_pa);
+    auto* planesB = reinterpret_cast<int8_t*>(h->ws + o_pb);
+
+    const Prob p{'N', 'N', m, n, k, {1.0, 0.0}, {0.0, 0.0}, A, lda, B, ldb, C, ldc, 1, nullptr};
+    Program prog;
+    Op ms;
+    ms.kind = Op::Memset;
+    ms.ptr = h->ws;
+    ms.bytes = zero_end;
+    prog.ops.push_back(ms);
+    std::vector<ScaleItem> sc{scale_item(p, true, maxA), scale_item(p, false, maxB)};
+    plan_scale(h, prog, sc);
+    for (int side = 0; side < 2; ++side) {  // digits: A rows contiguous, B columns k-contiguous
+        SplitItem it{};
+        it.X = side ? B : A;
+        it.ldx = side ? ldb : lda;
+        it.rows = side ? n : m;
+        it.k = k;
+        it.row_contig = side ? 0 : 1;
+        it.tk = tk;
+        it.s = L;
+        it.maxbits = side ? maxB : maxA;
+        it.planes = side ? planesB : planesA;
+        const PlaneGeom& g = side ? gb : ga;
+        it.rows_pad = g.rows_pad;
+        it.kb_total = g.kb_total;
+        it.plane_bytes = g.plane_bytes;
+        Op op;
+        op.kind = Op::Slice;
+        op.count = 1;
+        op.blocks = split_item_blocks(it, 0);
+        op.off = prog.add(&it, sizeof it);
+        prog.ops.push_back(op);
+    }
+    GemmConfig cfg;  // BN 256, raster 16
+    GemmItem g{};
+    g.planes_i = planesA;
+    g.planes_j = planesB;
+    g.pstride_i = ga.plane_bytes;
+    g.pstride_j = gb.plane_bytes;
+    g.m = m;
+    g.n = n;
+    g.kb_total = ga.kb_total;
+    g.tiles_i = static_cast<int>(gemm_tiles_i(m, cfg.bn));
+    g.tiles_j = static_cast<int>(ceil_div(n, kGemmJ));
+    g.tiles = static_cast<int64_t>(g.tiles_i) * g.tiles_j;
+    g.s = npairs;
+    g.groups = 1;
+    g.job0 = 0;
+    g.acc = acc;
+    g.acc_ld = n;
+    g.acc_plane = m * n;
+    for (int d = 0, t = 0; d < L; ++d)
+        for (int a = 0; a <= d; ++a, ++t) {
+            g.pair_a[t] = static_cast<uint8_t>(a);
+            g.pair_b[t] = static_cast<uint8_t>(d - a);
+            g.pair_d[t] = static_cast<uint8_t>(d);
+        }
+    Op go;
+    go.kind = Op::GemmOz1;
+    go.count = 1;
+    go.jobs = g.tiles * npairs;
+    go.cfg = cfg;
+    go.off = prog.add(&g, sizeof g);
+    prog.ops.push_back(go);
+    if ((st = check_grid(h, prog))) return st;
+    unsigned char* dev_desc = h->ws + o_desc;
+    if (prog.blob.size() > (64u << 10)) return fail(h, OZ2_EINTERNAL, "oz2: descriptor region too small");
+    if ((st = upload(h, prog, dev_desc))) return st;
+    issue(h, prog, dev_desc);
+    launch_oz1_horner(acc, m, n, L, maxA, maxB, tk, C, ldc, h->stream);
+    ++h->launches;
+    return end_call(h, nullptr);
 }
 
 // ref src/ozaki2_gpu.hpp:764-786 (plan for 2k: the 3M sums double the inner products)

@@ -238,6 +238,53 @@ __global__ void scale_c_kernel(double* C, int64_t ldc, int64_t m, int64_t n, dou
     }
 }
 
+// Ozaki Scheme I (the reference's comparison baseline, benchmarks/ozaki1_gpu.hpp:50-75): the
+// exact diagonal sums S_d, most significant first, in double-double Horner steps T = 128 T + S_d
+// (scaling by 128 is exact, so a contracted multiply-add rounds as the separate operations do),
+// then one ldexp by 7 (L - 1) - D_i - E_j, NaN for non-finite rows / columns. The sums are
+// stored row-major (acc[d][i n + j]); a block takes a 32 x 32 tile, reads it along j and writes
+// C along i through shared memory. Block (32, 8), grid (ceil(n / 32), rows of tiles strided).
+__global__ void __launch_bounds__(256) oz1_horner_kernel(const int64_t* __restrict__ acc, int64_t m, int64_t n, int L,
+                                                         const unsigned long long* __restrict__ maxA,
+                                                         const unsigned long long* __restrict__ maxB, int tk,
+                                                         double* __restrict__ C, int64_t ldc) {
+    __shared__ double tile[32][33];
+    const int64_t j0 = static_cast<int64_t>(blockIdx.x) * 32, plane = m * n;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int64_t j = j0 + tx;
+    const int Ej = j < n ? exponent_of(maxB[j], tk) : 0;
+    for (int64_t i0 = static_cast<int64_t>(blockIdx.y) * 32; i0 < m; i0 += static_cast<int64_t>(gridDim.y) * 32) {
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int64_t i = i0 + ty + 8 * r;
+            if (i >= m || j >= n) continue;
+            const int Di = exponent_of(maxA[i], tk);
+            double hi = 0.0, lo = 0.0;
+            for (int d = 0; d < L; ++d) {
+                const double sd = static_cast<double>(acc[d * plane + i * n + j]);
+                if (d > 0) {
+                    hi *= 128.0;
+                    lo *= 128.0;
+                }
+                const double sm = hi + sd, bb = sm - hi;
+                const double err = (hi - (sm - bb)) + (sd - bb) + lo;
+                hi = sm + err;
+                lo = err - (hi - sm);
+            }
+            double v = ldexp(hi + lo, 7 * (L - 1) - Di - Ej);
+            if (Di == kNonFinite || Ej == kNonFinite) v = __longlong_as_double(0x7FF8000000000000ll);
+            tile[ty + 8 * r][tx] = v;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int64_t jj = j0 + ty + 8 * r, ii = i0 + tx;
+            if (ii < m && jj < n) C[ii + jj * ldc] = tile[tx][ty + 8 * r];
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace
 
 int64_t crt_item_blocks(CrtItem& it, int64_t block0) {
@@ -259,6 +306,13 @@ void launch_crt(const CrtItem* d_items, int count, int64_t blocks, const Plan& p
     crt_constants(plan, P.cc);
     for (int t = 0; t < plan.s; ++t) P.mod_m[t] = plan.m[t];
     crt_dispatch<2>(plan.s, P, blocks, cplx, st);
+}
+
+void launch_oz1_horner(const int64_t* acc, int64_t m, int64_t n, int L, const unsigned long long* maxA,
+                       const unsigned long long* maxB, int tk, double* C, int64_t ldc, cudaStream_t st) {
+    if (m <= 0 || n <= 0) return;
+    dim3 grid(static_cast<unsigned>(ceil_div(n, 32)), static_cast<unsigned>(std::min<int64_t>(ceil_div(m, 32), 65535)));
+    oz1_horner_kernel<<<grid, dim3(32, 8), 0, st>>>(acc, m, n, L, maxA, maxB, tk, C, ldc);
 }
 
 void launch_write_blob(const void* src, size_t bytes, void* dst, cudaStream_t st) {

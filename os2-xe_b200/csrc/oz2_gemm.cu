@@ -83,7 +83,9 @@ __device__ __forceinline__ Job decode(const GemmParams& P, int64_t job) {
     return J;
 }
 
-template <int BN>
+// OZ1: the Ozaki Scheme I baseline (job t = digit pair, int64 atomic sums per anti-diagonal
+// instead of residues)
+template <int BN, bool OZ1>
 __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __grid_constant__ GemmParams P) {
     using C = Cfg<BN>;
     extern __shared__ uint8_t smem_raw[];
@@ -132,8 +134,9 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
             for (int64_t job = blockIdx.x; ok && job < P.jobs; job += nprog) {
                 const Job J = decode(P, job);
                 const int64_t kb_total = J.I->kb_total, row_block = kb_total * kTileBytes;
-                const int8_t* srcJ = J.I->planes_j + J.gt * J.I->pstride_j + J.tj * row_block;
-                const int8_t* srcI = J.I->planes_i + J.gt * J.I->pstride_i + (static_cast<int64_t>(J.ti) * (BN / 128)) * row_block;
+                const int pj = OZ1 ? J.I->pair_b[J.gt] : J.gt, pi = OZ1 ? J.I->pair_a[J.gt] : J.gt;
+                const int8_t* srcJ = J.I->planes_j + pj * J.I->pstride_j + J.tj * row_block;
+                const int8_t* srcI = J.I->planes_i + pi * J.I->pstride_i + (static_cast<int64_t>(J.ti) * (BN / 128)) * row_block;
                 for (int64_t kb = 0; ok && kb < kb_total; ++kb) {
                     if (!dev::mbar_wait(empty(stage), phase ^ 1u, abort_flag, P.err, dev::kErrTimeoutEmpty)) {
                         ok = false;
@@ -215,10 +218,11 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
         for (int64_t job = blockIdx.x; ok && job < P.jobs; job += nprog) {
             const Job J = decode(P, job);
             const int t = J.gt % J.I->s;
-            const uint32_t m = J.I->mod_m[t], mu = J.I->mod_mu[t], kbias = J.I->mod_kbias[t];
+            const uint32_t m = OZ1 ? 1u : J.I->mod_m[t], mu = OZ1 ? 0u : J.I->mod_mu[t],
+                           kbias = OZ1 ? 0u : J.I->mod_kbias[t];
             const int64_t j = static_cast<int64_t>(J.tj) * kGemmJ + quarter * 32 + lane;
             const int64_t mm = J.I->m, nn = J.I->n;
-            uint8_t* rowj = J.I->resid + J.gt * J.I->rstride + j * 32;  // + (i / 32) * 32 n
+            uint8_t* rowj = OZ1 ? nullptr : J.I->resid + J.gt * J.I->rstride + j * 32;  // + (i / 32) * 32 n
             for (int64_t c = 0; c < J.nch; ++c, ++local) {
                 const int acc = local & 1;
                 const uint32_t use = static_cast<uint32_t>(local >> 1);
@@ -243,7 +247,18 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
                     if (cc + 1 < kChunks) dev::tmem_load_32x32(taddr + (cc + 1) * 32, v[(cc + 1) & 1]);
                     const int64_t i0 = static_cast<int64_t>(J.ti) * BN + (half * kChunks + cc) * 32;
                     uint8_t* blk = rowj + (i0 >> 5) * (32 * nn);  // this chunk's 32 bytes of row j
-                    if (j < nn && i0 < mm) {
+                    if constexpr (OZ1) {
+                        if (j < nn) {  // a warp's lanes are 32 consecutive j: 256 contiguous bytes per row i
+                            unsigned long long* dst = reinterpret_cast<unsigned long long*>(
+                                J.I->acc + J.I->pair_d[J.gt] * J.I->acc_plane + j);
+                            const int64_t ld = J.I->acc_ld;
+#pragma unroll
+                            for (int b = 0; b < 32; ++b)
+                                if (i0 + b < mm)
+                                    atomicAdd(dst + (i0 + b) * ld, static_cast<unsigned long long>(
+                                                                       static_cast<long long>(static_cast<int32_t>(cur[b]))));
+                        }
+                    } else if (j < nn && i0 < mm) {
                         uint32_t ow[8] = {0, 0, 0, 0, 0, 0, 0, 0};
                         if (accumulate) {
                             const uint4 o0 = *reinterpret_cast<const uint4*>(blk);
@@ -288,19 +303,22 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
     }
 }
 
-template <int BN>
+template <int BN, bool OZ1 = false>
 void launch_bn(const GemmParams& P, int grid, cudaStream_t st) {
-    gemm_i8_modm_kernel<BN><<<grid, kGemmThreads, Cfg<BN>::kSmemBytes, st>>>(P);
+    gemm_i8_modm_kernel<BN, OZ1><<<grid, kGemmThreads, Cfg<BN>::kSmemBytes, st>>>(P);
 }
 
 }  // namespace
 
 cudaError_t prepare_gemm_kernels() {
-    cudaError_t e = cudaFuncSetAttribute(gemm_i8_modm_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(gemm_i8_modm_kernel<256, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          Cfg<256>::kSmemBytes);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(gemm_i8_modm_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(gemm_i8_modm_kernel<128, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  Cfg<128>::kSmemBytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(gemm_i8_modm_kernel<256, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 Cfg<256>::kSmemBytes);
     return e;
 }
 
@@ -314,6 +332,14 @@ void launch_gemm(const GemmItem* d_items, int count, int64_t jobs, const GemmCon
     const int grid = static_cast<int>(std::min<int64_t>(ctas, jobs));
     if (cfg.bn == 128) launch_bn<128>(P, grid, st);
     else launch_bn<256>(P, grid, st);
+}
+
+void launch_gemm_oz1(const GemmItem* d_items, int count, int64_t jobs, const GemmConfig& cfg, int num_sms, int* err,
+                     cudaStream_t st) {
+    if (count <= 0 || jobs <= 0) return;
+    GemmParams P{d_items, count, cfg.group_j > 0 ? cfg.group_j : 16, jobs, err};
+    const int grid = static_cast<int>(std::min<int64_t>(num_sms, jobs));
+    launch_bn<256, true>(P, grid, st);
 }
 
 }  // namespace oz2

@@ -78,6 +78,8 @@ struct SplitItem {
 };
 
 // ---- gemm: one item per problem; jobs = groups * s * tiles, each job runs all k chunks
+constexpr int kMaxOz1Pairs = 45;  // Ozaki Scheme I: L (L + 1) / 2 digit pairs, L <= 9
+
 struct GemmItem {
     const int8_t* planes_i;  // I side (op(A) rows), plane rows padded to 256
     const int8_t* planes_j;  // J side (op(B) columns), plane rows padded to 128
@@ -86,6 +88,11 @@ struct GemmItem {
     int64_t tiles, job0;
     int tiles_i, tiles_j, s, groups;
     uint32_t mod_m[kMaxModuli], mod_mu[kMaxModuli], mod_kbias[kMaxModuli];
+    // Ozaki-I mode only: job index t is the digit pair (pair_a[t], pair_b[t]) on anti-diagonal
+    // pair_d[t]; the int32 products are added into acc[d][i acc_ld + j] (int64)
+    int64_t* acc;
+    int64_t acc_ld, acc_plane;
+    uint8_t pair_a[kMaxOz1Pairs], pair_b[kMaxOz1Pairs], pair_d[kMaxOz1Pairs];
 };
 
 // ---- crt: one item per problem; all items of a launch share s
@@ -118,6 +125,15 @@ struct GemmConfig {
 };
 void launch_gemm(const GemmItem* d_items, int count, int64_t jobs, const GemmConfig& cfg, int num_sms, int* err,
                  cudaStream_t st);
+// the same GEMM for the Ozaki Scheme I baseline: digit-pair jobs, int64 atomic sums per diagonal
+void launch_gemm_oz1(const GemmItem* d_items, int count, int64_t jobs, const GemmConfig& cfg, int num_sms, int* err,
+                     cudaStream_t st);
+// Ozaki Scheme I digits: item.s = L balanced base-128 digits of RNE(x 2^e), e = tk - frexp_exp(max)
+void launch_slice(const SplitItem* d_items, const SplitItem* h_items, int count, int64_t blocks, cudaStream_t st);
+// Ozaki Scheme I: C = 2^(7 (L - 1) - D_i - E_j) * Horner_d(acc[d]) in double-double, NaN for
+// non-finite rows / columns
+void launch_oz1_horner(const int64_t* acc, int64_t m, int64_t n, int L, const unsigned long long* maxA,
+                       const unsigned long long* maxB, int tk, double* C, int64_t ldc, cudaStream_t st);
 int64_t gemm_tiles_i(int64_t m, int bn);
 
 // all items of one CRT launch share s (the CRT table is a kernel parameter)

@@ -270,6 +270,62 @@ __global__ void __launch_bounds__(256) split_kernel(const SplitItem* __restrict_
     }
 }
 
+// Ozaki Scheme I digits (the reference's comparison baseline, benchmarks/ozaki1_gpu.hpp:31-40):
+// x = RNE(v 2^e) as on the narrow split path (tk = 7L - 2 <= 61), then L balanced base-128
+// digits in [-64, 63], most significant in plane 0, written in the same plane layout and with
+// the same thread mapping as split_kernel's narrow real path (16 elements per thread).
+template <bool ROWC>
+__global__ void __launch_bounds__(256) slice_kernel(const SplitItem* __restrict__ items, int count) {
+    constexpr int EPT = 16;
+    const SplitItem* __restrict__ I = items + find_item(items, count, blockIdx.x);
+    const int64_t local = static_cast<int64_t>(blockIdx.x) - I->block0;
+    const int64_t bx = local % I->rblocks, by = local / I->rblocks;
+    int64_t r, k0;
+    if (ROWC) {
+        r = bx * 32 + (threadIdx.x & 31);
+        k0 = by * (8 * EPT) + (threadIdx.x >> 5) * EPT;
+    } else {
+        r = bx * 8 + (threadIdx.x >> 5);
+        k0 = by * (32 * EPT) + (threadIdx.x & 31) * EPT;
+    }
+    const int64_t kb_total = I->kb_total, plane_bytes = I->plane_bytes, ldx = I->ldx, k = I->k;
+    if (r >= I->rows_pad || k0 >= kb_total * kTileK) return;
+    const int ndig = I->s;
+    const int64_t rb = r >> 7;
+    const int rr = static_cast<int>(r & 127);
+    const int c = static_cast<int>((k0 >> 4) & 7);
+    int8_t* out = I->planes + (rb * kb_total + (k0 >> 7)) * kTileBytes + rr * kTileK + ((c ^ (rr & 7)) << 4);
+    long long x[EPT];
+#pragma unroll
+    for (int q = 0; q < EPT; ++q) x[q] = 0;
+    if (r < I->rows && k0 < k) {
+        const int e = exponent_of(I->maxbits[r], I->tk);
+        if (e != kNonFinite) {
+            const int e1 = e >> 1;
+            const double s1 = pow2(e1), s2 = pow2(e - e1);
+#pragma unroll
+            for (int q = 0; q < EPT; ++q) {
+                const int64_t p = k0 + q;
+                if (p < k) x[q] = __double2ll_rn((__ldg(I->X + (ROWC ? r + p * ldx : p + r * ldx)) * s1) * s2);
+            }
+        }
+    }
+    // least significant digit first, into planes ndig - 1 .. 0
+    for (int i = ndig - 1; i >= 0; --i) {
+        uint32_t b[EPT];
+#pragma unroll
+        for (int q = 0; q < EPT; ++q) {
+            const long long d = ((x[q] + 64) & 127) - 64;
+            x[q] = (x[q] - d) >> 7;
+            b[q] = static_cast<uint32_t>(d);
+        }
+        uint32_t w[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) w[q] = pack_bytes(b[4 * q], b[4 * q + 1], b[4 * q + 2], b[4 * q + 3]);
+        *reinterpret_cast<uint4*>(out + i * plane_bytes) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+}
+
 template <int NLIMB, bool CPLX>
 void split_dispatch(const SplitItem* d, int count, int64_t blocks, bool rowc, cudaStream_t st) {
     if (rowc) split_kernel<NLIMB, CPLX, true><<<static_cast<unsigned>(blocks), 256, 0, st>>>(d, count);
@@ -325,6 +381,12 @@ void launch_scale(const ScaleItem* d, const ScaleItem* h, int count, int64_t blo
         if (cplx) scale_kernel<true, false><<<g, 256, 0, st>>>(d, count);
         else scale_kernel<false, false><<<g, 256, 0, st>>>(d, count);
     }
+}
+
+void launch_slice(const SplitItem* d, const SplitItem* h, int count, int64_t blocks, cudaStream_t st) {
+    if (count <= 0 || blocks <= 0) return;
+    if (h[0].row_contig) slice_kernel<true><<<static_cast<unsigned>(blocks), 256, 0, st>>>(d, count);
+    else slice_kernel<false><<<static_cast<unsigned>(blocks), 256, 0, st>>>(d, count);
 }
 
 void launch_split(const SplitItem* d, const SplitItem* h, int count, int64_t blocks, cudaStream_t st) {

@@ -32,6 +32,7 @@ _lib.oz2_dgemm.argtypes = [_vp, _chr, _chr, _i64, _i64, _i64, _dbl, _vp, _i64, _
                            _vp, _i32, _vp]
 _lib.oz2_zgemm.argtypes = [_vp, _chr, _chr, _i64, _i64, _i64, _vp, _vp, _i64, _vp, _i64, _vp, _vp, _i64, _i32,
                            _vp, _i32, _vp]
+_lib.oz2_ozaki1_dgemm.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i32]
 _lib.oz2_precision_bits.argtypes = [_i64, _i32, C.POINTER(_i32)]
 _lib.oz2_precision_bits_complex.argtypes = [_i64, _i32, C.POINTER(_i32)]
 _lib.oz2_moduli_for_bits.argtypes = [_i64, _i32, C.POINTER(_i32)]
@@ -392,6 +393,12 @@ class Ozaki2:
         d = done.cuda_event if hasattr(done, "cuda_event") else done
         _raise(_lib.oz2_dgemm(self._h, _op(ta), _op(tb), m, n, k, float(alpha), _addr(A), lda, _addr(B), ldb,
                               float(beta), _addr(C_), ldc, num_moduli, ev, nev, d), self._h)
+
+    def ozaki1(self, m, n, k, A, lda, B, ldb, C_, ldc, L):
+        """C = A B by Ozaki Scheme I with L 7-bit digits (7 L - 2 bits per element), the
+        reference's comparison baseline oz1::Ozaki1::gemm (benchmarks/ozaki1_gpu.hpp:85-147):
+        column-major, untransposed, no alpha / beta"""
+        _raise(_lib.oz2_ozaki1_dgemm(self._h, m, n, k, _addr(A), lda, _addr(B), ldb, _addr(C_), ldc, L), self._h)
 
     def zgemm(self, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C_, ldc, num_moduli, deps=None, done=None):
         alpha, beta = complex(alpha), complex(beta)

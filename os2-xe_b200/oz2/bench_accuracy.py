@@ -1,10 +1,12 @@
 """Accuracy of the emulated DGEMM / ZGEMM against a double-double product, one CSV row per
 (distribution, k, method, s): the rows and columns of the reference's accuracy bench
 (benchmarks/bench_accuracy.cpp:190-285), with this library's emulation (`ozaki2`,
-`ozaki2_3m`) beside native cuBLAS (`dgemm_gpu`, `zgemm_gpu`).
+`ozaki2_3m`) beside native cuBLAS (`dgemm_gpu`, `zgemm_gpu`) and the Ozaki Scheme I baseline
+(`ozaki1`, real only: the s column holds its L (L + 1) / 2 GEMMs, tk = 7 L - 2, as the reference's
+rows do, :256-261).
 
-    python -m oz2.bench_accuracy [--k 256,1024,4096] [--s 4-24] [--dist urand,phi0.5,phi2,phi4]
-                                 [--mn 512] [--complex] [--seed 1]
+    python -m oz2.bench_accuracy [--k 256,1024,4096] [--s 4-24] [--L 4-9]
+                                 [--dist urand,phi0.5,phi2,phi4] [--mn 512] [--complex] [--seed 1]
 
 Distributions (m = n = mn, inner dimension k; the same definitions as the reference's `gen`,
 seeded here by numpy's PCG64, so the values differ):
@@ -83,7 +85,7 @@ def row(dist, k, method, s, tk, m5):
     return "%s,%d,%s,%d,%d,%.4g,%.4g,%.6f,%.4g,%.4g" % ((dist, k, method, s, tk) + tuple(m5))
 
 
-def run_real(oz, torch, dist, k, mn, svals, seed):
+def run_real(oz, torch, dist, k, mn, svals, seed, Ls=()):
     import oz2
     m = n = mn
     A = generate(m, k, dist, seed * 1000 + 11 + k, True)
@@ -104,6 +106,12 @@ def run_real(oz, torch, dist, k, mn, svals, seed):
             continue
         oz.gemm("N", "N", m, n, k, 1.0, dA, m, dB, k, 0.0, C, m, s)
         out.append(row(dist, k, "ozaki2", s, tk, metrics(torch, C, hi, lo, ab)))
+    for L in Ls:
+        try:
+            oz.ozaki1(m, n, k, dA, m, dB, k, C, m, L)
+        except ValueError:
+            continue
+        out.append(row(dist, k, "ozaki1", L * (L + 1) // 2, 7 * L - 2, metrics(torch, C, hi, lo, ab)))
     return out
 
 
@@ -113,7 +121,7 @@ def two_sum(a, b):
     return s, (a - (s - bb)) + (b - bb)
 
 
-def run_complex(oz, torch, dist, k, mn, svals, seed):
+def run_complex(oz, torch, dist, k, mn, svals, seed, Ls=()):
     """ZGEMM rows: the double-double product assembled from the four real double-double
     products (Re = ArBr - AiBi, Im = ArBi + AiBr) and |A||B| = (|Ar|+|Ai|)(|Br|+|Bi|)"""
     import oz2
@@ -161,6 +169,7 @@ def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--k", default="256,1024,4096,16384")
     ap.add_argument("--s", default="4-24")
+    ap.add_argument("--L", default="4-9")
     ap.add_argument("--dist", default="urand,phi0.5,phi2,phi4")
     ap.add_argument("--mn", type=int, default=512)
     ap.add_argument("--complex", action="store_true")
@@ -174,7 +183,7 @@ def main(argv=None):
     for dist in a.dist.split(","):
         for k in parse_ints(a.k):
             run = run_complex if a.complex else run_real
-            for line in run(oz, torch, dist, k, a.mn, parse_ints(a.s), a.seed):
+            for line in run(oz, torch, dist, k, a.mn, parse_ints(a.s), a.seed, parse_ints(a.L)):
                 print(line, flush=True)
                 lines.append(line)
     oz.close()

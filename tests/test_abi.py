@@ -62,8 +62,10 @@ def test_cpp_header_compiles():
             "void use(oz2::Ozaki2& oz) { std::vector<oz2::Problem> ps(1); oz.gemm_grouped(ps);\n"
             "  oz2::AdaptiveStats st = oz.gemm_adaptive(ps, 53, oz2::Adaptive::Mlp); (void)st;\n"
             "  oz.set_mlp_weights({}); oz.set_adaptive_options(512, 0.99f); oz.autotune_grouped(ps); }\n"
-            "int main(int argc, char**) { if (argc > 5) { oz2::Ozaki2 oz; use(oz); }\n"
-            "  return oz2::Ozaki2::moduli_for_bits(1024, 53) == 15 ? 0 : 1; }\n")
+            "void use1(oz1::Ozaki1& o) { o.gemm(1, 1, 1, nullptr, 1, nullptr, 1, nullptr, 1, 4); }\n"
+            "int main(int argc, char**) { if (argc > 5) { oz2::Ozaki2 oz; use(oz); oz1::Ozaki1 o; use1(o); }\n"
+            "  return oz2::Ozaki2::moduli_for_bits(1024, 53) == 15 && oz1::Ozaki1::num_gemms(9) == 45 &&\n"
+            "    oz1::Ozaki1::precision_bits(9) == 61 ? 0 : 1; }\n")
     exe = os.path.join(ROOT, "os2-xe_b200", "_build", "hdr_check")
     os.makedirs(os.path.dirname(exe), exist_ok=True)
     r = subprocess.run(["/usr/bin/g++", "-std=c++17", "-x", "c++", "-", "-I" + os.path.join(ROOT, "include"),
