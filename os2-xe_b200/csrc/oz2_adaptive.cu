@@ -188,7 +188,8 @@ __device__ __forceinline__ dd dd_add_prod(dd acc, double a, double b) {  // acc 
 // the block sums added into a second accumulator: its error is at most
 // (gamma_32 + gamma_(k/32 + 1) (1 + gamma_32)) (|A||B|)_ij < (34 + k/32) 2^-52 (|A||B|)_ij, far
 // below the k 2^-53 (|A||B|)_ij tolerance, and that error is added to the tolerance. A is read
-// once per tile.
+// once per tile. A thread holds two rows (i and i + kProbeThreads) and the chunk of B's columns
+// sits in shared memory as [p][column], so one 16-byte shared load feeds eight FP64 FMAs.
 __device__ __forceinline__ uint64_t mix64(uint64_t z) {
     z += 0x9E3779B97F4A7C15ull;
     z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
@@ -196,90 +197,112 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
     return z ^ (z >> 31);
 }
 
-__global__ void __launch_bounds__(kProbeRows, 6) probe_kernel(const ProbeItem* __restrict__ items, int count,
-                                                    int* __restrict__ fail) {
+__global__ void __launch_bounds__(kProbeThreads, 3) probe_kernel(const ProbeItem* __restrict__ items, int count,
+                                                                 int* __restrict__ fail) {
+    constexpr int R = kProbeRowsPerThread, NC = kProbeCols;
+    static_assert(NC == 8, "the shared-memory row of B is read as four double2");
     const ProbeItem* I = items + find_block_item(items, count, blockIdx.x);
     const int64_t rblk = static_cast<int64_t>(blockIdx.x) - I->block0;
     const int64_t mt = I->mt, nt = I->nt, k = I->k;
-    const int ncol = static_cast<int>(min(static_cast<int64_t>(kProbeCols), nt));
-    __shared__ int64_t cols[kProbeCols];
-    __shared__ double bs[kProbeCols][kProbeChunk];
-    if (threadIdx.x < ncol) {
+    const int ncol = static_cast<int>(min(static_cast<int64_t>(NC), nt));
+    __shared__ int64_t cols[NC];
+    __shared__ __align__(16) double bs[kProbeChunk][NC];
+    if (threadIdx.x < NC) {
         const int c = threadIdx.x;
-        if (nt >= kProbeCols) {
-            const int64_t span = nt / kProbeCols;
+        int64_t j = c;
+        if (nt >= NC) {
+            const int64_t span = nt / NC;
             const uint64_t h = mix64(I->seed ^ static_cast<uint64_t>(c));
-            cols[c] = c * span + static_cast<int64_t>(h % static_cast<uint64_t>(span));
-        } else {
-            cols[c] = c;
+            j = c * span + static_cast<int64_t>(h % static_cast<uint64_t>(span));
         }
+        cols[c] = j;
     }
     __syncthreads();
-    const int64_t i = rblk * kProbeRows + threadIdx.x;
-    const bool live = i < mt;
-    double z[kProbeCols], zp[kProbeCols], za[kProbeCols];
+    const int64_t i0 = rblk * kProbeRows + threadIdx.x;
+    bool live[R];
+    const double* Ai[R];
+    const int64_t astep = I->a_rowc ? I->lda : 1;
 #pragma unroll
-    for (int c = 0; c < kProbeCols; ++c) z[c] = zp[c] = za[c] = 0.0;
+    for (int r = 0; r < R; ++r) {
+        const int64_t i = i0 + r * kProbeThreads;
+        live[r] = i < mt;
+        Ai[r] = I->a_rowc ? I->A + i : I->A + i * I->lda;  // dereferenced only for live rows
+    }
+    double z[R][NC], zp[R][NC], za[R][NC];
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) z[r][c] = zp[r][c] = za[r][c] = 0.0;
     for (int64_t p0 = 0; p0 < k; p0 += kProbeChunk) {
         const int pn = static_cast<int>(min(static_cast<int64_t>(kProbeChunk), k - p0));
-        for (int e = threadIdx.x; e < ncol * pn; e += blockDim.x) {
+        for (int e = threadIdx.x; e < NC * pn; e += blockDim.x) {
             const int c = e / pn, q = e - c * pn;
-            const int64_t j = cols[c], p = p0 + q;
-            bs[c][q] = I->b_rowc ? I->B[j + p * I->ldb] : I->B[p + j * I->ldb];
-        }
-        for (int e = ncol * pn + threadIdx.x; e < kProbeCols * pn; e += blockDim.x) {
-            const int c = e / pn, q = e - c * pn;
-            bs[c][q] = 0.0;  // columns beyond nt: never checked
+            double v = 0.0;  // columns beyond nt: never checked
+            if (c < ncol) {
+                const int64_t j = cols[c], p = p0 + q;
+                v = I->b_rowc ? I->B[j + p * I->ldb] : I->B[p + j * I->ldb];
+            }
+            bs[q][c] = v;
         }
         __syncthreads();
-        if (live) {
-            const double* __restrict__ Ai = I->a_rowc ? I->A + i : I->A + i * I->lda;
-            const int64_t astep = I->a_rowc ? I->lda : 1;
+        if (live[0]) {
             for (int q0 = 0; q0 < pn; q0 += 32) {  // kProbeChunk is a multiple of 32
-                const int qn = min(32, pn - q0);
-                for (int q1 = q0; q1 < q0 + qn; q1 += 8) {
-                    // eight loads of A in flight before their products
-                    double av[8];
+                const int qe = min(q0 + 32, pn);
+                for (int q1 = q0; q1 < qe; q1 += 4) {
+                    // the next four terms of both rows' loads in flight before their products
+                    double av[R][4];
 #pragma unroll
-                    for (int u = 0; u < 8; ++u)
-                        av[u] = q1 + u < q0 + qn ? __ldg(Ai + (p0 + q1 + u) * astep) : 0.0;
+                    for (int r = 0; r < R; ++r)
 #pragma unroll
-                    for (int u = 0; u < 8; ++u) {
-                        const int q = min(q1 + u, pn - 1);  // av[u] = 0 past the chunk
+                        for (int u = 0; u < 4; ++u)
+                            av[r][u] = live[r] && q1 + u < qe ? __ldg(Ai[r] + (p0 + q1 + u) * astep) : 0.0;
 #pragma unroll
-                        for (int c = 0; c < kProbeCols; ++c) {
-                            const double b = bs[c][q];
-                            zp[c] = fma(av[u], b, zp[c]);
-                            za[c] = fma(fabs(av[u]), fabs(b), za[c]);
-                        }
+                    for (int u = 0; u < 4; ++u) {
+                        const int q = min(q1 + u, pn - 1);  // av = 0 past the chunk
+                        const double2* b2 = reinterpret_cast<const double2*>(bs[q]);
+                        const double2 b01 = b2[0], b23 = b2[1], b45 = b2[2], b67 = b2[3];
+                        const double b[NC] = {b01.x, b01.y, b23.x, b23.y, b45.x, b45.y, b67.x, b67.y};
+#pragma unroll
+                        for (int r = 0; r < R; ++r)
+#pragma unroll
+                            for (int c = 0; c < NC; ++c) {
+                                zp[r][c] = fma(av[r][u], b[c], zp[r][c]);
+                                za[r][c] = fma(fabs(av[r][u]), fabs(b[c]), za[r][c]);
+                            }
                     }
                 }
 #pragma unroll
-                for (int c = 0; c < kProbeCols; ++c) {
-                    z[c] += zp[c];
-                    zp[c] = 0.0;
-                }
+                for (int r = 0; r < R; ++r)
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) {
+                        z[r][c] += zp[r][c];
+                        zp[r][c] = 0.0;
+                    }
             }
         }
         __syncthreads();
     }
-    if (!live) return;
     bool bad = false;
     const double kd = static_cast<double>(k);
 #pragma unroll
-    for (int c = 0; c < kProbeCols; ++c) {
-        if (c < ncol) {
-            const double cv = I->C[i + cols[c] * I->ldc];
-            // C - alpha z in double-double (alpha z exact as a two-product)
-            const dd az{I->alpha * z[c], fma(I->alpha, z[c], -I->alpha * z[c])};
-            const dd diff = dd_add(dd{cv, 0.0}, dd{-az.hi, -az.lo});
-            const double err = fabs(diff.hi + diff.lo);
-            // target k 2^-t |A||B| (za's own rounding widened by k 2^-50), plus the summation
-            // error of z, plus the rounding of C itself (2^-52 |C|)
-            const double tol = fabs(I->alpha) * za[c] *
-                                   (I->tol_scale * (1.0 + kd * 0x1p-50) + (34.0 + kd / 32.0) * 0x1p-52) +
-                               0x1p-52 * fabs(cv) + 1e-300;
-            bad |= !(err <= tol);
+    for (int r = 0; r < R; ++r) {
+        if (!live[r]) continue;
+        const int64_t i = i0 + r * kProbeThreads;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            if (c < ncol) {
+                const double cv = I->C[i + cols[c] * I->ldc];
+                // C - alpha z in double-double (alpha z exact as a two-product)
+                const dd az{I->alpha * z[r][c], fma(I->alpha, z[r][c], -I->alpha * z[r][c])};
+                const dd diff = dd_add(dd{cv, 0.0}, dd{-az.hi, -az.lo});
+                const double err = fabs(diff.hi + diff.lo);
+                // target k 2^-t |A||B| (za's own rounding widened by k 2^-50), plus the summation
+                // error of z, plus the rounding of C itself (2^-52 |C|)
+                const double tol = fabs(I->alpha) * za[r][c] *
+                                       (I->tol_scale * (1.0 + kd * 0x1p-50) + (34.0 + kd / 32.0) * 0x1p-52) +
+                                   0x1p-52 * fabs(cv) + 1e-300;
+                bad |= !(err <= tol);
+            }
         }
     }
     if (bad) atomicOr(fail + I->tile, 1);
@@ -408,7 +431,7 @@ int64_t probe_item_blocks(ProbeItem& it, int64_t block0) {
 
 void launch_probe(const ProbeItem* d, int count, int64_t blocks, int* fail, cudaStream_t st) {
     if (count <= 0 || blocks <= 0) return;
-    probe_kernel<<<static_cast<unsigned>(blocks), kProbeRows, 0, st>>>(d, count, fail);
+    probe_kernel<<<static_cast<unsigned>(blocks), kProbeThreads, 0, st>>>(d, count, fail);
 }
 
 void launch_dd_gemm_nn(int64_t m, int64_t n, int64_t k, const double* A, int64_t lda, const double* B, int64_t ldb,

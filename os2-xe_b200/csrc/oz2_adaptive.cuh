@@ -24,7 +24,9 @@ constexpr int kAdaptiveStats = 10;
 constexpr int kMlpParams = kHidden * kFeatures + kHidden + kHidden * kHidden + kHidden + kClasses * kHidden + kClasses;
 constexpr int kProbeCols = 8;    // columns per probed tile, each entry checked on its own
 constexpr int kProbeChunk = 512;  // inner-index chunk of the probe's B columns in shared memory
-constexpr int kProbeRows = 128;   // tile rows per probe block (one per thread)
+constexpr int kProbeThreads = 128;
+constexpr int kProbeRowsPerThread = 2;
+constexpr int kProbeRows = kProbeThreads * kProbeRowsPerThread;  // tile rows per probe block
 
 // histogram of exponent gaps for the rows [0, rows) of one panel (rows of op(A) or columns of
 // op(B)), all k; layout like ScaleItem

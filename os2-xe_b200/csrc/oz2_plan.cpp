@@ -184,15 +184,17 @@ void mod_constants(const Plan& p, ModConst* out) {
         c.m = m;
         c.mu = static_cast<uint32_t>((uint64_t{1} << 32) / m);
         c.h = h;
-        for (int j = 1; j <= 4; ++j) c.c[j - 1] = pow2_mod(21 * j, m);
         c.koff3 = (h + m - pow2_mod(62, m)) % m;
         c.koff5 = (h + m - pow2_mod(104, m)) % m;
         c.kbias = m * static_cast<uint32_t>(((uint64_t{1} << 31) + m - 1) / m);
+        for (int w = 0; w < 4; ++w) {
+            c.cb[w] = 0;
+            for (int b = 0; b < 4; ++b) c.cb[w] |= pow2_mod(8 * (4 * w + b), m) << (8 * b);
+        }
         // division by a constant with an exact multiply-high (Granlund and Montgomery, 1994):
-        // with M = ceil(2^(N + 8) / m) and m <= 2^8, floor(v M / 2^(N + 8)) = floor(v / m) for
-        // every v < 2^N; M < 2^32 for the moduli here (m >= 157)
-        c.mx30 = static_cast<uint32_t>(((uint64_t{1} << 38) + m - 1) / m);
-        c.mx31 = static_cast<uint32_t>(((uint64_t{1} << 39) + m - 1) / m);
+        // with M = ceil(2^32 / m) = (2^32 + e) / m, 0 <= e < m <= 2^8, floor(v M / 2^32) =
+        // floor(v / m) for every v < 2^24 (the added v e / (m 2^32) stays below 1 / m)
+        c.m32 = static_cast<uint32_t>(((uint64_t{1} << 32) + m - 1) / m);
     }
 }
 

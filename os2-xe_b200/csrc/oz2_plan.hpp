@@ -31,13 +31,12 @@ struct ModConst {
     uint32_t m;      // modulus
     uint32_t mu;     // floor(2^32 / m), Barrett
     uint32_t h;      // (m - 1) / 2: residues are kept symmetric in [-h, m-1-h]
-    uint32_t c[4];   // 2^(21 j) mod m, j = 1..4 (21-bit limb weights)
-    uint32_t koff3;  // (h - 2^62 mod m) mod m: narrow limb offset (tk <= 62)
-    uint32_t koff5;  // (h - 2^104 mod m) mod m: wide limb offset
+    uint32_t koff3;  // (h - 2^62 mod m) mod m: narrow offset (tk <= 62)
+    uint32_t koff5;  // (h - 2^104 mod m) mod m: wide offset
     uint32_t kbias;  // m ceil(2^31 / m): c + kbias is in [0, 2^32) for every int32 GEMM sum c
                      // (|c| < 2^31 - 2^21) and congruent to c modulo m
-    uint32_t mx30;   // ceil(2^38 / m): floor(v / m) = umulhi(v, mx30) >> 6 exactly for v < 2^30
-    uint32_t mx31;   // ceil(2^39 / m): floor(v / m) = umulhi(v, mx31) >> 7 exactly for v < 2^31
+    uint32_t cb[4];  // bytes 2^(8 l) mod m, l = 0..15, four per word (byte-limb weights)
+    uint32_t m32;    // ceil(2^32 / m): floor(v / m) = umulhi(v, m32) exactly for v < 2^24
 };
 
 struct Plan {

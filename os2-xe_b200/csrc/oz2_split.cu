@@ -15,7 +15,6 @@ namespace oz2 {
 namespace {
 
 constexpr uint64_t kAbsMask = 0x7FFFFFFFFFFFFFFFull;
-constexpr uint32_t kMask21 = 0x1FFFFFu;
 
 __device__ __forceinline__ int exponent_of(unsigned long long b, int tk) {
     if (b >= 0x7FF0000000000000ull) return kNonFinite;
@@ -89,22 +88,23 @@ __device__ __forceinline__ double pow2(int k) {
 // computed in floating point: y = v 2^e as two exact power-of-two products (e = e1 + e2 keeps
 // both factors normal for every e the split sees; a product that underflows means
 // |y| < 2^-1022, which rounds to 0 like the exact value), then one round-to-nearest-even
-// conversion. Narrow path (tk <= 62): x fits int64, limbs of 2^62 + x.
-__device__ __forceinline__ void offset_limbs_fp(double v, double s1, double s2, uint32_t (&L)[3]) {
+// conversion. The offset integer 2^62 + x (narrow path, tk <= 62: x fits int64) as two 32-bit
+// words.
+__device__ __forceinline__ void offset_words_fp(double v, double s1, double s2, uint32_t (&W)[2]) {
     const long long x = __double2ll_rn((v * s1) * s2);
     const uint64_t xo = static_cast<uint64_t>(x + (1ll << 62));
-    L[0] = static_cast<uint32_t>(xo) & kMask21;
-    L[1] = static_cast<uint32_t>(xo >> 21) & kMask21;
-    L[2] = static_cast<uint32_t>(xo >> 42) & kMask21;
+    W[0] = static_cast<uint32_t>(xo);
+    W[1] = static_cast<uint32_t>(xo >> 32);
 }
 
-// Wide path (62 < tk <= 100) in floating point: y = v 2^e as above, a = |rint(y)| < 2^101 split
-// exactly into hi = trunc(a 2^-64) and lo = a - hi 2^64 (both exact: power-of-two scaling, and
-// lo keeps a subset of a's 53 significant bits), then 2^104 +- (hi:lo) in 21-bit limbs.
-__device__ __forceinline__ void offset_limbs_fp_wide(double v, double s1, double s2, uint32_t (&L)[5]) {
+// Wide path (62 < tk <= 100): y = v 2^e as above, a = |rint(y)| < 2^101 split exactly into
+// hi = trunc(a 2^-64) and lo = a - hi 2^64 (both exact: power-of-two scaling, and lo keeps a
+// subset of a's 53 significant bits), then 2^104 +- (hi:lo) as four 32-bit words (the top two
+// bytes zero).
+__device__ __forceinline__ void offset_words_fp_wide(double v, double s1, double s2, uint32_t (&W)[4]) {
     const double y = rint((v * s1) * s2);
     const double a = fabs(y);
-    const double hd = trunc(a * 5.421010862427522e-20);  // 2^-64
+    const double hd = trunc(a * 5.421010862427522e-20);     // 2^-64
     const double ld = fma(hd, -18446744073709551616.0, a);  // a - hd 2^64, exact
     const uint64_t hi = __double2ull_rz(hd), lo = __double2ull_rz(ld);
     uint64_t ol, oh;
@@ -115,23 +115,22 @@ __device__ __forceinline__ void offset_limbs_fp_wide(double v, double s1, double
         ol = lo;
         oh = (1ull << 40) + hi;
     }
-    L[0] = static_cast<uint32_t>(ol) & kMask21;
-    L[1] = static_cast<uint32_t>(ol >> 21) & kMask21;
-    L[2] = static_cast<uint32_t>(ol >> 42) & kMask21;
-    L[3] = static_cast<uint32_t>((ol >> 63) | (oh << 1)) & kMask21;
-    L[4] = static_cast<uint32_t>(oh >> 20) & kMask21;
+    W[0] = static_cast<uint32_t>(ol);
+    W[1] = static_cast<uint32_t>(ol >> 32);
+    W[2] = static_cast<uint32_t>(oh);
+    W[3] = static_cast<uint32_t>(oh >> 32);
 }
 
-// (x + h) mod m in [0, m) for the value x whose offset limbs are L; the symmetric residue is this
-// minus h. The limb sum v stays below 2^30 (three limbs) or 2^31 (five limbs), where the
-// multiply-high quotient of the plan's mx30 / mx31 is exact, so no correction step follows.
-template <int NLIMB>
-__device__ __forceinline__ uint32_t shifted_residue(const uint32_t (&L)[NLIMB], const ModConst& c) {
-    uint32_t v = L[0] + (NLIMB == 3 ? c.koff3 : c.koff5);
+// (x + h) mod m in [0, m) from the bytes of the offset integer: v = koff + sum_l byte_l (2^(8 l)
+// mod m) by byte dot products (at most 14 nonzero bytes, so v < 255 + 14 255^2 < 2^20), then
+// the exact multiply-high quotient by ceil(2^32 / m). Two (four) dot products, one multiply-high
+// and one multiply-subtract per residue.
+template <int NW>
+__device__ __forceinline__ uint32_t byte_residue(const uint32_t (&W)[NW], const ModConst& c) {
+    uint32_t v = NW == 2 ? c.koff3 : c.koff5;
 #pragma unroll
-    for (int j = 1; j < NLIMB; ++j) v += L[j] * c.c[j - 1];
-    const uint32_t q = NLIMB == 3 ? __umulhi(v, c.mx30) >> 6 : __umulhi(v, c.mx31) >> 7;
-    return v - q * c.m;
+    for (int j = 0; j < NW; ++j) v = __dp4a(W[j], c.cb[j], v);
+    return v - __umulhi(v, c.m32) * c.m;
 }
 
 // low bytes of a, b, c, d as one little-endian word
@@ -139,9 +138,10 @@ __device__ __forceinline__ uint32_t pack_bytes(uint32_t a, uint32_t b, uint32_t 
     return __byte_perm(__byte_perm(a, b, 0x0040), __byte_perm(c, d, 0x0040), 0x5410);
 }
 
-// elements per thread: 16 (one 16-byte chunk of every plane) on the real narrow path; 8 (half a
-// chunk) on the wide path and for complex inputs, whose limbs per element (five, or two groups)
-// would otherwise hold 128 to 200 registers
+// NLIMB: 3 selects the narrow path (two words per offset integer), 5 the wide one (four words).
+// Elements per thread: 16 (one 16-byte chunk of every plane) on the real narrow path; 8 (half a
+// chunk) on the wide path and for complex inputs, whose words per element (four, or two groups)
+// would otherwise hold 128 registers
 template <int NLIMB, bool CPLX>
 __host__ __device__ constexpr int split_ept() {
     return NLIMB == 3 && !CPLX ? 16 : 8;
@@ -196,7 +196,8 @@ __global__ void __launch_bounds__(256) split_kernel(const SplitItem* __restrict_
     const bool live = e != kNonFinite;
 
     constexpr int NG = CPLX ? 2 : 1;
-    uint32_t L[NG][EPT][NLIMB];
+    constexpr int NW = NLIMB == 3 ? 2 : 4;  // 32-bit words of the offset integer
+    uint32_t L[NG][EPT][NW];
     const int e1 = e >> 1;
     const double s1 = pow2(live ? e1 : 0), s2 = pow2(live ? e - e1 : 0);
 #pragma unroll
@@ -214,11 +215,11 @@ __global__ void __launch_bounds__(256) split_kernel(const SplitItem* __restrict_
             }
         }
         if constexpr (NLIMB == 3) {
-            offset_limbs_fp(v0, s1, s2, L[0][q]);
-            if (CPLX) offset_limbs_fp(v1, s1, s2, L[NG - 1][q]);
+            offset_words_fp(v0, s1, s2, L[0][q]);
+            if (CPLX) offset_words_fp(v1, s1, s2, L[NG - 1][q]);
         } else {
-            offset_limbs_fp_wide(v0, s1, s2, L[0][q]);
-            if (CPLX) offset_limbs_fp_wide(v1, s1, s2, L[NG - 1][q]);
+            offset_words_fp_wide(v0, s1, s2, L[0][q]);
+            if (CPLX) offset_words_fp_wide(v1, s1, s2, L[NG - 1][q]);
         }
     }
 
@@ -226,7 +227,7 @@ __global__ void __launch_bounds__(256) split_kernel(const SplitItem* __restrict_
         const ModConst mc = I->mc[t];
         uint32_t b0[EPT], b1[EPT], b2[EPT];  // residue bytes in the low 8 bits
         if (mc.m == 256) {
-            // 2^21 j = 0 mod 256 and 2^62 = 0 mod 256: the residue byte is the low byte of 2^62 + x
+            // 2^62 = 2^104 = 0 mod 256: the residue byte is the low byte of the offset integer
 #pragma unroll
             for (int q = 0; q < EPT; ++q) {
                 b0[q] = L[0][q][0];
@@ -238,10 +239,10 @@ __global__ void __launch_bounds__(256) split_kernel(const SplitItem* __restrict_
         } else {
 #pragma unroll
             for (int q = 0; q < EPT; ++q) {
-                const uint32_t r0 = shifted_residue<NLIMB>(L[0][q], mc);
+                const uint32_t r0 = byte_residue<NW>(L[0][q], mc);
                 b0[q] = r0;
                 if (CPLX) {
-                    const uint32_t r1 = shifted_residue<NLIMB>(L[NG - 1][q], mc);
+                    const uint32_t r1 = byte_residue<NW>(L[NG - 1][q], mc);
                     // (x0 + x1 + h) mod m from the two shifted residues
                     uint32_t r2 = r0 + r1 + (mc.m - mc.h);
                     r2 = min(r2, r2 - mc.m);
