@@ -405,6 +405,8 @@ void plan_tasks(Program& prog, const std::vector<Task>& tasks, const GemmConfig&
             g.mod_m[q] = mc[q].m;
             g.mod_mu[q] = mc[q].mu;
             g.mod_kbias[q] = mc[q].kbias;
+            g.mod_kbias30[q] = mc[q].kbias30;
+            g.mod_mx31[q] = mc[q].mx31;
         }
         jobs += g.tiles * p.G * g.s;
         gi.push_back(g);

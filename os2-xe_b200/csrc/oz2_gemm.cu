@@ -68,17 +68,23 @@ __device__ __forceinline__ Job decode(const GemmParams& P, int64_t job) {
     }
     Job J;
     J.I = P.items + lo;
-    const int64_t local = job - J.I->job0;
-    const int64_t tiles = J.I->tiles;
-    J.gt = static_cast<int>(local / tiles);
-    const int64_t tile = local - static_cast<int64_t>(J.gt) * tiles;
-    const int tiles_i = J.I->tiles_i, tiles_j = J.I->tiles_j;
-    const int64_t per_grp = static_cast<int64_t>(P.group_j) * tiles_i;
-    const int64_t grp = tile / per_grp, rem = tile - grp * per_grp;
-    const int first_j = static_cast<int>(grp) * P.group_j;
-    const int gj = min(P.group_j, tiles_j - first_j);
-    J.tj = first_j + static_cast<int>(rem % gj);
-    J.ti = static_cast<int>(rem / gj);
+    // 32-bit arithmetic: an item's jobs (groups * s * tiles) are bounded by its residue planes,
+    // s m n bytes of device memory, so they stay far below 2^32 (one 64-bit division costs
+    // several times a 32-bit one, and every warp decodes every job)
+    const uint32_t local = static_cast<uint32_t>(job - J.I->job0);
+    const uint32_t tiles = static_cast<uint32_t>(J.I->tiles);
+    const uint32_t gt = local / tiles;
+    J.gt = static_cast<int>(gt);
+    const uint32_t tile = local - gt * tiles;
+    const uint32_t tiles_i = static_cast<uint32_t>(J.I->tiles_i), tiles_j = static_cast<uint32_t>(J.I->tiles_j);
+    const uint32_t group_j = static_cast<uint32_t>(P.group_j);
+    const uint32_t per_grp = group_j * tiles_i;
+    const uint32_t grp = tile / per_grp, rem = tile - grp * per_grp;
+    const uint32_t first_j = grp * group_j;
+    const uint32_t gj = min(group_j, tiles_j - first_j);
+    const uint32_t qj = rem / gj;
+    J.tj = static_cast<int>(first_j + (rem - qj * gj));
+    J.ti = static_cast<int>(qj);
     J.nch = (J.I->kb_total + kChunkKB - 1) / kChunkKB;
     return J;
 }
@@ -220,6 +226,10 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
             const int t = J.gt % J.I->s;
             const uint32_t m = OZ1 ? 1u : J.I->mod_m[t], mu = OZ1 ? 0u : J.I->mod_mu[t],
                            kbias = OZ1 ? 0u : J.I->mod_kbias[t];
+            // at most kExactKB k-blocks (one chunk): |c| <= kExactSum, so u = c + kbias30 < 2^31 and
+            // the multiply-high quotient is exact; otherwise Barrett with one correction step
+            const bool exact = !OZ1 && J.I->kb_total <= kExactKB;
+            const uint32_t kbias30 = OZ1 ? 0u : J.I->mod_kbias30[t], mx31 = OZ1 ? 0u : J.I->mod_mx31[t];
             const int64_t j = static_cast<int64_t>(J.tj) * kGemmJ + quarter * 32 + lane;
             const int64_t mm = J.I->m, nn = J.I->n;
             uint8_t* rowj = OZ1 ? nullptr : J.I->resid + J.gt * J.I->rstride + j * 32;  // + (i / 32) * 32 n
@@ -257,6 +267,23 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
                                 if (i0 + b < mm)
                                     atomicAdd(dst + (i0 + b) * ld, static_cast<unsigned long long>(
                                                                        static_cast<long long>(static_cast<int32_t>(cur[b]))));
+                        }
+                    } else if (exact) {
+                        if (j < nn && i0 < mm) {
+                            uint32_t w[8];
+#pragma unroll
+                            for (int q = 0; q < 8; ++q) {
+                                uint32_t r4[4];
+#pragma unroll
+                                for (int b = 0; b < 4; ++b) {
+                                    const uint32_t u = cur[4 * q + b] + kbias30;  // in [0, 2^31)
+                                    r4[b] = u - (__umulhi(u, mx31) >> 7) * m;    // in [0, m)
+                                }
+                                w[q] = __byte_perm(__byte_perm(r4[0], r4[1], 0x0040),
+                                                   __byte_perm(r4[2], r4[3], 0x0040), 0x5410);
+                            }
+                            *reinterpret_cast<uint4*>(blk) = make_uint4(w[0], w[1], w[2], w[3]);
+                            *reinterpret_cast<uint4*>(blk + 16) = make_uint4(w[4], w[5], w[6], w[7]);
                         }
                     } else if (j < nn && i0 < mm) {
                         uint32_t ow[8] = {0, 0, 0, 0, 0, 0, 0, 0};

@@ -88,6 +88,7 @@ struct GemmItem {
     int64_t tiles, job0;
     int tiles_i, tiles_j, s, groups;
     uint32_t mod_m[kMaxModuli], mod_mu[kMaxModuli], mod_kbias[kMaxModuli];
+    uint32_t mod_kbias30[kMaxModuli], mod_mx31[kMaxModuli];  // exact quotient, kb_total <= kExactKB
     // Ozaki-I mode only: job index t is the digit pair (pair_a[t], pair_b[t]) on anti-diagonal
     // pair_d[t]; the int32 products are added into acc[d][i acc_ld + j] (int64)
     int64_t* acc;

@@ -208,6 +208,8 @@ extern "C" int oz2_dgemm_noalloc(void* stream, char ta, char tb, int64_t m, int6
         g.mod_m[t] = mc[t].m;
         g.mod_mu[t] = mc[t].mu;
         g.mod_kbias[t] = mc[t].kbias;
+        g.mod_kbias30[t] = mc[t].kbias30;
+        g.mod_mx31[t] = mc[t].mx31;
     }
     CrtItem& c = T.c;
     c.resid = resid;

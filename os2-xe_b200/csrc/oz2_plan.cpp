@@ -187,6 +187,10 @@ void mod_constants(const Plan& p, ModConst* out) {
         c.koff3 = (h + m - pow2_mod(62, m)) % m;
         c.koff5 = (h + m - pow2_mod(104, m)) % m;
         c.kbias = m * static_cast<uint32_t>(((uint64_t{1} << 31) + m - 1) / m);
+        c.kbias30 = m * ((kExactSum + m - 1) / m);
+        // Granlund and Montgomery (1994): with M = ceil(2^39 / m) = (2^39 + e) / m, e < m <= 2^8,
+        // floor(v M / 2^39) = floor(v / m) for every v < 2^31 (v e / (m 2^39) < 1 / m)
+        c.mx31 = static_cast<uint32_t>(((uint64_t{1} << 39) + m - 1) / m);
         for (int w = 0; w < 4; ++w) {
             c.cb[w] = 0;
             for (int b = 0; b < 4; ++b) c.cb[w] |= pow2_mod(8 * (4 * w + b), m) << (8 * b);

@@ -27,6 +27,11 @@ OZ2_HD constexpr int limbs_for(int s) {
 }
 
 // Constants of one modulus as the kernels use them.
+// GEMM sums of at most kExactKB k-blocks of 128 products of int8 residues are bounded by
+// kExactSum = 511 * 128 * 128^2 < 2^30, so c + kbias30 < 2^31 and the epilogue's quotient is exact
+constexpr int kExactKB = 511;
+constexpr uint32_t kExactSum = 511u * 128u * 16384u;
+
 struct ModConst {
     uint32_t m;      // modulus
     uint32_t mu;     // floor(2^32 / m), Barrett
@@ -35,6 +40,9 @@ struct ModConst {
     uint32_t koff5;  // (h - 2^104 mod m) mod m: wide offset
     uint32_t kbias;  // m ceil(2^31 / m): c + kbias is in [0, 2^32) for every int32 GEMM sum c
                      // (|c| < 2^31 - 2^21) and congruent to c modulo m
+    uint32_t kbias30;  // m ceil(kExactSum / m): c + kbias30 is in [0, 2^31) for every int32 GEMM sum
+                       // c of at most kExactKB k-blocks (|c| <= kExactSum) and congruent to c
+    uint32_t mx31;     // ceil(2^39 / m): floor(v / m) = umulhi(v, mx31) >> 7 exactly for v < 2^31
     uint32_t cb[4];  // bytes 2^(8 l) mod m, l = 0..15, four per word (byte-limb weights)
     uint32_t m32;    // ceil(2^32 / m): floor(v / m) = umulhi(v, m32) exactly for v < 2^24
 };

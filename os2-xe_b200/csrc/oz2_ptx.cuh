@@ -48,6 +48,22 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
     return ok != 0;
 }
 
+// The same test with a suspend-time hint: a thread whose phase is pending sleeps until the phase
+// completes or about `ns` nanoseconds pass, instead of spinning, so waiting roles leave the issue
+// slots of their scheduler to the epilogue warps.
+constexpr uint32_t kWaitSleepNs = 20000;
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity), "n"(kWaitSleepNs)
+        : "memory");
+    return ok != 0;
+}
+
 // Waits for the phase of `bar` with the given parity. Returns false when the CTA-wide abort
 // flag is raised by another role, or when the wait exceeds kWaitLimitNs (then it raises the
 // flag and records `code` in the global error word).
@@ -56,7 +72,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatil
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = global_timer_ns();
     for (uint32_t it = 1;; ++it) {
-        if (mbar_try_wait(bar, parity)) return true;
+        if (mbar_try_wait_sleep(bar, parity)) return true;
         if ((it & 63) == 0) {
             if (*abort_flag) return false;
             if (global_timer_ns() - t0 > kWaitLimitNs) {
