@@ -265,6 +265,62 @@ class Timer:
         self.ms = self.e0.elapsed_time(self.e1)
 
 
+def sharded_leg(a, oz2, torch, dev, stream, dist, world, rank):
+    """One DGEMM m = n = k = 8192, s = 16, alpha 1.5, beta -0.5, U[-1,1), split over the ranks as
+    C blocks (strong scaling, oz2.sharded): every rank holds the same A, B and C (one seed), times
+    its block (CUDA events, max over ranks), then the all-gather of the blocks, and checks the
+    gathered C against its own unsharded call bit for bit (mismatches summed over ranks)."""
+    from oz2 import sharded
+    n = a.size
+    m = k = n
+    g = torch.Generator(device=dev)
+    g.manual_seed(4321)
+    A = torch.rand(m * k, dtype=torch.float64, device=dev, generator=g) * 2 - 1
+    B = torch.rand(k * n, dtype=torch.float64, device=dev, generator=g) * 2 - 1
+    C0 = torch.rand(m * n, dtype=torch.float64, device=dev, generator=g) * 2 - 1
+    C = C0.clone()
+    oz = oz2.Ozaki2(stream)
+    sho = sharded.ShardedOzaki2(oz)
+    reps = 10
+
+    def local():
+        C.copy_(C0)
+        sho.local_gemm("N", "N", m, n, k, 1.5, A, m, B, k, -0.5, C, m, a.s)
+
+    for _ in range(3):
+        local()
+    with Timer(torch, stream) as t:
+        for _ in range(reps):
+            local()
+    copy_ms = 0.0
+    with Timer(torch, stream) as tc:
+        for _ in range(reps):
+            C.copy_(C0)
+    copy_ms = tc.ms / reps
+    ms_local = max(t.ms / reps - copy_ms, 1e-6)
+    dist.barrier()
+    with Timer(torch, stream) as tg:
+        sho.gather(C, m, m, n)
+    ms_gather = tg.ms
+    full = C0.clone()
+    oz.gemm("N", "N", m, n, k, 1.5, A, m, B, k, -0.5, full, m, a.s)
+    torch.cuda.synchronize()
+    bad = torch.tensor([float((C.view(torch.int64) != full.view(torch.int64)).sum().item())], device=dev)
+    dist.all_reduce(bad, op=dist.ReduceOp.SUM)
+    ms_l, _ = over_ranks(dist, torch, world, dev, ms_local, 0.0)
+    ms_g, _ = over_ranks(dist, torch, world, dev, ms_gather, 0.0)
+    (r0, r1), (c0, c1) = sho.block(m, n)
+    oz.close()
+    del A, B, C0, C, full
+    torch.cuda.empty_cache()
+    flops = 2.0 * m * n * k
+    return {"workload": f"dgemm {n}x{n}x{n} op=NN s={a.s} alpha=1.5 beta=-0.5 U[-1,1), C blocks over {world} ranks",
+            "grid": list(sharded.grid_shape(world, m, n)), "rank0_block": [[r0, r1], [c0, c1]],
+            "scaling": "strong", "ms_block_max": ms_l, "tflops_blocks": flops / (ms_l * 1e-3) / 1e12,
+            "ms_gather": ms_g, "tflops_with_gather": flops / ((ms_l + ms_g) * 1e-3) / 1e12,
+            "entries_differing_from_unsharded": int(bad.item())}
+
+
 def grouped_leg(oz2, torch, dev, stream, reps=5):
     """512 DGEMMs, m, n, k log-uniform in [32, 2048], ops uniform over NN/NT/TN/TT, s uniform in
     14..20, U[-1,1): one grouped call (autotuned GEMM configuration, replayed from a CUDA graph)
@@ -719,6 +775,8 @@ def main():
         extras["dgemm_8192"] = dgemm_leg(a, oz2, torch, dev, stream, rank)
         extras["zgemm_4096"] = zgemm_leg(oz2, torch, dev, stream, rank)
         extras["grouped_c4"] = grouped_leg(oz2, torch, dev, stream)
+        if world > 1:
+            extras["dgemm_8192_sharded"] = sharded_leg(a, oz2, torch, dev, stream, dist, world, rank)
         if world == 1:  # the host-core baseline is quoted at one GPU only
             line["cpu_baseline"] = cpu_sample(a)
     line["extras"] = extras
