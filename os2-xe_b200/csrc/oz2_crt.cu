@@ -37,23 +37,35 @@ __device__ __forceinline__ double scale_pow2(double d, int E) {
     return ldexp(d, E);
 }
 
-// Exact reconstruction + single rounding; r[t] in [0, m_t).
-// q = round(Sum r_t y_t / m_t) from 24-bit fixed-point fractions F_t (error < 2^-12, far
-// below the 1/4 margin that |x| <= M/4 leaves, so q is the reference's FP32 quotient), then
-// x = Sum r_t W_t - q M modulo 2^(32 NL) in 64-bit words, rounded once to double.
+// Exact reconstruction + single rounding. R[g] holds the residues r_t in [0, m_t) of the moduli
+// 4g..4g+3 as bytes (zero past s). Every sum is a chain of two-way byte dot products (dp2a):
+// q = round(Sum r_t y_t / m_t) from the 16-bit fractions F16_t (error below 24 * 255 * 2^-16 <
+// 0.1, inside the 1/4 margin that |x| <= M/4 leaves, so q is the reference's FP32 quotient),
+// and Sum r_t W_t limb by limb over 16-bit limbs of W_t (each limb sum below 24 * 255 * 2^16 <
+// 2^29), then x = Sum r_t W_t - q M modulo 2^(32 NL) in 64-bit words, rounded once to double.
 template <int S, int NL>
-__device__ __forceinline__ double crt_value(const uint32_t (&r)[S], const CrtConst& cc, int shift) {
-    uint64_t uf = 0;
+__device__ __forceinline__ double crt_value(const uint32_t (&R)[(S + 3) / 4], const CrtConst& cc, int shift) {
+    constexpr int Q = (S + 3) / 4;
+    uint32_t uf = 1u << 15;  // rounding offset of the quotient
+#pragma unroll
+    for (int g = 0; g < Q; ++g) {
+        uf = __dp2a_lo(cc.Fq[g][0], R[g], uf);
+        uf = __dp2a_hi(cc.Fq[g][1], R[g], uf);
+    }
+    const int64_t q = static_cast<int64_t>(uf >> 16);
     uint64_t acc[NL];
 #pragma unroll
-    for (int l = 0; l < NL; ++l) acc[l] = 0;
+    for (int l = 0; l < NL; ++l) {
+        uint32_t a0 = 0, a1 = 0;  // 16-bit limbs 2l and 2l + 1
 #pragma unroll
-    for (int t = 0; t < S; ++t) {
-        uf += static_cast<uint64_t>(r[t]) * cc.F[t];
-#pragma unroll
-        for (int l = 0; l < NL; ++l) acc[l] += static_cast<uint64_t>(r[t]) * cc.W[t][l];
+        for (int g = 0; g < Q; ++g) {
+            a0 = __dp2a_lo(cc.Wq[g][2 * l][0], R[g], a0);
+            a0 = __dp2a_hi(cc.Wq[g][2 * l][1], R[g], a0);
+            a1 = __dp2a_lo(cc.Wq[g][2 * l + 1][0], R[g], a1);
+            a1 = __dp2a_hi(cc.Wq[g][2 * l + 1][1], R[g], a1);
+        }
+        acc[l] = static_cast<uint64_t>(a0) + (static_cast<uint64_t>(a1) << 16);
     }
-    const int64_t q = static_cast<int64_t>((uf + (1u << 23)) >> 24);
     uint32_t w[NL];
     int64_t carry = 0;
 #pragma unroll
@@ -106,6 +118,22 @@ __device__ __forceinline__ uint32_t sub_mod(uint32_t a, uint32_t b, uint32_t m) 
     return min(r, r - m);
 }
 
+// low bytes of a, b, c, d as one little-endian word
+__device__ __forceinline__ uint32_t pack4(uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+    return __byte_perm(__byte_perm(a, b, 0x0040), __byte_perm(c, d, 0x0040), 0x5410);
+}
+
+// 4 x 4 byte transpose: word t of `in` holds entries e = 0..3 of modulus 4g + t; word e of `out`
+// holds moduli 4g..4g+3 of entry e
+__device__ __forceinline__ void transpose4(uint32_t a, uint32_t b, uint32_t c, uint32_t d, uint32_t (&out)[4]) {
+    const uint32_t t0 = __byte_perm(a, b, 0x5140), t1 = __byte_perm(a, b, 0x7362);
+    const uint32_t t2 = __byte_perm(c, d, 0x5140), t3 = __byte_perm(c, d, 0x7362);
+    out[0] = __byte_perm(t0, t2, 0x5410);
+    out[1] = __byte_perm(t0, t2, 0x7632);
+    out[2] = __byte_perm(t1, t3, 0x5410);
+    out[3] = __byte_perm(t1, t3, 0x7632);
+}
+
 template <int S, bool CPLX>
 __global__ void __launch_bounds__(256) crt_kernel(const __grid_constant__ CrtParams P) {
     constexpr int NL = limbs_for(S);
@@ -130,13 +158,25 @@ __global__ void __launch_bounds__(256) crt_kernel(const __grid_constant__ CrtPar
         const int Ej = exponent_of(I->maxB[j], tk);
         const uint8_t* base = I->resid + (i0 >> 5) * (32 * I->n) + j * 32 + (i0 & 31);
         // one 32-bit word per plane = the residues of the 4 entries i0..i0+3
-        uint32_t w0[S], w1[CPLX ? S : 1], w2[CPLX ? S : 1];
+        constexpr int Q = (S + 3) / 4;
+        uint32_t w0[4 * Q], w1[CPLX ? 4 * Q : 1], w2[CPLX ? 4 * Q : 1];
 #pragma unroll
-        for (int t = 0; t < S; ++t) {
-            w0[t] = __ldg(reinterpret_cast<const uint32_t*>(base + t * rstride));
+        for (int t = 0; t < 4 * Q; ++t) {
+            w0[t] = t < S ? __ldg(reinterpret_cast<const uint32_t*>(base + t * rstride)) : 0u;
             if (CPLX) {
-                w1[t] = __ldg(reinterpret_cast<const uint32_t*>(base + gstride + t * rstride));
-                w2[t] = __ldg(reinterpret_cast<const uint32_t*>(base + 2 * gstride + t * rstride));
+                w1[t] = t < S ? __ldg(reinterpret_cast<const uint32_t*>(base + gstride + t * rstride)) : 0u;
+                w2[t] = t < S ? __ldg(reinterpret_cast<const uint32_t*>(base + 2 * gstride + t * rstride)) : 0u;
+            }
+        }
+        // real: the residue bytes regrouped per entry, four moduli per word
+        uint32_t Rq[CPLX ? 1 : 4][CPLX ? 1 : Q];
+        if constexpr (!CPLX) {
+#pragma unroll
+            for (int g = 0; g < Q; ++g) {
+                uint32_t o[4];
+                transpose4(w0[4 * g], w0[4 * g + 1], w0[4 * g + 2], w0[4 * g + 3], o);
+#pragma unroll
+                for (int e = 0; e < 4; ++e) Rq[e][g] = o[e];
             }
         }
 #pragma unroll
@@ -148,27 +188,34 @@ __global__ void __launch_bounds__(256) crt_kernel(const __grid_constant__ CrtPar
             const int shift = nonfinite ? 0 : De + Ej;
             const uint32_t sel = 0x4440 + e;  // byte e of a word, zero-extended
             double* cp = I->C + (CPLX ? 2 : 1) * (i + j * I->ldc);
-            if (!CPLX) {
-                uint32_t r[S];
-#pragma unroll
-                for (int t = 0; t < S; ++t) r[t] = __byte_perm(w0[t], 0, sel);
-                double v = crt_value<S, NL>(r, P.cc, shift);
+            if constexpr (!CPLX) {
+                double v = crt_value<S, NL>(Rq[e], P.cc, shift);
                 if (nonfinite) v = __longlong_as_double(0x7FF8000000000000ll);
                 // the reference's unfused alpha*v + beta*c, one rounding per operation
                 const double av = __dmul_rn(ar, v);
                 cp[0] = br == 0.0 ? av : __dadd_rn(av, __dmul_rn(br, cp[0]));
             } else {
-                uint32_t rr[S], ri[S];
+                uint32_t rr[4 * Q], ri[4 * Q];
 #pragma unroll
-                for (int t = 0; t < S; ++t) {
-                    const uint32_t m = P.mod_m[t];
-                    const uint32_t p0 = __byte_perm(w0[t], 0, sel), p1 = __byte_perm(w1[t], 0, sel);
-                    const uint32_t p2 = __byte_perm(w2[t], 0, sel);
-                    rr[t] = sub_mod(p0, p1, m);                  // Re = P0 - P1
-                    ri[t] = sub_mod(sub_mod(p2, p0, m), p1, m);  // Im = P2 - P0 - P1
+                for (int t = 0; t < 4 * Q; ++t) {
+                    if (t < S) {
+                        const uint32_t m = P.mod_m[t];
+                        const uint32_t p0 = __byte_perm(w0[t], 0, sel), p1 = __byte_perm(w1[t], 0, sel);
+                        const uint32_t p2 = __byte_perm(w2[t], 0, sel);
+                        rr[t] = sub_mod(p0, p1, m);                  // Re = P0 - P1
+                        ri[t] = sub_mod(sub_mod(p2, p0, m), p1, m);  // Im = P2 - P0 - P1
+                    } else {
+                        rr[t] = ri[t] = 0;
+                    }
                 }
-                double vr = crt_value<S, NL>(rr, P.cc, shift);
-                double vi = crt_value<S, NL>(ri, P.cc, shift);
+                uint32_t Rr[Q], Ri[Q];
+#pragma unroll
+                for (int g = 0; g < Q; ++g) {
+                    Rr[g] = pack4(rr[4 * g], rr[4 * g + 1], rr[4 * g + 2], rr[4 * g + 3]);
+                    Ri[g] = pack4(ri[4 * g], ri[4 * g + 1], ri[4 * g + 2], ri[4 * g + 3]);
+                }
+                double vr = crt_value<S, NL>(Rr, P.cc, shift);
+                double vi = crt_value<S, NL>(Ri, P.cc, shift);
                 if (nonfinite) vr = vi = __longlong_as_double(0x7FF8000000000000ll);
                 double orr = __dsub_rn(__dmul_rn(ar, vr), __dmul_rn(ai, vi));
                 double oi = __dadd_rn(__dmul_rn(ar, vi), __dmul_rn(ai, vr));

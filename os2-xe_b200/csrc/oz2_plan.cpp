@@ -1,6 +1,7 @@
 // oz2_plan.cpp - see oz2_plan.hpp.
 #include "oz2_plan.hpp"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -207,8 +208,13 @@ void crt_constants(const Plan& p, CrtConst& out) {
     out.s = p.s;
     out.nl = p.nl;
     for (int t = 0; t < p.s; ++t) {
-        for (int l = 0; l < p.nl; ++l) out.W[t][l] = p.W[t][l];
-        out.F[t] = static_cast<uint32_t>(((static_cast<uint64_t>(p.y[t]) << 24) + p.m[t] / 2) / p.m[t]);
+        const int g = t / 4, half = (t / 2) & 1, sh = 16 * (t & 1);
+        for (int l = 0; l < 2 * p.nl; ++l) {
+            const uint32_t w16 = (p.W[t][l / 2] >> (16 * (l & 1))) & 0xFFFFu;
+            out.Wq[g][l][half] |= w16 << sh;
+        }
+        const uint64_t f = ((static_cast<uint64_t>(p.y[t]) << 16) + p.m[t] / 2) / p.m[t];
+        out.Fq[g][half] |= static_cast<uint32_t>(std::min<uint64_t>(f, 0xFFFFu)) << sh;
     }
     for (int l = 0; l < p.nl; ++l) out.M[l] = p.M[l];
 }

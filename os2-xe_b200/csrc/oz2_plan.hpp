@@ -70,11 +70,18 @@ void mod_constants(const Plan& p, ModConst* out);
 
 // CRT table: Sum_t r_t W_t - q M with q = round(Sum_t r_t y_t / m_t) from an estimate whose
 // error is far below 1/4 (ref src/ozaki2_gpu.hpp:526-588 uses FP32; here 24-bit fixed point)
+constexpr int kQuads = (kMaxModuli + 3) / 4;  // moduli in groups of four (one residue byte each)
+
 struct CrtConst {
     int s, nl;
-    uint32_t W[kMaxModuli][kMaxLimbs];
     uint32_t M[kMaxLimbs];
-    uint32_t F[kMaxModuli];  // round(y_t / m_t * 2^24): fixed-point quotient weights
+    // W_t = (M / m_t) y_t in 16-bit limbs, paired for two-way byte dot products: for the moduli
+    // 4g..4g+3 and limb l, Wq[g][l][0] = W16[4g][l] | W16[4g+1][l] << 16 and Wq[g][l][1] the same
+    // for 4g+2, 4g+3 (zero past s)
+    uint32_t Wq[kQuads][2 * kMaxLimbs][2];
+    // F16_t = min(round(y_t / m_t 2^16), 2^16 - 1), paired the same way: fixed-point quotient
+    // weights (error per term below 2^-16, so the quotient estimate is off by less than 0.1)
+    uint32_t Fq[kQuads][2];
 };
 void crt_constants(const Plan& p, CrtConst& out);
 
