@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--seed", type=int, default=2025)
     ap.add_argument("--size", type=int, default=8192, help="m = n = k of the DGEMM extra")
     ap.add_argument("--s", type=int, default=16, help="moduli of the DGEMM extra")
+    ap.add_argument("--k", type=int, default=0, help="inner dimension of the DGEMM extra (default: --size)")
     ap.add_argument("--no-extras", action="store_true", help="skip the DGEMM, grouped and CPU legs")
     ap.add_argument("--dgemm-only", action="store_true",
                     help="time only the DGEMM of --size and --s (a profiling aid; not the headline)")
@@ -366,7 +367,8 @@ def dgemm_leg(a, oz2, torch, dev, stream, rank):
     stage times, the GEMM kernel against the int8 roofline, end to end with host buffers, and
     native cuBLAS DGEMM / cuBLASLt int8 at the same shape."""
     n = a.size
-    m = k = n
+    m = n
+    k = a.k or n
     ldc = m + 16
     g = torch.Generator(device=dev)
     g.manual_seed(1234 + rank)
@@ -408,7 +410,7 @@ def dgemm_leg(a, oz2, torch, dev, stream, rank):
     ulp, cr = oz.accuracy(blk, blk, C2, m, hi, lo)
     ratio = oz.error_ratio(blk, blk, k, C2, m, hi, lo, ab, TARGET_BITS)
     del C2, hi, lo, ab
-    out = {"workload": f"dgemm {n}x{n}x{n} op=NN s={a.s} alpha=1.5 beta=-0.5 ldc=m+16 U[-1,1)",
+    out = {"workload": f"dgemm {m}x{n}x{k} op=NN s={a.s} alpha=1.5 beta=-0.5 ldc=m+16 U[-1,1)",
            "accuracy": {"block": f"C[0:{blk}, 0:{blk}] of A B (alpha 1, beta 0) against double-double",
                         "ulp_max": ulp, "cr_frac": cr / (blk * blk), "dgemm_level_ratio": ratio},
            "tflops": flops / (ms * 1e-3) / 1e12, "ms": ms, "steps": steps,
@@ -601,6 +603,12 @@ def main():
     def analytic_batched(b):
         return oz.gemm_adaptive([as_args(p) for p in batches[b]], TARGET_BITS, oz.ADAPTIVE_ANALYTIC_PROBLEM)
 
+    def certified_tiles(b):
+        return oz.gemm_adaptive([as_args(p) for p in batches[b]], TARGET_BITS, oz.ADAPTIVE_CERTIFIED_TILE)
+
+    def certified_problem(b):
+        return oz.gemm_adaptive([as_args(p) for p in batches[b]], TARGET_BITS, oz.ADAPTIVE_CERTIFIED_PROBLEM)
+
     def analytic_plain(b):
         for p, sv in zip(batches[b], s_an[b]):
             if sv > oz2.K_MAX_MODULI:  # no moduli set reaches the target: native FP64 (cuBLAS)
@@ -620,7 +628,8 @@ def main():
     def refrule_grouped(b):
         oz.gemm_grouped([as_args(p, max(2, ref_rule(p["n"], TARGET_BITS))) for p in batches[b]])
 
-    forms = {"adaptive_mlp_batched": adaptive, "analytic_per_problem_batched": analytic_batched,
+    forms = {"adaptive_mlp_batched": adaptive, "adaptive_certified_batched": certified_tiles,
+             "certified_per_problem_batched": certified_problem, "analytic_per_problem_batched": analytic_batched,
              "analytic_per_problem_plain_calls": analytic_plain, "native_fp64_cublas": native_fp64,
              "s24_grouped": s24_grouped,
              "reference_rule_grouped": refrule_grouped}

@@ -94,20 +94,26 @@ int oz2_autotune_grouped(oz2_handle h, int count, const oz2_dgemm_problem* probl
  * FP64 GEMM for target_bits = 53 ("DGEMM-level error"). Per tile of tile x tile entries (default
  * 512), s comes from
  *   mode 0: the MLP (oz2_mlp_set_weights; a tile takes the largest class over itself and its
- *           up to 8 neighbours in the problem), capped by the analytic s, for problems with
- *           beta = 0 (others take the analytic s); a problem whose tiles then differ by at most
- *           one takes the largest for all; tiles below their analytic s are probed (C x against
- *           A (B x) with x = e_j for 8 columns j, each entry checked) and rerun at the analytic s
- *           when the probe fails; without weights it behaves as mode 1
- * A problem whose tiles all share one s runs as one task (as a plain call would).
+ *           up to 8 neighbours in the problem), capped by the judge's s, for problems with
+ *           beta = 0 and tiles without a certificate (the others take the judge's s); tiles below
+ *           the judge's s are probed (C x against A (B x) with x = e_j for 8 columns j, each entry
+ *           checked) and rerun at it when the probe fails; without weights it behaves as mode 4
  *   mode 1: the analytic s of the tile: smallest s whose tk >= R + 2 + t - floor(log2(k - 1)),
  *           R the largest exponent gap below the row / column maximum in the tile's panels
  *   mode 2: the analytic s of the whole problem (the largest over its tiles)
  *   mode 3: each problem's own num_moduli (tiled like the other modes)
- * In modes 0-2 a tile that no s <= 24 brings to the target (analytic s or MLP class 25) runs as a
- * native FP64 GEMM (cuBLAS DGEMM), the whole problem in one call when all its tiles do.
+ *   mode 4: the judge's s of the tile (no MLP, no probe: every tile meets the target)
+ *   mode 5: the judge's s of the whole problem (the largest over its tiles)
+ * The judge of a tile is the smaller of its analytic s and, for problems with a tile whose analytic
+ * s is 23 or more (k <= 65472), its certified s: the smallest s for which a rigorous entrywise
+ * bound of the emulation's error (row / column sums of |A| and |B| against a bf16 lower bound of
+ * |A||B| from a tcgen05 GEMM) meets the target in every entry of the tile. In modes 0 and 4 a
+ * problem runs as one task at the largest s of its tiles (or in native FP64) when that costs no
+ * more than its tiles as chosen, counting a tile task 12 % dearer and native FP64 as 63 moduli.
+ * In modes 0-2, 4 and 5 a tile that no s <= 24 brings to the target (judge or MLP class 25) runs as
+ * a native FP64 GEMM (cuBLAS DGEMM), the whole problem in one call when all its tiles do.
  * stats (may be NULL, 10 entries): tiles, sum of s over emulated tiles (reruns included), probed
- * tiles, rerun tiles, sum of s of the reruns (25 for native), sum of analytic s (25 for native),
+ * tiles, rerun tiles, sum of s of the reruns (25 for native), sum of the judge's s (25 for native),
  * MLP used, int8 multiply-adds of the emulated tiles (s m_t n_t k summed, reruns included),
  * native tiles, native FP64 multiply-adds. Synchronises the stream. With profiling on,
  * oz2_stage_times reports scale (with the tile statistics, features and MLP), split, GEMM and CRT

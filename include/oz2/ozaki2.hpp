@@ -60,7 +60,7 @@ struct GemmConfig {
 };
 
 // how gemm_adaptive picks s per tile (oz2_dgemm_adaptive modes)
-enum class Adaptive { Mlp = 0, AnalyticTile = 1, AnalyticProblem = 2, Fixed = 3 };
+enum class Adaptive { Mlp = 0, AnalyticTile = 1, AnalyticProblem = 2, Fixed = 3, CertifiedTile = 4, CertifiedProblem = 5 };
 
 struct AdaptiveStats {
     int64_t tiles = 0, sum_s = 0, probed = 0, rerun = 0, rerun_sum_s = 0, analytic_sum_s = 0, mlp = 0,

@@ -12,6 +12,8 @@ Definitions (no counterpart in the reference, whose number of moduli is fixed pe
   Ozaki2::gemm for this k) reach R + 2 + t - floor(log2(k - 1)), R the largest gap of the tile's
   two panels, t the target bits; 25 (the tile runs as a native FP64 GEMM) when none does.
 """
+import math
+
 import numpy as np
 
 TILE = 512
@@ -104,3 +106,34 @@ def tile_features(oracle, problems, target_bits=53, tile=TILE):
 def problem_analytic_s(oracle, ta, tb, m, n, k, A, B, target_bits=53, tile=TILE):
     """the largest analytic s over the problem's tiles (the per-problem fixed analytic s)"""
     return int(tile_features(oracle, [(ta, tb, m, n, k, A, B)], target_bits, tile)[1].max())
+
+
+def certified_s(oracle, opA, opB, target_bits=53):
+    """certified s of one tile: op(A) (m x k) and op(B) (k x n) as numpy arrays, restating the
+    entrywise a-priori bound of the library's certificate with the FP64 product |op(A)||op(B)| in
+    place of its bf16 lower bound (so the library's s is this one or above). 25 when no s
+    reaches it, the two roundings use up the target or an input is non-finite."""
+    k = opA.shape[1]
+    t = float(target_bits)
+    Bu = k - 2.0 ** (t - 52.0)
+    if Bu <= 0 or not (np.all(np.isfinite(opA)) and np.all(np.isfinite(opB))):
+        return 25
+    ma, mb = np.abs(opA).max(axis=1), np.abs(opB).max(axis=0)
+    e = np.where(ma > 0, np.frexp(ma)[1], 0)
+    f = np.where(mb > 0, np.frexp(mb)[1], 0)
+    Ra = np.abs(opA).sum(axis=1) * np.ldexp(1.0, -e)
+    Sb = np.abs(opB).sum(axis=0) * np.ldexp(1.0, -f)
+    G = (np.abs(opA) @ np.abs(opB)) * np.ldexp(1.0, -e)[:, None] * np.ldexp(1.0, -f)[None, :]
+    live = (Ra[:, None] > 0) & (Sb[None, :] > 0)
+    if not np.any(live):
+        return 2
+    if np.any(G[live] == 0):
+        return 25
+    q1 = ((Ra[:, None] + Sb[None, :]) / np.where(live, G, 1.0))[live].max()
+    q2 = (1.0 / np.where(live, G, 1.0))[live].max()
+    c = 1.0 - 2.0 ** -6
+    l1 = math.log2(q1 * (1 + 2.0 ** -20)) + t - 1.0 - math.log2(Bu * c * (1 - 2.0 ** -10))
+    l2 = 0.5 * (math.log2(q2 * (1 + 2.0 ** -20)) + t + 10.0 - math.log2(Bu / k * c))
+    need = math.ceil(max(l1, l2) + 1e-9)
+    tk = tk_table(oracle, k)
+    return next((s for s in range(2, 25) if tk[s] > 0 and tk[s] >= need), 25)

@@ -15,7 +15,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 BUILD = os.path.join(HERE, "_build")
 OUT = os.path.join(HERE, "oz2", "liboz2.so")
-SOURCES = ["oz2_plan.cpp", "oz2_split.cu", "oz2_gemm.cu", "oz2_crt.cu", "oz2_api.cu", "oz2_noalloc.cu", "oz2_adaptive.cu", "oz2_mlp.cu"]
+SOURCES = ["oz2_plan.cpp", "oz2_split.cu", "oz2_gemm.cu", "oz2_crt.cu", "oz2_api.cu", "oz2_noalloc.cu", "oz2_adaptive.cu",
+           "oz2_mlp.cu", "oz2_certify.cu"]
 NVCC = os.environ.get("OZ2_NVCC", "/usr/local/cuda/bin/nvcc")
 HOST_CXX = "/usr/bin/g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -64,6 +64,36 @@ struct ProbeItem {
     int64_t block0;
 };
 
+// ---- certified s (a rigorous entrywise a-priori bound, see oz2_certify.cu)
+// one panel side of a problem: the scaled magnitudes |x| 2^-e_r of its rows (rows of op(A) or
+// columns of op(B)) as bf16 planes in the GEMM's tiled layout (128 x 128-byte swizzled tiles,
+// 64 elements per 128-byte row, padding rows and k zero), and their sums R'_r in FP64
+struct CertPrepItem {
+    const double* X;
+    int64_t ldx, rows, k;
+    int row_contig;                     // rows contiguous (X[r + p ldx]) or k contiguous (X[p + r ldx])
+    const unsigned long long* maxbits;  // row maxima (raw bits) of the rows
+    uint8_t* planes;
+    int64_t rows_pad, kb_total;         // plane geometry (kb_total 128-byte blocks of 64 elements)
+    double* rsum;                       // R'_r (0 for a zero or non-finite row)
+    int64_t block0, blocks;
+};
+// one C tile: the two maxima the certificate GEMM left for it, its rows' and columns' maxima
+struct CertTileItem {
+    const unsigned int* q;  // FP32 bits: max (R'_i + S'_j) / G_ij, max 1 / G_ij (0 when all exact)
+    const unsigned long long* maxa;
+    const unsigned long long* maxb;
+    int64_t mb, nb, k;
+    int target_bits;
+    int tk[kMaxModuli + 1];
+    int* s_out;  // smallest certified s, kNativeS where none is (or the tile has a non-finite row)
+};
+constexpr int kCertRowsPerBlock = 32;   // rows-contiguous prep: 32 rows x 8 k slices per block
+constexpr int64_t kCertMaxK = 65472;     // one k chunk of the GEMM (1023 blocks of 64 bf16)
+int64_t cert_prep_blocks(CertPrepItem& it, int64_t block0);
+void launch_cert_prep(const CertPrepItem* d, const CertPrepItem* h, int count, int64_t blocks, cudaStream_t st);
+void launch_cert_tiles(const CertTileItem* d, int count, cudaStream_t st);
+
 int64_t stat_item_blocks(StatItem& it, int64_t block0);
 void launch_panel_stats(const StatItem* d, const StatItem* h, int count, int64_t blocks, cudaStream_t st);
 void launch_tile_features(const FeatureItem* d, int count, float* feat, int* s_analytic, cudaStream_t st);

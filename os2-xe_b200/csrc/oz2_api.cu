@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <limits>
 #include <map>
 #include <memory>
@@ -907,8 +908,171 @@ struct TileRef {
     int ia, jb;    // panel indices
 };
 
-// mode: 0 MLP per tile (analytic cap, probe, rerun at analytic s), 1 analytic per tile,
-// 2 analytic per problem (the largest of its tiles), 3 the problems' own num_moduli
+// The certified s of every tile (oz2_certify.cu): per group of problems that fits the budget,
+// bf16 planes of the scaled magnitudes and the row / column sums, one persistent tcgen05 GEMM
+// launch over all the group's problems whose epilogue keeps two maxima per tile, then one thread
+// per tile. A problem with k above one GEMM chunk, or whose planes exceed the budget on their
+// own, keeps kNativeS (no certificate: its tiles take the analytic s).
+int certify_tiles(oz2_context* h, const std::vector<Prob>& base, const std::vector<TileRef>& tiles, int64_t T,
+                  const std::function<unsigned long long*(int)>& maxA, const std::function<unsigned long long*(int)>& maxB,
+                  const std::map<int64_t, std::vector<int>>& tk_cache, const std::vector<char>& want, int target_bits,
+                  unsigned int* d_q, int* d_sc) {
+    const size_t budget = h->ws_limit ? h->ws_limit / 2 : (size_t{4} << 30);
+    std::vector<int64_t> first_tile(base.size(), -1), ntile(base.size(), 0);
+    for (int64_t t = 0; t < static_cast<int64_t>(tiles.size()); ++t) {
+        const int q = tiles[t].prob;
+        if (first_tile[q] < 0) first_tile[q] = t;
+        ++ntile[q];
+    }
+    auto bytes_of = [&](const Prob& p) {
+        return align256(plane_geom(p.m, 2 * p.k, kGemmIPad).plane_bytes) +
+               align256(plane_geom(p.n, 2 * p.k, kGemmJ).plane_bytes) + align256(8 * static_cast<size_t>(p.m)) +
+               align256(8 * static_cast<size_t>(p.n));
+    };
+    size_t q0 = 0;
+    while (q0 < base.size()) {
+        std::vector<size_t> group;
+        size_t q1 = q0, total = 0;
+        for (; q1 < base.size(); ++q1) {
+            const Prob& p = base[q1];
+            if (!want[q1] || p.k > kCertMaxK || bytes_of(p) > budget) continue;  // no certificate for this one
+            if (!group.empty() && total + bytes_of(p) > budget) break;
+            total += bytes_of(p);
+            group.push_back(q1);
+        }
+        q0 = q1;
+        if (group.empty()) continue;
+        struct Buf {
+            size_t pa, pb, ra, sb;
+            PlaneGeom ga, gb;
+        };
+        std::vector<Buf> buf(group.size());
+        size_t off = 0;
+        auto carve = [&](size_t b) {
+            const size_t o = off;
+            off += align256(b);
+            return o;
+        };
+        int64_t nt = 0;
+        for (size_t g = 0; g < group.size(); ++g) {
+            const Prob& p = base[group[g]];
+            Buf& b = buf[g];
+            b.ga = plane_geom(p.m, 2 * p.k, kGemmIPad);
+            b.gb = plane_geom(p.n, 2 * p.k, kGemmJ);
+            b.pa = carve(b.ga.plane_bytes);
+            b.pb = carve(b.gb.plane_bytes);
+            b.ra = carve(8 * static_cast<size_t>(p.m));
+            b.sb = carve(8 * static_cast<size_t>(p.n));
+            nt += ntile[group[g]];
+        }
+        const size_t odesc = off;
+        const size_t desc = 2 * align256(2 * group.size() * sizeof(CertPrepItem)) +
+                            align256(group.size() * sizeof(GemmItem)) + align256(nt * sizeof(CertTileItem));
+        int st = ensure_ws2(h, odesc + desc + 4096);
+        if (st) return st;
+        unsigned char* w = h->ws2;
+        size_t dpos = odesc;
+        // bf16 planes of the scaled magnitudes and the sums, grouped by layout
+        std::vector<CertPrepItem> prep[2];
+        for (size_t g = 0; g < group.size(); ++g) {
+            const int q = static_cast<int>(group[g]);
+            const Prob& p = base[q];
+            const Buf& b = buf[g];
+            for (int side = 0; side < 2; ++side) {
+                CertPrepItem it{};
+                it.X = side ? p.B : p.A;
+                it.ldx = side ? p.ldb : p.lda;
+                it.rows = side ? p.n : p.m;
+                it.k = p.k;
+                it.row_contig = side ? !is_n(p.tb) : is_n(p.ta);
+                it.maxbits = side ? maxB(q) : maxA(q);
+                it.planes = reinterpret_cast<uint8_t*>(w + (side ? b.pb : b.pa));
+                it.rows_pad = side ? b.gb.rows_pad : b.ga.rows_pad;
+                it.kb_total = b.ga.kb_total;
+                it.rsum = reinterpret_cast<double*>(w + (side ? b.sb : b.ra));
+                prep[it.row_contig].push_back(it);
+            }
+        }
+        for (int lay = 0; lay < 2; ++lay) {
+            if (prep[lay].empty()) continue;
+            int64_t blocks = 0;
+            for (auto& it : prep[lay]) blocks += cert_prep_blocks(it, blocks);
+            unsigned char* dd = w + dpos;
+            const size_t nbytes = prep[lay].size() * sizeof(CertPrepItem);
+            if ((st = put_blob(h, prep[lay].data(), nbytes, dd))) return st;
+            launch_cert_prep(reinterpret_cast<const CertPrepItem*>(dd), prep[lay].data(),
+                             static_cast<int>(prep[lay].size()), blocks, h->stream);
+            ++h->launches;
+            dpos += align256(nbytes);
+        }
+        // the GEMM over all problems of the group: one job per (256 x 128) tile, s = 1
+        std::vector<GemmItem> gi(group.size());
+        int64_t jobs = 0;
+        for (size_t g = 0; g < group.size(); ++g) {
+            const int q = static_cast<int>(group[g]);
+            const Prob& p = base[q];
+            const Buf& b = buf[g];
+            GemmItem& it = gi[g];
+            it = GemmItem{};
+            it.planes_i = reinterpret_cast<const int8_t*>(w + b.pa);
+            it.planes_j = reinterpret_cast<const int8_t*>(w + b.pb);
+            it.m = p.m;
+            it.n = p.n;
+            it.kb_total = b.ga.kb_total;
+            it.tiles_i = static_cast<int>(gemm_tiles_i(p.m, 256));
+            it.tiles_j = static_cast<int>(ceil_div(p.n, kGemmJ));
+            it.tiles = static_cast<int64_t>(it.tiles_i) * it.tiles_j;
+            it.s = 1;
+            it.groups = 1;
+            it.job0 = jobs;
+            it.cert_ra = reinterpret_cast<const double*>(w + b.ra);
+            it.cert_sb = reinterpret_cast<const double*>(w + b.sb);
+            it.cert_q = d_q + 2 * first_tile[q];
+            it.cert_tile = T;
+            it.cert_na = ceil_div(p.m, T);
+            jobs += it.tiles;
+        }
+        unsigned char* dg = w + dpos;
+        if ((st = put_blob(h, gi.data(), gi.size() * sizeof(GemmItem), dg))) return st;
+        dpos += align256(gi.size() * sizeof(GemmItem));
+        launch_gemm_cert(reinterpret_cast<const GemmItem*>(dg), static_cast<int>(gi.size()), jobs, h->num_sms,
+                         h->d_err, h->stream);
+        ++h->launches;
+        // s per tile
+        std::vector<CertTileItem> ti;
+        ti.reserve(nt);
+        for (size_t g = 0; g < group.size(); ++g) {
+            const int q = static_cast<int>(group[g]);
+            const Prob& p = base[q];
+            const std::vector<int>& tk = tk_cache.at(p.k);
+            for (int64_t t = first_tile[q]; t < first_tile[q] + ntile[q]; ++t) {
+                const TileRef& r = tiles[t];
+                CertTileItem it{};
+                it.q = d_q + 2 * t;
+                it.maxa = maxA(q) + r.i0;
+                it.maxb = maxB(q) + r.j0;
+                it.mb = r.mb;
+                it.nb = r.nb;
+                it.k = p.k;
+                it.target_bits = target_bits;
+                for (int s = 0; s <= kMaxModuli; ++s) it.tk[s] = tk[s];
+                it.s_out = d_sc + t;
+                ti.push_back(it);
+            }
+        }
+        unsigned char* dt = w + dpos;
+        if ((st = put_blob(h, ti.data(), ti.size() * sizeof(CertTileItem), dt))) return st;
+        launch_cert_tiles(reinterpret_cast<const CertTileItem*>(dt), static_cast<int>(ti.size()), h->stream);
+        ++h->launches;
+    }
+    return OZ2_OK;
+}
+
+// mode: 0 MLP per tile for tiles without a certificate (judge cap, probe, rerun at the judge's s;
+// certified tiles take the judge's s), 1 analytic per tile,
+// 2 analytic per problem (the largest of its tiles), 3 the problems' own num_moduli, 4 certified
+// per tile, 5 certified per problem. The judge of a tile is the smaller of its analytic and
+// certified s (modes 0, 4, 5; the analytic s alone in modes 1 and 2).
 int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>& fixed_s, int target_bits,
                  int mode, float* feat_out = nullptr, int* sa_out = nullptr, int64_t* ntiles_out = nullptr) {
     const int64_t T = h->adaptive_tile;
@@ -944,10 +1108,12 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
     }
     const size_t ohist = carve1(static_cast<size_t>(npanels) * (kGapBins + 1) * 4);
     const size_t ofail = carve1(static_cast<size_t>(ntiles) * 4);
+    const size_t ocq = carve1(static_cast<size_t>(ntiles) * 8);  // the certificate's two maxima per tile
     const size_t zero_end = off;
     const size_t ofeat = carve1(static_cast<size_t>(ntiles) * kFeatures * 4);
     const size_t osa = carve1(static_cast<size_t>(ntiles) * 4);
     const size_t osm = carve1(static_cast<size_t>(ntiles) * 4);
+    const size_t osc = carve1(static_cast<size_t>(ntiles) * 4);
     const size_t desc_bytes = 1024 + base.size() * 2 * sizeof(ScaleItem) + npanels * sizeof(StatItem) +
                               ntiles * (sizeof(FeatureItem) + sizeof(ProbeItem)) + 16 * 256;
     const size_t odesc = carve1(desc_bytes);
@@ -961,6 +1127,8 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
     float* d_feat = reinterpret_cast<float*>(ws + ofeat);
     int* d_sa = reinterpret_cast<int*>(ws + osa);
     int* d_sm = reinterpret_cast<int*>(ws + osm);
+    int* d_sc = reinterpret_cast<int*>(ws + osc);
+    unsigned int* d_q = reinterpret_cast<unsigned int*>(ws + ocq);
     OZ2_CUDA(h, cudaMemsetAsync(ws, 0, zero_end, h->stream));
 
     Program ph1;
@@ -1046,11 +1214,30 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
         launch_mlp_infer(h->d_mlp, static_cast<int>(ntiles), d_feat, h->mlp_threshold, d_sm, nullptr, h->stream);
         ++h->launches;
     }
-    mark(h, kScale);  // statistics, features and the MLP count with the scale stage
-    std::vector<int> s_an(ntiles), s_ml(ntiles, kMaxModuli);
+    constexpr int kNoCertificate = 0x7F7F7F7F;  // the device's fill byte 0x7F: above every s
+    std::vector<int> s_an(ntiles), s_ml(ntiles, kMaxModuli), s_ce(ntiles, kNoCertificate);
     OZ2_CUDA(h, cudaMemcpyAsync(s_an.data(), d_sa, ntiles * 4, cudaMemcpyDeviceToHost, h->stream));
     if (use_mlp) OZ2_CUDA(h, cudaMemcpyAsync(s_ml.data(), d_sm, ntiles * 4, cudaMemcpyDeviceToHost, h->stream));
     OZ2_CUDA(h, cudaStreamSynchronize(h->stream));
+    // The certificate costs about three moduli of emulation over the problem and saves about four
+    // where the analytic s is emulated, far more where it is native: it runs for the problems
+    // with a tile at kCertFromS or above.
+    constexpr int kCertFromS = 23;
+    const bool certify = mode == 0 || mode == 4 || mode == 5;
+    if (certify && mode >= 0) {
+        std::vector<char> want(base.size(), 0);
+        bool any = false;
+        for (int64_t t = 0; t < ntiles; ++t)
+            if (s_an[t] >= kCertFromS) any = want[tiles[t].prob] = 1;
+        if (any) {
+            OZ2_CUDA(h, cudaMemsetAsync(d_sc, 0x7F, ntiles * 4, h->stream));  // kNoCertificate
+            if ((st = certify_tiles(h, base, tiles, T, maxA, maxB, tk_cache, want, target_bits, d_q, d_sc)))
+                return st;
+            OZ2_CUDA(h, cudaMemcpyAsync(s_ce.data(), d_sc, ntiles * 4, cudaMemcpyDeviceToHost, h->stream));
+            OZ2_CUDA(h, cudaStreamSynchronize(h->stream));
+        }
+    }
+    mark(h, kScale);  // statistics, certificate, features and the MLP count with the scale stage
     if (mode < 0) {  // features only
         if (feat_out)
             OZ2_CUDA(h, cudaMemcpyAsync(feat_out, d_feat, ntiles * kFeatures * 4, cudaMemcpyDeviceToDevice, h->stream));
@@ -1082,18 +1269,28 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
         }
         s_ml.swap(pooled);
     }
+    // the judge: the smaller of the analytic and the certified s (both meet the target)
+    std::vector<int> s_jd(ntiles);
+    for (int64_t t = 0; t < ntiles; ++t) s_jd[t] = certify ? std::min(s_an[t], std::max(s_ce[t], 2)) : s_an[t];
     std::vector<int> s_tile(ntiles);
     std::vector<int> prob_max(base.size(), 2);
-    for (int64_t t = 0; t < ntiles; ++t) prob_max[tiles[t].prob] = std::max(prob_max[tiles[t].prob], s_an[t]);
+    for (int64_t t = 0; t < ntiles; ++t) prob_max[tiles[t].prob] = std::max(prob_max[tiles[t].prob], s_jd[t]);
     for (int64_t t = 0; t < ntiles; ++t) {
         const int q = tiles[t].prob;
         int sv;
         switch (mode) {
             // the probe and the rerun need C's old values gone (beta = 0): other problems keep
-            // the analytic s
-            case 0: sv = use_mlp && base[q].beta[0] == 0.0 ? std::min(s_ml[t], s_an[t]) : s_an[t]; break;
-            case 1: sv = s_an[t]; break;
-            case 2: sv = prob_max[q]; break;
+            // the judge's s
+            // a tile with a certificate takes it (rigorous, within about a modulus of the smallest
+            // s that meets the target); the MLP chooses for the others, below the analytic s
+            case 0:
+                sv = use_mlp && base[q].beta[0] == 0.0 && s_ce[t] == kNoCertificate ? std::min(s_ml[t], s_jd[t])
+                                                                                     : s_jd[t];
+                break;
+            case 1:
+            case 4: sv = s_jd[t]; break;
+            case 2:
+            case 5: sv = prob_max[q]; break;
             default: sv = fixed_s[q]; break;
         }
         if (sv >= kNativeS) {
@@ -1105,18 +1302,32 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
         while (sv < kMaxModuli && tk[sv] == 0) ++sv;
         s_tile[t] = std::max(2, std::min(kMaxModuli, sv));
     }
-    if (use_mlp) {
-        // a problem whose tiles' s differ by at most one (none native) takes the largest for all
-        // of them: it then runs as one task, its panels split once
-        std::vector<int> lo(base.size(), kNativeS), hi(base.size(), 0);
-        for (int64_t t = 0; t < ntiles; ++t) {
-            lo[tiles[t].prob] = std::min(lo[tiles[t].prob], s_tile[t]);
-            hi[tiles[t].prob] = std::max(hi[tiles[t].prob], s_tile[t]);
-        }
+    if (mode == 0 || mode == 4) {
+        // Per problem, the cheaper of its tiles as chosen and one whole-problem task (a larger s
+        // only adds bits; native FP64 always meets the target). Work per tile ~ s mb nb k for an
+        // emulated tile (a tile task costing kTileTax more than the same work in a whole-problem
+        // task: more splits of the same panels, shorter GEMM tasks) and ~ kNativeCost mb nb k
+        // for a native one (per-tile cuBLAS calls kTileTax more than one whole call). Measured
+        // on B200: native FP64 costs as much as about 63 moduli of emulation.
+        constexpr double kTileTax = 1.12, kNativeCost = 63.0;
+        std::vector<double> tiles_cost(base.size(), 0.0), area(base.size(), 0.0);
+        std::vector<int> hi(base.size(), 0);
         for (int64_t t = 0; t < ntiles; ++t) {
             const int q = tiles[t].prob;
-            if (hi[q] <= kMaxModuli && hi[q] - lo[q] <= 1) s_tile[t] = hi[q];
+            const double a = static_cast<double>(tiles[t].mb) * tiles[t].nb;
+            const int sv = s_tile[t];
+            tiles_cost[q] += kTileTax * a * (sv >= kNativeS ? kNativeCost : sv);
+            area[q] += a;
+            hi[q] = std::max(hi[q], sv);
         }
+        std::vector<int> whole(base.size(), 0);  // 0 keep the tiles, else the s of one task
+        for (size_t q = 0; q < base.size(); ++q) {
+            const double emu = hi[q] <= kMaxModuli ? hi[q] * area[q] : 1e300;
+            const double nat = kNativeCost * area[q];
+            if (std::min(emu, nat) <= tiles_cost[q]) whole[q] = emu <= nat ? hi[q] : kNativeS;
+        }
+        for (int64_t t = 0; t < ntiles; ++t)
+            if (whole[tiles[t].prob]) s_tile[t] = whole[tiles[t].prob];
     }
 
     // ---- phase 2: tiles with their s, panels split once per (panel, s); batches by budget
@@ -1190,6 +1401,9 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
             free_b += h->ws2_size;
             const size_t reserve = (size_t{512} << 20) + total / 32;
             limit = free_b > reserve ? free_b - reserve : 0;
+            // a batch of 16 GiB of planes and residues keeps every SM busy for milliseconds; more
+            // only takes memory from the rest of the process (the caller's tensors, other calls)
+            limit = std::min(limit, size_t{16} << 30);
         }
         // a problem whose tiles all run here at one s is one task: its GEMM jobs then share the
         // planes through the L2 across the whole problem, as in a plain call
@@ -1341,7 +1555,7 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
         for (const int64_t t : porder) {
             const TileRef& r = tiles[t];
             const Prob& p = base[r.prob];
-            if (p.beta[0] != 0.0 || s_tile[t] >= s_an[t]) continue;  // analytic s needs no probe
+            if (p.beta[0] != 0.0 || s_tile[t] >= s_jd[t]) continue;  // the judge's s needs no probe
             ProbeItem it{};
             it.a_rowc = is_n(p.ta);
             it.b_rowc = !is_n(p.tb);
@@ -1377,7 +1591,7 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
             for (int64_t t = 0; t < ntiles; ++t)
                 if (failed[t]) {
                     redo.push_back(t);
-                    redo_s.push_back(s_an[t]);
+                    redo_s.push_back(s_jd[t]);
                 }
             h->astats[3] = static_cast<int64_t>(redo.size());
             if (!redo.empty()) {
@@ -1389,7 +1603,7 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
             }
         }
     }
-    for (int64_t t = 0; t < ntiles; ++t) h->astats[5] += s_an[t];
+    for (int64_t t = 0; t < ntiles; ++t) h->astats[5] += s_jd[t];
     h->astats[6] = use_mlp ? 1 : 0;
     return OZ2_OK;
 }
@@ -1715,7 +1929,7 @@ int oz2_dgemm_adaptive(oz2_handle h, int count, const oz2_dgemm_problem* problem
     if (!h) return fail(nullptr, OZ2_EINVAL, "oz2: null handle");
     if (count < 0 || (count > 0 && !problems)) return fail(h, OZ2_EINVAL, "oz2: bad problem list");
     if (target_bits < 1 || target_bits > 120) return fail(h, OZ2_EINVAL, "oz2: target_bits must be in [1, 120]");
-    if (mode < 0 || mode > 3) return fail(h, OZ2_EINVAL, "oz2: mode must be 0..3");
+    if (mode < 0 || mode > 5) return fail(h, OZ2_EINVAL, "oz2: mode must be 0..5");
     h->marks.clear();
     if (h->plans.size() > 8192) h->plans.clear();
     std::vector<Prob> probs;

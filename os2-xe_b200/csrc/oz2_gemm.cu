@@ -89,10 +89,15 @@ __device__ __forceinline__ Job decode(const GemmParams& P, int64_t job) {
     return J;
 }
 
-// OZ1: the Ozaki Scheme I baseline (job t = digit pair, int64 atomic sums per anti-diagonal
-// instead of residues)
-template <int BN, bool OZ1>
+// KIND: kKindResidue the Ozaki-II GEMM (int8 planes, residues mod m); kKindOz1 the Ozaki Scheme I
+// baseline (job t = digit pair, int64 atomic sums per anti-diagonal instead of residues);
+// kKindCert the certificate (bf16 planes of scaled magnitudes, kind::f16 MMAs, the largest
+// (R'_i + S'_j) / G_ij and 1 / G_ij per adaptive tile instead of residues)
+constexpr int kKindResidue = 0, kKindOz1 = 1, kKindCert = 2;
+
+template <int BN, int KIND>
 __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __grid_constant__ GemmParams P) {
+    constexpr bool OZ1 = KIND == kKindOz1, CERT = KIND == kKindCert;
     using C = Cfg<BN>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t{1023});
@@ -196,8 +201,14 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
                         const uint32_t sI = sJ + C::kStageJ;
 #pragma unroll
                         for (int kk = 0; kk < kTileK / 32; ++kk) {
-                            dev::mma_i8(d_tmem, dev::sw128_kmajor_desc(sJ + kk * 32), dev::sw128_kmajor_desc(sI + kk * 32),
-                                        C::kIdesc, (kb > kb0 || kk > 0) ? 1u : 0u);
+                            if constexpr (CERT)
+                                dev::mma_bf16(d_tmem, dev::sw128_kmajor_desc(sJ + kk * 32),
+                                              dev::sw128_kmajor_desc(sI + kk * 32), dev::idesc_bf16(kGemmJ, BN),
+                                              (kb > kb0 || kk > 0) ? 1u : 0u);
+                            else
+                                dev::mma_i8(d_tmem, dev::sw128_kmajor_desc(sJ + kk * 32),
+                                            dev::sw128_kmajor_desc(sI + kk * 32), C::kIdesc,
+                                            (kb > kb0 || kk > 0) ? 1u : 0u);
                         }
                         issued = true;
                         dev::tc_commit(empty(stage));
@@ -224,15 +235,19 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
         for (int64_t job = blockIdx.x; ok && job < P.jobs; job += nprog) {
             const Job J = decode(P, job);
             const int t = J.gt % J.I->s;
-            const uint32_t m = OZ1 ? 1u : J.I->mod_m[t], mu = OZ1 ? 0u : J.I->mod_mu[t],
-                           kbias = OZ1 ? 0u : J.I->mod_kbias[t];
+            constexpr bool RES = KIND == kKindResidue;
+            const uint32_t m = RES ? J.I->mod_m[t] : 1u, mu = RES ? J.I->mod_mu[t] : 0u,
+                           kbias = RES ? J.I->mod_kbias[t] : 0u;
             // at most kExactKB k-blocks (one chunk): |c| <= kExactSum, so u = c + kbias30 < 2^31 and
             // the multiply-high quotient is exact; otherwise Barrett with one correction step
-            const bool exact = !OZ1 && J.I->kb_total <= kExactKB;
-            const uint32_t kbias30 = OZ1 ? 0u : J.I->mod_kbias30[t], mx31 = OZ1 ? 0u : J.I->mod_mx31[t];
+            const bool exact = RES && J.I->kb_total <= kExactKB;
+            const uint32_t kbias30 = RES ? J.I->mod_kbias30[t] : 0u, mx31 = RES ? J.I->mod_mx31[t] : 0u;
             const int64_t j = static_cast<int64_t>(J.tj) * kGemmJ + quarter * 32 + lane;
             const int64_t mm = J.I->m, nn = J.I->n;
-            uint8_t* rowj = OZ1 ? nullptr : J.I->resid + J.gt * J.I->rstride + j * 32;  // + (i / 32) * 32 n
+            uint8_t* rowj = RES ? J.I->resid + J.gt * J.I->rstride + j * 32 : nullptr;  // + (i / 32) * 32 n
+            // certificate: this lane's column sum (zero for a padding column or an all-zero column,
+            // whose entries are skipped)
+            const float sj = CERT && j < nn ? static_cast<float>(J.I->cert_sb[j]) : 0.0f;
             for (int64_t c = 0; c < J.nch; ++c, ++local) {
                 const int acc = local & 1;
                 const uint32_t use = static_cast<uint32_t>(local >> 1);
@@ -257,7 +272,40 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
                     if (cc + 1 < kChunks) dev::tmem_load_32x32(taddr + (cc + 1) * 32, v[(cc + 1) & 1]);
                     const int64_t i0 = static_cast<int64_t>(J.ti) * BN + (half * kChunks + cc) * 32;
                     uint8_t* blk = rowj + (i0 >> 5) * (32 * nn);  // this chunk's 32 bytes of row j
-                    if constexpr (OZ1) {
+                    if constexpr (CERT) {
+                        // the warp's 32 lanes are 32 consecutive j of one adaptive tile column
+                        // (cert_tile is a multiple of 128), its 32 columns i0.. one tile row
+                        float q1 = 0.0f, q2 = 0.0f;
+                        if (sj > 0.0f) {
+#pragma unroll
+                            for (int b = 0; b < 32; ++b) {
+                                const int64_t i = i0 + b;
+                                const float ri = i < mm ? static_cast<float>(__ldg(J.I->cert_ra + i)) : 0.0f;
+                                if (ri > 0.0f) {
+                                    const float g = __uint_as_float(cur[b]);
+                                    if (g > 0.0f) {
+                                        const float rg = __fdividef(1.0f, g);  // within 2 ulp
+                                        q1 = fmaxf(q1, (ri + sj) * rg);
+                                        q2 = fmaxf(q2, rg);
+                                    } else {
+                                        q1 = q2 = __int_as_float(0x7F800000);
+                                    }
+                                }
+                            }
+                        }
+#pragma unroll
+                        for (int o = 16; o > 0; o >>= 1) {
+                            q1 = fmaxf(q1, __shfl_xor_sync(0xFFFFFFFFu, q1, o));
+                            q2 = fmaxf(q2, __shfl_xor_sync(0xFFFFFFFFu, q2, o));
+                        }
+                        if (lane == 0 && i0 < mm && q1 > 0.0f) {
+                            const int64_t T = J.I->cert_tile;
+                            const int64_t jw = static_cast<int64_t>(J.tj) * kGemmJ + quarter * 32;
+                            unsigned int* slot = J.I->cert_q + 2 * ((jw / T) * J.I->cert_na + i0 / T);
+                            atomicMax(slot, __float_as_uint(q1));  // non-negative floats order as their bits
+                            atomicMax(slot + 1, __float_as_uint(q2));
+                        }
+                    } else if constexpr (OZ1) {
                         if (j < nn) {  // a warp's lanes are 32 consecutive j: 256 contiguous bytes per row i
                             unsigned long long* dst = reinterpret_cast<unsigned long long*>(
                                 J.I->acc + J.I->pair_d[J.gt] * J.I->acc_plane + j);
@@ -330,21 +378,24 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
     }
 }
 
-template <int BN, bool OZ1 = false>
+template <int BN, int KIND = kKindResidue>
 void launch_bn(const GemmParams& P, int grid, cudaStream_t st) {
-    gemm_i8_modm_kernel<BN, OZ1><<<grid, kGemmThreads, Cfg<BN>::kSmemBytes, st>>>(P);
+    gemm_i8_modm_kernel<BN, KIND><<<grid, kGemmThreads, Cfg<BN>::kSmemBytes, st>>>(P);
 }
 
 }  // namespace
 
 cudaError_t prepare_gemm_kernels() {
-    cudaError_t e = cudaFuncSetAttribute(gemm_i8_modm_kernel<256, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         Cfg<256>::kSmemBytes);
+    cudaError_t e = cudaFuncSetAttribute(gemm_i8_modm_kernel<256, kKindResidue>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg<256>::kSmemBytes);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(gemm_i8_modm_kernel<128, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(gemm_i8_modm_kernel<128, kKindResidue>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  Cfg<128>::kSmemBytes);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(gemm_i8_modm_kernel<256, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(gemm_i8_modm_kernel<256, kKindOz1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 Cfg<256>::kSmemBytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(gemm_i8_modm_kernel<256, kKindCert>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  Cfg<256>::kSmemBytes);
     return e;
 }
@@ -366,7 +417,14 @@ void launch_gemm_oz1(const GemmItem* d_items, int count, int64_t jobs, const Gem
     if (count <= 0 || jobs <= 0) return;
     GemmParams P{d_items, count, cfg.group_j > 0 ? cfg.group_j : 16, jobs, err};
     const int grid = static_cast<int>(std::min<int64_t>(num_sms, jobs));
-    launch_bn<256, true>(P, grid, st);
+    launch_bn<256, kKindOz1>(P, grid, st);
+}
+
+void launch_gemm_cert(const GemmItem* d_items, int count, int64_t jobs, int num_sms, int* err, cudaStream_t st) {
+    if (count <= 0 || jobs <= 0) return;
+    GemmParams P{d_items, count, 16, jobs, err};
+    const int grid = static_cast<int>(std::min<int64_t>(num_sms, jobs));
+    launch_bn<256, kKindCert>(P, grid, st);
 }
 
 }  // namespace oz2

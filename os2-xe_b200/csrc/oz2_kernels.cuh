@@ -94,6 +94,13 @@ struct GemmItem {
     int64_t* acc;
     int64_t acc_ld, acc_plane;
     uint8_t pair_a[kMaxOz1Pairs], pair_b[kMaxOz1Pairs], pair_d[kMaxOz1Pairs];
+    // certificate mode only: bf16 planes (64 elements per 128-byte row), the scaled sums R' of
+    // op(A)'s rows and S' of op(B)'s columns, and per adaptive tile (cert_tile rows and columns,
+    // cert_na tiles down a column of tiles) two FP32 maxima as bits: (R'_i + S'_j) / G_ij, 1 / G_ij
+    const double* cert_ra;
+    const double* cert_sb;
+    unsigned int* cert_q;
+    int64_t cert_tile, cert_na;
 };
 
 // ---- crt: one item per problem; all items of a launch share s
@@ -126,6 +133,9 @@ struct GemmConfig {
 };
 void launch_gemm(const GemmItem* d_items, int count, int64_t jobs, const GemmConfig& cfg, int num_sms, int* err,
                  cudaStream_t st);
+// the same GEMM on bf16 planes of scaled magnitudes, with the certificate's maxima in the
+// epilogue instead of residues (one job per tile; items as for launch_gemm with s = 1)
+void launch_gemm_cert(const GemmItem* d_items, int count, int64_t jobs, int num_sms, int* err, cudaStream_t st);
 // the same GEMM for the Ozaki Scheme I baseline: digit-pair jobs, int64 atomic sums per diagonal
 void launch_gemm_oz1(const GemmItem* d_items, int count, int64_t jobs, const GemmConfig& cfg, int num_sms, int* err,
                      cudaStream_t st);

@@ -125,6 +125,17 @@ __device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t adesc, uint64_t
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
         : "memory");
 }
+// the same with bf16 A and B (kind::f16, K = 16 per instruction: the same 32 bytes of each
+// 128-byte swizzled row as kind::i8), FP32 accumulators
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
 // 32 lanes x 32 consecutive 32-bit columns: thread i of the warp gets lane (base lane + i)
 __device__ __forceinline__ void tmem_load_32x32(uint32_t taddr, uint32_t (&r)[32]) {
     asm volatile(
@@ -159,6 +170,16 @@ __host__ __device__ constexpr uint32_t idesc_i8(int M, int N) {
     return (2u << 4)                                  // D format: s32
            | (1u << 7)                                // A format: signed 8-bit
            | (1u << 10)                               // B format: signed 8-bit
+           | (static_cast<uint32_t>(N >> 3) << 17)    // N / 8
+           | (static_cast<uint32_t>(M >> 4) << 24);   // M / 16
+}
+
+// Instruction descriptor of tcgen05.mma kind::f16 with bf16 A and B (both the same type), both
+// K-major, FP32 D.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
+    return (1u << 4)                                  // D format: f32
+           | (1u << 7)                                // A format: bf16
+           | (1u << 10)                               // B format: bf16
            | (static_cast<uint32_t>(N >> 3) << 17)    // N / 8
            | (static_cast<uint32_t>(M >> 4) << 24);   // M / 16
 }

@@ -290,12 +290,14 @@ class Ozaki2:
 
     # ---- adaptive number of moduli per tile (no counterpart in the reference)
     ADAPTIVE_MLP, ADAPTIVE_ANALYTIC_TILE, ADAPTIVE_ANALYTIC_PROBLEM, ADAPTIVE_FIXED = 0, 1, 2, 3
+    ADAPTIVE_CERTIFIED_TILE, ADAPTIVE_CERTIFIED_PROBLEM = 4, 5
 
     def gemm_adaptive(self, problems, target_bits=53, mode=0):
         """problems as for gemm_grouped (num_moduli is used by mode 3 only). Returns the stats
         dict: tiles, sum_s (emulated tiles, reruns included), probed, rerun, rerun_sum_s,
-        analytic_sum_s (25 counts a native tile), mlp, int8_macs (sum of s m_t n_t k over emulated
-        tiles), native_tiles, native_macs (tiles run as native FP64 GEMMs)."""
+        analytic_sum_s (the judge's s summed: the analytic s, or in modes 0, 4 and 5 the smaller of
+        the analytic and certified s; 25 counts a native tile), mlp, int8_macs (sum of s m_t n_t k
+        over emulated tiles), native_tiles, native_macs (tiles run as native FP64 GEMMs)."""
         arr = self._problems(problems)
         st = (_i64 * 10)()
         _raise(_lib.oz2_dgemm_adaptive(self._h, len(problems), arr, target_bits, mode, st), self._h)

@@ -187,15 +187,16 @@ def test_analytic_modes_meet_the_target(az, phi, offsets):
 
 
 def test_probe_reruns_tiles_run_at_too_few_moduli(az):
-    """an MLP that always answers s = 2: every tile is probed, fails and is rerun at its analytic
-    s, so the result equals the analytic mode's bit for bit"""
+    """an MLP that always answers s = 2 (on tiles whose analytic s stays below 23, so that no
+    certificate takes them over): every tile is probed, fails and is rerun at its judge's s, and
+    the result meets the target"""
     import torch
     m, n, k = 1030, 600, 700
-    A, B = nn_problem(71, m, n, k, 2.0, 20)
+    A, B = nn_problem(71, m, n, k, 1.0, 10)
     dA, dB = to_dev(A), to_dev(B)
     dC1 = torch.zeros(m * n, dtype=torch.float64, device="cuda")
     az.set_mlp_weights(None)
-    ref = az.gemm_adaptive([("N", "N", m, n, k, 1.5, dA, m, dB, k, 0.0, dC1, m, 16)], 53, az.ADAPTIVE_ANALYTIC_TILE)
+    ref = az.gemm_adaptive([("N", "N", m, n, k, 1.5, dA, m, dB, k, 0.0, dC1, m, 16)], 53, az.ADAPTIVE_CERTIFIED_TILE)
     az.set_mlp_weights(const_class_params(0))
     try:
         dC0 = torch.zeros(m * n, dtype=torch.float64, device="cuda")
@@ -204,8 +205,9 @@ def test_probe_reruns_tiles_run_at_too_few_moduli(az):
         az.set_mlp_weights(None)
     assert st["mlp"] == 1
     assert st["probed"] == st["tiles"] and st["rerun"] == st["tiles"]
-    assert st["rerun_sum_s"] == ref["analytic_sum_s"]
-    assert torch.equal(dC0.view(torch.int64), dC1.view(torch.int64))
+    assert st["rerun_sum_s"] == ref["analytic_sum_s"] == st["analytic_sum_s"]
+    dC0 /= 1.5
+    assert dd_check(az, m, n, k, dA, dB, dC0) <= 1.0
 
 
 def smallest_s(az, dA, dB, m, n, k):
@@ -240,18 +242,21 @@ def test_probe_passes_tiles_that_meet_the_target(az):
         st = az.gemm_adaptive([("N", "N", m, n, k, 1.0, dA, m, dB, k, 0.0, dC, m, 16)], 53, az.ADAPTIVE_MLP)
     finally:
         az.set_mlp_weights(None)
-    assert st["probed"] == 1 and st["rerun"] == 0 and st["sum_s"] == s_min
+    # probed when s_min is below the judge (the certified s is within a modulus or two of s_min)
+    assert st["analytic_sum_s"] >= s_min
+    assert st["probed"] == (1 if st["analytic_sum_s"] > s_min else 0)
+    assert st["rerun"] == 0 and st["sum_s"] == s_min
     assert dd_check(az, m, n, k, dA, dB, dC) <= 1.0
 
 
-def test_mode0_without_weights_is_the_tile_analytic_mode(az):
+def test_mode0_without_weights_is_the_certified_tile_mode(az):
     import torch
     m, n, k = 800, 900, 333
     A, B = nn_problem(91, m, n, k, 3.0, 10)
     dA, dB = to_dev(A), to_dev(B)
     az.set_mlp_weights(None)
     out = []
-    for mode in (az.ADAPTIVE_MLP, az.ADAPTIVE_ANALYTIC_TILE):
+    for mode in (az.ADAPTIVE_MLP, az.ADAPTIVE_CERTIFIED_TILE):
         dC = torch.zeros(m * n, dtype=torch.float64, device="cuda")
         st = az.gemm_adaptive([("N", "N", m, n, k, 1.0, dA, m, dB, k, 0.0, dC, m, 16)], 53, mode)
         out.append((st, dC))
@@ -274,7 +279,7 @@ def test_mlp_keeps_analytic_s_when_beta_is_nonzero(az):
         az.set_mlp_weights(None)
     assert st["probed"] == 0 and st["sum_s"] == st["analytic_sum_s"]
     dC1 = C0.clone()
-    az.gemm_adaptive([("N", "N", m, n, k, 1.0, dA, m, dB, k, 0.5, dC1, m, 16)], 53, az.ADAPTIVE_ANALYTIC_TILE)
+    az.gemm_adaptive([("N", "N", m, n, k, 1.0, dA, m, dB, k, 0.5, dC1, m, 16)], 53, az.ADAPTIVE_CERTIFIED_TILE)
     assert torch.equal(dC.view(torch.int64), dC1.view(torch.int64))
 
 
@@ -410,3 +415,75 @@ def test_whole_problem_and_tile_tasks_agree(az):
     dC = torch.zeros(m * n, dtype=torch.float64, device="cuda")
     az.gemm("N", "N", m, n, k, 1.0, dA, m, dB, k, 0.0, dC, m, 16)
     assert torch.equal(out[0].view(torch.int64), dC.view(torch.int64))
+
+
+@pytest.mark.parametrize("m,n,k,phi,offsets", [(700, 900, 600, 0.0, 0), (1030, 600, 777, 3.0, 20),
+                                               (600, 1100, 1500, 6.0, 40), (520, 520, 300, 8.0, 40)])
+def test_certified_modes_meet_the_target(az, m, n, k, phi, offsets):
+    """modes 4 (certified s per tile) and 5 (per problem): every output within the target, the
+    judge never above the analytic rule, the same result on every run, and op(A) = T / op(B) = T
+    on explicitly transposed copies (the k-contiguous certificate layouts) equal to NN bit for bit"""
+    import torch
+    A, B = nn_problem(300 + m, m, n, k, phi, offsets)
+    dA, dB = to_dev(A), to_dev(B)
+    dC = torch.zeros(m * n, dtype=torch.float64, device="cuda")
+    an = az.gemm_adaptive([("N", "N", m, n, k, 1.0, dA, m, dB, k, 0.0, dC, m, 16)], 53, az.ADAPTIVE_ANALYTIC_TILE)
+    outs = []
+    for mode in (az.ADAPTIVE_CERTIFIED_TILE, az.ADAPTIVE_CERTIFIED_PROBLEM, az.ADAPTIVE_CERTIFIED_TILE):
+        dC = torch.zeros(m * n, dtype=torch.float64, device="cuda")
+        st = az.gemm_adaptive([("N", "N", m, n, k, 1.0, dA, m, dB, k, 0.0, dC, m, 16)], 53, mode)
+        assert dd_check(az, m, n, k, dA, dB, dC) <= 1.0, (mode, st)
+        assert st["analytic_sum_s"] <= an["analytic_sum_s"]
+        assert st["probed"] == 0 and st["mlp"] == 0
+        outs.append((st, dC))
+    assert torch.equal(outs[0][1].view(torch.int64), outs[2][1].view(torch.int64))
+    At = to_dev(np.asfortranarray(A.T))  # k x m: op(A) = T gives A
+    Bt = to_dev(np.asfortranarray(B.T))  # n x k
+    dT = torch.zeros(m * n, dtype=torch.float64, device="cuda")
+    az.gemm_adaptive([("T", "T", m, n, k, 1.0, At, k, Bt, n, 0.0, dT, m, 16)], 53, az.ADAPTIVE_CERTIFIED_TILE)
+    assert torch.equal(dT.view(torch.int64), outs[0][1].view(torch.int64))
+    if phi >= 6.0:
+        assert outs[0][0]["native_tiles"] <= an["native_tiles"]
+
+
+@pytest.mark.parametrize("seed,n,k,phi", [(1, 300, 400, 0.0), (2, 512, 1000, 2.5), (3, 256, 2000, 4.0),
+                                          (4, 400, 333, 6.0), (5, 512, 512, 1.0), (6, 500, 700, 5.0),
+                                          (7, 384, 1500, 7.0)])
+def test_certified_s_matches_the_restatement(oracle, az, seed, n, k, phi):
+    """one tile per problem: where the analytic s is 23 or more the device's judge lies between
+    the restated certificate (FP64 |A||B|) and one modulus above it (the device's bf16 lower
+    bound is a little smaller); below 23 no certificate runs and the judge is the analytic s"""
+    import torch
+    A, B = nn_problem(700 + seed, n, n, k, phi, 30)
+    dA, dB = to_dev(A), to_dev(B)
+    dC = torch.zeros(n * n, dtype=torch.float64, device="cuda")
+    st = az.gemm_adaptive([("N", "N", n, n, k, 1.0, dA, n, dB, k, 0.0, dC, n, 16)], 53, az.ADAPTIVE_CERTIFIED_TILE)
+    assert st["tiles"] == 1
+    s_np = adaptive_oracle.certified_s(oracle, A, B)
+    _, s_an = adaptive_oracle.tile_features(oracle, [("N", "N", n, n, k, A, B)])
+    if int(s_an[0]) < 23:
+        assert st["analytic_sum_s"] == int(s_an[0])
+        return
+    lo_s, hi_s = min(int(s_an[0]), s_np), min(int(s_an[0]), s_np + 1)
+    assert lo_s <= st["analytic_sum_s"] <= hi_s, (st, s_np, int(s_an[0]))
+
+
+def test_certified_tiles_override_the_mlp(az):
+    """an MLP that always answers s = 2 on heavy-tailed inputs (analytic s 23 or more): the
+    certified tiles take their certificate and are not probed, and every output meets the target"""
+    import torch
+    m, n, k = 1030, 600, 700
+    A, B = nn_problem(171, m, n, k, 5.0, 40)
+    dA, dB = to_dev(A), to_dev(B)
+    ref = az.gemm_adaptive([("N", "N", m, n, k, 1.0, dA, m, dB, k, 0.0, torch.zeros(m * n, dtype=torch.float64,
+                                                                                    device="cuda"), m, 16)],
+                           53, az.ADAPTIVE_CERTIFIED_TILE)
+    az.set_mlp_weights(const_class_params(0))
+    try:
+        dC = torch.zeros(m * n, dtype=torch.float64, device="cuda")
+        st = az.gemm_adaptive([("N", "N", m, n, k, 1.0, dA, m, dB, k, 0.0, dC, m, 16)], 53, az.ADAPTIVE_MLP)
+    finally:
+        az.set_mlp_weights(None)
+    assert st["mlp"] == 1 and st["probed"] == 0
+    assert st["sum_s"] == ref["sum_s"] and st["native_tiles"] == ref["native_tiles"]
+    assert dd_check(az, m, n, k, dA, dB, dC) <= 1.0
