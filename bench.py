@@ -60,7 +60,8 @@ def parse():
 def workload(a):
     return {"workload": f"adaptive-s stream: batches of {a.batch} dgemm, m=n=k log-uniform [256,4096], "
                         "(u-0.5)exp(phi g), phi~U[0,8] per problem, rows of A / columns of B scaled by "
-                        "2^U[-40,40], alpha=1 beta=0, target 53 bits, MLP s per 512x512 tile + probe",
+                        "2^U[-40,40], alpha=1 beta=0, target 53 bits, s per 512x512 tile: certified "
+                        "(problems with analytic s >= 23) or MLP + probe",
             "batch": a.batch, "tile": 512, "target_bits": TARGET_BITS, "seed": a.seed,
             "l2": "each batch holds several GB, larger than the 126 MB L2; no flush"}
 
