@@ -844,9 +844,8 @@ int ensure_ws2(oz2_context* h, size_t bytes) {
     return OZ2_OK;
 }
 
-// C[i0:i0+mb, j0:j0+nb] = alpha op(A) op(B) + beta C in native FP64 (cuBLAS DGEMM, default math:
-// no emulation), for tiles whose inputs span more exponent range than 24 moduli cover
-int native_gemm(oz2_context* h, cudaStream_t st, const Prob& p, int64_t i0, int64_t j0, int64_t mb, int64_t nb) {
+// the handle's cuBLAS handle, created on first use and bound to stream st
+int cublas_on(oz2_context* h, cudaStream_t st) {
     if (!h->cublas) {
         if (cublasCreate(&h->cublas) != CUBLAS_STATUS_SUCCESS) {
             h->cublas = nullptr;
@@ -862,6 +861,14 @@ int native_gemm(oz2_context* h, cudaStream_t st, const Prob& p, int64_t i0, int6
         h->cublas_stream = st;
         h->cublas_bound = true;
     }
+    return OZ2_OK;
+}
+
+// C[i0:i0+mb, j0:j0+nb] = alpha op(A) op(B) + beta C in native FP64 (cuBLAS DGEMM, default math:
+// no emulation), for tiles whose inputs span more exponent range than 24 moduli cover
+int native_gemm(oz2_context* h, cudaStream_t st, const Prob& p, int64_t i0, int64_t j0, int64_t mb, int64_t nb) {
+    const int sb = cublas_on(h, st);
+    if (sb) return sb;
     const double* A = p.A + (is_n(p.ta) ? i0 : i0 * p.lda);
     const double* B = p.B + (is_n(p.tb) ? j0 * p.ldb : j0);
     double* C = p.C + i0 + j0 * p.ldc;
@@ -869,6 +876,26 @@ int native_gemm(oz2_context* h, cudaStream_t st, const Prob& p, int64_t i0, int6
     const cublasStatus_t cs = cublasDgemm_64(h->cublas, is_n(p.ta) ? CUBLAS_OP_N : CUBLAS_OP_T,
                                              is_n(p.tb) ? CUBLAS_OP_N : CUBLAS_OP_T, mb, nb, p.k, &al, A, p.lda, B,
                                              p.ldb, &be, C, p.ldc);
+    if (cs != CUBLAS_STATUS_SUCCESS) return fail(h, OZ2_ECUDA, "oz2: native FP64 GEMM failed");
+    ++h->launches;
+    return OZ2_OK;
+}
+
+// `count` tiles of one row of tiles in native FP64, side by side: C[i0:i0+mb, j0 + b nb ...] for
+// b < count, one strided batched cuBLAS DGEMM (op(A)'s rows shared, op(B)'s columns and C advance
+// by nb per tile). One 512 x 512 tile alone fills well under half of the SMs; a row of them fills
+// them all.
+int native_gemm_row(oz2_context* h, cudaStream_t st, const Prob& p, int64_t i0, int64_t j0, int64_t mb, int64_t nb,
+                    int64_t count) {
+    const int sb = cublas_on(h, st);
+    if (sb) return sb;
+    const double* A = p.A + (is_n(p.ta) ? i0 : i0 * p.lda);
+    const double* B = p.B + (is_n(p.tb) ? j0 * p.ldb : j0);
+    double* C = p.C + i0 + j0 * p.ldc;
+    const double al = p.alpha[0], be = p.beta[0];
+    const cublasStatus_t cs = cublasDgemmStridedBatched_64(
+        h->cublas, is_n(p.ta) ? CUBLAS_OP_N : CUBLAS_OP_T, is_n(p.tb) ? CUBLAS_OP_N : CUBLAS_OP_T, mb, nb, p.k, &al, A,
+        p.lda, 0, B, p.ldb, is_n(p.tb) ? nb * p.ldb : nb, &be, C, p.ldc, nb * p.ldc, count);
     if (cs != CUBLAS_STATUS_SUCCESS) return fail(h, OZ2_ECUDA, "oz2: native FP64 GEMM failed");
     ++h->launches;
     return OZ2_OK;
@@ -1355,20 +1382,40 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
             std::fill(native_count.begin(), native_count.end(), 0);
             for (int64_t t : native) ++native_count[tiles[t].prob];
             std::vector<bool> whole_done(base.size(), false);
+            // other native tiles by (problem, row of tiles), in column order
+            std::map<std::pair<int, int64_t>, std::vector<int64_t>> rows_of;
             for (int64_t t : native) {
                 const TileRef& r = tiles[t];
                 const Prob& p = base[r.prob];
                 h->astats[8] += 1;
                 h->astats[9] += r.mb * r.nb * p.k;
-                int st2;
                 if (native_count[r.prob] == prob_tiles[r.prob]) {
                     if (whole_done[r.prob]) continue;
                     whole_done[r.prob] = true;
-                    st2 = native_gemm(h, h->nat_stream, p, 0, 0, p.m, p.n);
+                    const int st2 = native_gemm(h, h->nat_stream, p, 0, 0, p.m, p.n);
+                    if (st2) return st2;
                 } else {
-                    st2 = native_gemm(h, h->nat_stream, p, r.i0, r.j0, r.mb, r.nb);
+                    rows_of[{r.prob, r.i0}].push_back(t);
                 }
-                if (st2) return st2;
+            }
+            for (auto& kv : rows_of) {
+                std::vector<int64_t>& ts = kv.second;
+                std::sort(ts.begin(), ts.end(), [&](int64_t x, int64_t y) { return tiles[x].j0 < tiles[y].j0; });
+                const Prob& p = base[kv.first.first];
+                size_t a = 0;
+                while (a < ts.size()) {
+                    // a run of adjacent full-width tiles goes in one batched call
+                    size_t b = a + 1;
+                    while (b < ts.size() && tiles[ts[b]].j0 == tiles[ts[b - 1]].j0 + T && tiles[ts[b]].nb == T &&
+                           tiles[ts[a]].nb == T)
+                        ++b;
+                    const TileRef& r = tiles[ts[a]];
+                    const int st2 = b - a > 1 ? native_gemm_row(h, h->nat_stream, p, r.i0, r.j0, r.mb, T,
+                                                                static_cast<int64_t>(b - a))
+                                              : native_gemm(h, h->nat_stream, p, r.i0, r.j0, r.mb, r.nb);
+                    if (st2) return st2;
+                    a = b;
+                }
             }
             if (h->profiling) {
                 OZ2_CUDA(h, cudaEventRecord(h->nat_t1, h->nat_stream));
