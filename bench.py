@@ -714,7 +714,7 @@ def main():
     for name, fn in forms.items():
         if name == "adaptive_mlp_batched":
             continue
-        tf, msf = timed(fn, a.steps, min(a.warmup, 1))
+        tf, msf = timed(fn, a.steps, a.warmup)
         fixed[name] = {"tflops": tf, "ms_per_step": msf, "adaptive_speedup": value / tf}
 
     tiles = max(adaptive_stats.get("tiles", 0), 1)

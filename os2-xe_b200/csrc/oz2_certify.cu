@@ -109,7 +109,24 @@ __global__ void __launch_bounds__(256) cert_prep_kernel(const CertPrepItem* __re
         if (r < I->rows_pad) {
             const Scale sc = r < rows ? row_scale(I->maxbits[r]) : Scale{1.0, 1.0, false};
             const int64_t per = (nchunk + 7) / 8, c0 = warp * per, c1 = min(nchunk, c0 + per);
-            for (int64_t c = c0; c < c1; ++c) chunk(r, c, sc, I->X + r, ldx, sum);
+            const double* x = I->X + r;
+            for (int64_t c = c0; c < c1; c += 2) {  // two chunks' sixteen loads in flight
+                double v[16];
+#pragma unroll
+                for (int u = 0; u < 16; ++u) {
+                    const int64_t p = 8 * c + u;
+                    v[u] = sc.live && p < k && c + u / 8 < c1 ? (fabs(__ldg(x + p * ldx)) * sc.s1) * sc.s2 : 0.0;
+                }
+#pragma unroll
+                for (int h2 = 0; h2 < 2; ++h2) {
+                    if (c + h2 >= c1) break;
+                    const double* w = v + 8 * h2;
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) sum += w[u];
+                    *chunk_ptr(I->planes, kb_total, r, c + h2) = make_uint4(
+                        bf16x2(w[0], w[1]), bf16x2(w[2], w[3]), bf16x2(w[4], w[5]), bf16x2(w[6], w[7]));
+                }
+            }
         }
         part[warp][lane] = sum;
         __syncthreads();
@@ -131,15 +148,18 @@ __global__ void __launch_bounds__(256) cert_prep_kernel(const CertPrepItem* __re
     }
 }
 
-// One thread per tile: the certified s from the GEMM's two maxima, kNativeS for a tile with a
-// non-finite row or column (those rows' outputs are NaN at any s; the analytic rule decides).
+// One warp per tile: the lanes scan the tile's row and column maxima for a non-finite one
+// (kNativeS then: those rows' outputs are NaN at any s and the analytic rule decides), lane 0
+// turns the GEMM's two maxima into the certified s.
 __global__ void __launch_bounds__(128) cert_tile_kernel(const CertTileItem* __restrict__ items, int count) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = blockIdx.x * 4 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
     if (t >= count) return;
     const CertTileItem* I = items + t;
-    bool nonfinite = false;
-    for (int64_t i = 0; i < I->mb && !nonfinite; ++i) nonfinite = I->maxa[i] >= 0x7FF0000000000000ull;
-    for (int64_t j = 0; j < I->nb && !nonfinite; ++j) nonfinite = I->maxb[j] >= 0x7FF0000000000000ull;
+    bool bad = false;
+    for (int64_t i = lane; i < I->mb; i += 32) bad |= I->maxa[i] >= 0x7FF0000000000000ull;
+    for (int64_t j = lane; j < I->nb; j += 32) bad |= I->maxb[j] >= 0x7FF0000000000000ull;
+    const bool nonfinite = __any_sync(0xFFFFFFFFu, bad);
+    if (lane != 0) return;
     const float q1 = __uint_as_float(I->q[0]), q2 = __uint_as_float(I->q[1]);
     int s = kNativeS;
     const double k = static_cast<double>(I->k), tb = static_cast<double>(I->target_bits);
@@ -179,7 +199,7 @@ void launch_cert_prep(const CertPrepItem* d, const CertPrepItem* h, int count, i
 
 void launch_cert_tiles(const CertTileItem* d, int count, cudaStream_t st) {
     if (count <= 0) return;
-    cert_tile_kernel<<<static_cast<unsigned>((count + 127) / 128), 128, 0, st>>>(d, count);
+    cert_tile_kernel<<<static_cast<unsigned>((count + 3) / 4), 128, 0, st>>>(d, count);
 }
 
 }  // namespace oz2
