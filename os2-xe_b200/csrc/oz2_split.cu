@@ -142,15 +142,33 @@ __device__ __forceinline__ uint32_t pack_bytes(uint32_t a, uint32_t b, uint32_t 
 // Elements per thread: 16 (one 16-byte chunk of every plane) on the real narrow path; 8 (half a
 // chunk) on the wide path and for complex inputs, whose words per element (four, or two groups)
 // would otherwise hold 128 registers
+constexpr int kSplitRowcK = 256;  // inner indices per block of the rows-contiguous split
+
 template <int NLIMB, bool CPLX>
 __host__ __device__ constexpr int split_ept() {
     return NLIMB == 3 && !CPLX ? 16 : 8;
 }
 
 // Each thread: one plane row r and EPT consecutive inner indices k0..k0+EPT-1 of every plane.
-// ROWC: a warp is 32 consecutive rows (coalesced loads along r), the 8 warps of a block are 8
-// consecutive EPT-wide pieces of the inner index. Otherwise a warp is one row and 32
-// consecutive pieces, the 8 warps are 8 rows.
+// Block (bx, by) and thread -> plane row r and the first k0 of its EPT consecutive inner indices.
+// ROWC: a warp is EPT consecutive rows times 32 / EPT consecutive EPT-wide pieces: the loads along
+// r stay coalesced (EPT rows of 8 bytes per inner index), and the lanes of one row cover 32
+// inner indices, a whole 32-byte sector of each plane row (two 16-byte chunks that the swizzle
+// keeps adjacent); the 8 warps of a block continue along the inner index, so a block is EPT rows
+// by 256 inner indices. Otherwise a warp is one row and 32 consecutive pieces, the 8 warps are 8
+// rows.
+template <int EPT, bool ROWC>
+__device__ __forceinline__ void split_coords(int64_t bx, int64_t by, int64_t& r, int64_t& k0) {
+    const int lane = static_cast<int>(threadIdx.x & 31), warp = static_cast<int>(threadIdx.x >> 5);
+    if (ROWC) {
+        r = bx * EPT + lane % EPT;
+        k0 = by * kSplitRowcK + (warp * (32 / EPT) + lane / EPT) * EPT;
+    } else {
+        r = bx * 8 + warp;
+        k0 = by * (32 * EPT) + lane * EPT;
+    }
+}
+
 template <int NLIMB, bool CPLX, bool ROWC>
 __global__ void __launch_bounds__(256) split_kernel(const SplitItem* __restrict__ items, int count) {
     constexpr int EPT = split_ept<NLIMB, CPLX>();
@@ -158,13 +176,7 @@ __global__ void __launch_bounds__(256) split_kernel(const SplitItem* __restrict_
     const int64_t local = static_cast<int64_t>(blockIdx.x) - I->block0;
     const int64_t bx = local % I->rblocks, by = local / I->rblocks;
     int64_t r, k0;
-    if (ROWC) {
-        r = bx * 32 + (threadIdx.x & 31);
-        k0 = by * (8 * EPT) + (threadIdx.x >> 5) * EPT;
-    } else {
-        r = bx * 8 + (threadIdx.x >> 5);
-        k0 = by * (32 * EPT) + (threadIdx.x & 31) * EPT;
-    }
+    split_coords<EPT, ROWC>(bx, by, r, k0);
     const int64_t kb_total = I->kb_total, plane_bytes = I->plane_bytes, ldx = I->ldx, k = I->k;
     const int64_t rows = I->rows;
     if (r >= I->rows_pad || k0 >= kb_total * kTileK) return;
@@ -282,13 +294,7 @@ __global__ void __launch_bounds__(256) slice_kernel(const SplitItem* __restrict_
     const int64_t local = static_cast<int64_t>(blockIdx.x) - I->block0;
     const int64_t bx = local % I->rblocks, by = local / I->rblocks;
     int64_t r, k0;
-    if (ROWC) {
-        r = bx * 32 + (threadIdx.x & 31);
-        k0 = by * (8 * EPT) + (threadIdx.x >> 5) * EPT;
-    } else {
-        r = bx * 8 + (threadIdx.x >> 5);
-        k0 = by * (32 * EPT) + (threadIdx.x & 31) * EPT;
-    }
+    split_coords<EPT, ROWC>(bx, by, r, k0);
     const int64_t kb_total = I->kb_total, plane_bytes = I->plane_bytes, ldx = I->ldx, k = I->k;
     if (r >= I->rows_pad || k0 >= kb_total * kTileK) return;
     const int ndig = I->s;
@@ -362,8 +368,8 @@ int64_t split_item_blocks(SplitItem& it, int64_t block0) {
     const int ept = it.tk > kNarrowScaleBits || it.cplx ? split_ept<5, false>() : split_ept<3, false>();
     const int64_t kpad = it.kb_total * kTileK;  // inner indices of the plane, padding included
     if (it.row_contig) {
-        it.rblocks = ceil_div(it.rows_pad, 32);
-        it.kblocks = ceil_div(kpad, 8 * ept);
+        it.rblocks = ceil_div(it.rows_pad, ept);
+        it.kblocks = ceil_div(kpad, kSplitRowcK);
     } else {
         it.rblocks = ceil_div(it.rows_pad, 8);
         it.kblocks = ceil_div(kpad, 32 * ept);
