@@ -159,6 +159,7 @@ int make_plan(int s, int64_t k, Plan& p) {
     if (T.status[s]) return T.status[s];
     const int tk = plan_tk(s, k);
     if (tk < 1) return 1;
+    if (tk > kWideScaleBits) return 5;  // never for the tables above (largest tk 91 at s = 24)
     p = T.plan[s];
     p.tk = tk;
     return 0;
@@ -186,7 +187,7 @@ void mod_constants(const Plan& p, ModConst* out) {
         c.mu = static_cast<uint32_t>((uint64_t{1} << 32) / m);
         c.h = h;
         c.koff3 = (h + m - pow2_mod(62, m)) % m;
-        c.koff5 = (h + m - pow2_mod(104, m)) % m;
+        c.koff5 = (h + m - pow2_mod(93, m)) % m;
         c.kbias = m * static_cast<uint32_t>(((uint64_t{1} << 31) + m - 1) / m);
         c.kbias30 = m * ((kExactSum + m - 1) / m);
         // Granlund and Montgomery (1994): with M = ceil(2^39 / m) = (2^39 + e) / m, e < m <= 2^8,

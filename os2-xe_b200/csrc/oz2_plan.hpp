@@ -18,6 +18,8 @@ constexpr int kBigWords = 8;       // 256-bit host integers
 constexpr int kMaxLimbs = 6;       // 32-bit limbs of M for s <= 24
 constexpr int kMaxScaleBits = 100;
 constexpr int kNarrowScaleBits = 62;
+// the split's wide offset (2^93 in three 32-bit words) holds |x| <= 2^92; every plan has tk <= 91
+constexpr int kWideScaleBits = 92;
 constexpr int kNonFinite = -2147483647 - 1;
 
 // 32-bit limbs of M per s: max(2, floor(log2 M / 32) + 1) (ref src/ozaki2_gpu.hpp:55-59, :168)
@@ -37,7 +39,7 @@ struct ModConst {
     uint32_t mu;     // floor(2^32 / m), Barrett
     uint32_t h;      // (m - 1) / 2: residues are kept symmetric in [-h, m-1-h]
     uint32_t koff3;  // (h - 2^62 mod m) mod m: narrow offset (tk <= 62)
-    uint32_t koff5;  // (h - 2^104 mod m) mod m: wide offset
+    uint32_t koff5;  // (h - 2^93 mod m) mod m: wide offset
     uint32_t kbias;  // m ceil(2^31 / m): c + kbias is in [0, 2^32) for every int32 GEMM sum c
                      // (|c| < 2^31 - 2^21) and congruent to c modulo m
     uint32_t kbias30;  // m ceil(kExactSum / m): c + kbias30 is in [0, 2^31) for every int32 GEMM sum

@@ -97,11 +97,11 @@ __device__ __forceinline__ void offset_words_fp(double v, double s1, double s2, 
     W[1] = static_cast<uint32_t>(xo >> 32);
 }
 
-// Wide path (62 < tk <= 100): y = v 2^e as above, a = |rint(y)| < 2^101 split exactly into
-// hi = trunc(a 2^-64) and lo = a - hi 2^64 (both exact: power-of-two scaling, and lo keeps a
-// subset of a's 53 significant bits), then 2^104 +- (hi:lo) as four 32-bit words (the top two
-// bytes zero).
-__device__ __forceinline__ void offset_words_fp_wide(double v, double s1, double s2, uint32_t (&W)[4]) {
+// Wide path (62 < tk <= 92; the largest tk of any plan is 91): y = v 2^e as above, a = |rint(y)|
+// <= 2^92 split exactly into hi = trunc(a 2^-64) and lo = a - hi 2^64 (both exact: power-of-two
+// scaling, and lo keeps a subset of a's 53 significant bits), then 2^93 +- (hi:lo), which lies in
+// (0, 2^94), as three 32-bit words.
+__device__ __forceinline__ void offset_words_fp_wide(double v, double s1, double s2, uint32_t (&W)[3]) {
     const double y = rint((v * s1) * s2);
     const double a = fabs(y);
     const double hd = trunc(a * 5.421010862427522e-20);     // 2^-64
@@ -110,21 +110,20 @@ __device__ __forceinline__ void offset_words_fp_wide(double v, double s1, double
     uint64_t ol, oh;
     if (y < 0.0) {
         ol = 0 - lo;
-        oh = (1ull << 40) - hi - (lo != 0 ? 1 : 0);
+        oh = (1ull << 29) - hi - (lo != 0 ? 1 : 0);
     } else {
         ol = lo;
-        oh = (1ull << 40) + hi;
+        oh = (1ull << 29) + hi;
     }
     W[0] = static_cast<uint32_t>(ol);
     W[1] = static_cast<uint32_t>(ol >> 32);
     W[2] = static_cast<uint32_t>(oh);
-    W[3] = static_cast<uint32_t>(oh >> 32);
 }
 
 // (x + h) mod m in [0, m) from the bytes of the offset integer: v = koff + sum_l byte_l (2^(8 l)
-// mod m) by byte dot products (at most 14 nonzero bytes, so v < 255 + 14 255^2 < 2^20), then
-// the exact multiply-high quotient by ceil(2^32 / m). Two (four) dot products, one multiply-high
-// and one multiply-subtract per residue.
+// mod m) by byte dot products (at most 12 bytes, so v < 255 + 12 255^2 < 2^20), then the exact
+// multiply-high quotient by ceil(2^32 / m). Two (three) dot products, one multiply-high and one
+// multiply-subtract per residue.
 template <int NW>
 __device__ __forceinline__ uint32_t byte_residue(const uint32_t (&W)[NW], const ModConst& c) {
     uint32_t v = NW == 2 ? c.koff3 : c.koff5;
@@ -138,10 +137,9 @@ __device__ __forceinline__ uint32_t pack_bytes(uint32_t a, uint32_t b, uint32_t 
     return __byte_perm(__byte_perm(a, b, 0x0040), __byte_perm(c, d, 0x0040), 0x5410);
 }
 
-// NLIMB: 3 selects the narrow path (two words per offset integer), 5 the wide one (four words).
+// NLIMB: 3 selects the narrow path (two words per offset integer), 5 the wide one (three words).
 // Elements per thread: 16 (one 16-byte chunk of every plane) on the real narrow path; 8 (half a
-// chunk) on the wide path and for complex inputs, whose words per element (four, or two groups)
-// would otherwise hold 128 registers
+// chunk) on the wide path (16 measured no faster) and for complex inputs (two groups of words)
 constexpr int kSplitRowcK = 256;  // inner indices per block of the rows-contiguous split
 
 template <int NLIMB, bool CPLX>
@@ -208,7 +206,7 @@ __global__ void __launch_bounds__(256) split_kernel(const SplitItem* __restrict_
     const bool live = e != kNonFinite;
 
     constexpr int NG = CPLX ? 2 : 1;
-    constexpr int NW = NLIMB == 3 ? 2 : 4;  // 32-bit words of the offset integer
+    constexpr int NW = NLIMB == 3 ? 2 : 3;  // 32-bit words of the offset integer
     uint32_t L[NG][EPT][NW];
     const int e1 = e >> 1;
     const double s1 = pow2(live ? e1 : 0), s2 = pow2(live ? e - e1 : 0);
@@ -239,7 +237,7 @@ __global__ void __launch_bounds__(256) split_kernel(const SplitItem* __restrict_
         const ModConst mc = I->mc[t];
         uint32_t b0[EPT], b1[EPT], b2[EPT];  // residue bytes in the low 8 bits
         if (mc.m == 256) {
-            // 2^62 = 2^104 = 0 mod 256: the residue byte is the low byte of the offset integer
+            // 2^62 = 2^93 = 0 mod 256: the residue byte is the low byte of the offset integer
 #pragma unroll
             for (int q = 0; q < EPT; ++q) {
                 b0[q] = L[0][q][0];
