@@ -798,7 +798,7 @@ def main():
                 stream.wait_event(b)
 
     e2e_run(2)
-    e2e_steps = max(2, min(a.steps, 6))
+    e2e_steps = max(2, a.steps)  # the pipeline's fill (first upload) and drain (last download) amortised over the steps
     with Timer(torch, stream) as t:
         e2e_run(e2e_steps)
     e2e_ms = t.ms / e2e_steps

@@ -90,12 +90,18 @@ struct oz2_context {
     std::vector<std::pair<int, cudaEvent_t>> marks;
     std::vector<cudaEvent_t> pool;
     size_t pool_used = 0;
-    // pinned staging ring for large descriptor blobs
+    // pinned staging ring for large descriptor blobs (read by a copy kernel through its device
+    // mapping)
     void* ring_host[kRing] = {};
+    void* ring_dev[kRing] = {};
     size_t ring_cap[kRing] = {};
     cudaEvent_t ring_ev[kRing] = {};
     bool ring_used[kRing] = {};
     int ring_next = 0;
+    // pinned buffer that kernels write small results into for the host to read
+    void* rb_host = nullptr;
+    void* rb_dev = nullptr;
+    size_t rb_cap = 0;
     // GEMM configuration: forced by the caller, tuned per problem-set shape, last used
     GemmConfig forced;
     bool has_forced = false;
@@ -483,7 +489,8 @@ int check_grid(oz2_context* h, const Program& prog) {
 
 // ---------------------------------------------------------------- issuing a program
 // copies host bytes to device memory on the stream: small blobs through a kernel parameter,
-// large ones through the pinned staging ring
+// large ones through the pinned staging ring and a copy kernel (no copy engine: see
+// launch_sm_copy)
 int put_blob(oz2_context* h, const void* data, size_t bytes, unsigned char* dev) {
     if (bytes == 0) return OZ2_OK;
     if (bytes <= kParamBlobBytes) {
@@ -498,16 +505,56 @@ int put_blob(oz2_context* h, const void* data, size_t bytes, unsigned char* dev)
     if (h->ring_cap[slot] < bytes) {
         // pinned allocations are slow and synchronise: grow in powers of two from 1 MiB
         if (h->ring_host[slot]) cudaFreeHost(h->ring_host[slot]);
-        h->ring_host[slot] = nullptr;
+        h->ring_host[slot] = h->ring_dev[slot] = nullptr;
+        h->ring_cap[slot] = 0;
         size_t cap = std::max(h->ring_cap[slot] * 2, size_t{1} << 20);
         while (cap < bytes) cap *= 2;
-        OZ2_CUDA(h, cudaHostAlloc(&h->ring_host[slot], cap, cudaHostAllocDefault));
+        OZ2_CUDA(h, cudaHostAlloc(&h->ring_host[slot], cap, cudaHostAllocMapped));
+        OZ2_CUDA(h, cudaHostGetDevicePointer(&h->ring_dev[slot], h->ring_host[slot], 0));
         h->ring_cap[slot] = cap;
     }
     std::memcpy(h->ring_host[slot], data, bytes);
-    OZ2_CUDA(h, cudaMemcpyAsync(dev, h->ring_host[slot], bytes, cudaMemcpyHostToDevice, h->stream));
+    launch_sm_copy(h->ring_dev[slot], dev, bytes, h->stream);
+    ++h->launches;
     OZ2_CUDA(h, cudaEventRecord(h->ring_ev[slot], h->stream));
     h->ring_used[slot] = true;
+    return OZ2_OK;
+}
+
+// reads small device arrays into host memory once the stream's work so far has run: a copy
+// kernel writes them into mapped pinned memory, the host waits for the stream and copies them
+// out (no copy engine: see launch_sm_copy)
+struct HostRead {
+    void* dst;
+    const void* src;
+    size_t bytes;
+};
+int read_back(oz2_context* h, std::initializer_list<HostRead> reads) {
+    size_t total = 0;
+    for (const HostRead& r : reads) total += (r.bytes + 15) & ~size_t{15};
+    if (h->rb_cap < total) {
+        OZ2_CUDA(h, cudaStreamSynchronize(h->stream));
+        if (h->rb_host) cudaFreeHost(h->rb_host);
+        h->rb_host = h->rb_dev = nullptr;
+        h->rb_cap = 0;
+        size_t cap = size_t{1} << 16;
+        while (cap < total) cap *= 2;
+        OZ2_CUDA(h, cudaHostAlloc(&h->rb_host, cap, cudaHostAllocMapped));
+        OZ2_CUDA(h, cudaHostGetDevicePointer(&h->rb_dev, h->rb_host, 0));
+        h->rb_cap = cap;
+    }
+    size_t off = 0;
+    for (const HostRead& r : reads) {
+        launch_sm_copy(r.src, static_cast<unsigned char*>(h->rb_dev) + off, r.bytes, h->stream);
+        ++h->launches;
+        off += (r.bytes + 15) & ~size_t{15};
+    }
+    OZ2_CUDA(h, cudaStreamSynchronize(h->stream));
+    off = 0;
+    for (const HostRead& r : reads) {
+        std::memcpy(r.dst, static_cast<const unsigned char*>(h->rb_host) + off, r.bytes);
+        off += (r.bytes + 15) & ~size_t{15};
+    }
     return OZ2_OK;
 }
 
@@ -518,9 +565,9 @@ int upload(oz2_context* h, const Program& prog, unsigned char* dev) {
 void issue(oz2_context* h, const Program& prog, const unsigned char* dev) {
     const unsigned char* hb = prog.blob.data();
     for (const Op& op : prog.ops) {
-        if (op.kind != Op::Memset && op.kind != Op::Mark) ++h->launches;
+        if (op.kind != Op::Mark) ++h->launches;
         switch (op.kind) {
-            case Op::Memset: cudaMemsetAsync(op.ptr, 0, op.bytes, h->stream); break;
+            case Op::Memset: launch_fill(op.ptr, 0, op.bytes, h->stream); break;
             case Op::Scale:
                 launch_scale(reinterpret_cast<const ScaleItem*>(dev + op.off), reinterpret_cast<const ScaleItem*>(hb + op.off),
                              op.count, op.blocks, h->stream);
@@ -1156,7 +1203,8 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
     int* d_sm = reinterpret_cast<int*>(ws + osm);
     int* d_sc = reinterpret_cast<int*>(ws + osc);
     unsigned int* d_q = reinterpret_cast<unsigned int*>(ws + ocq);
-    OZ2_CUDA(h, cudaMemsetAsync(ws, 0, zero_end, h->stream));
+    launch_fill(ws, 0, zero_end, h->stream);
+    ++h->launches;
 
     Program ph1;
     std::vector<ScaleItem> sc;
@@ -1243,9 +1291,10 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
     }
     constexpr int kNoCertificate = 0x7F7F7F7F;  // the device's fill byte 0x7F: above every s
     std::vector<int> s_an(ntiles), s_ml(ntiles, kMaxModuli), s_ce(ntiles, kNoCertificate);
-    OZ2_CUDA(h, cudaMemcpyAsync(s_an.data(), d_sa, ntiles * 4, cudaMemcpyDeviceToHost, h->stream));
-    if (use_mlp) OZ2_CUDA(h, cudaMemcpyAsync(s_ml.data(), d_sm, ntiles * 4, cudaMemcpyDeviceToHost, h->stream));
-    OZ2_CUDA(h, cudaStreamSynchronize(h->stream));
+    const size_t tile_bytes = static_cast<size_t>(ntiles) * 4;
+    if (use_mlp) st = read_back(h, {{s_an.data(), d_sa, tile_bytes}, {s_ml.data(), d_sm, tile_bytes}});
+    else st = read_back(h, {{s_an.data(), d_sa, tile_bytes}});
+    if (st) return st;
     // The certificate costs about three moduli of emulation over the problem and saves about four
     // where the analytic s is emulated, far more where it is native: it runs for the problems
     // with a tile at kCertFromS or above.
@@ -1257,18 +1306,18 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
         for (int64_t t = 0; t < ntiles; ++t)
             if (s_an[t] >= kCertFromS) any = want[tiles[t].prob] = 1;
         if (any) {
-            OZ2_CUDA(h, cudaMemsetAsync(d_sc, 0x7F, ntiles * 4, h->stream));  // kNoCertificate
+            launch_fill(d_sc, 0x7F, ntiles * 4, h->stream);  // kNoCertificate
+            ++h->launches;
             if ((st = certify_tiles(h, base, tiles, T, maxA, maxB, tk_cache, want, target_bits, d_q, d_sc)))
                 return st;
-            OZ2_CUDA(h, cudaMemcpyAsync(s_ce.data(), d_sc, ntiles * 4, cudaMemcpyDeviceToHost, h->stream));
-            OZ2_CUDA(h, cudaStreamSynchronize(h->stream));
+            if ((st = read_back(h, {{s_ce.data(), d_sc, tile_bytes}}))) return st;
         }
     }
     mark(h, kScale);  // statistics, certificate, features and the MLP count with the scale stage
     if (mode < 0) {  // features only
         if (feat_out)
-            OZ2_CUDA(h, cudaMemcpyAsync(feat_out, d_feat, ntiles * kFeatures * 4, cudaMemcpyDeviceToDevice, h->stream));
-        if (sa_out) OZ2_CUDA(h, cudaMemcpyAsync(sa_out, d_sa, ntiles * 4, cudaMemcpyDeviceToDevice, h->stream));
+            launch_sm_copy(d_feat, feat_out, ntiles * kFeatures * 4, h->stream);
+        if (sa_out) launch_sm_copy(d_sa, sa_out, ntiles * 4, h->stream);
         if (ntiles_out) *ntiles_out = ntiles;
         return OZ2_OK;
     }
@@ -1630,8 +1679,7 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
             ++h->launches;
             mark(h, kProbe);
             std::vector<int> failed(ntiles);
-            OZ2_CUDA(h, cudaMemcpyAsync(failed.data(), d_fail, ntiles * 4, cudaMemcpyDeviceToHost, h->stream));
-            OZ2_CUDA(h, cudaStreamSynchronize(h->stream));
+            if ((st = read_back(h, {{failed.data(), d_fail, static_cast<size_t>(ntiles) * 4}}))) return st;
             h->astats[2] = static_cast<int64_t>(pi.size());
             std::vector<int64_t> redo;
             std::vector<int> redo_s;
@@ -1739,6 +1787,7 @@ int oz2_destroy(oz2_handle h) {
         if (h->ring_host[i]) cudaFreeHost(h->ring_host[i]);
         if (h->ring_ev[i]) cudaEventDestroy(h->ring_ev[i]);
     }
+    if (h->rb_host) cudaFreeHost(h->rb_host);
     if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
     if (h->d_mlp) cudaFree(h->d_mlp);
     if (h->ws2) cudaFree(h->ws2);

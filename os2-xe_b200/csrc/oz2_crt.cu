@@ -264,6 +264,39 @@ void write_blob_n(const unsigned char* src, size_t n, unsigned char* dst, cudaSt
     write_blob_kernel<N><<<1, 256, 0, st>>>(bp, dst);
 }
 
+// VEC: both pointers 16-byte aligned, 16-byte words first
+template <bool VEC>
+__global__ void sm_copy_kernel(const unsigned char* __restrict__ src, unsigned char* __restrict__ dst, size_t bytes) {
+    const size_t tid = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
+    size_t tail = 0;
+    if (VEC) {
+        const size_t n16 = bytes / 16;
+        for (size_t i = tid; i < n16; i += stride)
+            reinterpret_cast<uint4*>(dst)[i] = reinterpret_cast<const uint4*>(src)[i];
+        tail = n16 * 16;
+    }
+    for (size_t i = tail + tid; i < bytes; i += stride) dst[i] = src[i];
+}
+
+template <bool VEC>
+__global__ void fill_kernel(unsigned char* __restrict__ dst, uint32_t word, size_t bytes) {
+    const size_t tid = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
+    size_t tail = 0;
+    if (VEC) {
+        const size_t n16 = bytes / 16;
+        for (size_t i = tid; i < n16; i += stride) reinterpret_cast<uint4*>(dst)[i] = make_uint4(word, word, word, word);
+        tail = n16 * 16;
+    }
+    for (size_t i = tail + tid; i < bytes; i += stride) dst[i] = static_cast<unsigned char>(word);
+}
+
+// blocks of 256 threads for `units` units of work, at most 4 per SM of a B200
+unsigned copy_blocks(size_t units) {
+    return static_cast<unsigned>(std::min<size_t>((units + 255) / 256 + 1, 4 * 148));
+}
+
 __global__ void scale_c_kernel(double* C, int64_t ldc, int64_t m, int64_t n, double br, double bi, int cplx) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= m) return;
@@ -372,6 +405,24 @@ void launch_write_blob(const void* src, size_t bytes, void* dst, cudaStream_t st
         else if (n <= 12288) write_blob_n<12288>(p + off, n, d, st);
         else write_blob_n<kParamBlobBytes>(p + off, n, d, st);
     }
+}
+
+void launch_sm_copy(const void* src, void* dst, size_t bytes, cudaStream_t st) {
+    if (bytes == 0) return;
+    const auto* s = static_cast<const unsigned char*>(src);
+    auto* d = static_cast<unsigned char*>(dst);
+    if (((reinterpret_cast<uintptr_t>(s) | reinterpret_cast<uintptr_t>(d)) & 15) == 0)
+        sm_copy_kernel<true><<<copy_blocks(bytes / 16), 256, 0, st>>>(s, d, bytes);
+    else
+        sm_copy_kernel<false><<<copy_blocks(bytes), 256, 0, st>>>(s, d, bytes);
+}
+
+void launch_fill(void* dst, unsigned char value, size_t bytes, cudaStream_t st) {
+    if (bytes == 0) return;
+    auto* d = static_cast<unsigned char*>(dst);
+    const uint32_t word = value * 0x01010101u;
+    if ((reinterpret_cast<uintptr_t>(d) & 15) == 0) fill_kernel<true><<<copy_blocks(bytes / 16), 256, 0, st>>>(d, word, bytes);
+    else fill_kernel<false><<<copy_blocks(bytes), 256, 0, st>>>(d, word, bytes);
 }
 
 void launch_scale_c(double* C, int64_t ldc, int64_t m, int64_t n, const double* beta, bool cplx, cudaStream_t st) {

@@ -158,6 +158,15 @@ cudaError_t prepare_gemm_kernels();
 constexpr size_t kParamBlobBytes = 30 * 1024;
 void launch_write_blob(const void* src, size_t bytes, void* dst, cudaStream_t st);
 
+// Copies bytes with SM loads and stores; either side may be pinned host memory, which unified
+// addressing maps into the device's address space. A call moves its own small data (item tables
+// in, tile decisions out) only through these kernels, in stream order on the SMs: a
+// cudaMemcpyAsync on the call's stream waits behind the bulk host copies other streams queued
+// on the copy engines.
+void launch_sm_copy(const void* src, void* dst, size_t bytes, cudaStream_t st);
+// bytes of dst set to `value`, by a kernel
+void launch_fill(void* dst, unsigned char value, size_t bytes, cudaStream_t st);
+
 // C = beta * C (beta == 0 writes zeros), the k == 0 / alpha == 0 path
 void launch_scale_c(double* C, int64_t ldc, int64_t m, int64_t n, const double* beta, bool cplx, cudaStream_t st);
 
