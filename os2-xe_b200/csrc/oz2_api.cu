@@ -98,6 +98,10 @@ struct oz2_context {
     cudaEvent_t ring_ev[kRing] = {};
     bool ring_used[kRing] = {};
     int ring_next = 0;
+    // the highest-priority stream for those copies: their few blocks are dispatched ahead of
+    // the native tiles' cuBLAS blocks on the other streams
+    cudaStream_t xfer = nullptr;
+    cudaEvent_t xfer_in = nullptr;
     // pinned buffer that kernels write small results into for the host to read
     void* rb_host = nullptr;
     void* rb_dev = nullptr;
@@ -488,9 +492,22 @@ int check_grid(oz2_context* h, const Program& prog) {
 }
 
 // ---------------------------------------------------------------- issuing a program
+// the transfer stream starts after everything issued to the caller's stream so far
+int xfer_fork(oz2_context* h) {
+    if (!h->xfer) {
+        int least = 0, greatest = 0;
+        OZ2_CUDA(h, cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        OZ2_CUDA(h, cudaStreamCreateWithPriority(&h->xfer, cudaStreamNonBlocking, greatest));
+        OZ2_CUDA(h, cudaEventCreateWithFlags(&h->xfer_in, cudaEventDisableTiming));
+    }
+    OZ2_CUDA(h, cudaEventRecord(h->xfer_in, h->stream));
+    OZ2_CUDA(h, cudaStreamWaitEvent(h->xfer, h->xfer_in, 0));
+    return OZ2_OK;
+}
+
 // copies host bytes to device memory on the stream: small blobs through a kernel parameter,
-// large ones through the pinned staging ring and a copy kernel (no copy engine: see
-// launch_sm_copy)
+// large ones through the pinned staging ring and a copy kernel on the transfer stream (no copy
+// engine: see launch_sm_copy)
 int put_blob(oz2_context* h, const void* data, size_t bytes, unsigned char* dev) {
     if (bytes == 0) return OZ2_OK;
     if (bytes <= kParamBlobBytes) {
@@ -514,9 +531,11 @@ int put_blob(oz2_context* h, const void* data, size_t bytes, unsigned char* dev)
         h->ring_cap[slot] = cap;
     }
     std::memcpy(h->ring_host[slot], data, bytes);
-    launch_sm_copy(h->ring_dev[slot], dev, bytes, h->stream);
+    if (int st = xfer_fork(h)) return st;  // the region's earlier readers have finished
+    launch_sm_copy(h->ring_dev[slot], dev, bytes, h->xfer);
     ++h->launches;
-    OZ2_CUDA(h, cudaEventRecord(h->ring_ev[slot], h->stream));
+    OZ2_CUDA(h, cudaEventRecord(h->ring_ev[slot], h->xfer));
+    OZ2_CUDA(h, cudaStreamWaitEvent(h->stream, h->ring_ev[slot], 0));
     h->ring_used[slot] = true;
     return OZ2_OK;
 }
@@ -543,13 +562,14 @@ int read_back(oz2_context* h, std::initializer_list<HostRead> reads) {
         OZ2_CUDA(h, cudaHostGetDevicePointer(&h->rb_dev, h->rb_host, 0));
         h->rb_cap = cap;
     }
+    if (int st = xfer_fork(h)) return st;
     size_t off = 0;
     for (const HostRead& r : reads) {
-        launch_sm_copy(r.src, static_cast<unsigned char*>(h->rb_dev) + off, r.bytes, h->stream);
+        launch_sm_copy(r.src, static_cast<unsigned char*>(h->rb_dev) + off, r.bytes, h->xfer);
         ++h->launches;
         off += (r.bytes + 15) & ~size_t{15};
     }
-    OZ2_CUDA(h, cudaStreamSynchronize(h->stream));
+    OZ2_CUDA(h, cudaStreamSynchronize(h->xfer));
     off = 0;
     for (const HostRead& r : reads) {
         std::memcpy(r.dst, static_cast<const unsigned char*>(h->rb_host) + off, r.bytes);
@@ -1793,6 +1813,8 @@ int oz2_destroy(oz2_handle h) {
     if (h->ws2) cudaFree(h->ws2);
     if (h->cublas) cublasDestroy(h->cublas);
     if (h->nat_stream) cudaStreamDestroy(h->nat_stream);
+    if (h->xfer) cudaStreamDestroy(h->xfer);
+    if (h->xfer_in) cudaEventDestroy(h->xfer_in);
     for (cudaEvent_t e : {h->nat_fork, h->nat_join, h->nat_t0, h->nat_t1})
         if (e) cudaEventDestroy(e);
     delete h;
