@@ -115,7 +115,10 @@ int oz2_autotune_grouped(oz2_handle h, int count, const oz2_dgemm_problem* probl
  * stats (may be NULL, 10 entries): tiles, sum of s over emulated tiles (reruns included), probed
  * tiles, rerun tiles, sum of s of the reruns (25 for native), sum of the judge's s (25 for native),
  * MLP used, int8 multiply-adds of the emulated tiles (s m_t n_t k summed, reruns included),
- * native tiles, native FP64 multiply-adds. Synchronises the stream. With profiling on,
+ * native tiles, native FP64 multiply-adds. The host waits in the middle of the call for the tile
+ * statistics (and in mode 0 for the probe). Those reads, and the uploads of item tables, are copy
+ * kernels on an internal highest-priority stream, not copy-engine transfers, so host-device copies
+ * that the caller queues on other streams do not delay the call. With profiling on,
  * oz2_stage_times reports scale (with the tile statistics, features and MLP), split, GEMM and CRT
  * summed over the tile batches; the probe and native tiles are in none of them. */
 int oz2_dgemm_adaptive(oz2_handle h, int count, const oz2_dgemm_problem* problems, int target_bits, int mode,
