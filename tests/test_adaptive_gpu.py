@@ -487,3 +487,49 @@ def test_certified_tiles_override_the_mlp(az):
     assert st["mlp"] == 1 and st["probed"] == 0
     assert st["sum_s"] == ref["sum_s"] and st["native_tiles"] == ref["native_tiles"]
     assert dd_check(az, m, n, k, dA, dB, dC) <= 1.0
+
+
+def test_results_do_not_depend_on_concurrent_host_copies(az):
+    """the call's own transfers (item tables in through the pinned ring, tile decisions out) run as
+    copy kernels on an internal stream: with large host copies queued on two other streams the
+    outputs are the same bits as without them, in the MLP mode (probe reads included) and the
+    certified tile mode, on a batch whose item tables exceed one kernel-parameter blob"""
+    import torch
+    model = az.load_model()
+    try:
+        rng = np.random.default_rng(77)
+        probs, outs = [], []
+        for q in range(16):
+            n = int(rng.integers(300, 1400))
+            A, B = nn_problem(900 + 2 * q, n, n, n, float(rng.uniform(0, 8)), 40)
+            probs.append((n, to_dev(A), to_dev(B)))
+
+        def run(mode):
+            Cs = [torch.zeros(n * n, dtype=torch.float64, device="cuda") for n, _, _ in probs]
+            az.gemm_adaptive([("N", "N", n, n, n, 1.0, dA, n, dB, n, 0.0, dC, n, 16)
+                              for (n, dA, dB), dC in zip(probs, Cs)], 53, mode)
+            return Cs
+
+        big = 1 << 26  # 512 MiB each way
+        h_in = torch.ones(big, dtype=torch.float64, pin_memory=True)
+        h_out = torch.empty(big, dtype=torch.float64, pin_memory=True)
+        d_in = torch.empty(big, dtype=torch.float64, device="cuda")
+        d_out = torch.ones(big, dtype=torch.float64, device="cuda")
+        up, down = torch.cuda.Stream(), torch.cuda.Stream()
+        for mode in (az.ADAPTIVE_MLP, az.ADAPTIVE_CERTIFIED_TILE):
+            quiet = run(mode)
+            torch.cuda.synchronize()
+            for _ in range(3):
+                with torch.cuda.stream(up):
+                    d_in.copy_(h_in, non_blocking=True)
+                with torch.cuda.stream(down):
+                    h_out.copy_(d_out, non_blocking=True)
+            busy = run(mode)
+            torch.cuda.synchronize()
+            az.check_device_error()
+            for (n, _, _), a, b in zip(probs, quiet, busy):
+                assert torch.equal(a.view(torch.int64), b.view(torch.int64)), (mode, n)
+        assert model["threshold"] > 0
+    finally:
+        az.set_mlp_weights(None)
+        az.set_adaptive_options(TILE, 0.9)
