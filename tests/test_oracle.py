@@ -189,6 +189,41 @@ def test_oracle_against_reference_build(oracle, ref):
         assert np.array_equal(bits(C1), bits(C2)), (ta, tb, m, n, k, s)
 
 
+def test_zgemm_oracle_against_reference_build(oracle, ref):
+    """random complex products through both CPU paths: every op pair, s across the narrow and wide
+    paths (the plan of 2k), alpha and beta complex"""
+    rng = np.random.default_rng(123)
+    for trial in range(8):
+        ta, tb = rng.choice(list("NTC")), rng.choice(list("NTC"))
+        m, n, k = (int(x) for x in rng.integers(1, 60, 3))
+        s = int(rng.integers(6, 25))
+        Ar, Ac = op_shape(ta, m, k)
+        Br, Bc = op_shape(tb, k, n)
+        A = make_mat(400 + trial, Ar, Ac, Ar + 1, "wide", 10, cplx=True)
+        B = make_mat(500 + trial, Br, Bc, Br + 2, "wide", 10, cplx=True)
+        C1 = make_mat(600 + trial, m, n, m + 2, "u", cplx=True, pad=0.125)
+        C2 = C1.copy(order="F")
+        al, be = complex(0.5, -1.25), complex(-0.75, 0.25)
+        st_o = oracle.zgemm(ta, tb, m, n, k, al, A, Ar + 1, B, Br + 2, be, C1, m + 2, s)
+        st_r = ref.zgemm(ta, tb, m, n, k, al, A, Ar + 1, B, Br + 2, be, C2, m + 2, s)
+        assert st_o == st_r == 0, (ta, tb, m, n, k, s)
+        assert np.array_equal(bits(C1), bits(C2)), (ta, tb, m, n, k, s)
+
+
+@pytest.mark.parametrize("k,s", [(1500, 12), (2100, 17), (3000, 20), (700, 24)])
+def test_long_k_oracle_against_reference_build(oracle, ref, k, s):
+    """longer k with wide exponent ranges: tk on both sides of the narrow / wide boundary (62)"""
+    m, n = 33, 29
+    A = make_mat(700 + k, m, k, m + 3, "wide", 30)
+    B = make_mat(800 + k, k, n, k + 1, "wide", 30)
+    C1 = make_mat(900 + k, m, n, m, "u")
+    C2 = C1.copy(order="F")
+    st_o = oracle.dgemm("N", "N", m, n, k, 1.0, A, m + 3, B, k + 1, 0.5, C1, m, s)
+    st_r, _ = ref.dgemm("N", "N", m, n, k, 1.0, A, m + 3, B, k + 1, 0.5, C2, m, s)
+    assert st_o == st_r == 0
+    assert np.array_equal(bits(C1), bits(C2)), oracle.plan(s, k).tk
+
+
 def test_reference_own_suite_passes():
     """the reference's tests/test_ozaki2.cpp, built for the host, passes its quick suite"""
     exe = os.path.join(ROOT, "oracle", "_ref", "test_ozaki2")
