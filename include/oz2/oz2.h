@@ -186,13 +186,24 @@ int oz2_stage_times(oz2_handle h, double* out4);
 int oz2_last_tiling(oz2_handle h, int64_t* out6);
 
 /* Ozaki2::set_tuning: src/ozaki2_gpu.hpp:713, Tuning :41-45. The reference's three knobs are
- * Xe2-specific; here they are accepted and reported back, and pow2_tiles keeps its meaning
- * (prefer power-of-two tile candidates). */
+ * Xe2-specific. pow2_tiles keeps its meaning: with it set (the default) the tiling of C under a
+ * workspace limit considers power-of-two tile edges first. batched_gemm and pad_lda are accepted
+ * and stored but change nothing here: every INT8 GEMM of a call is one persistent launch, and the
+ * planes are always written in a padded, pre-tiled layout. */
 int oz2_set_tuning(oz2_handle h, int batched_gemm, int pad_lda, int pow2_tiles);
 
 /* Device-side error word: non-zero after a kernel's bounded wait ran out (OZ2_ETIMEOUT).
  * Synchronises the handle's stream, returns and clears the word. */
 int oz2_check_device_error(oz2_handle h);
+
+/* Test of the failure path (no counterpart in the reference; process-wide, read at each GEMM
+ * launch, so set it only while no other call is being made). wait_limit_ns bounds every
+ * mbarrier wait of the INT8 GEMM (0 restores the 2 s default); with stall_mma != 0 the GEMM's
+ * MMA issuer issues nothing, so the copy and epilogue waits run out: the kernel records a code in
+ * the error word, drains its copies, frees its tensor memory and returns, the call's C is not
+ * valid, and oz2_check_device_error (oz2_noalloc_check_device_error for oz2_dgemm_noalloc)
+ * returns OZ2_ETIMEOUT. Calls after oz2_set_failure_test(0, 0) compute normally. */
+int oz2_set_failure_test(int64_t wait_limit_ns, int stall_mma);
 
 /* Emulated DGEMM for callers that cannot allocate device memory. No counterpart in the
  * reference. Same arguments, checks and results as oz2_dgemm, but no handle: it works on the
@@ -204,6 +215,12 @@ int oz2_check_device_error(oz2_handle h);
 int oz2_dgemm_noalloc(void* stream, char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha,
                       const double* A, int64_t lda, const double* B, int64_t ldb, double beta, double* C,
                       int64_t ldc, int num_moduli);
+/* The device error word of oz2_dgemm_noalloc (no counterpart in the reference): synchronises the
+ * stream, returns OZ2_ETIMEOUT (and clears the word) when a bounded wait of the last call's GEMM
+ * ran out, so its C is not valid; the next oz2_dgemm_noalloc clears the word as well, so check
+ * before it. Allocates nothing. Neither entry point may be used after cudaDeviceReset: the array's
+ * device address is looked up once per device. */
+int oz2_noalloc_check_device_error(void* stream);
 
 /* message of the last failed call on the handle (or of the last failed handle-less call) */
 const char* oz2_last_error(oz2_handle h);

@@ -2411,6 +2411,12 @@ int oz2_check_device_error(oz2_handle h) {
     return OZ2_OK;
 }
 
+int oz2_set_failure_test(int64_t wait_limit_ns, int stall_mma) {
+    if (wait_limit_ns < 0) return fail(nullptr, OZ2_EINVAL, "oz2: negative wait limit");
+    set_gemm_failure_test(static_cast<uint64_t>(wait_limit_ns), stall_mma);
+    return OZ2_OK;
+}
+
 const char* oz2_last_error(oz2_handle h) { return h ? h->err.c_str() : g_error.c_str(); }
 
 const char* oz2_status_string(int status) {

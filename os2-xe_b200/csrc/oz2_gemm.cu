@@ -21,6 +21,7 @@
 // Every mbarrier wait is time-bounded; on expiry the kernel records an error code, drains its
 // in-flight copies and MMAs, frees TMEM and returns.
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 
 #include "oz2_kernels.cuh"
@@ -51,6 +52,8 @@ struct GemmParams {
     int group_j;
     int64_t jobs;
     int* err;
+    uint64_t wait_ns;  // limit of every bounded mbarrier wait
+    int stall;         // failure-path test: the MMA issuer issues nothing, so the waits run out
 };
 
 struct Job {
@@ -149,7 +152,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
                 const int8_t* srcJ = J.I->planes_j + pj * J.I->pstride_j + J.tj * row_block;
                 const int8_t* srcI = J.I->planes_i + pi * J.I->pstride_i + (static_cast<int64_t>(J.ti) * (BN / 128)) * row_block;
                 for (int64_t kb = 0; ok && kb < kb_total; ++kb) {
-                    if (!dev::mbar_wait(empty(stage), phase ^ 1u, abort_flag, P.err, dev::kErrTimeoutEmpty)) {
+                    if (!dev::mbar_wait(empty(stage), phase ^ 1u, abort_flag, P.err, dev::kErrTimeoutEmpty,
+                                         P.wait_ns)) {
                         ok = false;
                         break;
                     }
@@ -176,7 +180,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
         if (lane == 0) {
             int stage = 0;
             uint32_t phase = 0;
-            bool ok = true, issued = false;
+            bool ok = !P.stall, issued = false;
             int local = 0;  // (job, chunk) pairs processed: selects the accumulator
             for (int64_t job = blockIdx.x; ok && job < P.jobs; job += nprog) {
                 const Job J = decode(P, job);
@@ -184,7 +188,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
                 for (int64_t c = 0; ok && c < J.nch; ++c, ++local) {
                     const int acc = local & 1;
                     const uint32_t use = static_cast<uint32_t>(local >> 1);
-                    if (!dev::mbar_wait(acc_empty(acc), (use & 1u) ^ 1u, abort_flag, P.err, dev::kErrTimeoutAccEmpty)) {
+                    if (!dev::mbar_wait(acc_empty(acc), (use & 1u) ^ 1u, abort_flag, P.err, dev::kErrTimeoutAccEmpty,
+                                         P.wait_ns)) {
                         ok = false;
                         break;
                     }
@@ -192,7 +197,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
                     const uint32_t d_tmem = tmem_base + static_cast<uint32_t>(acc) * BN;
                     const int64_t kb0 = c * kChunkKB, kb1 = min(kb_total, kb0 + kChunkKB);
                     for (int64_t kb = kb0; kb < kb1; ++kb) {
-                        if (!dev::mbar_wait(full(stage), phase, abort_flag, P.err, dev::kErrTimeoutFull)) {
+                        if (!dev::mbar_wait(full(stage), phase, abort_flag, P.err, dev::kErrTimeoutFull,
+                                             P.wait_ns)) {
                             ok = false;
                             break;
                         }
@@ -252,7 +258,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
                 const int acc = local & 1;
                 const uint32_t use = static_cast<uint32_t>(local >> 1);
                 int w_ok = 1;
-                if (lane == 0) w_ok = dev::mbar_wait(acc_full(acc), use & 1u, abort_flag, P.err, dev::kErrTimeoutAccFull);
+                if (lane == 0) w_ok = dev::mbar_wait(acc_full(acc), use & 1u, abort_flag, P.err, dev::kErrTimeoutAccFull,
+                                                  P.wait_ns);
                 w_ok = __shfl_sync(0xFFFFFFFFu, w_ok, 0);
                 if (!w_ok) {
                     ok = false;
@@ -378,6 +385,14 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
     }
 }
 
+// failure-path test settings, read at every launch (process-wide)
+std::atomic<uint64_t> g_wait_ns{dev::kWaitLimitNs};
+std::atomic<int> g_stall{0};
+
+GemmParams make_params(const GemmItem* d_items, int count, int group_j, int64_t jobs, int* err) {
+    return GemmParams{d_items, count, group_j, jobs, err, g_wait_ns.load(), g_stall.load()};
+}
+
 template <int BN, int KIND = kKindResidue>
 void launch_bn(const GemmParams& P, int grid, cudaStream_t st) {
     gemm_i8_modm_kernel<BN, KIND><<<grid, kGemmThreads, Cfg<BN>::kSmemBytes, st>>>(P);
@@ -400,12 +415,17 @@ cudaError_t prepare_gemm_kernels() {
     return e;
 }
 
+void set_gemm_failure_test(uint64_t wait_ns, int stall) {
+    g_wait_ns.store(wait_ns ? wait_ns : dev::kWaitLimitNs);
+    g_stall.store(stall ? 1 : 0);
+}
+
 int64_t gemm_tiles_i(int64_t m, int bn) { return ceil_div(m, bn); }
 
 void launch_gemm(const GemmItem* d_items, int count, int64_t jobs, const GemmConfig& cfg, int num_sms, int* err,
                  cudaStream_t st) {
     if (count <= 0 || jobs <= 0) return;
-    GemmParams P{d_items, count, cfg.group_j > 0 ? cfg.group_j : 16, jobs, err};
+    const GemmParams P = make_params(d_items, count, cfg.group_j > 0 ? cfg.group_j : 16, jobs, err);
     const int ctas = cfg.ctas > 0 ? std::min(cfg.ctas, num_sms) : num_sms;
     const int grid = static_cast<int>(std::min<int64_t>(ctas, jobs));
     if (cfg.bn == 128) launch_bn<128>(P, grid, st);
@@ -415,14 +435,14 @@ void launch_gemm(const GemmItem* d_items, int count, int64_t jobs, const GemmCon
 void launch_gemm_oz1(const GemmItem* d_items, int count, int64_t jobs, const GemmConfig& cfg, int num_sms, int* err,
                      cudaStream_t st) {
     if (count <= 0 || jobs <= 0) return;
-    GemmParams P{d_items, count, cfg.group_j > 0 ? cfg.group_j : 16, jobs, err};
+    const GemmParams P = make_params(d_items, count, cfg.group_j > 0 ? cfg.group_j : 16, jobs, err);
     const int grid = static_cast<int>(std::min<int64_t>(num_sms, jobs));
     launch_bn<256, kKindOz1>(P, grid, st);
 }
 
 void launch_gemm_cert(const GemmItem* d_items, int count, int64_t jobs, int num_sms, int* err, cudaStream_t st) {
     if (count <= 0 || jobs <= 0) return;
-    GemmParams P{d_items, count, 16, jobs, err};
+    const GemmParams P = make_params(d_items, count, 16, jobs, err);
     const int grid = static_cast<int>(std::min<int64_t>(num_sms, jobs));
     launch_bn<256, kKindCert>(P, grid, st);
 }

@@ -152,6 +152,11 @@ void launch_crt(const CrtItem* d_items, int count, int64_t blocks, const Plan& p
 
 // sets the GEMM kernels' shared-memory attribute (once per device, before any graph capture)
 cudaError_t prepare_gemm_kernels();
+// Failure-path test of the GEMM's bounded waits (process-wide, read at each launch): wait_ns
+// limits every mbarrier wait (0 = the 2 s default); with stall set the MMA issuer of every CTA
+// issues nothing, so the other roles' waits run out, record their code in the error word, drain
+// their copies, free TMEM and return.
+void set_gemm_failure_test(uint64_t wait_ns, int stall);
 
 // Copies up to kParamBlobBytes of host data to device memory by passing them as the parameter
 // of a one-block kernel: no staging buffer, no memcpy, capturable in a graph.

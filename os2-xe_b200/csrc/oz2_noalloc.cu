@@ -17,7 +17,14 @@
 //
 // Set-up: the first call on each device looks up the device address of the array with
 // cudaGetSymbolAddress while that device is current (in host code the array's name is only a
-// host-side stand-in). That first call should come before any stream capture.
+// host-side stand-in) and raises the GEMM kernels' dynamic shared-memory limit, which a process
+// that never created a handle has not done. That first call should come before any stream
+// capture. The address is kept per device for the life of the process: after cudaDeviceReset
+// the array may move, so this entry point must not be used after a device reset.
+//
+// Errors on the device: the GEMM's bounded waits record a code in the first word of the array.
+// oz2_noalloc_check_device_error reads (and clears) it; the next call clears it too, so check
+// after the call whose result matters and before the next one.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -63,6 +70,11 @@ int scratch_for_current_device(unsigned char** ptr, int* num_sms) {
         int sms = 0;
         e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (e != cudaSuccess) return reject(OZ2_ECUDA, std::string("oz2_dgemm_noalloc: ") + cudaGetErrorString(e));
+        // the GEMM needs more than 48 KiB of dynamic shared memory; oz2_create sets this for
+        // handle users, and a caller of this entry point may never have created a handle
+        e = oz2::prepare_gemm_kernels();
+        if (e != cudaSuccess)
+            return reject(OZ2_ECUDA, std::string("oz2_dgemm_noalloc: kernel set-up: ") + cudaGetErrorString(e));
         g_num_sms[dev] = sms;
         g_scratch_dev[dev] = static_cast<unsigned char*>(p);
     }
@@ -238,4 +250,27 @@ extern "C" int oz2_dgemm_noalloc(void* stream, char ta, char tb, int64_t m, int6
     launch_crt(&D->c, 1, crt_blocks, p, false, st);
     e = cudaGetLastError();
     return e == cudaSuccess ? OZ2_OK : reject(OZ2_ECUDA, std::string("oz2_dgemm_noalloc: ") + cudaGetErrorString(e));
+}
+
+extern "C" int oz2_noalloc_check_device_error(void* stream) {
+    using namespace oz2;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    unsigned char* scratch = nullptr;
+    int num_sms = 0;
+    const int rc = scratch_for_current_device(&scratch, &num_sms);
+    if (rc) return rc;
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return reject(OZ2_ECUDA, std::string("oz2_noalloc_check_device_error: ") + cudaGetErrorString(e));
+    int v = 0;
+    e = cudaMemcpy(&v, scratch, sizeof v, cudaMemcpyDeviceToHost);  // the error word at offset 0
+    if (e != cudaSuccess) return reject(OZ2_ECUDA, std::string("oz2_noalloc_check_device_error: ") + cudaGetErrorString(e));
+    if (v) {
+        e = cudaMemset(scratch, 0, sizeof v);
+        if (e != cudaSuccess)
+            return reject(OZ2_ECUDA, std::string("oz2_noalloc_check_device_error: ") + cudaGetErrorString(e));
+        char buf[96];
+        std::snprintf(buf, sizeof buf, "oz2_dgemm_noalloc: a device-side wait ran out (code %d)", v);
+        return reject(OZ2_ETIMEOUT, buf);
+    }
+    return OZ2_OK;
 }

@@ -13,7 +13,8 @@ enum : int { kErrNone = 0, kErrTimeoutFull = 1, kErrTimeoutEmpty = 2, kErrTimeou
              kErrTimeoutAccEmpty = 4, kErrTimeoutDrain = 5 };
 
 // A wait on an mbarrier phase that is still pending after this long is treated as a fault.
-// Healthy waits last microseconds.
+// Healthy waits last microseconds. The GEMM takes its limit as a kernel parameter (this value
+// unless a test of the failure path shortens it); draining waits always use this one.
 constexpr uint64_t kWaitLimitNs = 2000000000ull;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -65,17 +66,17 @@ __device__ __forceinline__ bool mbar_try_wait_sleep(uint32_t bar, uint32_t parit
 }
 
 // Waits for the phase of `bar` with the given parity. Returns false when the CTA-wide abort
-// flag is raised by another role, or when the wait exceeds kWaitLimitNs (then it raises the
-// flag and records `code` in the global error word).
+// flag is raised by another role, or when the wait exceeds limit_ns (then it raises the flag and
+// records `code` in the global error word).
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag, int* gerr,
-                                          int code) {
+                                          int code, uint64_t limit_ns) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = global_timer_ns();
     for (uint32_t it = 1;; ++it) {
         if (mbar_try_wait_sleep(bar, parity)) return true;
         if ((it & 63) == 0) {
             if (*abort_flag) return false;
-            if (global_timer_ns() - t0 > kWaitLimitNs) {
+            if (global_timer_ns() - t0 > limit_ns) {
                 *abort_flag = 1;
                 atomicExch(gerr, code);
                 return false;

@@ -44,6 +44,7 @@ _lib.oz2_stage_times.argtypes = [_vp, C.POINTER(_dbl)]
 _lib.oz2_last_tiling.argtypes = [_vp, C.POINTER(_i64)]
 _lib.oz2_set_tuning.argtypes = [_vp, _i32, _i32, _i32]
 _lib.oz2_check_device_error.argtypes = [_vp]
+_lib.oz2_set_failure_test.argtypes = [_i64, _i32]
 
 
 class DgemmProblem(C.Structure):
@@ -79,6 +80,13 @@ _lib.oz2_status_string.restype = C.c_char_p
 def lib():
     """The loaded ctypes library (for callers that bind further entry points)."""
     return _lib
+
+
+def set_failure_test(wait_limit_ns=0, stall_mma=False):
+    """Failure-path test of the INT8 GEMM's bounded waits (process-wide): wait_limit_ns bounds
+    every wait (0 = the 2 s default); with stall_mma the MMA issuer issues nothing, so the waits
+    run out and check_device_error raises TimeoutError. set_failure_test() restores normal runs."""
+    _raise(_lib.oz2_set_failure_test(int(wait_limit_ns), 1 if stall_mma else 0))
 
 
 def mlp_info():
