@@ -1,24 +1,27 @@
 #!/usr/bin/env python
 """Benchmark: emulated FP64 DGEMM (Ozaki Scheme II on the INT8 tensor cores) on B200.
 
-Headline workload (one step = one batched call over one batch of the stream): the adaptive-s
-stream, DGEMMs with m = n = k log-uniform in [256, 4096], inputs (u - 0.5) exp(phi g) with
-u ~ U[0,1), g ~ N(0,1), phi per problem uniform in [0, 8], the rows of A and the columns of B
-scaled by 2^e, e uniform in [-40, 40]; alpha = 1, beta = 0, target DGEMM-level error
-(|C - AB| <= k 2^-53 (|A||B|)_ij). The MLP picks s per 512 x 512 tile, tiles below their analytic
-s are probed and rerun at it on failure. Seeded synthetic inputs generated on the device; each
-batch (several GB) is larger than the 126 MB L2, so no flush is needed between steps.
-Metric: FP64-equivalent TFLOP/s = sum 2 m n k / t. Beside it, the fixed-s forms of the same
-stream (per-problem analytic s batched and as plain calls, s = 24, the reference's
-moduli_for_bits(k, 53)), each output of each form checked against a double-double product.
-Extras: the m = n = k = 8192 DGEMM at s = 16 (alpha 1.5, beta -0.5, ldc = m + 16) against cuBLAS
-DGEMM, and the grouped launch of 512 uneven DGEMMs.
+Headline workload: the adaptive-s stream of 10,000 DGEMMs with m = n = k log-uniform in
+[256, 4096], inputs (u - 0.5) exp(phi g) with u ~ U[0,1), g ~ N(0,1), phi per problem uniform in
+[0, 8], the rows of A and the columns of B scaled by 2^e, e uniform in [-40, 40]; alpha = 1,
+beta = 0, target DGEMM-level error (|C - AB| <= k 2^-53 (|A||B|)_ij). The stream is cut into
+`--steps` batches; one step = one batched adaptive call over one batch (10,000 / steps problems,
+at most 512), generated on the device with a seeded generator before the step and timed alone
+with CUDA events, so every timed problem is distinct; each batch (tens of GB) is far larger than
+the 126 MB L2. s is chosen per 512 x 512 tile: certified where a tile needs 23 or more moduli by
+the analytic rule, else by the MLP (probed, rerun at the judge's s on failure); tiles no s <= 24
+serves run in native FP64. Metric: FP64-equivalent TFLOP/s = sum 2 m n k / t. The fixed-s forms
+of the same batches (per-problem analytic s batched and as plain calls, the certified per-problem
+s, cuBLAS DGEMM for everything, s = 24, the reference's moduli_for_bits(k, 53)) are timed step by
+step on the same problems, and every output of every form is checked against a double-double
+product. Extras: the m = n = k = 8192 DGEMM at s = 16 (alpha 1.5, beta -0.5, ldc = m + 16)
+against cuBLAS DGEMM, the ZGEMM 4096^3, and the grouped launch of 512 uneven DGEMMs.
 
   python bench.py [--gpus N --steps K --warmup W]            this implementation
   python bench.py --impl reference [--steps K --warmup W]    the reference's CPU path
 
 Under torchrun every rank runs its own stream (weak scaling, no collective on the data path);
-value = all ranks' work / max over ranks of the device-timed region.
+value = all ranks' work / the sum over steps of the slowest rank's step time.
 """
 import argparse
 import json
@@ -37,16 +40,21 @@ sys.path.insert(0, os.path.join(ROOT, "os2-xe_b200"))
 METRIC = "FP64-equiv TFLOP/s at DGEMM-level error: adaptive-s batched vs fixed-s, 1 B200"
 UNIT = "TFLOP/s"
 TARGET_BITS = 53
-STREAM_BYTES = 48 << 30  # device bytes of distinct stream problems kept resident
+MAX_BATCH = 512          # problems per step: inputs, outputs and the check's references of a batch
+WORKSPACE = 24 << 30     # workspace limit of the bench's handle (the same for every form)
+E2E_BATCH = 64           # problems per step of the end-to-end leg (pinned host arenas)
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="oz2", choices=["oz2", "reference"])
-    ap.add_argument("--batch", type=int, default=64, help="problems per step of the adaptive-s stream")
+    ap.add_argument("--problems", type=int, default=10000, help="problems of the adaptive-s stream")
+    ap.add_argument("--batch", type=int, default=0,
+                    help="problems per step (default: problems / steps, at most %d)" % MAX_BATCH)
+    ap.add_argument("--forms", default="all", help="'all' or 'headline': the fixed-s forms beside the headline")
     ap.add_argument("--seed", type=int, default=2025)
     ap.add_argument("--size", type=int, default=8192, help="m = n = k of the DGEMM extra")
     ap.add_argument("--s", type=int, default=16, help="moduli of the DGEMM extra")
@@ -57,13 +65,19 @@ def parse():
     return ap.parse_args()
 
 
+def batch_size(a):
+    return a.batch or max(1, min(MAX_BATCH, -(-a.problems // a.steps)))
+
+
 def workload(a):
-    return {"workload": f"adaptive-s stream: batches of {a.batch} dgemm, m=n=k log-uniform [256,4096], "
-                        "(u-0.5)exp(phi g), phi~U[0,8] per problem, rows of A / columns of B scaled by "
-                        "2^U[-40,40], alpha=1 beta=0, target 53 bits, s per 512x512 tile: certified "
-                        "(problems with analytic s >= 23) or MLP + probe",
-            "batch": a.batch, "tile": 512, "target_bits": TARGET_BITS, "seed": a.seed,
-            "l2": "each batch holds several GB, larger than the 126 MB L2; no flush"}
+    b = batch_size(a)
+    timed = min(a.problems, b * a.steps)
+    return {"workload": f"adaptive-s stream of {a.problems} dgemm (the first {timed} timed, {b} per step, each "
+                        "batch generated before its step), m=n=k log-uniform [256,4096], (u-0.5)exp(phi g), "
+                        "phi~U[0,8] per problem, rows of A / columns of B scaled by 2^U[-40,40], alpha=1 beta=0, "
+                        "target 53 bits, s per 512x512 tile",
+            "problems": a.problems, "problems_timed": timed, "batch": b, "tile": 512, "target_bits": TARGET_BITS,
+            "seed": a.seed, "l2": "each batch holds tens of GB, far larger than the 126 MB L2; no flush"}
 
 
 def stream_specs(seed, count):
@@ -150,77 +164,132 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ CPU legs (reference / oracle)
-CPU_MAX_N = 1024  # problems of the stream the CPU sample takes (larger ones take minutes each)
-
-
-def cpu_stream(a, budget_s, start=0):
-    """The reference's own CPU path (oracle/_ref: src/ozaki2_gpu.hpp compiled for the host, all
-    host threads; the C oracle where it was not built) over the stream's problems with n <= 1024,
-    in stream order from `start`, until `budget_s` seconds of DGEMM time; each problem at its
-    per-problem analytic s (the fixed s that meets the target). Returns (flops, seconds, problems,
-    next start, kind)."""
+def host_problem(n, phi, seed):
+    """one problem of the stream generated by numpy (same distribution as the device generator,
+    not the same numbers): column-major A and B"""
     import numpy as np
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import adaptive_oracle
-    from pyoracle import Oracle, Ref, ref_available
-    threads = os.cpu_count() or 1
-    lib, kind = (Ref(), "reference") if ref_available() else (Oracle(), "port")
-    lib.set_threads(threads)
-    plan_oracle = Oracle()
-    flops = secs = 0.0
-    done = 0
-    i = start
-    specs = stream_specs(a.seed, 100000)
-    while secs < budget_s and i < len(specs):
-        n, phi, seed = specs[i]
-        i += 1
-        if n > CPU_MAX_N:
-            continue
-        rng = np.random.default_rng(seed)
-        A = (rng.random((n, n)) - 0.5) * np.exp(phi * rng.standard_normal((n, n)))
-        A = np.asfortranarray(A * np.ldexp(1.0, rng.integers(-40, 41, (n, 1))))
-        B = (rng.random((n, n)) - 0.5) * np.exp(phi * rng.standard_normal((n, n)))
-        B = np.asfortranarray(B * np.ldexp(1.0, rng.integers(-40, 41, (1, n))))
-        C = np.zeros((n, n), order="F")
-        sv = adaptive_oracle.problem_analytic_s(plan_oracle, "N", "N", n, n, n, A, B, TARGET_BITS)
-        t0 = time.perf_counter()
-        lib.dgemm("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n, sv)
-        secs += time.perf_counter() - t0
-        flops += 2.0 * n ** 3
-        done += 1
-    return flops, secs, done, i, kind, threads
+    rng = np.random.default_rng(seed)
+    A = (rng.random((n, n)) - 0.5) * np.exp(phi * rng.standard_normal((n, n)))
+    A = np.asfortranarray(A * np.ldexp(1.0, rng.integers(-40, 41, (n, 1))))
+    B = (rng.random((n, n)) - 0.5) * np.exp(phi * rng.standard_normal((n, n)))
+    B = np.asfortranarray(B * np.ldexp(1.0, rng.integers(-40, 41, (1, n))))
+    return A, B
+
+
+def blas_threads():
+    try:
+        from threadpoolctl import threadpool_info
+        return max((d.get("num_threads", 0) for d in threadpool_info() if d.get("user_api") == "blas"), default=0)
+    except Exception:  # noqa: BLE001
+        return 0
+
+
+class CpuStream:
+    """The reference's own CPU path (oracle/_ref: src/ozaki2_gpu.hpp built for the host, all host
+    threads; the C oracle where it was not built) over the stream's problems in stream order, each
+    at its per-problem analytic s (the fixed s that meets the target). The reference's Ozaki2::gemm
+    takes s <= 24 only (make_plan rejects more, src/ozaki2_gpu.hpp:160-161), so a problem whose
+    analytic s is 25 runs as host FP64 DGEMM (numpy's BLAS, the reference bench's --cpu path,
+    benchmarks/bench_ozaki2.cpp:133-142), and its time counts. Every call's status is checked."""
+
+    def __init__(self, a):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import adaptive_oracle
+        from pyoracle import Oracle, Ref, ref_available
+        self.ao = adaptive_oracle
+        self.threads = os.cpu_count() or 1
+        self.is_ref = ref_available()
+        self.lib = Ref() if self.is_ref else Oracle()
+        self.kind = "reference" if self.is_ref else "port"
+        self.lib.set_threads(self.threads)
+        self.plans = Oracle()
+        self.specs = stream_specs(a.seed, a.problems)
+        self.pos = 0
+        self.native = self.emulated = 0
+
+    def step(self, budget_s):
+        """problems from the current position until budget_s seconds of compute: (flops, seconds)"""
+        import numpy as np
+        flops = secs = 0.0
+        while secs < budget_s and self.pos < len(self.specs):
+            n, phi, seed = self.specs[self.pos]
+            self.pos += 1
+            A, B = host_problem(n, phi, seed)
+            C = np.zeros((n, n), order="F")
+            sv = self.ao.problem_analytic_s(self.plans, "N", "N", n, n, n, A, B, TARGET_BITS)
+            t0 = time.perf_counter()
+            if sv > 24:
+                np.matmul(A, B, out=C)
+                self.native += 1
+            else:
+                st = self.lib.dgemm("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n, sv)
+                st = st[0] if isinstance(st, tuple) else st
+                if st != 0:
+                    raise RuntimeError(f"CPU path failed on problem {self.pos - 1} (n={n}, s={sv}): status {st}")
+                self.emulated += 1
+            secs += time.perf_counter() - t0
+            flops += 2.0 * n ** 3
+        return flops, secs
+
+    def describe(self, problems, secs):
+        what = "src/ozaki2_gpu.hpp built for the host" if self.is_ref else "the C oracle"
+        return (f"{problems} problems of the same stream in stream order (numpy-generated, same distribution), "
+                f"{self.emulated} at their per-problem analytic s through {what}, {self.native} whose analytic s "
+                f"exceeds 24 as host FP64 DGEMM (numpy BLAS); {secs:.1f} s of compute, {self.threads} threads")
 
 
 def cpu_sample(a, budget_s=12.0):
-    flops, secs, done, _, kind, threads = cpu_stream(a, budget_s)
-    return {"value": flops / secs / 1e12, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": f"the first {done} problems of the same stream with n <= {CPU_MAX_N} (numpy-generated, same "
-                      f"distribution), each at its per-problem analytic s, "
-                      f"{'src/ozaki2_gpu.hpp built for the host' if kind == 'reference' else 'C oracle'}, "
-                      f"{secs:.1f} s of DGEMM time"}
+    cs = CpuStream(a)
+    flops, secs = cs.step(budget_s)
+    return {"value": flops / secs / 1e12, "unit": UNIT, "cores": cs.threads, "kind": cs.kind,
+            "sample": cs.describe(cs.pos, secs)}
+
+
+def cpu_dgemm_sample(a, budget_s=8.0):
+    """host FP64 DGEMM (numpy's BLAS, all its threads) over the stream's problems in stream order:
+    the reference bench's --cpu baseline (benchmarks/bench_ozaki2.cpp:133-142). DGEMM-level error
+    by construction."""
+    import numpy as np
+    flops = secs = 0.0
+    done = 0
+    for n, phi, seed in stream_specs(a.seed, a.problems):
+        if secs >= budget_s:
+            break
+        A, B = host_problem(n, phi, seed)
+        C = np.empty((n, n), order="F")
+        np.matmul(A, B, out=C)  # warm (BLAS threads, pages)
+        t0 = time.perf_counter()
+        np.matmul(A, B, out=C)
+        secs += time.perf_counter() - t0
+        flops += 2.0 * n ** 3
+        done += 1
+    threads = blas_threads()
+    return {"value": flops / secs / 1e12, "unit": UNIT, "cores": threads or (os.cpu_count() or 1),
+            "kind": "host fp64 dgemm",
+            "sample": f"the first {done} problems of the same stream (numpy-generated), numpy.matmul FP64 "
+                      f"(OpenBLAS, {threads or 'all'} threads), {secs:.1f} s of compute"}
 
 
 def run_reference_arm(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    pos = 0
+    cs = CpuStream(a)
     for _ in range(a.warmup):
-        _, _, _, pos, _, _ = cpu_stream(a, 1.0, pos)
+        cs.step(0.5)
+    first = cs.pos
+    cs.emulated = cs.native = 0  # the description counts the timed problems only
     flops = secs = 0.0
-    total = 0
     for _ in range(a.steps):
-        f, t, d, pos, kind, threads = cpu_stream(a, 4.0, pos)
-        flops, secs, total = flops + f, secs + t, total + d
+        f, t = cs.step(4.0)
+        flops, secs = flops + f, secs + t
     value = flops / secs / 1e12
-    sample = (f"{total} problems of the same stream with n <= {CPU_MAX_N} (numpy-generated, same distribution; "
-              f"about 4 s of DGEMM per step), each at its per-problem analytic s, all host threads, "
-              f"{'src/ozaki2_gpu.hpp built for the host' if kind == 'reference' else 'C oracle'}")
+    sample = cs.describe(cs.pos - first, secs) + "; about 4 s of compute per step"
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": a.gpus,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": secs / a.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 (int8 residues)",
             "data": "synthetic", "config": workload(a),
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cs.threads, "kind": cs.kind, "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -513,19 +582,11 @@ def zgemm_leg(oz2, torch, dev, stream, rank):
 
 
 # ------------------------------------------------------------------ the adaptive-s stream
-def stream_batches(a, torch, dev, rank):
-    """distinct batches of the stream kept on the device (up to STREAM_BYTES); the timed steps
-    cycle through them"""
-    specs = stream_specs(a.seed + 7919 * rank, a.steps * a.batch)
-    batches, used = [], 0
-    for b in range(a.steps):
-        part = specs[b * a.batch:(b + 1) * a.batch]
-        need = sum(24 * n * n for n, _, _ in part)
-        if batches and used + need > STREAM_BYTES:
-            break
-        batches.append([make_problem(torch, dev, n, phi, sd) for n, phi, sd in part])
-        used += need
-    return batches, used
+def step_specs(a, rank):
+    """the stream of this rank cut into steps: a list of (n, phi, seed) lists"""
+    b = batch_size(a)
+    specs = stream_specs(a.seed + 7919 * rank, min(a.problems, b * a.steps))
+    return [specs[i:i + b] for i in range(0, len(specs), b)]
 
 
 def over_ranks(dist, torch, world, dev, ms, flops):
@@ -548,212 +609,40 @@ def problem_analytic_s(oz, batch):
     return out
 
 
-def verify(oz, torch, batch, run, refs):
-    """runs `run` over the batch and measures every output against its double-double product:
-    (problems over the bound, largest ratio, largest ulp error, correctly rounded entries)"""
-    run()
-    torch.cuda.synchronize()
-    bad, worst, ulp, cr = 0, 0.0, 0.0, 0
+def dd_refs(oz, torch, dev, batch):
+    """the double-double product hi + lo and |A||B| of every problem of the batch (untimed)"""
+    refs = []
+    for p in batch:
+        n = p["n"]
+        hi = torch.empty(n * n, dtype=torch.float64, device=dev)
+        lo, ab = torch.empty_like(hi), torch.empty_like(hi)
+        oz.dd_reference(n, n, n, p["A"], n, p["B"], n, hi, lo, ab)
+        refs.append((hi, lo, ab))
+    return refs
+
+
+def check(oz, batch, refs, acc):
+    """measures every output of the batch against its double-double product and adds to acc:
+    problems, problems over the bound, largest ratio, largest ulp error, correctly rounded entries"""
     for p, (hi, lo, ab) in zip(batch, refs):
         n = p["n"]
         r = oz.error_ratio(n, n, n, p["C"], n, hi, lo, ab, TARGET_BITS)
-        worst = max(worst, r)
-        bad += r > 1.0
         u, c = oz.accuracy(n, n, p["C"], n, hi, lo)
-        ulp, cr = max(ulp, u), cr + c
-    return bad, worst, ulp, cr
+        acc["problems"] += 1
+        acc["over_bound"] += int(r > 1.0)
+        acc["max_ratio"] = max(acc["max_ratio"], r)
+        acc["ulp_max"] = max(acc["ulp_max"], u)
+        acc["cr_entries"] += c
+        acc["entries"] += n * n
 
 
-def main():
-    a = parse()
-    if a.impl == "reference":
-        return run_reference_arm(a)
-    import torch
-    import torch.distributed as dist
-    import oz2
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
-    dev = torch.device("cuda", local)
-    stream = torch.cuda.current_stream()
-    if a.dgemm_only:
-        out = dgemm_leg(a, oz2, torch, dev, stream, rank)
-        if rank == 0:
-            print(json.dumps({"dgemm_only": out}), flush=True)
-        if world > 1:
-            dist.barrier()
-            dist.destroy_process_group()
-        return
-    oz = oz2.Ozaki2(stream)
-    model = oz.load_model()
-    ref_rule = oz2.Ozaki2.moduli_for_bits
-
-    batches, resident = stream_batches(a, torch, dev, rank)
-    nb = len(batches)
-    s_an = [problem_analytic_s(oz, b) for b in batches]
-
-    # forms of the stream, each one call (or one call per problem) over a batch
-    def adaptive(b):
-        return oz.gemm_adaptive([as_args(p) for p in batches[b]], TARGET_BITS, oz.ADAPTIVE_MLP)
-
-    def analytic_batched(b):
-        return oz.gemm_adaptive([as_args(p) for p in batches[b]], TARGET_BITS, oz.ADAPTIVE_ANALYTIC_PROBLEM)
-
-    def certified_tiles(b):
-        return oz.gemm_adaptive([as_args(p) for p in batches[b]], TARGET_BITS, oz.ADAPTIVE_CERTIFIED_TILE)
-
-    def certified_problem(b):
-        return oz.gemm_adaptive([as_args(p) for p in batches[b]], TARGET_BITS, oz.ADAPTIVE_CERTIFIED_PROBLEM)
-
-    def analytic_plain(b):
-        for p, sv in zip(batches[b], s_an[b]):
-            if sv > oz2.K_MAX_MODULI:  # no moduli set reaches the target: native FP64 (cuBLAS)
-                n = p["n"]
-                torch.mm(p["B"].view(n, n), p["A"].view(n, n), out=p["C"].view(n, n))
-            else:
-                oz.gemm(*as_args(p, sv))
-
-    def native_fp64(b):  # cuBLAS DGEMM for every problem: DGEMM-level error by construction
-        for p in batches[b]:
-            n = p["n"]
-            torch.mm(p["B"].view(n, n), p["A"].view(n, n), out=p["C"].view(n, n))
-
-    def s24_grouped(b):
-        oz.gemm_grouped([as_args(p, 24) for p in batches[b]])
-
-    def refrule_grouped(b):
-        oz.gemm_grouped([as_args(p, max(2, ref_rule(p["n"], TARGET_BITS))) for p in batches[b]])
-
-    forms = {"adaptive_mlp_batched": adaptive, "adaptive_certified_batched": certified_tiles,
-             "certified_per_problem_batched": certified_problem, "analytic_per_problem_batched": analytic_batched,
-             "analytic_per_problem_plain_calls": analytic_plain, "native_fp64_cublas": native_fp64,
-             "s24_grouped": s24_grouped,
-             "reference_rule_grouped": refrule_grouped}
-
-    # every output of every form against the double-double product (untimed; also sizes the
-    # workspaces before the timed steps)
-    checks = {f: {"problems": 0, "over_bound": 0, "max_ratio": 0.0, "ulp_max": 0.0, "cr_frac": 0.0} for f in forms}
-    entries = sum(p["n"] ** 2 for b in batches for p in b)
-    adaptive_stats = {}
-    for b in range(nb):
-        refs = []
-        for p in batches[b]:
-            n = p["n"]
-            hi = torch.empty(n * n, dtype=torch.float64, device=dev)
-            lo, ab = torch.empty_like(hi), torch.empty_like(hi)
-            oz.dd_reference(n, n, n, p["A"], n, p["B"], n, hi, lo, ab)
-            refs.append((hi, lo, ab))
-        for name, fn in forms.items():
-            holder = {}
-            bad, worst, ulp, cr = verify(oz, torch, batches[b], lambda: holder.update(st=fn(b)), refs)
-            c = checks[name]
-            c["problems"] += len(batches[b])
-            c["over_bound"] += int(bad)
-            c["max_ratio"] = max(c["max_ratio"], worst)
-            c["ulp_max"] = max(c["ulp_max"], ulp)
-            c["cr_frac"] += cr / entries
-            if name == "adaptive_mlp_batched":
-                for key, v in holder["st"].items():
-                    adaptive_stats[key] = adaptive_stats.get(key, 0) + v
-        del refs
-    torch.cuda.empty_cache()
-    oz.check_device_error()
-
-    def timed(fn, steps, warmup):
-        for i in range(warmup):
-            fn(i % nb)
-        if world > 1:
-            dist.barrier()
-        flops = 0.0
-        with Timer(torch, stream) as t:
-            for i in range(steps):
-                fn(i % nb)
-                flops += flops_of(batches[i % nb])
-        ms = t.ms
-        ms, flops = over_ranks(dist, torch, world, dev, ms, flops)
-        return flops / (ms * 1e-3) / 1e12, ms / steps
-
-    # headline: the adaptive form
-    for i in range(a.warmup):
-        adaptive(i % nb)
-    if world > 1:
-        dist.barrier()
-    launches0 = oz.kernel_launches()
-    flops = 0.0
-    # the NVTX range lets a profiler capture the timed steps alone (ncu --nvtx --nvtx-include headline/)
-    torch.cuda.nvtx.range_push("headline")
-    with ClockSampler(local) as clk:
-        with Timer(torch, stream) as t:
-            for i in range(a.steps):
-                adaptive(i % nb)
-                flops += flops_of(batches[i % nb])
-    torch.cuda.nvtx.range_pop()
-    launches = oz.kernel_launches() - launches0
-    ms = t.ms
-    ms, flops = over_ranks(dist, torch, world, dev, ms, flops)
-    value = flops / (ms * 1e-3) / 1e12
-    ms_step = ms / a.steps
-    oz.check_device_error()
-
-    # stage times and the GEMM kernel against the int8 roofline (profiling pass, untimed)
-    oz.set_profiling(True)
-    st_sum, macs = [0.0] * 6, 0
-    for i in range(a.steps):
-        st = adaptive(i % nb)
-        macs += st["int8_macs"]
-        tt, at = oz.stage_times(), oz.adaptive_stage_times()
-        for j, v in enumerate((tt.scale_ms, tt.split_ms, tt.gemm_ms, tt.crt_ms, at["probe_ms"], at["native_ms"])):
-            st_sum[j] += v
-    oz.set_profiling(False)
-    peak, note = int8_peak()
-    achieved = 2.0 * macs / (st_sum[2] * 1e-3) / 1e12
-
-    fixed = {}
-    for name, fn in forms.items():
-        if name == "adaptive_mlp_batched":
-            continue
-        tf, msf = timed(fn, a.steps, a.warmup)
-        fixed[name] = {"tflops": tf, "ms_per_step": msf, "adaptive_speedup": value / tf}
-
-    tiles = max(adaptive_stats.get("tiles", 0), 1)
-    emulated = max(tiles + adaptive_stats.get("rerun", 0) - adaptive_stats.get("native_tiles", 0), 1)
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
-            "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64 (int8 residues, int32 accumulate)", "data": "synthetic",
-            "config": dict(workload(a), problems_timed=a.steps * a.batch,
-                           distinct_problems=sum(len(b) for b in batches), resident_gb=resident / 2 ** 30,
-                           model_threshold=model.get("threshold")),
-            "clocks": clk.summary(), "gpu_launches": launches,
-            "stage_ms_per_step": {"scale_stats_mlp": st_sum[0] / a.steps, "split": st_sum[1] / a.steps,
-                                  "gemm": st_sum[2] / a.steps, "crt": st_sum[3] / a.steps,
-                                  "probe": st_sum[4] / a.steps, "native_fp64": st_sum[5] / a.steps},
-            "roofline": {"bound": "tensor", "kernel": "gemm_i8_modm_kernel", "achieved": achieved, "peak": peak,
-                         "unit": "TOPS (int8)", "frac": achieved / peak, "peak_note": note,
-                         "algorithmic": "2 s m_t n_t k int8 ops per tile (reruns included), summed over the step",
-                         "traffic": None},
-            "fixed_s": fixed,
-            "error_check": {"bound": "|C - AB| <= k 2^-53 (|A||B|)_ij against a double-double product, per entry; "
-                                     "ulp_max in units of the spacing above |AB|, cr_frac = entries equal to RN(AB)",
-                            **checks},
-            "adaptive_tiles": {"tiles": adaptive_stats.get("tiles"),
-                               "native_tiles": adaptive_stats.get("native_tiles"),
-                               "mean_s_emulated": adaptive_stats.get("sum_s", 0) / emulated,
-                               "mean_analytic_s": adaptive_stats.get("analytic_sum_s", 0) / tiles,
-                               "analytic_note": "25 counts a tile the analytic rule sends to native FP64",
-                               "probed": adaptive_stats.get("probed"), "rerun": adaptive_stats.get("rerun")}}
-
-    # end to end through the public API: every step copies its A and B from pinned host memory,
-    # makes the batched call and copies every C back. The batch lives in one pinned host arena
-    # per direction (inputs: every A, then every B; outputs: every C), so each direction is a few
-    # large copies. Two sets of device arenas let step i + 1's inputs travel (one copy stream per
-    # direction) while step i computes and step i - 1's results come back; each step still moves
-    # all of its own bytes.
-    b0 = batches[0]
+def e2e_leg(oz, torch, dev, stream, b0, steps):
+    """end to end through the public API: every step copies its A and B from pinned host memory,
+    makes the batched adaptive call and copies every C back. The batch lives in one pinned host
+    arena per direction (inputs: every A, then every B; outputs: every C), so each direction is a
+    few large copies. Two sets of device arenas let step i + 1's inputs travel (one copy stream per
+    direction) while step i computes and step i - 1's results come back; each step still moves all
+    of its own bytes."""
     sizes = [p["n"] ** 2 for p in b0]
     slots = [(sz + 31) // 32 * 32 for sz in sizes]  # every matrix 256-byte aligned, as allocations are
     tot = sum(slots)
@@ -785,7 +674,7 @@ def main():
         for j in range(0, dst.numel(), c):
             dst[j:j + c].copy_(src[j:j + c], non_blocking=True)
 
-    def e2e_run(steps):
+    def run(nsteps):
         ready, done, back = [ev(), ev()], [None, None], [None, None]
         start = ev()
         start.record(stream)
@@ -799,8 +688,8 @@ def main():
             ready[i % 2].record(h2d)
 
         upload(0)
-        for i in range(steps):
-            if i + 1 < steps:
+        for i in range(nsteps):
+            if i + 1 < nsteps:
                 upload(i + 1)
             _, d_out, probs = sets[i % 2]
             stream.wait_event(ready[i % 2])
@@ -818,28 +707,219 @@ def main():
             if b is not None:
                 stream.wait_event(b)
 
-    # the same call on the device-resident batch, for the bitwise comparison below
-    oz.gemm_adaptive([as_args(p) for p in b0], TARGET_BITS, oz.ADAPTIVE_MLP)
-    e2e_run(2)
-    e2e_steps = max(2, a.steps)  # the pipeline's fill (first upload) and drain (last download) amortised over the steps
+    oz.gemm_adaptive([as_args(p) for p in b0], TARGET_BITS, oz.ADAPTIVE_MLP)  # device-resident, to compare
+    run(2)
     with Timer(torch, stream) as t:
-        e2e_run(e2e_steps)
-    e2e_ms = t.ms / e2e_steps
+        run(steps)
     torch.cuda.synchronize()
     same = sum(int(torch.equal(p["C"].cpu().view(torch.int64), c.view(torch.int64)))
                for p, c in zip(b0, views(h_out, 0)))
-    e2e_flops = flops_of(b0)
-    e2e_ms, e2e_flops = over_ranks(dist, torch, world, dev, e2e_ms, e2e_flops)
-    line["e2e"] = {"value": e2e_flops / (e2e_ms * 1e-3) / 1e12, "unit": UNIT,
-                   "h2d_bytes_per_step": 16 * tot, "d2h_bytes_per_step": 8 * tot, "ms_per_step": e2e_ms,
-                   "steps": e2e_steps, "outputs_equal_device_call": f"{same} of {len(b0)}",
-                   "note": "the first batch of the stream every step, from one pinned host arena per direction "
-                           "(8 copies each); step i + 1's inputs copy in while step i computes and step i - 1's "
-                           "results copy out (two device arena sets, one copy stream per direction)"}
+    out = {"ms_per_step": t.ms / steps, "flops_per_step": flops_of(b0), "h2d": 16 * tot, "d2h": 8 * tot,
+           "same": f"{same} of {len(b0)}"}
     del h_in, h_out, sets
+    return out
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        return run_reference_arm(a)
+    import torch
+    import torch.distributed as dist
+    import oz2
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    if a.dgemm_only:
+        out = dgemm_leg(a, oz2, torch, dev, stream, rank)
+        if rank == 0:
+            print(json.dumps({"dgemm_only": out}), flush=True)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    oz = oz2.Ozaki2(stream)
+    oz.set_workspace_limit(WORKSPACE)
+    model = oz.load_model()
+    ref_rule = oz2.Ozaki2.moduli_for_bits
+    steps = step_specs(a, rank)
+    ctx = {}  # per-batch data the forms read (per-problem analytic s)
+
+    def args_of(batch):
+        return [as_args(p) for p in batch]
+
+    # forms of the stream, each one call (or one call per problem) over a batch
+    def adaptive(b):
+        return oz.gemm_adaptive(args_of(b), TARGET_BITS, oz.ADAPTIVE_MLP)
+
+    def certified_tiles(b):
+        return oz.gemm_adaptive(args_of(b), TARGET_BITS, oz.ADAPTIVE_CERTIFIED_TILE)
+
+    def certified_problem(b):
+        return oz.gemm_adaptive(args_of(b), TARGET_BITS, oz.ADAPTIVE_CERTIFIED_PROBLEM)
+
+    def analytic_batched(b):
+        return oz.gemm_adaptive(args_of(b), TARGET_BITS, oz.ADAPTIVE_ANALYTIC_PROBLEM)
+
+    def analytic_plain(b):
+        for p, sv in zip(b, ctx["s_an"]):
+            if sv > oz2.K_MAX_MODULI:  # no moduli set reaches the target: native FP64 (cuBLAS)
+                n = p["n"]
+                torch.mm(p["B"].view(n, n), p["A"].view(n, n), out=p["C"].view(n, n))
+            else:
+                oz.gemm(*as_args(p, sv))
+
+    def native_fp64(b):  # cuBLAS DGEMM for every problem: DGEMM-level error by construction
+        for p in b:
+            n = p["n"]
+            torch.mm(p["B"].view(n, n), p["A"].view(n, n), out=p["C"].view(n, n))
+
+    def s24_grouped(b):
+        oz.gemm_grouped([as_args(p, 24) for p in b])
+
+    def refrule_grouped(b):
+        oz.gemm_grouped([as_args(p, max(2, ref_rule(p["n"], TARGET_BITS))) for p in b])
+
+    HEAD = "adaptive_mlp_batched"
+    forms = {HEAD: adaptive, "adaptive_certified_batched": certified_tiles,
+             "certified_per_problem_batched": certified_problem, "analytic_per_problem_batched": analytic_batched,
+             "analytic_per_problem_plain_calls": analytic_plain, "native_fp64_cublas": native_fp64,
+             "s24_grouped": s24_grouped, "reference_rule_grouped": refrule_grouped}
+    if a.forms == "headline":
+        forms = {HEAD: adaptive}
+    checks = {f: {"problems": 0, "over_bound": 0, "max_ratio": 0.0, "ulp_max": 0.0, "cr_entries": 0, "entries": 0}
+              for f in forms}
+    ms_sum = {f: 0.0 for f in forms}
+    flops_sum = 0.0
+    adaptive_stats, st_sum, macs, launches = {}, [0.0] * 6, 0, 0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed_step(fn, batch):
+        """one step bracketed by a barrier and a device synchronisation on both sides, timed with
+        CUDA events on the launching stream; the slowest rank's time"""
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        ret = fn(batch)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if world > 1:
+            x = torch.tensor([ms], dtype=torch.float64, device=dev)
+            dist.all_reduce(x, op=dist.ReduceOp.MAX)
+            ms = float(x[0])
+        return ms, ret
+
+    # warm-up: every form on the first batch (also sizes the workspaces)
+    batch = [make_problem(torch, dev, n, phi, sd) for n, phi, sd in steps[0]]
+    ctx["s_an"] = problem_analytic_s(oz, batch)
+    for _ in range(a.warmup):
+        for fn in forms.values():
+            fn(batch)
+    torch.cuda.synchronize()
+    oz.check_device_error()
+
+    # timed steps: each batch generated (untimed), then every form timed on it and checked
+    torch.cuda.nvtx.range_push("stream")
+    with ClockSampler(local) as clk:
+        for i, part in enumerate(steps):
+            if i > 0:
+                del batch
+                torch.cuda.empty_cache()
+                batch = [make_problem(torch, dev, n, phi, sd) for n, phi, sd in part]
+                ctx["s_an"] = problem_analytic_s(oz, batch)
+            refs = dd_refs(oz, torch, dev, batch)
+            flops_sum += flops_of(batch)
+            for name, fn in forms.items():
+                l0 = oz.kernel_launches() if name == HEAD else 0
+                if name == HEAD:
+                    torch.cuda.nvtx.range_push("headline")
+                ms, ret = timed_step(fn, batch)
+                if name == HEAD:
+                    torch.cuda.nvtx.range_pop()
+                    launches += oz.kernel_launches() - l0
+                    for key, v in ret.items():
+                        adaptive_stats[key] = adaptive_stats.get(key, 0) + v
+                ms_sum[name] += ms
+                check(oz, batch, refs, checks[name])
+            # stage times and the GEMM against the int8 roofline: a profiling pass of the headline
+            # form on the same batch (untimed)
+            oz.set_profiling(True)
+            st = adaptive(batch)
+            macs += st["int8_macs"]
+            tt, at = oz.stage_times(), oz.adaptive_stage_times()
+            for j, v in enumerate((tt.scale_ms, tt.split_ms, tt.gemm_ms, tt.crt_ms, at["probe_ms"], at["native_ms"])):
+                st_sum[j] += v
+            oz.set_profiling(False)
+            del refs
+            if rank == 0:
+                print(f"step {i + 1}/{len(steps)}: {len(batch)} problems, headline {ms_sum[HEAD]:.1f} ms so far, "
+                      f"device memory peak {torch.cuda.max_memory_allocated() / 2 ** 30:.1f} GiB", file=sys.stderr,
+                      flush=True)
+    torch.cuda.nvtx.range_pop()
+    oz.check_device_error()
+    nsteps = len(steps)
+    _, flops_all = over_ranks(dist, torch, world, dev, 0.0, flops_sum)
+    value = flops_all / (ms_sum[HEAD] * 1e-3) / 1e12
+    peak, note = int8_peak()
+    achieved = 2.0 * macs / (st_sum[2] * 1e-3) / 1e12
+
+    def summary_of(c):
+        return {"problems": c["problems"], "over_bound": c["over_bound"], "max_ratio": c["max_ratio"],
+                "ulp_max": c["ulp_max"], "cr_frac": c["cr_entries"] / max(c["entries"], 1)}
+
+    fixed = {name: {"tflops": flops_all / (ms_sum[name] * 1e-3) / 1e12, "ms_per_step": ms_sum[name] / nsteps,
+                    "adaptive_speedup": ms_sum[name] / ms_sum[HEAD]} for name in forms if name != HEAD}
+    tiles = max(adaptive_stats.get("tiles", 0), 1)
+    emulated = max(tiles + adaptive_stats.get("rerun", 0) - adaptive_stats.get("native_tiles", 0), 1)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": nsteps, "warmup": a.warmup,
+            "ms_per_step": ms_sum[HEAD] / nsteps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 (int8 residues, int32 accumulate)", "data": "synthetic",
+            "config": dict(workload(a), model_threshold=model.get("threshold"), workspace_limit_gib=WORKSPACE >> 30),
+            "clocks": clk.summary(), "gpu_launches": launches,
+            "stage_ms_per_step": {"scale_stats_mlp": st_sum[0] / nsteps, "split": st_sum[1] / nsteps,
+                                  "gemm": st_sum[2] / nsteps, "crt": st_sum[3] / nsteps,
+                                  "probe": st_sum[4] / nsteps, "native_fp64": st_sum[5] / nsteps},
+            "roofline": {"bound": "tensor", "kernel": "gemm_i8_modm_kernel", "achieved": achieved, "peak": peak,
+                         "unit": "TOPS (int8)", "frac": achieved / peak, "peak_note": note,
+                         "algorithmic": "2 s m_t n_t k int8 ops per tile (reruns included), summed over the steps",
+                         "traffic": None},
+            "fixed_s": fixed,
+            "error_check": {"bound": "|C - AB| <= k 2^-53 (|A||B|)_ij against a double-double product, per entry; "
+                                     "ulp_max in units of the spacing above |AB|, cr_frac = entries equal to RN(AB)",
+                            **{f: summary_of(c) for f, c in checks.items()}},
+            "adaptive_tiles": {"tiles": adaptive_stats.get("tiles"),
+                               "native_tiles": adaptive_stats.get("native_tiles"),
+                               "mean_s_emulated": adaptive_stats.get("sum_s", 0) / emulated,
+                               "mean_analytic_s": adaptive_stats.get("analytic_sum_s", 0) / tiles,
+                               "analytic_note": "25 counts a tile the analytic rule sends to native FP64",
+                               "probed": adaptive_stats.get("probed"), "rerun": adaptive_stats.get("rerun")}}
+    del batch
+    torch.cuda.empty_cache()
+
+    # end to end with host buffers, on the first E2E_BATCH problems of the stream
+    b0 = [make_problem(torch, dev, n, phi, sd) for n, phi, sd in steps[0][:E2E_BATCH]]
+    e2e_steps = max(2, a.steps)  # the pipeline's fill and drain amortised over the steps
+    e = e2e_leg(oz, torch, dev, stream, b0, e2e_steps)
+    e2e_ms, e2e_flops = over_ranks(dist, torch, world, dev, e["ms_per_step"], e["flops_per_step"])
+    line["e2e"] = {"value": e2e_flops / (e2e_ms * 1e-3) / 1e12, "unit": UNIT,
+                   "h2d_bytes_per_step": e["h2d"], "d2h_bytes_per_step": e["d2h"], "ms_per_step": e2e_ms,
+                   "steps": e2e_steps, "outputs_equal_device_call": e["same"],
+                   "note": f"the first {len(b0)} problems of the stream every step (one adaptive call), from one "
+                           "pinned host arena per direction (8 copies each); step i + 1's inputs copy in while step "
+                           "i computes and step i - 1's results copy out (two device arena sets, one copy stream "
+                           "per direction)"}
+    del b0
     oz.check_device_error()
     oz.close()
-    del batches
     torch.cuda.empty_cache()
 
     extras = {}
@@ -849,9 +929,18 @@ def main():
         extras["grouped_c4"] = grouped_leg(oz2, torch, dev, stream)
         if world > 1:
             extras["dgemm_8192_sharded"] = sharded_leg(a, oz2, torch, dev, stream, dist, world, rank)
-        if world == 1:  # the host-core baseline is quoted at one GPU only
+        if world == 1:  # the host-core baselines are quoted at one GPU only
             line["cpu_baseline"] = cpu_sample(a)
+            line["cpu_baseline_dgemm"] = cpu_dgemm_sample(a)
     line["extras"] = extras
+    # last, where a truncated log keeps it: the headline's accuracy and its speed-up over each form
+    hc = checks[HEAD]
+    line["summary"] = {"problems_timed": hc["problems"], "over_bound": hc["over_bound"],
+                       "max_ratio": hc["max_ratio"], "ulp_max": hc["ulp_max"],
+                       "cr_frac": hc["cr_entries"] / max(hc["entries"], 1),
+                       "speedup_over": {f: round(v["adaptive_speedup"], 3) for f, v in fixed.items()},
+                       "forms_over_bound": {f: c["over_bound"] for f, c in checks.items()},
+                       "roofline_frac": round(achieved / peak, 3), "e2e": line["e2e"]["value"]}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

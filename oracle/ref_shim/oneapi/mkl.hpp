@@ -23,9 +23,9 @@ enum class compute_mode { unset, standard };
 namespace column_major {
 namespace detail {
 // Dot products of two rows of op(A) with two columns of op(B), all k-contiguous int8:
-// out = {a0.b0, a1.b0, a0.b1, a1.b1}. AVX2 where the CPU has it (sign-extension to int16 and
-// pairwise multiply-add into int32 lanes: exact, |sum| < 2^31 as in the reference's own bound),
-// plain loops otherwise.
+// out = {a0.b0, a1.b0, a0.b1, a1.b1}. AVX-512 VNNI or AVX2 where the CPU has them (sign-extension
+// to int16 and pairwise multiply-add into int32 lanes: exact, |sum| < 2^31 as in the reference's
+// own bound), plain loops otherwise.
 #if defined(__x86_64__)
 __attribute__((target("avx2"))) static inline void dot2x2_avx2(const int8_t* a0, const int8_t* a1,
                                                                const int8_t* b0, const int8_t* b1, int64_t k,
@@ -55,6 +55,31 @@ __attribute__((target("avx2"))) static inline void dot2x2_avx2(const int8_t* a0,
         out[3] += a1[p] * b1[p];
     }
 }
+__attribute__((target("avx512f,avx512bw,avx512vnni"))) static inline void dot2x2_vnni(
+    const int8_t* a0, const int8_t* a1, const int8_t* b0, const int8_t* b1, int64_t k, int32_t* out) {
+    __m512i s00 = _mm512_setzero_si512(), s10 = s00, s01 = s00, s11 = s00;
+    int64_t p = 0;
+    for (; p + 32 <= k; p += 32) {
+        const __m512i x0 = _mm512_cvtepi8_epi16(_mm256_loadu_si256(reinterpret_cast<const __m256i*>(a0 + p)));
+        const __m512i x1 = _mm512_cvtepi8_epi16(_mm256_loadu_si256(reinterpret_cast<const __m256i*>(a1 + p)));
+        const __m512i y0 = _mm512_cvtepi8_epi16(_mm256_loadu_si256(reinterpret_cast<const __m256i*>(b0 + p)));
+        const __m512i y1 = _mm512_cvtepi8_epi16(_mm256_loadu_si256(reinterpret_cast<const __m256i*>(b1 + p)));
+        s00 = _mm512_dpwssd_epi32(s00, x0, y0);
+        s10 = _mm512_dpwssd_epi32(s10, x1, y0);
+        s01 = _mm512_dpwssd_epi32(s01, x0, y1);
+        s11 = _mm512_dpwssd_epi32(s11, x1, y1);
+    }
+    out[0] = _mm512_reduce_add_epi32(s00);
+    out[1] = _mm512_reduce_add_epi32(s10);
+    out[2] = _mm512_reduce_add_epi32(s01);
+    out[3] = _mm512_reduce_add_epi32(s11);
+    for (; p < k; ++p) {
+        out[0] += a0[p] * b0[p];
+        out[1] += a1[p] * b0[p];
+        out[2] += a0[p] * b1[p];
+        out[3] += a1[p] * b1[p];
+    }
+}
 #endif
 static inline void dot2x2_plain(const int8_t* a0, const int8_t* a1, const int8_t* b0, const int8_t* b1, int64_t k,
                                 int32_t* out) {
@@ -67,12 +92,15 @@ static inline void dot2x2_plain(const int8_t* a0, const int8_t* a1, const int8_t
     }
     out[0] = s00, out[1] = s10, out[2] = s01, out[3] = s11;
 }
-static inline bool have_avx2() {
+// 2: AVX-512 VNNI, 1: AVX2, 0: plain loops (chosen once, from the CPU the process runs on)
+static inline int simd_level() {
 #if defined(__x86_64__)
-    static const bool ok = __builtin_cpu_supports("avx2");
-    return ok;
+    static const int lv = __builtin_cpu_supports("avx512vnni") && __builtin_cpu_supports("avx512bw")
+                              ? 2
+                              : (__builtin_cpu_supports("avx2") ? 1 : 0);
+    return lv;
 #else
-    return false;
+    return 0;
 #endif
 }
 
@@ -94,7 +122,7 @@ inline void i8_gemm(transpose ta, transpose tb, int64_t m, int64_t n, int64_t k,
             bt[static_cast<size_t>(j) * k + p] = tb == transpose::nontrans ? b[p + j * ldb] : b[j + p * ldb];
     constexpr int64_t kBlk = 64;
     const int64_t bi = (m2 + kBlk - 1) / kBlk, bj = (n2 + kBlk - 1) / kBlk;
-    const bool avx2 = have_avx2();
+    const int simd = simd_level();
 #pragma omp parallel for schedule(dynamic)
     for (int64_t blk = 0; blk < bi * bj; ++blk) {
         const int64_t i0 = (blk % bi) * kBlk, j0 = (blk / bi) * kBlk;
@@ -105,7 +133,8 @@ inline void i8_gemm(transpose ta, transpose tb, int64_t m, int64_t n, int64_t k,
                 const int8_t* b0 = &bt[static_cast<size_t>(j) * k];
                 int32_t o[4] = {0, 0, 0, 0};
 #if defined(__x86_64__)
-                if (avx2) dot2x2_avx2(a0, a0 + k, b0, b0 + k, k, o);
+                if (simd == 2) dot2x2_vnni(a0, a0 + k, b0, b0 + k, k, o);
+                else if (simd == 1) dot2x2_avx2(a0, a0 + k, b0, b0 + k, k, o);
                 else dot2x2_plain(a0, a0 + k, b0, b0 + k, k, o);
 #else
                 dot2x2_plain(a0, a0 + k, b0, b0 + k, k, o);

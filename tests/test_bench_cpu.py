@@ -34,3 +34,37 @@ def test_reference_arm_prints_the_contract_line():
 
 def test_reference_arm_other_ranks_print_nothing():
     assert run_arm({"RANK": "1", "WORLD_SIZE": "2"}) == []
+
+
+def _stream(monkeypatch, s_value, status=0):
+    import importlib
+    import types
+    sys.path.insert(0, ROOT)
+    bench = importlib.import_module("bench")
+    a = types.SimpleNamespace(seed=2025, problems=3, steps=1, batch=0)
+    cs = bench.CpuStream(a)
+    cs.specs = [(64, 1.0, 11), (96, 2.0, 12), (80, 0.5, 13)]  # small problems of the stream's kind
+    monkeypatch.setattr(cs.ao, "problem_analytic_s", lambda *args, **kw: s_value)
+    if status:
+        monkeypatch.setattr(cs.lib, "dgemm", lambda *args, **kw: (status, None))
+    return cs
+
+
+def test_cpu_stream_runs_problems_beyond_24_moduli_as_host_dgemm(monkeypatch):
+    cs = _stream(monkeypatch, 25)
+    flops, secs = cs.step(60.0)
+    assert cs.native == 3 and cs.emulated == 0
+    assert flops == 2.0 * (64 ** 3 + 96 ** 3 + 80 ** 3) and secs > 0
+
+
+def test_cpu_stream_runs_the_reference_at_the_analytic_s(monkeypatch):
+    cs = _stream(monkeypatch, 20)
+    flops, secs = cs.step(60.0)
+    assert cs.emulated == 3 and cs.native == 0 and secs > 0
+
+
+def test_cpu_stream_fails_loudly_on_a_failed_call(monkeypatch):
+    import pytest
+    cs = _stream(monkeypatch, 20, status=1)
+    with pytest.raises(RuntimeError):
+        cs.step(60.0)
