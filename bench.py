@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--batch", type=int, default=0,
                     help="problems per step (default: problems / steps, at most %d)" % MAX_BATCH)
     ap.add_argument("--forms", default="all", help="'all' or 'headline': the fixed-s forms beside the headline")
+    ap.add_argument("--probe-study", action="store_true",
+                    help="instead of the bench line: problems over the bound per MLP threshold and probe kind")
     ap.add_argument("--seed", type=int, default=2025)
     ap.add_argument("--size", type=int, default=8192, help="m = n = k of the DGEMM extra")
     ap.add_argument("--s", type=int, default=16, help="moduli of the DGEMM extra")
@@ -720,6 +722,47 @@ def e2e_leg(oz, torch, dev, stream, b0, steps):
     return out
 
 
+def probe_study(a, oz, torch, dev):
+    """What the probes catch: the MLP mode at lowered decision thresholds (more tiles below their
+    judge's s) over the first batches of the stream, with no probe, the column probe, the Freivalds
+    probe and both; per setting the problems over the bound after the reruns, the probed and rerun
+    tiles, and the step time. Prints one JSON line."""
+    model = oz.load_model()
+    steps = step_specs(a, 0)
+    rows = []
+    for part in steps:
+        batch = [make_problem(torch, dev, n, phi, sd) for n, phi, sd in part]
+        refs = dd_refs(oz, torch, dev, batch)
+        for thr in (0.999, 0.99, 0.95, 0.9):
+            for kind, name in ((3, "none"), (0, "columns"), (1, "freivalds"), (2, "both")):
+                oz.set_adaptive_options(512, thr)
+                oz.set_probe_kind(kind)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                st = oz.gemm_adaptive([as_args(p) for p in batch], TARGET_BITS, oz.ADAPTIVE_MLP)
+                torch.cuda.synchronize()
+                ms = (time.perf_counter() - t0) * 1e3
+                acc = {"problems": 0, "over_bound": 0, "max_ratio": 0.0, "ulp_max": 0.0, "cr_entries": 0,
+                       "entries": 0}
+                check(oz, batch, refs, acc)
+                rows.append({"threshold": thr, "probe": name, "problems": acc["problems"],
+                             "over_bound": acc["over_bound"], "max_ratio": acc["max_ratio"],
+                             "probed": st["probed"], "rerun": st["rerun"], "ms": ms})
+        del batch, refs
+        torch.cuda.empty_cache()
+    oz.set_probe_kind(0)
+    oz.set_adaptive_options(512, model.get("threshold", 0.999))
+    merged = {}
+    for r in rows:
+        key = (r["threshold"], r["probe"])
+        m = merged.setdefault(key, {"threshold": r["threshold"], "probe": r["probe"], "problems": 0,
+                                    "over_bound": 0, "max_ratio": 0.0, "probed": 0, "rerun": 0, "ms": 0.0})
+        for f in ("problems", "over_bound", "probed", "rerun", "ms"):
+            m[f] += r[f]
+        m["max_ratio"] = max(m["max_ratio"], r["max_ratio"])
+    print(json.dumps({"probe_study": list(merged.values()), "config": workload(a)}), flush=True)
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -747,6 +790,10 @@ def main():
         return
     oz = oz2.Ozaki2(stream)
     oz.set_workspace_limit(WORKSPACE)
+    if a.probe_study:
+        probe_study(a, oz, torch, dev)
+        oz.close()
+        return
     model = oz.load_model()
     ref_rule = oz2.Ozaki2.moduli_for_bits
     steps = step_specs(a, rank)
@@ -828,7 +875,8 @@ def main():
     oz.check_device_error()
 
     # timed steps: each batch generated (untimed), then every form timed on it and checked
-    torch.cuda.nvtx.range_push("stream")
+    by_form = {}
+    gbytes = [0, 0, 0]
     with ClockSampler(local) as clk:
         for i, part in enumerate(steps):
             if i > 0:
@@ -859,12 +907,23 @@ def main():
             for j, v in enumerate((tt.scale_ms, tt.split_ms, tt.gemm_ms, tt.crt_ms, at["probe_ms"], at["native_ms"])):
                 st_sum[j] += v
             oz.set_profiling(False)
+            gb = oz.adaptive_gemm_bytes()
+            gbytes = [gbytes[0] + gb["plane_bytes"], gbytes[1] + gb["residue_bytes"], gbytes[2] + gb["batches"]]
+            if i == 0:  # the stage times of every adaptive-call form on the first batch (untimed)
+                for name, fn in forms.items():
+                    if fn not in (adaptive, certified_tiles, certified_problem, analytic_batched):
+                        continue
+                    oz.set_profiling(True)
+                    fn(batch)
+                    tt, at = oz.stage_times(), oz.adaptive_stage_times()
+                    oz.set_profiling(False)
+                    by_form[name] = {"scale_stats": tt.scale_ms, "split": tt.split_ms, "gemm": tt.gemm_ms,
+                                     "crt": tt.crt_ms, "probe": at["probe_ms"], "native_fp64": at["native_ms"]}
             del refs
             if rank == 0:
                 print(f"step {i + 1}/{len(steps)}: {len(batch)} problems, headline {ms_sum[HEAD]:.1f} ms so far, "
                       f"device memory peak {torch.cuda.max_memory_allocated() / 2 ** 30:.1f} GiB", file=sys.stderr,
                       flush=True)
-    torch.cuda.nvtx.range_pop()
     oz.check_device_error()
     nsteps = len(steps)
     _, flops_all = over_ranks(dist, torch, world, dev, 0.0, flops_sum)
@@ -891,7 +950,9 @@ def main():
             "roofline": {"bound": "tensor", "kernel": "gemm_i8_modm_kernel", "achieved": achieved, "peak": peak,
                          "unit": "TOPS (int8)", "frac": achieved / peak, "peak_note": note,
                          "algorithmic": "2 s m_t n_t k int8 ops per tile (reruns included), summed over the steps",
-                         "traffic": None},
+                         "algorithmic_bytes_per_launch": (gbytes[0] + gbytes[1]) / max(gbytes[2], 1),
+                         "launches": gbytes[2], "traffic": None},
+            "stage_ms_first_batch_by_form": by_form,
             "fixed_s": fixed,
             "error_check": {"bound": "|C - AB| <= k 2^-53 (|A||B|)_ij against a double-double product, per entry; "
                                      "ulp_max in units of the spacing above |AB|, cr_frac = entries equal to RN(AB)",
@@ -900,7 +961,7 @@ def main():
                                "native_tiles": adaptive_stats.get("native_tiles"),
                                "mean_s_emulated": adaptive_stats.get("sum_s", 0) / emulated,
                                "mean_analytic_s": adaptive_stats.get("analytic_sum_s", 0) / tiles,
-                               "analytic_note": "25 counts a tile the analytic rule sends to native FP64",
+                               "analytic_note": "33 counts a tile the analytic rule sends to native FP64",
                                "probed": adaptive_stats.get("probed"), "rerun": adaptive_stats.get("rerun")}}
     del batch
     torch.cuda.empty_cache()

@@ -101,7 +101,7 @@ int oz2_autotune_grouped(oz2_handle h, int count, const oz2_dgemm_problem* probl
  *   mode 1: the analytic s of the tile: smallest s whose tk >= R + 2 + t - floor(log2(k - 1)),
  *           R the largest exponent gap below the row / column maximum in the tile's panels
  *   mode 2: the analytic s of the whole problem (the largest over its tiles)
- *   mode 3: each problem's own num_moduli (tiled like the other modes)
+ *   mode 3: each problem's own num_moduli, 2..32 (tiled like the other modes)
  *   mode 4: the judge's s of the tile (no MLP, no probe: every tile meets the target)
  *   mode 5: the judge's s of the whole problem (the largest over its tiles)
  * The judge of a tile is the smaller of its analytic s and, for problems with a tile whose analytic
@@ -110,10 +110,15 @@ int oz2_autotune_grouped(oz2_handle h, int count, const oz2_dgemm_problem* probl
  * |A||B| from a tcgen05 GEMM) meets the target in every entry of the tile. In modes 0 and 4 a
  * problem runs as one task at the largest s of its tiles (or in native FP64) when that costs no
  * more than its tiles as chosen, counting a tile task 12 % dearer and native FP64 as 63 moduli.
- * In modes 0-2, 4 and 5 a tile that no s <= 24 brings to the target (judge or MLP class 25) runs as
- * a native FP64 GEMM (cuBLAS DGEMM), the whole problem in one call when all its tiles do.
+ * Above s = 24 the adaptive path uses moduli sets of its own (s = 25..32: pairwise-coprime
+ * integers <= 256 taken greedily from the top; up to 124 bits per element), so a tile whose
+ * judge needs more than the 91 bits of 24 moduli still runs emulated; the MLP's last class means
+ * "more than 24" and answers 25. In modes 0-2, 4 and 5 a tile that no s <= 32 brings to the
+ * target runs as a native FP64 GEMM (cuBLAS DGEMM), the whole problem in one call when all its
+ * tiles do; the analytic rule sends a tile there when a gap reaches 63 binades (its histogram's
+ * last bin).
  * stats (may be NULL, 10 entries): tiles, sum of s over emulated tiles (reruns included), probed
- * tiles, rerun tiles, sum of s of the reruns (25 for native), sum of the judge's s (25 for native),
+ * tiles, rerun tiles, sum of s of the reruns (33 for native), sum of the judge's s (33 for native),
  * MLP used, int8 multiply-adds of the emulated tiles (s m_t n_t k summed, reruns included),
  * native tiles, native FP64 multiply-adds. The host waits in the middle of the call for the tile
  * statistics (and in mode 0 for the probe). Those reads, and the uploads of item tables, are copy
@@ -126,10 +131,22 @@ int oz2_dgemm_adaptive(oz2_handle h, int count, const oz2_dgemm_problem* problem
 /* tile edge (multiple of 128) and the MLP decision threshold: s is the smallest class whose
  * cumulative predicted probability reaches it */
 int oz2_set_adaptive_options(oz2_handle h, int tile, float threshold);
+/* the probe of mode 0 (no counterpart in the reference): 0 (default) checks kProbeCols = 8
+ * stratified random columns of each probed tile entry by entry against A B summed in FP64; 1 is the
+ * Freivalds test, C x against alpha A (B x) in double-double for two random vectors x with
+ * x_j = +-2^-f_j (f_j the exponent of op(B)'s column maximum), row by row against alpha k 2^-t
+ * (|A| (|B| |x|))_i; 2 runs both (a tile fails when either fails); 3 runs none, so the MLP's s
+ * stands unchecked (for measuring what the probes catch). A tile that meets the target passes
+ * every kind; a failing tile is rerun at its judge's s. */
+int oz2_set_probe_kind(oz2_handle h, int kind);
 /* with profiling on: device time of the last oz2_dgemm_adaptive's probe and of its native FP64
  * tiles (out2 = {probe_ms, native_ms}) */
 int oz2_adaptive_stage_times(oz2_handle h, double* out2);
-/* out4 = {parameters, features, classes (s = 2..24, 25 = native FP64), hidden width} of the MLP */
+/* algorithmic bytes of the last oz2_dgemm_adaptive's INT8 GEMMs (no counterpart in the reference):
+ * out3 = {plane bytes read (each split panel once), residue bytes written, tile batches (one GEMM
+ * launch each)}; the yardstick for the GEMM's measured DRAM traffic */
+int oz2_adaptive_gemm_bytes(oz2_handle h, int64_t* out3);
+/* out4 = {parameters, features, classes (s = 2..24 and one for more than 24), hidden width} of the MLP */
 int oz2_mlp_info(int* out4);
 /* loads the MLP parameters (host floats); NULL unloads */
 int oz2_mlp_set_weights(oz2_handle h, const float* params, int nparams);

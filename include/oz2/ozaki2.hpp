@@ -6,6 +6,7 @@
 
 #include <cuda_runtime_api.h>
 
+#include <array>
 #include <complex>
 #include <cstddef>
 #include <cstdint>
@@ -61,6 +62,8 @@ struct GemmConfig {
 
 // how gemm_adaptive picks s per tile (oz2_dgemm_adaptive modes)
 enum class Adaptive { Mlp = 0, AnalyticTile = 1, AnalyticProblem = 2, Fixed = 3, CertifiedTile = 4, CertifiedProblem = 5 };
+// the probe of Adaptive::Mlp (oz2_set_probe_kind)
+enum class Probe { Columns = 0, Freivalds = 1, Both = 2, None = 3 };
 
 struct AdaptiveStats {
     int64_t tiles = 0, sum_s = 0, probed = 0, rerun = 0, rerun_sum_s = 0, analytic_sum_s = 0, mlp = 0,
@@ -199,6 +202,13 @@ public:
     }
     void set_adaptive_options(int tile, float threshold) {
         detail::check(oz2_set_adaptive_options(h_, tile, threshold), h_);
+    }
+    void set_probe_kind(Probe kind) { detail::check(oz2_set_probe_kind(h_, static_cast<int>(kind)), h_); }
+    // {plane bytes read, residue bytes written, GEMM launches} of the last gemm_adaptive
+    std::array<int64_t, 3> adaptive_gemm_bytes() const {
+        std::array<int64_t, 3> v{};
+        detail::check(oz2_adaptive_gemm_bytes(h_, v.data()), h_);
+        return v;
     }
 
     // synchronises the stream; throws std::runtime_error if a kernel's bounded wait ran out

@@ -10,13 +10,17 @@ Definitions (no counterpart in the reference, whose number of moduli is fixed pe
   counted apart.
   analytic s = the smallest s in 2..24 whose bits per element tk (the plan of the reference's
   Ozaki2::gemm for this k) reach R + 2 + t - floor(log2(k - 1)), R the largest gap of the tile's
-  two panels, t the target bits; 25 (the tile runs as a native FP64 GEMM) when none does.
+  two panels, t the target bits, over s = 2..32 (the library's extended sets above 24); 33 (the
+  tile runs as a native FP64 GEMM) when none does or when R reaches the last gap bin (63: every
+  gap of 63 binades or more, which bounds nothing).
 """
 import math
 
 import numpy as np
 
 TILE = 512
+MAX_S = 32   # the library's extended moduli sets reach s = 32 in the adaptive path
+NATIVE = 33  # the s of a tile run as a native FP64 GEMM
 QUANTILES = (0.5, 0.75, 0.9, 0.99)
 
 
@@ -58,10 +62,10 @@ def floor_log2_km1(k):
 
 
 def tk_table(oracle, k):
-    tk = [0] * 25
-    for s in range(2, 25):
+    tk = [0] * (MAX_S + 1)
+    for s in range(2, MAX_S + 1):
         try:
-            tk[s] = oracle.plan(s, k).tk
+            tk[s] = oracle.plan_ext(s, k).tk
         except ValueError:
             tk[s] = 0
     return tk
@@ -69,7 +73,9 @@ def tk_table(oracle, k):
 
 def analytic_s(tk, R, k, target_bits=53):
     need = R + 2 + target_bits - floor_log2_km1(k)
-    return next((s for s in range(2, 25) if tk[s] >= need), 25)
+    if R >= 63:
+        return NATIVE
+    return next((s for s in range(2, MAX_S + 1) if tk[s] >= need), NATIVE)
 
 
 def tile_features(oracle, problems, target_bits=53, tile=TILE):
@@ -111,13 +117,13 @@ def problem_analytic_s(oracle, ta, tb, m, n, k, A, B, target_bits=53, tile=TILE)
 def certified_s(oracle, opA, opB, target_bits=53):
     """certified s of one tile: op(A) (m x k) and op(B) (k x n) as numpy arrays, restating the
     entrywise a-priori bound of the library's certificate with the FP64 product |op(A)||op(B)| in
-    place of its bf16 lower bound (so the library's s is this one or above). 25 when no s
+    place of its bf16 lower bound (so the library's s is this one or above). 33 when no s <= 32
     reaches it, the two roundings use up the target or an input is non-finite."""
     k = opA.shape[1]
     t = float(target_bits)
     Bu = k - 2.0 ** (t - 52.0)
     if Bu <= 0 or not (np.all(np.isfinite(opA)) and np.all(np.isfinite(opB))):
-        return 25
+        return NATIVE
     ma, mb = np.abs(opA).max(axis=1), np.abs(opB).max(axis=0)
     e = np.where(ma > 0, np.frexp(ma)[1], 0)
     f = np.where(mb > 0, np.frexp(mb)[1], 0)
@@ -128,7 +134,7 @@ def certified_s(oracle, opA, opB, target_bits=53):
     if not np.any(live):
         return 2
     if np.any(G[live] == 0):
-        return 25
+        return NATIVE
     q1 = ((Ra[:, None] + Sb[None, :]) / np.where(live, G, 1.0))[live].max()
     q2 = (1.0 / np.where(live, G, 1.0))[live].max()
     c = 1.0 - 2.0 ** -6
@@ -136,4 +142,4 @@ def certified_s(oracle, opA, opB, target_bits=53):
     l2 = 0.5 * (math.log2(q2 * (1 + 2.0 ** -20)) + t + 10.0 - math.log2(Bu / k * c))
     need = math.ceil(max(l1, l2) + 1e-9)
     tk = tk_table(oracle, k)
-    return next((s for s in range(2, 25) if tk[s] > 0 and tk[s] >= need), 25)
+    return next((s for s in range(2, MAX_S + 1) if tk[s] > 0 and tk[s] >= need), NATIVE)

@@ -28,9 +28,13 @@ static const uint16_t kSeqMid[13] = {256, 253, 251, 249, 247, 245, 241, 239, 233
 static const uint16_t kSeqLarge[24] = {256, 253, 251, 249, 247, 241, 239, 235, 233, 229, 227, 223,
                                        217, 211, 199, 197, 193, 191, 181, 179, 173, 167, 163, 157}; /* 14..24 */
 
+/* the product library's extended sets (s = 25..32; no counterpart in the reference) */
+static const uint16_t kSeqExt[32] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 217, 211, 199, 197, 193,
+                                     191, 181, 179, 173, 167, 163, 157, 151, 149, 139, 137, 131, 127, 113, 109, 107};
+
 int oz2o_moduli(int s, uint32_t* out) {
-    if (s < 2 || s > OZ2O_MAX_MODULI) return OZ2O_EINVAL;
-    const uint16_t* seq = s <= 6 ? kSeqSmall : (s <= 13 ? kSeqMid : kSeqLarge);
+    if (s < 2 || s > OZ2O_MAX_MODULI_EXT) return OZ2O_EINVAL;
+    const uint16_t* seq = s <= 6 ? kSeqSmall : (s <= 13 ? kSeqMid : (s <= OZ2O_MAX_MODULI ? kSeqLarge : kSeqExt));
     for (int t = 0; t < s; ++t) out[t] = seq[t];
     return OZ2O_OK;
 }
@@ -122,9 +126,15 @@ static int64_t mod_inverse(int64_t a, int64_t m) {
     return (t % m + m) % m;
 }
 
-/* plan: ref src/ozaki2_gpu.hpp:159-200 */
+/* plan: ref src/ozaki2_gpu.hpp:159-200 (s <= 24); the same rule with tk capped at 124 for the
+ * extended sets */
 int oz2o_make_plan(int s, int64_t k, oz2o_plan* p) {
-    if (s < 2 || s > OZ2O_MAX_MODULI || k < 1) return OZ2O_EINVAL;
+    if (s > OZ2O_MAX_MODULI) return OZ2O_EINVAL;
+    return oz2o_make_plan_ext(s, k, p);
+}
+
+int oz2o_make_plan_ext(int s, int64_t k, oz2o_plan* p) {
+    if (s < 2 || s > OZ2O_MAX_MODULI_EXT || k < 1) return OZ2O_EINVAL;
     memset(p, 0, sizeof *p);
     p->s = s;
     oz2o_moduli(s, p->m);
@@ -135,7 +145,8 @@ int oz2o_make_plan(int s, int64_t k, oz2o_plan* p) {
     p->nl = (int)floor(p->log2M / 32.0) + 1;
     if (p->nl < 2) p->nl = 2;
     int tk = (int)floor((p->log2M - 2.0 - log2((double)k)) / 2.0);
-    if (tk > 100) tk = 100;
+    const int cap = s <= OZ2O_MAX_MODULI ? 100 : 124;
+    if (tk > cap) tk = cap;
     for (;; --tk) {
         if (tk < 1) return OZ2O_EINVAL;
         big lhs; big_u64(&lhs, (uint64_t)k);
@@ -183,7 +194,7 @@ int oz2o_exponent(uint64_t maxbits, int tk) {
     return tk - e2;
 }
 
-/* x = RNE(v 2^e) from the bits of v (ref src/ozaki2_gpu.hpp:251-289). |v 2^e| <= 2^100 here. */
+/* x = RNE(v 2^e) from the bits of v (ref src/ozaki2_gpu.hpp:251-289). |v 2^e| <= 2^124 here. */
 void oz2o_scaled_int(double v, int e, int* neg, uint64_t* lo, uint64_t* hi) {
     uint64_t bits;
     memcpy(&bits, &v, 8);
@@ -247,7 +258,7 @@ void oz2o_split(const double* X, int64_t ldx, int64_t rows, int64_t cols, const 
  * ------------------------------------------------------------------------------------------ */
 double oz2o_crt(const oz2o_plan* p, const int64_t* r, int shift) {
     const int s = p->s;
-    int64_t a[OZ2O_MAX_MODULI];
+    int64_t a[OZ2O_MAX_MODULI_EXT];
     for (int i = 0; i < s; ++i) {
         const int64_t mi = p->m[i];
         int64_t v = ((r[i] % mi) + mi) % mi;
@@ -354,8 +365,21 @@ static int64_t dot_i8(const int8_t* a, const int8_t* b, int64_t k) {
 
 static double nan_value(void) { return __builtin_nan(""); }
 
+static int dgemm_impl(char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha, const double* A, int64_t lda,
+                      const double* B, int64_t ldb, double beta, double* C, int64_t ldc, int s, int ext);
+
 int oz2o_dgemm(char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha, const double* A, int64_t lda,
                const double* B, int64_t ldb, double beta, double* C, int64_t ldc, int s) {
+    return dgemm_impl(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s, 0);
+}
+
+int oz2o_dgemm_ext(char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha, const double* A, int64_t lda,
+                   const double* B, int64_t ldb, double beta, double* C, int64_t ldc, int s) {
+    return dgemm_impl(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s, 1);
+}
+
+static int dgemm_impl(char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha, const double* A, int64_t lda,
+                      const double* B, int64_t ldb, double beta, double* C, int64_t ldc, int s, int ext) {
     if (check_args(ta, tb, m, n, k, lda, ldb, ldc)) return OZ2O_EINVAL;
     if (m == 0 || n == 0) return OZ2O_OK;
     if (k == 0 || alpha == 0.0) {
@@ -364,7 +388,7 @@ int oz2o_dgemm(char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha, 
         return OZ2O_OK;
     }
     oz2o_plan p;
-    int st = oz2o_make_plan(s, k, &p);
+    int st = ext ? oz2o_make_plan_ext(s, k, &p) : oz2o_make_plan(s, k, &p);
     if (st) return st;
     int* D = (int*)malloc(sizeof(int) * (size_t)m);
     int* E = (int*)malloc(sizeof(int) * (size_t)n);
@@ -394,7 +418,7 @@ int oz2o_dgemm(char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha, 
 #pragma omp parallel for schedule(dynamic, 1)
     for (int64_t j = 0; j < n; ++j)
         for (int64_t i = 0; i < m; ++i) {
-            int64_t r[OZ2O_MAX_MODULI];
+            int64_t r[OZ2O_MAX_MODULI_EXT];
             for (int t = 0; t < s; ++t)
                 r[t] = dot_i8(Ar + ((size_t)t * m + i) * k, Br + ((size_t)t * n + j) * k, k);
             double v = oz2o_crt(&p, r, D[i] + E[j]);

@@ -32,7 +32,8 @@
 extern "C" {
 #endif
 
-#define OZ2O_MAX_MODULI 24
+#define OZ2O_MAX_MODULI 24      /* the reference's range of s */
+#define OZ2O_MAX_MODULI_EXT 32  /* the product's adaptive path: its own sets for s = 25..32 */
 #define OZ2O_BIG_WORDS 8
 #define OZ2O_NON_FINITE (-2147483647 - 1)
 
@@ -41,9 +42,9 @@ typedef struct {
     int nl;       /* 32-bit limbs needed for M */
     int tk;       /* bits per scaled element */
     double log2M;
-    uint32_t m[OZ2O_MAX_MODULI];
-    uint32_t y[OZ2O_MAX_MODULI];                 /* (M/m_t)^-1 mod m_t */
-    uint32_t W[OZ2O_MAX_MODULI][OZ2O_BIG_WORDS]; /* (M/m_t) * y_t */
+    uint32_t m[OZ2O_MAX_MODULI_EXT];
+    uint32_t y[OZ2O_MAX_MODULI_EXT];                 /* (M/m_t)^-1 mod m_t */
+    uint32_t W[OZ2O_MAX_MODULI_EXT][OZ2O_BIG_WORDS]; /* (M/m_t) * y_t */
     uint32_t M[OZ2O_BIG_WORDS];
 } oz2o_plan;
 
@@ -55,6 +56,10 @@ typedef struct {
 
 int oz2o_moduli(int s, uint32_t* out);
 int oz2o_make_plan(int s, int64_t k, oz2o_plan* p);
+/* s in [2, 32]: the reference's plans up to 24, above that the product library's extended sets
+ * (no counterpart in the reference; pairwise-coprime moduli <= 256 greedily from the top, tk up
+ * to 124), restated so the GPU's extended path can be checked bit for bit */
+int oz2o_make_plan_ext(int s, int64_t k, oz2o_plan* p);
 int oz2o_precision_bits(int64_t k, int s, int* out);
 int oz2o_moduli_for_bits(int64_t k, int bits);
 
@@ -76,6 +81,9 @@ void oz2o_split(const double* X, int64_t ldx, int64_t rows, int64_t cols, const 
 double oz2o_crt(const oz2o_plan* p, const int64_t* r, int shift);
 
 /* full emulated DGEMM on the CPU, C = alpha op(A) op(B) + beta C, ops 'N','T','C' */
+/* oz2o_dgemm at s in [2, 32] through oz2o_make_plan_ext (the product's adaptive path) */
+int oz2o_dgemm_ext(char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha, const double* A, int64_t lda,
+                   const double* B, int64_t ldb, double beta, double* C, int64_t ldc, int s);
 int oz2o_dgemm(char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha, const double* A, int64_t lda,
                const double* B, int64_t ldb, double beta, double* C, int64_t ldc, int s);
 /* complex (interleaved re,im) ZGEMM via exact 3M; alpha, beta are [re, im] */

@@ -30,8 +30,8 @@ def _op(c):
 
 class Plan(C.Structure):
     _fields_ = [("s", _i32), ("nl", _i32), ("tk", _i32), ("log2M", _dbl),
-                ("m", C.c_uint32 * 24), ("y", C.c_uint32 * 24),
-                ("W", (C.c_uint32 * 8) * 24), ("M", C.c_uint32 * 8)]
+                ("m", C.c_uint32 * 32), ("y", C.c_uint32 * 32),
+                ("W", (C.c_uint32 * 8) * 32), ("M", C.c_uint32 * 8)]
 
     def big(self, words):
         return sum(int(w) << (32 * i) for i, w in enumerate(words))
@@ -50,6 +50,7 @@ class Oracle:
             raise FileNotFoundError(f"{path} is not built (make -C oracle)")
         L = self.lib = C.CDLL(path)
         L.oz2o_make_plan.argtypes = [_i32, _i64, C.POINTER(Plan)]
+        L.oz2o_make_plan_ext.argtypes = [_i32, _i64, C.POINTER(Plan)]
         L.oz2o_precision_bits.argtypes = [_i64, _i32, C.POINTER(_i32)]
         L.oz2o_moduli_for_bits.argtypes = [_i64, _i32]
         L.oz2o_exponent.argtypes = [C.c_uint64, _i32]
@@ -60,6 +61,7 @@ class Oracle:
         L.oz2o_crt.restype = _dbl
         gemm_args = [_chr, _chr, _i64, _i64, _i64]
         L.oz2o_dgemm.argtypes = gemm_args + [_dbl, _vp, _i64, _vp, _i64, _dbl, _vp, _i64, _i32]
+        L.oz2o_dgemm_ext.argtypes = gemm_args + [_dbl, _vp, _i64, _vp, _i64, _dbl, _vp, _i64, _i32]
         L.oz2o_zgemm.argtypes = gemm_args + [_vp, _vp, _i64, _vp, _i64, _vp, _vp, _i64, _i32]
         L.oz2o_exponents.argtypes = gemm_args + [_vp, _i64, _vp, _i64, _i32, _i32, _vp, _vp]
         L.oz2o_dd_gemm.argtypes = gemm_args + [_vp, _i64, _vp, _i64, _vp, _vp]
@@ -84,6 +86,14 @@ class Oracle:
         st = self.lib.oz2o_make_plan(s, k, C.byref(p))
         if st:
             raise ValueError(f"oracle plan(s={s}, k={k}) status {st}")
+        return p
+
+    def plan_ext(self, s, k):
+        """the plan for s in [2, 32]: the reference's up to 24, the library's extended sets above"""
+        p = Plan()
+        st = self.lib.oz2o_make_plan_ext(s, k, C.byref(p))
+        if st:
+            raise ValueError(f"oracle plan_ext(s={s}, k={k}) status {st}")
         return p
 
     def precision_bits(self, k, s):
@@ -115,6 +125,10 @@ class Oracle:
 
     def dgemm(self, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C_, ldc, s):
         return self.lib.oz2o_dgemm(_op(ta), _op(tb), m, n, k, alpha, _ptr(A), lda, _ptr(B), ldb, beta, _ptr(C_),
+                                   ldc, s)
+
+    def dgemm_ext(self, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C_, ldc, s):
+        return self.lib.oz2o_dgemm_ext(_op(ta), _op(tb), m, n, k, alpha, _ptr(A), lda, _ptr(B), ldb, beta, _ptr(C_),
                                    ldc, s)
 
     def zgemm(self, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C_, ldc, s):

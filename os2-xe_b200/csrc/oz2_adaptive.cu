@@ -7,8 +7,8 @@
 //              analytic s: the smallest s
 //              whose bits per element tk reach R + 2 + t - floor(log2(k - 1)), R the largest
 //              gap. Every product term then carries a relative error <= 3 * 2^(R - tk), so
-//              |C - AB| <= k 2^-t |A||B| holds entry by entry (the DGEMM-level target); 25 (native
-//              FP64) where even 24 moduli do not reach it.
+//              |C - AB| <= k 2^-t |A||B| holds entry by entry (the DGEMM-level target); kNativeS
+//              (native FP64) where even 32 moduli (the extended sets above 24) do not reach it.
 //   probe    : Freivalds-style check of a computed tile, C x against A (B x) in double-double
 //              with x = e_j for kProbeCols stratified random columns j: each entry (i, j) of those
 //              columns against its own tolerance k 2^-t (|A||B|)_ij plus the rounding of C, so a
@@ -144,17 +144,19 @@ __global__ void tile_features_kernel(const FeatureItem* __restrict__ items, int 
     // edge tiles hold fewer rows / columns: fewer entries, other statistics
     f[16] = static_cast<float>(I.rows_a) / 512.0f;
     f[17] = static_cast<float>(I.rows_b) / 512.0f;
-    // analytic s: tk >= R + 2 + t - floor(log2(k - 1))
+    // analytic s: tk >= R + 2 + t - floor(log2(k - 1)); the last gap bin holds every gap of 63 or
+    // more, so R = 63 bounds nothing: native FP64
     const int R = max(ra, rb);
     int lg = 0;
     for (int64_t v = I.k - 1; v > 1; v >>= 1) ++lg;
     const int need = R + 2 + I.target_bits - lg;
     int s = kNativeS;  // no moduli set suffices: native FP64
-    for (int c = 2; c <= kMaxModuli; ++c)
-        if (I.tk[c] >= need) {
-            s = c;
-            break;
-        }
+    if (R < kGapBins - 1)
+        for (int c = 2; c <= kMaxModuliExt; ++c)
+            if (I.tk[c] >= need) {
+                s = c;
+                break;
+            }
     s_analytic[t] = s;
 }
 
@@ -308,6 +310,152 @@ __global__ void __launch_bounds__(kProbeThreads, 3) probe_kernel(const ProbeItem
     if (bad) atomicOr(fail + I->tile, 1);
 }
 
+// ---------------------------------------------------------------- Freivalds probe
+// x_vj = +-2^-f_j: the sign from the item's seed, f_j the frexp exponent of op(B)'s column maximum
+// (0 for a zero or non-finite column: nothing to test there)
+__device__ __forceinline__ double freivalds_x(const FreivaldsItem* I, int v, int64_t j) {
+    const unsigned long long b = I->maxb[j];
+    if (b == 0 || b >= 0x7FF0000000000000ull) return 0.0;
+    const int f = frexp_exp_bits(b);
+    const double mag = ldexp(1.0, -f);
+    const uint64_t h = mix64(I->seed ^ (static_cast<uint64_t>(v) << 40) ^ static_cast<uint64_t>(j));
+    return (h & 1) ? -mag : mag;
+}
+// acc + x for a double x (exact error term kept)
+__device__ __forceinline__ dd dd_add_d(dd acc, double x) {
+    dd s = two_sum(acc.hi, x);
+    s.lo += acc.lo;
+    return two_sum(s.hi, s.lo);
+}
+
+// pass 1: thread (p, v) of the block's kFreivaldsP inner indices: u_v,p = sum_j op(B)(p, j) x_vj in
+// double-double (each product exact) and ub_v,p = sum_j |op(B)(p, j)| |x_vj|
+__global__ void __launch_bounds__(kFreivaldsP * kFreivaldsVecs) freivalds_bx_kernel(
+    const FreivaldsItem* __restrict__ items, int count) {
+    constexpr int JC = 32, V = kFreivaldsVecs, P = kFreivaldsP;
+    const FreivaldsItem* I = items + find_block_item(items, count, blockIdx.x);
+    const int64_t p0 = (static_cast<int64_t>(blockIdx.x) - I->block0) * P;
+    const int64_t k = I->k, nt = I->nt;
+    const int tp = threadIdx.x % P, v = threadIdx.x / P;
+    __shared__ double bs[JC][P + 1];
+    __shared__ double xs[V][JC];
+    dd u{0.0, 0.0};
+    double ub = 0.0;
+    for (int64_t j0 = 0; j0 < nt; j0 += JC) {
+        if (threadIdx.x < V * JC) {
+            const int vv = threadIdx.x / JC, jj = threadIdx.x % JC;
+            xs[vv][jj] = j0 + jj < nt ? freivalds_x(I, vv, j0 + jj) : 0.0;
+        }
+        for (int e = threadIdx.x; e < JC * P; e += blockDim.x) {
+            int jj, pp;
+            if (I->b_rowc) {  // op(B)(p, j) at B[j + p ldb]: j contiguous
+                jj = e % JC;
+                pp = e / JC;
+            } else {          // B[p + j ldb]: p contiguous
+                pp = e % P;
+                jj = e / P;
+            }
+            const int64_t p = p0 + pp, j = j0 + jj;
+            double b = 0.0;
+            if (p < k && j < nt) b = I->b_rowc ? I->B[j + p * I->ldb] : I->B[p + j * I->ldb];
+            bs[jj][pp] = b;
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int jj = 0; jj < JC; ++jj) {
+            const double b = bs[jj][tp], x = xs[v][jj];
+            u = dd_add_d(u, b * x);  // a power-of-two scaling: exact unless it underflows
+            ub = fma(fabs(b), fabs(x), ub);
+        }
+        __syncthreads();
+    }
+    const int64_t p = p0 + tp;
+    if (p < k) {
+        I->work[(3 * v + 0) * k + p] = u.hi;
+        I->work[(3 * v + 1) * k + p] = u.lo;
+        I->work[(3 * v + 2) * k + p] = ub;
+    }
+}
+
+// pass 2: one thread per tile row i: z_v = alpha (op(A) u_v)_i and y_v = (C x_v)_i in double-double,
+// zb_v = (|op(A)| ub_v)_i and yb_v = (|C| |x_v|)_i in FP64; the row fails when |z_v - y_v| exceeds
+// |alpha| k 2^-t zb_v (the target summed over the row with weights |x_vj|) widened by the FP64
+// rounding of zb (k + nt + 8 terms), plus one rounding of C (2^-52 yb_v), plus the probe's own
+// double-double errors (below 2^-90 of the magnitudes), plus the underflow floor
+__global__ void __launch_bounds__(kFreivaldsRows) freivalds_check_kernel(const FreivaldsItem* __restrict__ items,
+                                                                         int count, int* __restrict__ fail) {
+    constexpr int V = kFreivaldsVecs, PC = 256;
+    const FreivaldsItem* I = items + find_block_item(items, count, blockIdx.x);
+    const int64_t i = (static_cast<int64_t>(blockIdx.x) - I->block0) * kFreivaldsRows + threadIdx.x;
+    const int64_t k = I->k, nt = I->nt, mt = I->mt;
+    const bool live = i < mt;
+    __shared__ double us[V][3][PC];
+    dd z[V], y[V];
+    double zb[V], yb[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        z[v] = y[v] = dd{0.0, 0.0};
+        zb[v] = yb[v] = 0.0;
+    }
+    for (int64_t p0 = 0; p0 < k; p0 += PC) {
+        const int pn = static_cast<int>(min(static_cast<int64_t>(PC), k - p0));
+        for (int e = threadIdx.x; e < V * 3 * PC; e += blockDim.x) {
+            const int q = e % PC, w = e / PC;  // w = 3 v + component
+            us[w / 3][w % 3][q] = q < pn ? I->work[w * k + p0 + q] : 0.0;
+        }
+        __syncthreads();
+        if (live) {
+            for (int q = 0; q < pn; ++q) {
+                const int64_t p = p0 + q;
+                const double a = I->a_rowc ? __ldg(I->A + i + p * I->lda) : __ldg(I->A + p + i * I->lda);
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                    z[v] = dd_add_prod(z[v], a, us[v][0][q]);
+                    z[v].lo = fma(a, us[v][1][q], z[v].lo);
+                    zb[v] = fma(fabs(a), us[v][2][q], zb[v]);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    __shared__ double xs[V][PC];
+    for (int64_t j0 = 0; j0 < nt; j0 += PC) {
+        const int jn = static_cast<int>(min(static_cast<int64_t>(PC), nt - j0));
+        for (int e = threadIdx.x; e < V * PC; e += blockDim.x) {
+            const int q = e % PC, v = e / PC;
+            xs[v][q] = q < jn ? freivalds_x(I, v, j0 + q) : 0.0;
+        }
+        __syncthreads();
+        if (live) {
+            for (int q = 0; q < jn; ++q) {
+                const double c = I->C[i + (j0 + q) * I->ldc];
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                    y[v] = dd_add_d(y[v], c * xs[v][q]);
+                    yb[v] = fma(fabs(c), fabs(xs[v][q]), yb[v]);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (!live) return;
+    const double al = I->alpha, kd = static_cast<double>(k) + static_cast<double>(nt) + 8.0;
+    bool bad = false;
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        // alpha z as a double-double: two-product of the high part, the low part rounded once
+        const double zh = al * z[v].hi;
+        const dd az = two_sum(zh, fma(al, z[v].hi, -zh) + al * z[v].lo);
+        const dd diff = dd_add(az, dd{-y[v].hi, -y[v].lo});
+        const double err = fabs(diff.hi + diff.lo);
+        const double mag = fabs(al) * zb[v];
+        const double tol = mag * I->tol_scale * (1.0 + kd * 0x1p-50) + 0x1p-52 * yb[v] + 0x1p-90 * (mag + yb[v]) +
+                           1e-300;
+        bad |= !(err <= tol);
+    }
+    if (bad) atomicOr(fail + I->tile, 1);
+}
+
 // ---------------------------------------------------------------- double-double reference
 // C_hi + C_lo ~= op(A) op(B) and |op(A)| |op(B)| for an m x n block, N/N column-major inputs.
 __global__ void __launch_bounds__(256) dd_gemm_nn_kernel(int64_t m, int64_t n, int64_t k, const double* __restrict__ A,
@@ -432,6 +580,21 @@ int64_t probe_item_blocks(ProbeItem& it, int64_t block0) {
 void launch_probe(const ProbeItem* d, int count, int64_t blocks, int* fail, cudaStream_t st) {
     if (count <= 0 || blocks <= 0) return;
     probe_kernel<<<static_cast<unsigned>(blocks), kProbeThreads, 0, st>>>(d, count, fail);
+}
+
+int64_t freivalds_blocks_pass1(FreivaldsItem& it, int64_t block0) {
+    it.block0 = block0;
+    return (it.k + kFreivaldsP - 1) / kFreivaldsP;
+}
+int64_t freivalds_blocks_pass2(FreivaldsItem& it, int64_t block0) {
+    it.block0 = block0;
+    return (it.mt + kFreivaldsRows - 1) / kFreivaldsRows;
+}
+void launch_freivalds(const FreivaldsItem* d1, int64_t blocks1, const FreivaldsItem* d2, int64_t blocks2, int count,
+                      int* fail, cudaStream_t st) {
+    if (count <= 0 || blocks1 <= 0 || blocks2 <= 0) return;
+    freivalds_bx_kernel<<<static_cast<unsigned>(blocks1), kFreivaldsP * kFreivaldsVecs, 0, st>>>(d1, count);
+    freivalds_check_kernel<<<static_cast<unsigned>(blocks2), kFreivaldsRows, 0, st>>>(d2, count, fail);
 }
 
 void launch_dd_gemm_nn(int64_t m, int64_t n, int64_t k, const double* A, int64_t lda, const double* B, int64_t ldb,

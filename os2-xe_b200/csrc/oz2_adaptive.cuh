@@ -15,10 +15,12 @@ namespace oz2 {
 constexpr int kGapBins = 64;     // exponent gaps 0..63 (63 = "63 or more"), plus a zero counter
 constexpr int kFeatures = 18;
 constexpr int kHidden = 32;
-// s = 2..24 run emulated; kNativeS marks a tile that no s <= 24 brings to the target, run as a
-// native FP64 GEMM
-constexpr int kNativeS = kMaxModuli + 1;
-constexpr int kClasses = kNativeS - 1;  // s = 2..25
+// s = 2..32 run emulated (s = 25..32 with the extended moduli sets); kNativeS marks a tile that no
+// s <= 32 brings to the target, run as a native FP64 GEMM
+constexpr int kNativeS = kMaxModuliExt + 1;
+// the MLP's classes: s = 2..24 and one for "more than 24" (s = 25 as its answer: a lower bound
+// that the probe checks, or the judge's s where a certificate takes the tile)
+constexpr int kClasses = kMaxModuli;
 // per-call statistics of oz2_dgemm_adaptive
 constexpr int kAdaptiveStats = 10;
 constexpr int kMlpParams = kHidden * kFeatures + kHidden + kHidden * kHidden + kHidden + kClasses * kHidden + kClasses;
@@ -47,7 +49,7 @@ struct FeatureItem {
     const unsigned long long* maxbits_b;
     int64_t rows_a, rows_b, k;
     int target_bits;
-    int tk[kMaxModuli + 1];  // tk[s] for s = 2..24 (0 where s is too small for k)
+    int tk[kMaxModuliExt + 1];  // tk[s] for s = 2..32 (0 where s is too small for k)
 };
 
 // probe of one computed tile (pointers at the tile's first row / column)
@@ -63,6 +65,34 @@ struct ProbeItem {
     int tile;         // index into the failure flags
     int64_t block0;
 };
+
+// Freivalds probe of one computed tile (the north star's C x against A (B x) in double-double):
+// kFreivaldsVecs random vectors x_v with x_vj = +-2^-f_j (f_j the frexp exponent of op(B)'s
+// column maximum, 0 for a zero or non-finite column), so every product with x is exact. Pass 1
+// (one block per kFreivaldsP inner indices): u_v = op(B) x_v in double-double and ub_v = |op(B)||x_v|.
+// Pass 2 (one block per kFreivaldsRows tile rows): per row i, |alpha (op(A) u_v)_i - (C x_v)_i| <=
+// alpha k 2^-t (|op(A)| ub_v)_i widened for the probe's own roundings. A tile that meets the
+// target entry by entry always passes; the test sees an error entry only through its row sum.
+constexpr int kFreivaldsVecs = 2;
+constexpr int kFreivaldsP = 64;     // inner indices per pass-1 block
+constexpr int kFreivaldsRows = 128;  // tile rows per pass-2 block (one per thread)
+struct FreivaldsItem {
+    const double* A;  // op(A) rows of the tile
+    const double* B;  // op(B) columns of the tile
+    const double* C;
+    const unsigned long long* maxb;  // column maxima (raw bits) of op(B) for the tile's columns
+    double* work;     // 3 kFreivaldsVecs k doubles: u_v hi, u_v lo, ub_v
+    int64_t lda, ldb, ldc, mt, nt, k;
+    int a_rowc, b_rowc;
+    double alpha, tol_scale;  // tol_scale = k 2^-t
+    uint64_t seed;
+    int tile;
+    int64_t block0;
+};
+int64_t freivalds_blocks_pass1(FreivaldsItem& it, int64_t block0);
+int64_t freivalds_blocks_pass2(FreivaldsItem& it, int64_t block0);
+void launch_freivalds(const FreivaldsItem* d1, int64_t blocks1, const FreivaldsItem* d2, int64_t blocks2, int count,
+                      int* fail, cudaStream_t st);
 
 // ---- certified s (a rigorous entrywise a-priori bound, see oz2_certify.cu)
 // one panel side of a problem: the scaled magnitudes |x| 2^-e_r of its rows (rows of op(A) or
@@ -85,7 +115,7 @@ struct CertTileItem {
     const unsigned long long* maxb;
     int64_t mb, nb, k;
     int target_bits;
-    int tk[kMaxModuli + 1];
+    int tk[kMaxModuliExt + 1];
     int* s_out;  // smallest certified s, kNativeS where none is (or the tile has a non-finite row)
 };
 constexpr int kCertRowsPerBlock = 32;   // rows-contiguous prep: 32 rows x 8 k slices per block

@@ -122,9 +122,11 @@ struct oz2_context {
     bool mlp_loaded = false;
     float mlp_threshold = 0.9f;
     int adaptive_tile = 512;
+    int probe_kind = 0;  // 0: kProbeCols columns entry by entry, 1: Freivalds, 2: both, 3: none
     uint8_t* ws2 = nullptr;
     size_t ws2_size = 0;
     int64_t astats[kAdaptiveStats] = {};
+    int64_t gbytes[3] = {};  // last adaptive call's GEMM: plane bytes read, residue bytes written, tile batches
     cublasHandle_t cublas = nullptr;  // native FP64 GEMM of tiles no moduli set brings to the target
     cudaStream_t cublas_stream = nullptr;
     bool cublas_bound = false;        // cublas_stream is set on the handle
@@ -197,7 +199,15 @@ int end_call(oz2_context* h, void* done) {
 }
 
 // plans are cached per (s, k); k is the plan's inner length (2k for complex)
-int get_plan(oz2_context* h, int s, int64_t k, const Plan** out) {
+// ext: the adaptive path's range s <= 32 (the extended sets above 24); the reference-facing calls
+// keep s <= 24
+int get_plan(oz2_context* h, int s, int64_t k, const Plan** out, bool ext = false) {
+    if (!ext && s > kMaxModuli) {
+        char buf[160];
+        return fail(h, OZ2_EINVAL, plan_error_text(s, k, 1, buf, sizeof buf));
+    }
+    if (ext && (s < 2 || s > kMaxModuliExt))
+        return fail(h, OZ2_EINVAL, "oz2: num_moduli must be in [2, " + std::to_string(kMaxModuliExt) + "]");
     auto key = std::make_pair(s, k);
     auto it = h->plans.find(key);
     if (it != h->plans.end()) {
@@ -205,7 +215,7 @@ int get_plan(oz2_context* h, int s, int64_t k, const Plan** out) {
         return OZ2_OK;
     }
     auto p = std::make_unique<Plan>();
-    const int st = make_plan(s, k, *p);
+    const int st = make_plan_ext(s, k, *p);
     if (st) {
         char buf[160];
         plan_error_text(s, k, st, buf, sizeof buf);
@@ -359,12 +369,12 @@ int64_t crt_geom(CrtItem& it, int64_t b0) { return crt_item_blocks(it, b0); }
 
 // Appends split, GEMM and CRT operations for a list of tasks (launches grouped by kernel variant)
 void plan_tasks(Program& prog, const std::vector<Task>& tasks, const GemmConfig& cfg) {
-    // split: group by (row_contig, complex, wide limb path)
+    // split: group by (row_contig, complex, limb path: narrow, wide, widest)
     std::map<std::tuple<int, int, int>, std::vector<SplitItem>> split_groups;
     for (const Task& t : tasks) {
         const Prob& p = *t.p;
         const ModConst* mc = p.plan->mc;
-        const bool wide = p.plan->tk > kNarrowScaleBits;
+        const int wide = p.plan->tk > kWideScaleBits ? 2 : (p.plan->tk > kNarrowScaleBits ? 1 : 0);
         if (t.split_b) {
             SplitItem it = side_item(p, false, t.j0, t.nb, t.maxB, t.planesB, mc);
             split_groups[{it.row_contig, it.cplx, wide}].push_back(it);
@@ -932,7 +942,7 @@ int cublas_on(oz2_context* h, cudaStream_t st) {
 }
 
 // C[i0:i0+mb, j0:j0+nb] = alpha op(A) op(B) + beta C in native FP64 (cuBLAS DGEMM, default math:
-// no emulation), for tiles whose inputs span more exponent range than 24 moduli cover
+// no emulation), for tiles whose inputs span more exponent range than 32 moduli cover
 int native_gemm(oz2_context* h, cudaStream_t st, const Prob& p, int64_t i0, int64_t j0, int64_t mb, int64_t nb) {
     const int sb = cublas_on(h, st);
     if (sb) return sb;
@@ -993,7 +1003,7 @@ int native_join(oz2_context* h) {
 
 // tk[s] for one k (0 where s is too small)
 void tk_table(int64_t k, int* tk) {
-    for (int s = 0; s <= kMaxModuli; ++s) tk[s] = s >= 2 ? plan_tk(s, k) : 0;
+    for (int s = 0; s <= kMaxModuliExt; ++s) tk[s] = s >= 2 ? plan_tk(s, k) : 0;
 }
 
 struct TileRef {
@@ -1149,7 +1159,7 @@ int certify_tiles(oz2_context* h, const std::vector<Prob>& base, const std::vect
                 it.nb = r.nb;
                 it.k = p.k;
                 it.target_bits = target_bits;
-                for (int s = 0; s <= kMaxModuli; ++s) it.tk[s] = tk[s];
+                for (int s = 0; s <= kMaxModuliExt; ++s) it.tk[s] = tk[s];
                 it.s_out = d_sc + t;
                 ti.push_back(it);
             }
@@ -1171,6 +1181,7 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
                  int mode, float* feat_out = nullptr, int* sa_out = nullptr, int64_t* ntiles_out = nullptr) {
     const int64_t T = h->adaptive_tile;
     for (int q = 0; q < kAdaptiveStats; ++q) h->astats[q] = 0;
+    for (int64_t& g : h->gbytes) g = 0;
     // ---- phase 1: maxima, panel statistics, tile features, analytic s, MLP
     std::vector<TileRef> tiles;
     std::vector<int64_t> pa0(base.size()), pb0(base.size());
@@ -1209,7 +1220,8 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
     const size_t osm = carve1(static_cast<size_t>(ntiles) * 4);
     const size_t osc = carve1(static_cast<size_t>(ntiles) * 4);
     const size_t desc_bytes = 1024 + base.size() * 2 * sizeof(ScaleItem) + npanels * sizeof(StatItem) +
-                              ntiles * (sizeof(FeatureItem) + sizeof(ProbeItem)) + 16 * 256;
+                              ntiles * (sizeof(FeatureItem) + sizeof(ProbeItem) + 2 * sizeof(FreivaldsItem)) +
+                              16 * 256;
     const size_t odesc = carve1(desc_bytes);
     int st = ensure_workspace(h, off);
     if (st) return st;
@@ -1283,11 +1295,11 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
         f.target_bits = target_bits;
         auto it = tk_cache.find(p.k);
         if (it == tk_cache.end()) {
-            std::vector<int> tk(kMaxModuli + 1);
+            std::vector<int> tk(kMaxModuliExt + 1);
             tk_table(p.k, tk.data());
             it = tk_cache.emplace(p.k, tk).first;
         }
-        for (int s = 0; s <= kMaxModuli; ++s) f.tk[s] = it->second[s];
+        for (int s = 0; s <= kMaxModuliExt; ++s) f.tk[s] = it->second[s];
     }
     const size_t ofi = ph1.add(fi.data(), fi.size() * sizeof(FeatureItem));
     if (ph1.blob.size() > desc_bytes) return fail(h, OZ2_EINTERNAL, "oz2: descriptor region too small");
@@ -1395,8 +1407,8 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
         }
         // never below the smallest s that k admits
         const std::vector<int>& tk = tk_cache[base[q].k];
-        while (sv < kMaxModuli && tk[sv] == 0) ++sv;
-        s_tile[t] = std::max(2, std::min(kMaxModuli, sv));
+        while (sv < kMaxModuliExt && tk[sv] == 0) ++sv;
+        s_tile[t] = std::max(2, std::min(kMaxModuliExt, sv));
     }
     if (mode == 0 || mode == 4) {
         // Per problem, the cheaper of its tiles as chosen and one whole-problem task (a larger s
@@ -1418,7 +1430,7 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
         }
         std::vector<int> whole(base.size(), 0);  // 0 keep the tiles, else the s of one task
         for (size_t q = 0; q < base.size(); ++q) {
-            const double emu = hi[q] <= kMaxModuli ? hi[q] * area[q] : 1e300;
+            const double emu = hi[q] <= kMaxModuliExt ? hi[q] * area[q] : 1e300;
             const double nat = kNativeCost * area[q];
             if (std::min(emu, nat) <= tiles_cost[q]) whole[q] = emu <= nat ? hi[q] : kNativeS;
         }
@@ -1502,7 +1514,7 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
             if (it != prob_for.end()) return it->second;
             auto np = std::make_unique<Prob>(base[q]);
             const Plan* plan;
-            if (get_plan(h, sv, base[q].k, &plan)) return nullptr;
+            if (get_plan(h, sv, base[q].k, &plan, true)) return nullptr;
             np->plan = plan;
             Prob* raw = np.get();
             probs.push_back(std::move(np));
@@ -1584,6 +1596,8 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
                     if (i > start && off2 + add + (1 << 20) > limit) break;
                     const size_t oa = carve2(pa), ob = carve2(pb);
                     batch.push_back(Slot{oa, ob, carve2(rs)});
+                    h->gbytes[0] += static_cast<int64_t>(pa + pb);
+                    h->gbytes[1] += static_cast<int64_t>(rs);
                     continue;
                 }
                 const TileRef& r = tiles[un.tile];
@@ -1592,9 +1606,12 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
                 if (i > start && off2 + add + (1 << 20) > limit) break;
                 if (newa) panels[{r.ia, 0, sv}] = {carve2(pa), true};
                 if (newb) panels[{r.jb, 1, sv}] = {carve2(pb), true};
+                h->gbytes[0] += static_cast<int64_t>((newa ? pa : 0) + (newb ? pb : 0));
+                h->gbytes[1] += static_cast<int64_t>(rs);
                 batch.push_back(Slot{panels[{r.ia, 0, sv}].first, panels[{r.jb, 1, sv}].first, carve2(rs)});
             }
             const size_t obase_desc = off2;
+            h->gbytes[2] += 1;
             const size_t need = off2 + align256(batch.size() * (2 * sizeof(SplitItem) + sizeof(GemmItem) +
                                                                 sizeof(CrtItem) + 1024) + 8192);
             int st2 = ensure_ws2(h, need);
@@ -1671,6 +1688,7 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
         for (const int64_t t : porder) {
             const TileRef& r = tiles[t];
             const Prob& p = base[r.prob];
+            if (h->probe_kind == 3) break;  // no probe: the MLP's s stands (for measurements)
             if (p.beta[0] != 0.0 || s_tile[t] >= s_jd[t]) continue;  // the judge's s needs no probe
             ProbeItem it{};
             it.a_rowc = is_n(p.ta);
@@ -1693,10 +1711,61 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
         }
         if (!pi.empty()) {
             unsigned char* pd = ws + odesc;  // phase-1 descriptors are consumed by now (stream order)
-            if ((st = put_blob(h, pi.data(), pi.size() * sizeof(ProbeItem), pd))) return st;
+            // Freivalds items: the same tiles, their column maxima and 3 kFreivaldsVecs k doubles
+            // of work each in the tile workspace, whose planes and residues are dead by now
+            std::vector<FreivaldsItem> f1, f2;
+            int64_t fb1 = 0, fb2 = 0;
+            if (h->probe_kind != 0) {
+                size_t fwork = 0;
+                for (const ProbeItem& q : pi) fwork += align256(3 * kFreivaldsVecs * q.k * sizeof(double));
+                if ((st = ensure_ws2(h, fwork))) return st;
+                size_t fo = 0;
+                for (const ProbeItem& q : pi) {
+                    const TileRef& r = tiles[q.tile];
+                    FreivaldsItem it{};
+                    it.A = q.A;
+                    it.B = q.B;
+                    it.C = q.C;
+                    it.maxb = maxB(r.prob) + r.j0;
+                    it.work = reinterpret_cast<double*>(h->ws2 + fo);
+                    fo += align256(3 * kFreivaldsVecs * q.k * sizeof(double));
+                    it.lda = q.lda;
+                    it.ldb = q.ldb;
+                    it.ldc = q.ldc;
+                    it.mt = q.mt;
+                    it.nt = q.nt;
+                    it.k = q.k;
+                    it.a_rowc = q.a_rowc;
+                    it.b_rowc = q.b_rowc;
+                    it.alpha = q.alpha;
+                    it.tol_scale = q.tol_scale;
+                    it.seed = q.seed;
+                    it.tile = q.tile;
+                    f1.push_back(it);
+                    fb1 += freivalds_blocks_pass1(f1.back(), fb1);
+                    f2.push_back(it);
+                    fb2 += freivalds_blocks_pass2(f2.back(), fb2);
+                }
+            }
+            const size_t o1 = align256(pi.size() * sizeof(ProbeItem));
+            const size_t o2 = o1 + align256(f1.size() * sizeof(FreivaldsItem));
+            if (h->probe_kind != 1 && (st = put_blob(h, pi.data(), pi.size() * sizeof(ProbeItem), pd))) return st;
+            if (h->probe_kind != 0) {
+                if ((st = put_blob(h, f1.data(), f1.size() * sizeof(FreivaldsItem), pd + o1))) return st;
+                if ((st = put_blob(h, f2.data(), f2.size() * sizeof(FreivaldsItem), pd + o2))) return st;
+            }
             mark(h, kBegin);
-            launch_probe(reinterpret_cast<const ProbeItem*>(pd), static_cast<int>(pi.size()), blocks, d_fail, h->stream);
-            ++h->launches;
+            if (h->probe_kind != 1) {
+                launch_probe(reinterpret_cast<const ProbeItem*>(pd), static_cast<int>(pi.size()), blocks, d_fail,
+                             h->stream);
+                ++h->launches;
+            }
+            if (h->probe_kind != 0) {
+                launch_freivalds(reinterpret_cast<const FreivaldsItem*>(pd + o1), fb1,
+                                 reinterpret_cast<const FreivaldsItem*>(pd + o2), fb2, static_cast<int>(f1.size()),
+                                 d_fail, h->stream);
+                h->launches += 2;
+            }
             mark(h, kProbe);
             std::vector<int> failed(ntiles);
             if ((st = read_back(h, {{failed.data(), d_fail, static_cast<size_t>(ntiles) * 4}}))) return st;
@@ -1756,9 +1825,9 @@ int validate_adaptive(oz2_handle h, int count, const oz2_dgemm_problem* pr, std:
     for (int i = 0; i < count; ++i) {
         const oz2_dgemm_problem& q = pr[i];
         if (q.m == 0 || q.n == 0 || q.k == 0 || q.alpha == 0.0) continue;
-        if (need_fixed) {
+        if (need_fixed) {  // mode 3 takes the extended sets too (s up to 32)
             const Plan* plan;
-            int st = get_plan(h, q.num_moduli, q.k, &plan);
+            int st = get_plan(h, q.num_moduli, q.k, &plan, true);
             if (st) return fail(h, st, "oz2: problem " + std::to_string(i) + ": " + h->err);
         }
         out.push_back(Prob{q.ta, q.tb, q.m, q.n, q.k, {q.alpha, 0.0}, {q.beta, 0.0}, q.A, q.lda, q.B, q.ldb, q.C, q.ldc, 1,
@@ -2064,6 +2133,7 @@ int oz2_dgemm_adaptive(oz2_handle h, int count, const oz2_dgemm_problem* problem
         }
     }
     for (int q = 0; q < kAdaptiveStats; ++q) h->astats[q] = 0;
+    for (int64_t& g : h->gbytes) g = 0;
     h->native_ms = 0.0;
     if (!probs.empty()) st = run_adaptive(h, probs, fixed_s, target_bits, mode);
     const int sj = native_join(h);  // on every path: the stream must cover the native tiles
@@ -2086,6 +2156,13 @@ int oz2_tile_features(oz2_handle h, int count, const oz2_dgemm_problem* problems
         return st;
     if (ntiles) *ntiles = nt;
     return end_call(h, nullptr);
+}
+
+int oz2_set_probe_kind(oz2_handle h, int kind) {
+    if (!h) return fail(nullptr, OZ2_EINVAL, "oz2: null handle");
+    if (kind < 0 || kind > 3) return fail(h, OZ2_EINVAL, "oz2: probe kind must be 0, 1, 2 or 3");
+    h->probe_kind = kind;
+    return OZ2_OK;
 }
 
 int oz2_set_adaptive_options(oz2_handle h, int tile, float threshold) {
@@ -2380,6 +2457,12 @@ int oz2_adaptive_stage_times(oz2_handle h, double* out2) {
         OZ2_CUDA(h, cudaEventElapsedTime(&ms, h->marks[i - 1].second, h->marks[i].second));
         out2[stg - kProbe] += ms;
     }
+    return OZ2_OK;
+}
+
+int oz2_adaptive_gemm_bytes(oz2_handle h, int64_t* out3) {
+    if (!h || !out3) return fail(h, OZ2_EINVAL, "oz2: null argument");
+    for (int i = 0; i < 3; ++i) out3[i] = h->gbytes[i];
     return OZ2_OK;
 }
 

@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(128) cert_tile_kernel(const CertTileItem* __re
             const double l1 = log2(static_cast<double>(q1) * (1.0 + 0x1p-20)) + tb - 1.0 - log2(B * c * (1.0 - 0x1p-10));
             const double l2 = 0.5 * (log2(static_cast<double>(q2) * (1.0 + 0x1p-20)) + tb + 10.0 - log2(B / k * c));
             const double need = ceil(fmax(l1, l2) + 1e-9);
-            for (int q = 2; q <= kMaxModuli; ++q)
+            for (int q = 2; q <= kMaxModuliExt; ++q)
                 if (I->tk[q] > 0 && static_cast<double>(I->tk[q]) >= need) {
                     s = q;
                     break;

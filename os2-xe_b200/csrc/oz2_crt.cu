@@ -18,7 +18,7 @@ struct CrtParams {
     const CrtItem* items;
     int count;
     CrtConst cc;
-    uint32_t mod_m[kMaxModuli];
+    uint32_t mod_m[kMaxModuliExt];
 };
 
 __device__ __forceinline__ int exponent_of(unsigned long long b, int tk) {
@@ -231,15 +231,21 @@ __global__ void __launch_bounds__(256) crt_kernel(const __grid_constant__ CrtPar
     }
 }
 
+// complex CRTs stop at s = 24 (zgemm is the reference's call); the extended sets are real only
 template <int S>
 void crt_launch_s(const CrtParams& P, int64_t blocks, bool cplx, cudaStream_t st) {
-    if (cplx) crt_kernel<S, true><<<static_cast<unsigned>(blocks), 256, 0, st>>>(P);
-    else crt_kernel<S, false><<<static_cast<unsigned>(blocks), 256, 0, st>>>(P);
+    if constexpr (S <= kMaxModuli) {
+        if (cplx) {
+            crt_kernel<S, true><<<static_cast<unsigned>(blocks), 256, 0, st>>>(P);
+            return;
+        }
+    }
+    crt_kernel<S, false><<<static_cast<unsigned>(blocks), 256, 0, st>>>(P);
 }
 
 template <int S>
 void crt_dispatch(int s, const CrtParams& P, int64_t blocks, bool cplx, cudaStream_t st) {
-    if constexpr (S <= kMaxModuli) {
+    if constexpr (S <= kMaxModuliExt) {
         if (s == S) return crt_launch_s<S>(P, blocks, cplx, st);
         crt_dispatch<S + 1>(s, P, blocks, cplx, st);
     }

@@ -74,7 +74,7 @@ struct SplitItem {
     int8_t* planes;                     // s planes (complex: 3 groups of s)
     int64_t plane_bytes, kb_total, rows_pad;
     int64_t block0, rblocks, kblocks;   // blocks = rblocks * kblocks
-    ModConst mc[kMaxModuli];
+    ModConst mc[kMaxModuliExt];
 };
 
 // ---- gemm: one item per problem; jobs = groups * s * tiles, each job runs all k chunks
@@ -87,8 +87,8 @@ struct GemmItem {
     int64_t pstride_i, pstride_j, rstride, ldr, m, n, kb_total;
     int64_t tiles, job0;
     int tiles_i, tiles_j, s, groups;
-    uint32_t mod_m[kMaxModuli], mod_mu[kMaxModuli], mod_kbias[kMaxModuli];
-    uint32_t mod_kbias30[kMaxModuli], mod_mx31[kMaxModuli];  // exact quotient, kb_total <= kExactKB
+    uint32_t mod_m[kMaxModuliExt], mod_mu[kMaxModuliExt], mod_kbias[kMaxModuliExt];
+    uint32_t mod_kbias30[kMaxModuliExt], mod_mx31[kMaxModuliExt];  // exact quotient, kb_total <= kExactKB
     // Ozaki-I mode only: job index t is the digit pair (pair_a[t], pair_b[t]) on anti-diagonal
     // pair_d[t]; the int32 products are added into acc[d][i acc_ld + j] (int64)
     int64_t* acc;

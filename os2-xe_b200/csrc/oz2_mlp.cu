@@ -1,6 +1,6 @@
 // oz2_mlp.cu - the small MLP that picks the number of moduli per C tile: inference (one thread
 // per tile, weights in shared memory) and training (one block, mini-batches of 256 samples,
-// cross-entropy over s = 2..24, Adam), both hand-written.
+// cross-entropy over s = 2..24 and "more than 24", Adam), both hand-written.
 #include <cmath>
 
 #include "oz2_adaptive.cuh"

@@ -161,7 +161,7 @@ extern "C" int oz2_dgemm_noalloc(void* stream, char ta, char tb, int64_t m, int6
 
     // item tables (one problem), written into the scratch by a kernel that takes them as its
     // parameter: host memory only, no staging buffer
-    ModConst mc[kMaxModuli];
+    ModConst mc[kMaxModuliExt];
     mod_constants(p, mc);
     struct Tables {
         ScaleItem sc[2];

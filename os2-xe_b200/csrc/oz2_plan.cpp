@@ -15,6 +15,11 @@ constexpr uint16_t kSeqSmall[6] = {256, 255, 253, 251, 247, 241};
 constexpr uint16_t kSeqMid[13] = {256, 253, 251, 249, 247, 245, 241, 239, 233, 229, 227, 223, 211};
 constexpr uint16_t kSeqLarge[24] = {256, 253, 251, 249, 247, 241, 239, 235, 233, 229, 227, 223,
                                     217, 211, 199, 197, 193, 191, 181, 179, 173, 167, 163, 157};
+// Extended sets (s = 25..32, the adaptive path only; no counterpart in the reference): prefixes of
+// the greedy sequence of pairwise-coprime integers <= 256 taken from the top (each the largest
+// one coprime with all before it), so M grows by the most a further modulus can give.
+constexpr uint16_t kSeqExt[32] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 217, 211, 199, 197, 193,
+                                  191, 181, 179, 173, 167, 163, 157, 151, 149, 139, 137, 131, 127, 113, 109, 107};
 
 struct Big {
     uint32_t w[kBigWords] = {};
@@ -97,15 +102,15 @@ uint32_t pow2_mod(int e, uint32_t m) {
 namespace {
 // everything of a plan but tk depends on s alone: built once per s
 struct Templates {
-    Plan plan[kMaxModuli + 1];
-    int status[kMaxModuli + 1];
+    Plan plan[kMaxModuliExt + 1];
+    int status[kMaxModuliExt + 1];
     Templates() {
-        for (int s = 2; s <= kMaxModuli; ++s) status[s] = build(s, plan[s]);
+        for (int s = 2; s <= kMaxModuliExt; ++s) status[s] = build(s, plan[s]);
     }
     static int build(int s, Plan& p) {
         p = Plan{};
         p.s = s;
-        const uint16_t* seq = s <= 6 ? kSeqSmall : (s <= 13 ? kSeqMid : kSeqLarge);
+        const uint16_t* seq = s <= 6 ? kSeqSmall : (s <= 13 ? kSeqMid : (s <= kMaxModuli ? kSeqLarge : kSeqExt));
         Big M = Big::of(1);
         for (int t = 0; t < s; ++t) {
             p.m[t] = seq[t];
@@ -136,15 +141,17 @@ const Templates& templates() {
 }  // namespace
 
 int plan_tk(int s, int64_t k) {
-    if (s < 2 || s > kMaxModuli || k < 1) return 0;
+    if (s < 2 || s > kMaxModuliExt || k < 1) return 0;
     const Templates& T = templates();
     if (T.status[s]) return 0;
     const Plan& p = T.plan[s];
     Big M;
     std::memcpy(M.w, p.M, sizeof M.w);
-    // largest tk <= 100 with k 2^(2 tk + 2) <= M, so that |x| <= M/4 for every result entry
+    // largest tk <= 100 (124 for the extended sets) with k 2^(2 tk + 2) <= M, so that |x| <= M/4 for
+    // every result entry
     int tk = static_cast<int>(std::floor((p.log2M - 2.0 - std::log2(static_cast<double>(k))) / 2.0));
-    if (tk > kMaxScaleBits) tk = kMaxScaleBits;
+    const int cap = s <= kMaxModuli ? kMaxScaleBits : kMaxScaleBitsExt;
+    if (tk > cap) tk = cap;
     for (;; --tk) {
         if (tk < 1) return 0;
         Big lhs = Big::of(static_cast<uint64_t>(k));
@@ -153,16 +160,22 @@ int plan_tk(int s, int64_t k) {
     }
 }
 
-int make_plan(int s, int64_t k, Plan& p) {
-    if (s < 2 || s > kMaxModuli || k < 1) return 1;
+int make_plan_ext(int s, int64_t k, Plan& p) {
+    if (s < 2 || s > kMaxModuliExt || k < 1) return 1;
     const Templates& T = templates();
     if (T.status[s]) return T.status[s];
     const int tk = plan_tk(s, k);
     if (tk < 1) return 1;
-    if (tk > kWideScaleBits) return 5;  // never for the tables above (largest tk 91 at s = 24)
+    // never for the tables above: the largest tk is 91 at s = 24 and 118 at s = 32
+    if (tk > (s <= kMaxModuli ? kWideScaleBits : kMaxScaleBitsExt)) return 5;
     p = T.plan[s];
     p.tk = tk;
     return 0;
+}
+
+int make_plan(int s, int64_t k, Plan& p) {
+    if (s < 2 || s > kMaxModuli || k < 1) return 1;
+    return make_plan_ext(s, k, p);
 }
 
 const char* plan_error_text(int s, int64_t k, int status, char* buf, int len) {
@@ -188,6 +201,7 @@ void mod_constants(const Plan& p, ModConst* out) {
         c.h = h;
         c.koff3 = (h + m - pow2_mod(62, m)) % m;
         c.koff5 = (h + m - pow2_mod(93, m)) % m;
+        c.koff7 = (h + m - pow2_mod(125, m)) % m;
         c.kbias = m * static_cast<uint32_t>(((uint64_t{1} << 31) + m - 1) / m);
         c.kbias30 = m * ((kExactSum + m - 1) / m);
         // Granlund and Montgomery (1994): with M = ceil(2^39 / m) = (2^39 + e) / m, e < m <= 2^8,

@@ -13,18 +13,26 @@
 
 namespace oz2 {
 
-constexpr int kMaxModuli = 24;
+constexpr int kMaxModuli = 24;     // the reference's range of s (Ozaki2::gemm / zgemm)
+// The adaptive path (no counterpart in the reference) may go further, to s = 32, with moduli sets
+// of its own: tiles whose certified error bound needs more than the 91 bits per element of 24
+// moduli run emulated instead of in native FP64.
+constexpr int kMaxModuliExt = 32;
 constexpr int kBigWords = 8;       // 256-bit host integers
-constexpr int kMaxLimbs = 6;       // 32-bit limbs of M for s <= 24
-constexpr int kMaxScaleBits = 100;
+constexpr int kMaxLimbs = 8;       // 32-bit limbs of M for s <= 32
+constexpr int kMaxScaleBits = 100;     // tk cap of the reference's plans (s <= 24)
+constexpr int kMaxScaleBitsExt = 124;  // tk cap of the extended plans (s = 25..32)
 constexpr int kNarrowScaleBits = 62;
-// the split's wide offset (2^93 in three 32-bit words) holds |x| <= 2^92; every plan has tk <= 91
+// the split's wide offset (2^93 in three 32-bit words) holds |x| <= 2^92; every plan with
+// s <= 24 has tk <= 91
 constexpr int kWideScaleBits = 92;
+// the widest offset (2^125 in four 32-bit words) holds |x| <= 2^124 (extended plans)
 constexpr int kNonFinite = -2147483647 - 1;
 
 // 32-bit limbs of M per s: max(2, floor(log2 M / 32) + 1) (ref src/ozaki2_gpu.hpp:55-59, :168)
 OZ2_HD constexpr int limbs_for(int s) {
-    constexpr int t[kMaxModuli + 1] = {0, 0, 2, 2, 2, 2, 2, 2, 2, 3, 3, 3, 3, 4, 4, 4, 4, 5, 5, 5, 5, 6, 6, 6, 6};
+    constexpr int t[kMaxModuliExt + 1] = {0, 0, 2, 2, 2, 2, 2, 2, 2, 3, 3, 3, 3, 4, 4, 4, 4,
+                                          5, 5, 5, 5, 6, 6, 6, 6, 6, 7, 7, 7, 7, 8, 8, 8};
     return t[s];
 }
 
@@ -40,6 +48,7 @@ struct ModConst {
     uint32_t h;      // (m - 1) / 2: residues are kept symmetric in [-h, m-1-h]
     uint32_t koff3;  // (h - 2^62 mod m) mod m: narrow offset (tk <= 62)
     uint32_t koff5;  // (h - 2^93 mod m) mod m: wide offset
+    uint32_t koff7;  // (h - 2^125 mod m) mod m: widest offset (extended plans)
     uint32_t kbias;  // m ceil(2^31 / m): c + kbias is in [0, 2^32) for every int32 GEMM sum c
                      // (|c| < 2^31 - 2^21) and congruent to c modulo m
     uint32_t kbias30;  // m ceil(kExactSum / m): c + kbias30 is in [0, 2^31) for every int32 GEMM sum
@@ -54,17 +63,19 @@ struct Plan {
     int nl = 0;
     int tk = 0;
     double log2M = 0;
-    uint32_t m[kMaxModuli] = {};
-    uint32_t y[kMaxModuli] = {};             // (M/m_t)^-1 mod m_t
-    uint32_t W[kMaxModuli][kBigWords] = {};  // CRT weights (M/m_t) y_t
+    uint32_t m[kMaxModuliExt] = {};
+    uint32_t y[kMaxModuliExt] = {};             // (M/m_t)^-1 mod m_t
+    uint32_t W[kMaxModuliExt][kBigWords] = {};  // CRT weights (M/m_t) y_t
     uint32_t M[kBigWords] = {};
-    ModConst mc[kMaxModuli] = {};            // per-modulus kernel constants (mod_constants)
+    ModConst mc[kMaxModuliExt] = {};            // per-modulus kernel constants (mod_constants)
 };
 
 // Returns 0, or 1 (invalid: s out of [2, 24], k < 1, s too small for k), or 5 (overflow).
 // ref src/ozaki2_gpu.hpp:159-200
 int make_plan(int s, int64_t k, Plan& p);
-// tk of make_plan(s, k), or 0 where that plan is invalid (s too small for k)
+// the same for s in [2, 32]: the reference's plans for s <= 24, the extended sets above
+int make_plan_ext(int s, int64_t k, Plan& p);
+// tk of make_plan_ext(s, k), or 0 where that plan is invalid (s too small for k)
 int plan_tk(int s, int64_t k);
 const char* plan_error_text(int s, int64_t k, int status, char* buf, int len);
 
@@ -72,7 +83,7 @@ void mod_constants(const Plan& p, ModConst* out);
 
 // CRT table: Sum_t r_t W_t - q M with q = round(Sum_t r_t y_t / m_t) from an estimate whose
 // error is far below 1/4 (ref src/ozaki2_gpu.hpp:526-588 uses FP32; here 24-bit fixed point)
-constexpr int kQuads = (kMaxModuli + 3) / 4;  // moduli in groups of four (one residue byte each)
+constexpr int kQuads = (kMaxModuliExt + 3) / 4;  // moduli in groups of four (one residue byte each)
 
 struct CrtConst {
     int s, nl;
@@ -82,7 +93,8 @@ struct CrtConst {
     // for 4g+2, 4g+3 (zero past s)
     uint32_t Wq[kQuads][2 * kMaxLimbs][2];
     // F16_t = min(round(y_t / m_t 2^16), 2^16 - 1), paired the same way: fixed-point quotient
-    // weights (error per term below 2^-16, so the quotient estimate is off by less than 0.1)
+    // weights (error per term below 2^-16, so for s <= 32 the quotient estimate is off by less than
+    // 1/8, inside the 1/4 margin that |x| <= M/4 leaves)
     uint32_t Fq[kQuads][2];
 };
 void crt_constants(const Plan& p, CrtConst& out);

@@ -120,13 +120,36 @@ __device__ __forceinline__ void offset_words_fp_wide(double v, double s1, double
     W[2] = static_cast<uint32_t>(oh);
 }
 
+// Widest path (92 < tk <= 124, the extended moduli sets of the adaptive path): as the wide path
+// with a = |rint(y)| <= 2^124, hi = trunc(a 2^-64) < 2^60, and the offset 2^125 +- (hi:lo), which
+// lies in (0, 2^126), as four 32-bit words.
+__device__ __forceinline__ void offset_words_fp_widest(double v, double s1, double s2, uint32_t (&W)[4]) {
+    const double y = rint((v * s1) * s2);
+    const double a = fabs(y);
+    const double hd = trunc(a * 5.421010862427522e-20);     // 2^-64
+    const double ld = fma(hd, -18446744073709551616.0, a);  // a - hd 2^64, exact
+    const uint64_t hi = __double2ull_rz(hd), lo = __double2ull_rz(ld);
+    uint64_t ol, oh;
+    if (y < 0.0) {
+        ol = 0 - lo;
+        oh = (1ull << 61) - hi - (lo != 0 ? 1 : 0);
+    } else {
+        ol = lo;
+        oh = (1ull << 61) + hi;
+    }
+    W[0] = static_cast<uint32_t>(ol);
+    W[1] = static_cast<uint32_t>(ol >> 32);
+    W[2] = static_cast<uint32_t>(oh);
+    W[3] = static_cast<uint32_t>(oh >> 32);
+}
+
 // (x + h) mod m in [0, m) from the bytes of the offset integer: v = koff + sum_l byte_l (2^(8 l)
-// mod m) by byte dot products (at most 12 bytes, so v < 255 + 12 255^2 < 2^20), then the exact
-// multiply-high quotient by ceil(2^32 / m). Two (three) dot products, one multiply-high and one
-// multiply-subtract per residue.
+// mod m) by byte dot products (at most 16 bytes, so v < 255 + 16 255^2 < 2^20), then the exact
+// multiply-high quotient by ceil(2^32 / m). Two (three, four) dot products, one multiply-high
+// and one multiply-subtract per residue.
 template <int NW>
 __device__ __forceinline__ uint32_t byte_residue(const uint32_t (&W)[NW], const ModConst& c) {
-    uint32_t v = NW == 2 ? c.koff3 : c.koff5;
+    uint32_t v = NW == 2 ? c.koff3 : (NW == 3 ? c.koff5 : c.koff7);
 #pragma unroll
     for (int j = 0; j < NW; ++j) v = __dp4a(W[j], c.cb[j], v);
     return v - __umulhi(v, c.m32) * c.m;
@@ -137,7 +160,8 @@ __device__ __forceinline__ uint32_t pack_bytes(uint32_t a, uint32_t b, uint32_t 
     return __byte_perm(__byte_perm(a, b, 0x0040), __byte_perm(c, d, 0x0040), 0x5410);
 }
 
-// NLIMB: 3 selects the narrow path (two words per offset integer), 5 the wide one (three words).
+// NLIMB: 3 selects the narrow path (two words per offset integer), 5 the wide one (three words),
+// 7 the widest (four words; real operands only: the complex path keeps s <= 24).
 // Elements per thread: 16 (one 16-byte chunk of every plane) on the real narrow path; 8 (half a
 // chunk) on the wide path (16 measured no faster) and for complex inputs (two groups of words)
 constexpr int kSplitRowcK = 256;  // inner indices per block of the rows-contiguous split
@@ -206,7 +230,7 @@ __global__ void __launch_bounds__(256) split_kernel(const SplitItem* __restrict_
     const bool live = e != kNonFinite;
 
     constexpr int NG = CPLX ? 2 : 1;
-    constexpr int NW = NLIMB == 3 ? 2 : 3;  // 32-bit words of the offset integer
+    constexpr int NW = NLIMB == 3 ? 2 : (NLIMB == 5 ? 3 : 4);  // 32-bit words of the offset integer
     uint32_t L[NG][EPT][NW];
     const int e1 = e >> 1;
     const double s1 = pow2(live ? e1 : 0), s2 = pow2(live ? e - e1 : 0);
@@ -227,9 +251,11 @@ __global__ void __launch_bounds__(256) split_kernel(const SplitItem* __restrict_
         if constexpr (NLIMB == 3) {
             offset_words_fp(v0, s1, s2, L[0][q]);
             if (CPLX) offset_words_fp(v1, s1, s2, L[NG - 1][q]);
-        } else {
+        } else if constexpr (NLIMB == 5) {
             offset_words_fp_wide(v0, s1, s2, L[0][q]);
             if (CPLX) offset_words_fp_wide(v1, s1, s2, L[NG - 1][q]);
+        } else {
+            offset_words_fp_widest(v0, s1, s2, L[0][q]);
         }
     }
 
@@ -237,7 +263,7 @@ __global__ void __launch_bounds__(256) split_kernel(const SplitItem* __restrict_
         const ModConst mc = I->mc[t];
         uint32_t b0[EPT], b1[EPT], b2[EPT];  // residue bytes in the low 8 bits
         if (mc.m == 256) {
-            // 2^62 = 2^93 = 0 mod 256: the residue byte is the low byte of the offset integer
+            // 2^62 = 2^93 = 2^125 = 0 mod 256: the residue byte is the low byte of the offset integer
 #pragma unroll
             for (int q = 0; q < EPT; ++q) {
                 b0[q] = L[0][q][0];
@@ -397,6 +423,10 @@ void launch_slice(const SplitItem* d, const SplitItem* h, int count, int64_t blo
 void launch_split(const SplitItem* d, const SplitItem* h, int count, int64_t blocks, cudaStream_t st) {
     if (count <= 0 || blocks <= 0) return;
     const bool wide = h[0].tk > kNarrowScaleBits, rowc = h[0].row_contig != 0;
+    if (h[0].tk > kWideScaleBits) {  // extended sets: real operands only
+        split_dispatch<7, false>(d, count, blocks, rowc, st);
+        return;
+    }
     if (h[0].cplx) {
         if (wide) split_dispatch<5, true>(d, count, blocks, rowc, st);
         else split_dispatch<3, true>(d, count, blocks, rowc, st);

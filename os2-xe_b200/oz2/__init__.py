@@ -18,7 +18,8 @@ LIB_PATH = os.path.join(HERE, "liboz2.so")
 
 OK, EINVAL, ENOMEM, EINTERNAL, ETIMEOUT, EOVERFLOW, ECUDA = range(7)
 K_MAX_MODULI = 24
-NATIVE_S = 25  # adaptive s of a tile run as a native FP64 GEMM
+K_MAX_MODULI_EXT = 32  # the adaptive path's extended sets (s = 25..32, no counterpart in the reference)
+NATIVE_S = 33  # adaptive s of a tile run as a native FP64 GEMM
 
 if not os.path.exists(LIB_PATH):
     raise ImportError(f"{LIB_PATH} is not built: run python os2-xe_b200/build.py")
@@ -64,6 +65,8 @@ _lib.oz2_autotune_grouped.argtypes = [_vp, _i32, C.POINTER(DgemmProblem), C.POIN
 _lib.oz2_dgemm_adaptive.argtypes = [_vp, _i32, C.POINTER(DgemmProblem), _i32, _i32, C.POINTER(_i64)]
 _lib.oz2_set_adaptive_options.argtypes = [_vp, _i32, C.c_float]
 _lib.oz2_adaptive_stage_times.argtypes = [_vp, C.POINTER(_dbl)]
+_lib.oz2_adaptive_gemm_bytes.argtypes = [_vp, C.POINTER(_i64)]
+_lib.oz2_set_probe_kind.argtypes = [_vp, _i32]
 _lib.oz2_mlp_info.argtypes = [C.POINTER(_i32)]
 _lib.oz2_mlp_set_weights.argtypes = [_vp, _vp, _i32]
 _lib.oz2_mlp_train.argtypes = [_vp, _i32, _vp, _vp, _i32, C.c_float, C.c_uint, _vp, _vp]
@@ -304,7 +307,7 @@ class Ozaki2:
         """problems as for gemm_grouped (num_moduli is used by mode 3 only). Returns the stats
         dict: tiles, sum_s (emulated tiles, reruns included), probed, rerun, rerun_sum_s,
         analytic_sum_s (the judge's s summed: the analytic s, or in modes 0, 4 and 5 the smaller of
-        the analytic and certified s; 25 counts a native tile), mlp, int8_macs (sum of s m_t n_t k
+        the analytic and certified s; 33 counts a native tile), mlp, int8_macs (sum of s m_t n_t k
         over emulated tiles), native_tiles, native_macs (tiles run as native FP64 GEMMs)."""
         arr = self._problems(problems)
         st = (_i64 * 10)()
@@ -318,6 +321,20 @@ class Ozaki2:
         out = (_dbl * 2)()
         _raise(_lib.oz2_adaptive_stage_times(self._h, out), self._h)
         return {"probe_ms": out[0], "native_ms": out[1]}
+
+    def adaptive_gemm_bytes(self):
+        """{plane_bytes, residue_bytes, batches} of the last gemm_adaptive's INT8 GEMM launches"""
+        out = (_i64 * 3)()
+        _raise(_lib.oz2_adaptive_gemm_bytes(self._h, out), self._h)
+        return {"plane_bytes": out[0], "residue_bytes": out[1], "batches": out[2]}
+
+    PROBE_COLUMNS, PROBE_FREIVALDS, PROBE_BOTH, PROBE_NONE = 0, 1, 2, 3
+
+    def set_probe_kind(self, kind):
+        """mode 0's probe: PROBE_COLUMNS (8 columns entry by entry), PROBE_FREIVALDS (C x against
+        alpha A (B x) in double-double, two random vectors), PROBE_BOTH, or PROBE_NONE (the MLP's s
+        unchecked: for measuring what the probes catch)"""
+        _raise(_lib.oz2_set_probe_kind(self._h, int(kind)), self._h)
 
     def set_adaptive_options(self, tile=512, threshold=0.9):
         _raise(_lib.oz2_set_adaptive_options(self._h, tile, threshold), self._h)

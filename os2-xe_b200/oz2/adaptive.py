@@ -4,8 +4,9 @@ Labels come from the emulator itself: for a sample tile (512 x 512 x k, or an ed
 fewer rows or columns, of a problem with inputs (u - 0.5) exp(phi g), per-row / per-column
 exponent offsets), the label is the smallest s whose result meets the DGEMM-level target, every
 entry within k 2^-53 (|A||B|)_ij of the exact product, measured against the library's
-double-double reference (oz2_dd_reference); 25 when no s <= 24 does (the tile runs as a native
-FP64 GEMM). Features are the
+double-double reference (oz2_dd_reference); 25 when no s <= 24 does (the MLP's last class: "more
+than 24", which the library resolves with its judge, up to the extended sets' s = 32 or native
+FP64). Features are the
 library's own tile features (oz2_tile_features). Training runs the hand-written CUDA kernel
 (oz2_mlp_train). The model is saved as JSON: parameters, decision threshold, tile, provenance.
 """
@@ -112,7 +113,7 @@ NATIVE_COST = 36.0  # a native FP64 tile costs about as much as 36 moduli of emu
 
 
 def tile_cost(s):
-    return NATIVE_COST if s > 24 else float(s)
+    return NATIVE_COST if s > 32 else float(s)
 
 
 def evaluate(oz, params, feats, labels, s_an, thresholds=THRESHOLDS):

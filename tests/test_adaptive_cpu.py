@@ -34,8 +34,15 @@ def test_analytic_s_rule(oracle):
     # R = 0: need tk >= 2 + 53 - 9 = 46
     s0 = ao.analytic_s(tk, 0, k)
     assert tk[s0] >= 46 and tk[s0 - 1] < 46
-    # beyond what 24 moduli give: native FP64
-    assert ao.analytic_s(tk, 63, k) == 25
+    # the last gap bin (63 binades or more) bounds nothing: native FP64
+    assert ao.analytic_s(tk, 63, k) == ao.NATIVE == 33
+    # beyond what 24 moduli give: the extended sets (tk 85 at s = 24 for k = 1024)
+    s1 = ao.analytic_s(tk, 45, k)
+    assert 24 < s1 <= 32 and tk[s1] >= 45 + 2 + 53 - 9 > tk[24]
+    # the extended plans follow the reference's tk rule, with M from the library's own sets
+    for s in range(25, 33):
+        p = oracle.plan_ext(s, k)
+        assert p.tk == tk[s] and k * 2 ** (2 * p.tk + 2) <= p.Mint < k * 2 ** (2 * p.tk + 4)
     assert ao.floor_log2_km1(1) == 0 and ao.floor_log2_km1(2) == 0 and ao.floor_log2_km1(1025) == 10
 
 
