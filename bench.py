@@ -43,6 +43,9 @@ TARGET_BITS = 53
 MAX_BATCH = 512          # problems per step: inputs, outputs and the check's references of a batch
 WORKSPACE = 24 << 30     # workspace limit of the bench's handle (the same for every form)
 E2E_BATCH = 64           # problems per step of the end-to-end leg (pinned host arenas)
+# DRAM bytes / algorithmic bytes of the residue GEMM on this stream, from one ncu capture of a
+# small case (profiles/gemm_i8_modm_kernel_traffic_adaptive_stream.md): 44.35 GB over 44.37 GB
+GEMM_TRAFFIC_RATIO = 0.9994
 
 
 def parse():
@@ -951,7 +954,11 @@ def main():
                          "unit": "TOPS (int8)", "frac": achieved / peak, "peak_note": note,
                          "algorithmic": "2 s m_t n_t k int8 ops per tile (reruns included), summed over the steps",
                          "algorithmic_bytes_per_launch": (gbytes[0] + gbytes[1]) / max(gbytes[2], 1),
-                         "launches": gbytes[2], "traffic": None},
+                         "launches": gbytes[2],
+                         "traffic": GEMM_TRAFFIC_RATIO * (gbytes[0] + gbytes[1]) / max(gbytes[2], 1),
+                         "traffic_note": "DRAM bytes per launch: the measured DRAM/algorithmic ratio of an ncu "
+                                         "capture of a small case of this stream times this run's algorithmic "
+                                         "bytes per launch (planes read once, residues written)"},
             "stage_ms_first_batch_by_form": by_form,
             "fixed_s": fixed,
             "error_check": {"bound": "|C - AB| <= k 2^-53 (|A||B|)_ij against a double-double product, per entry; "

@@ -47,7 +47,7 @@ def build(jobs=8, verbose_ptxas=False, quiet=True):
         for _, log in results:
             sys.stderr.write(log)
     if not os.path.exists(OUT) or any(os.path.getmtime(o) > os.path.getmtime(OUT) for o in objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-ccbin", HOST_CXX, "-o", OUT] + objs + ["-lcuda", "-lcublas"]
+        cmd = [NVCC] + ARCH + ["-shared", "-ccbin", HOST_CXX, "-Xlinker", "--no-undefined", "-o", OUT] + objs + ["-lcuda", "-lcublas"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

@@ -428,6 +428,7 @@ void plan_tasks(Program& prog, const std::vector<Task>& tasks, const GemmConfig&
             g.mod_kbias[q] = mc[q].kbias;
             g.mod_kbias30[q] = mc[q].kbias30;
             g.mod_mx31[q] = mc[q].mx31;
+            g.mod_mxs[q] = mc[q].mxs;
         }
         jobs += g.tiles * p.G * g.s;
         gi.push_back(g);
@@ -464,6 +465,7 @@ void plan_tasks(Program& prog, const std::vector<Task>& tasks, const GemmConfig&
         c.br = p.beta[0];
         c.bi = p.beta[1];
         c.C = p.C + w * (t.i0 + t.j0 * p.ldc);
+        c.mma = crt_uses_mma(*p.plan, cplx) ? 1 : 0;
         auto& grp = crt_groups[{p.plan->s, cplx}];
         grp.first = p.plan;
         grp.second.push_back(c);
@@ -620,7 +622,7 @@ void issue(oz2_context* h, const Program& prog, const unsigned char* dev) {
                 break;
             case Op::Crt:
                 launch_crt(reinterpret_cast<const CrtItem*>(dev + op.off), op.count, op.blocks, *op.plan, op.cplx,
-                           h->stream);
+                           h->d_err, h->stream);
                 break;
             case Op::ScaleC: launch_scale_c(static_cast<double*>(op.ptr), op.ldc, op.m, op.n, op.beta, op.cplx, h->stream); break;
             case Op::Mark: mark(h, op.stage); break;

@@ -10,6 +10,7 @@
 #include <cstring>
 
 #include "oz2_kernels.cuh"
+#include "oz2_ptx.cuh"
 
 namespace oz2 {
 namespace {
@@ -43,6 +44,9 @@ __device__ __forceinline__ double scale_pow2(double d, int E) {
 // 0.1, inside the 1/4 margin that |x| <= M/4 leaves, so q is the reference's FP32 quotient),
 // and Sum r_t W_t limb by limb over 16-bit limbs of W_t (each limb sum below 24 * 255 * 2^16 <
 // 2^29), then x = Sum r_t W_t - q M modulo 2^(32 NL) in 64-bit words, rounded once to double.
+template <int NL>
+__device__ __forceinline__ double crt_finish(const uint64_t (&acc)[NL], int64_t q, const uint32_t* Mw, int shift);
+
 template <int S, int NL>
 __device__ __forceinline__ double crt_value(const uint32_t (&R)[(S + 3) / 4], const CrtConst& cc, int shift) {
     constexpr int Q = (S + 3) / 4;
@@ -66,11 +70,19 @@ __device__ __forceinline__ double crt_value(const uint32_t (&R)[(S + 3) / 4], co
         }
         acc[l] = static_cast<uint64_t>(a0) + (static_cast<uint64_t>(a1) << 16);
     }
+    return crt_finish<NL>(acc, q, cc.M, shift);
+}
+
+// From the 32-bit limb sums acc[l] = sum_t r_t W_t[l] (below 2^46) and the quotient q: x = sum_t
+// r_t W_t - q M modulo 2^(32 NL) in 64-bit words (|x| <= M/4, two's complement), its magnitude's
+// leading 64 bits with a sticky bit for the rest, one RNE to double, 2^-shift.
+template <int NL>
+__device__ __forceinline__ double crt_finish(const uint64_t (&acc)[NL], int64_t q, const uint32_t* Mw, int shift) {
     uint32_t w[NL];
     int64_t carry = 0;
 #pragma unroll
     for (int l = 0; l < NL; ++l) {
-        const int64_t v = static_cast<int64_t>(acc[l]) - q * static_cast<int64_t>(cc.M[l]) + carry;
+        const int64_t v = static_cast<int64_t>(acc[l]) - q * static_cast<int64_t>(Mw[l]) + carry;
         w[l] = static_cast<uint32_t>(v);
         carry = v >> 32;
     }
@@ -231,6 +243,197 @@ __global__ void __launch_bounds__(256) crt_kernel(const __grid_constant__ CrtPar
     }
 }
 
+// ---------------------------------------------------------------- tensor-core CRT (real, 8 limbs)
+// The limb sums sum_t r_t W_t are a small integer matrix product: per entry e, D[e][b] = sum_t
+// r_et Wb[t][b] with r_et the residue bytes and Wb[t][b] byte b of W_t (b < 4 NL), plus two
+// columns of the 16-bit quotient fractions F16_t (low and high byte). One tcgen05.mma kind::i8
+// (unsigned bytes, M = 128 entries, N = 64 columns, K = 32 moduli, zero-padded) computes them
+// for 128 entries: every sum is below 32 * 255^2 < 2^21, exact in the int32 accumulators. The
+// threads then do only the carry chain and the rounding of the dp2a kernel (crt_finish), so the
+// results are the same bits; the integer-multiply pipe, which bounds the dp2a kernel, is left
+// to the few 64-bit products of the carry chain.
+// A CTA is 4 warps; a tile is 32 rows i x 4 columns j (warp q: column j0 + q, its lanes the
+// rows: TMEM lane 32 q + l is entry (i0 + l, j0 + q), so each warp stores 32 consecutive C
+// entries of a column). Persistent over the tiles of all items of the launch.
+constexpr int kCrtN = 64;                               // MMA N: 4 NL limb bytes + 2 quotient bytes
+constexpr uint32_t kCrtIdesc = (2u << 4)                  // D: s32; A, B: unsigned 8-bit, K-major
+                               | (static_cast<uint32_t>(kCrtN >> 3) << 17) | (static_cast<uint32_t>(128 >> 4) << 24);
+constexpr int kCrtSmem = 1024 + 2 * 128 * 128 + kCrtN * 128 + 64;  // align slack, two A tiles, B, barriers + slot
+
+struct CrtMmaParams {
+    const CrtItem* items;
+    int count;
+    int64_t tiles;
+    int s, nl;
+    uint32_t M[kMaxLimbs];
+    alignas(16) uint8_t wb[kCrtN][32];  // B operand rows: byte b of W_t for t = 0..31 (zero past s); F16 bytes at 4 nl, 4 nl + 1
+    int* err;
+    uint64_t wait_ns;
+};
+
+// the residue words of one tile for this thread: column j0 + warp, rows i0 + 4 (lane % 8) .. + 3,
+// moduli 8 (lane / 8) .. + 7 (one 32-bit word = 4 rows per modulus; zero past s or n)
+struct TileRef {
+    const CrtItem* I;
+    int64_t i0, j0;
+};
+__device__ __forceinline__ void crt_tile_load(const TileRef& T, int s, uint32_t (&wv)[8]) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t j = T.j0 + warp, n = T.I->n;
+    const int rq = lane & 7, mg = lane >> 3;
+    const uint8_t* base = T.I->resid + (T.i0 >> 5) * (32 * n) + j * 32 + 4 * rq;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+        const int t = 8 * mg + u;
+        wv[u] = j < n && t < s ? __ldg(reinterpret_cast<const uint32_t*>(base + t * T.I->rstride)) : 0u;
+    }
+}
+// the words regrouped per entry (4 x 4 byte transposes), 8 bytes per entry into its 128-byte
+// swizzled K-major row (K bytes 8 (lane / 8) .. + 7)
+__device__ __forceinline__ void crt_tile_store(uint8_t* sA, const uint32_t (&wv)[8]) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int rq = lane & 7, mg = lane >> 3;
+    uint32_t lo[4], hi[4];
+    transpose4(wv[0], wv[1], wv[2], wv[3], lo);
+    transpose4(wv[4], wv[5], wv[6], wv[7], hi);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int e = 32 * warp + 4 * rq + u;
+        const int c = mg >> 1;  // 16-byte chunk of the 32 K bytes
+        *reinterpret_cast<uint2*>(sA + e * 128 + ((c ^ (e & 7)) << 4) + 8 * (mg & 1)) = make_uint2(lo[u], hi[u]);
+    }
+}
+
+// Software-pipelined over the CTA's tiles: while the MMA of tile k runs, the threads load tile
+// k + 1's residues into registers and finish tile k - 1 from the other accumulator (two A tiles,
+// two 64-column accumulators, two barriers).
+template <int NL>
+__global__ void __launch_bounds__(128) crt_mma_kernel(const __grid_constant__ CrtMmaParams P) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t{1023});
+    uint8_t* sA0 = smem;                      // two 128 rows x 128 B tiles, K-major, 128-byte swizzle
+    uint8_t* sB = smem + 2 * 128 * 128;       // kCrtN rows x 128 B
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sB + kCrtN * 128);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 2);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x < kCrtN) {  // B: the W bytes of the plan (only the 32 K bytes of each row are read)
+        const int b = threadIdx.x;
+        const uint4* src = reinterpret_cast<const uint4*>(P.wb[b]);
+#pragma unroll
+        for (int c = 0; c < 2; ++c) *reinterpret_cast<uint4*>(sB + b * 128 + ((c ^ (b & 7)) << 4)) = src[c];
+    }
+    if (threadIdx.x == 0) {
+        dev::mbar_init(dev::smem_addr(bar), 1);
+        dev::mbar_init(dev::smem_addr(bar + 1), 1);
+        *abort_flag = 0;
+        dev::fence_barrier_init();
+    }
+    if (warp == 0) {
+        dev::tmem_alloc(dev::smem_addr(tmem_slot), 2 * kCrtN);
+        dev::tmem_relinquish();
+    }
+    dev::tc_fence_before();
+    __syncthreads();
+    dev::tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    int item = 0;
+    {  // the item of this CTA's first tile; later tiles only move forward
+        int hi = P.count - 1;
+        while (item < hi) {
+            const int mid = (item + hi + 1) >> 1;
+            if (P.items[mid].block0 <= static_cast<int64_t>(blockIdx.x)) item = mid;
+            else hi = mid - 1;
+        }
+    }
+    auto tile_ref = [&](int64_t tile) {
+        while (item + 1 < P.count && P.items[item + 1].block0 <= tile) ++item;
+        const CrtItem* I = P.items + item;
+        const int64_t local = tile - I->block0;
+        return TileRef{I, (local % I->iblocks) * 32, (local / I->iblocks) * 4};
+    };
+    const int64_t ntiles = P.tiles > blockIdx.x ? (P.tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    uint32_t wv[8];
+    TileRef cur{}, prev{};
+    if (ntiles > 0) {
+        cur = tile_ref(blockIdx.x);
+        crt_tile_load(cur, P.s, wv);
+    }
+    bool ok = true;
+    for (int64_t kk = 0; kk <= ntiles && ok; ++kk) {
+        const int buf = static_cast<int>(kk & 1);
+        if (kk < ntiles) {
+            crt_tile_store(sA0 + buf * 128 * 128, wv);
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        }
+        dev::tc_fence_before();
+        __syncthreads();
+        if (kk < ntiles && threadIdx.x == 0) {
+            dev::tc_fence_after();
+            dev::mma_i8(tmem + static_cast<uint32_t>(buf * kCrtN),
+                        dev::sw128_kmajor_desc(dev::smem_addr(sA0 + buf * 128 * 128)),
+                        dev::sw128_kmajor_desc(dev::smem_addr(sB)), kCrtIdesc, 0u);
+            dev::tc_commit(dev::smem_addr(bar + buf));
+        }
+        TileRef nxt{};
+        if (kk + 1 < ntiles) {  // the next tile's loads run under this iteration's waits and arithmetic
+            nxt = tile_ref(blockIdx.x + (kk + 1) * gridDim.x);
+            crt_tile_load(nxt, P.s, wv);
+        }
+        if (kk > 0) {  // finish tile kk - 1
+            const int pb = buf ^ 1;
+            const uint32_t parity = static_cast<uint32_t>(((kk - 1) >> 1) & 1);
+            const int w_ok = dev::mbar_wait(dev::smem_addr(bar + pb), parity, abort_flag, P.err,
+                                            dev::kErrTimeoutAccFull, P.wait_ns) ? 1 : 0;
+            if (!__syncthreads_and(w_ok)) {
+                ok = false;
+                break;
+            }
+            dev::tc_fence_after();
+            uint32_t d0[32], d1[32];
+            const uint32_t taddr = tmem + (static_cast<uint32_t>(32 * warp) << 16) + static_cast<uint32_t>(pb * kCrtN);
+            dev::tmem_load_32x32(taddr, d0);
+            dev::tmem_load_32x32(taddr + 32, d1);
+            dev::tmem_load_wait();
+            const CrtItem* __restrict__ I = prev.I;
+            const int64_t i = prev.i0 + lane, j = prev.j0 + warp;
+            if (i < I->m && j < I->n) {
+                uint64_t acc[NL];
+#pragma unroll
+                for (int l = 0; l < NL; ++l) {
+                    const uint32_t b0 = 4 * l < 32 ? d0[(4 * l) & 31] : d1[(4 * l) & 31];
+                    const uint32_t b1 = 4 * l + 1 < 32 ? d0[(4 * l + 1) & 31] : d1[(4 * l + 1) & 31];
+                    const uint32_t b2 = 4 * l + 2 < 32 ? d0[(4 * l + 2) & 31] : d1[(4 * l + 2) & 31];
+                    const uint32_t b3 = 4 * l + 3 < 32 ? d0[(4 * l + 3) & 31] : d1[(4 * l + 3) & 31];
+                    acc[l] = static_cast<uint64_t>(b0) + (static_cast<uint64_t>(b1) << 8) +
+                             (static_cast<uint64_t>(b2) << 16) + (static_cast<uint64_t>(b3) << 24);
+                }
+                const uint32_t f0 = 4 * NL < 32 ? d0[(4 * NL) & 31] : d1[(4 * NL) & 31];
+                const uint32_t f1 = 4 * NL + 1 < 32 ? d0[(4 * NL + 1) & 31] : d1[(4 * NL + 1) & 31];
+                const uint32_t uf = (1u << 15) + f0 + (f1 << 8);
+                const int64_t q = static_cast<int64_t>(uf >> 16);
+                const int tk = I->tk;
+                const int Ej = exponent_of(I->maxB[j], tk), De = exponent_of(I->maxA[i], tk);
+                const bool nonfinite = De == kNonFinite || Ej == kNonFinite;
+                double v = crt_finish<NL>(acc, q, P.M, nonfinite ? 0 : De + Ej);
+                if (nonfinite) v = __longlong_as_double(0x7FF8000000000000ll);
+                double* cp = I->C + i + j * I->ldc;
+                // the reference's unfused alpha*v + beta*c, one rounding per operation
+                const double av = __dmul_rn(I->ar, v);
+                *cp = I->br == 0.0 ? av : __dadd_rn(av, __dmul_rn(I->br, *cp));
+            }
+        }
+        prev = cur;
+        cur = nxt;
+    }
+    dev::tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        dev::tc_fence_after();
+        dev::tmem_dealloc(tmem, 2 * kCrtN);
+    }
+}
+
 // complex CRTs stop at s = 24 (zgemm is the reference's call); the extended sets are real only
 template <int S>
 void crt_launch_s(const CrtParams& P, int64_t blocks, bool cplx, cudaStream_t st) {
@@ -375,6 +578,10 @@ __global__ void __launch_bounds__(256) oz1_horner_kernel(const int64_t* __restri
 
 int64_t crt_item_blocks(CrtItem& it, int64_t block0) {
     it.block0 = block0;
+    if (it.mma) {  // tensor-core CRT: tiles of 32 rows x 4 columns
+        it.iblocks = ceil_div(it.m, 32);
+        return it.m > 0 ? it.iblocks * ceil_div(it.n, 4) : 0;
+    }
     const int64_t quads = ceil_div(it.m, 4);
     int tq = 1;
     while (tq < 8 && tq < quads) tq *= 2;  // a warp reads 4 columns x 32 rows: one 128-byte line per plane
@@ -384,7 +591,46 @@ int64_t crt_item_blocks(CrtItem& it, int64_t block0) {
     return it.m > 0 ? ceil_div(it.n, it.jb) * it.iblocks : 0;
 }
 
-void launch_crt(const CrtItem* d_items, int count, int64_t blocks, const Plan& plan, bool cplx, cudaStream_t st) {
+namespace {
+int sm_count() {
+    static int cached[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    if (!cached[dev]) {
+        int v = 0;
+        cached[dev] = cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && v > 0 ? v : 148;
+    }
+    return cached[dev];
+}
+}  // namespace
+
+void launch_crt(const CrtItem* d_items, int count, int64_t blocks, const Plan& plan, bool cplx, int* err,
+                cudaStream_t st) {
+    if (crt_uses_mma(plan, cplx)) {
+        if (count <= 0 || blocks <= 0) return;
+        static thread_local CrtMmaParams P;
+        P = CrtMmaParams{};
+        P.items = d_items;
+        P.count = count;
+        P.tiles = blocks;
+        P.s = plan.s;
+        P.nl = plan.nl;
+        for (int l = 0; l < plan.nl; ++l) P.M[l] = plan.M[l];
+        for (int t = 0; t < plan.s; ++t) {
+            for (int b = 0; b < 4 * plan.nl; ++b) P.wb[b][t] = static_cast<uint8_t>(plan.W[t][b / 4] >> (8 * (b % 4)));
+            // the 16-bit quotient fraction of crt_constants, as two bytes
+            const uint64_t f = ((static_cast<uint64_t>(plan.y[t]) << 16) + plan.m[t] / 2) / plan.m[t];
+            const uint32_t f16 = static_cast<uint32_t>(std::min<uint64_t>(f, 0xFFFFu));
+            P.wb[4 * plan.nl][t] = static_cast<uint8_t>(f16);
+            P.wb[4 * plan.nl + 1][t] = static_cast<uint8_t>(f16 >> 8);
+        }
+        P.err = err;
+        P.wait_ns = dev::kWaitLimitNs;
+        // four CTAs per SM: 4 x 128 of the 512 TMEM columns (and 4 x 41 KB of shared memory)
+        const int grid = static_cast<int>(std::min<int64_t>(blocks, static_cast<int64_t>(sm_count()) * 4));
+        crt_mma_kernel<8><<<grid, 128, kCrtSmem, st>>>(P);  // crt_uses_mma: 8 limbs only
+        return;
+    }
     if (count <= 0 || blocks <= 0) return;
     CrtParams P{};
     P.items = d_items;

@@ -248,6 +248,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
             // the multiply-high quotient is exact; otherwise Barrett with one correction step
             const bool exact = RES && J.I->kb_total <= kExactKB;
             const uint32_t kbias30 = RES ? J.I->mod_kbias30[t] : 0u, mx31 = RES ? J.I->mod_mx31[t] : 0u;
+            const uint32_t mxs = RES ? J.I->mod_mxs[t] : 7u;
             const int64_t j = static_cast<int64_t>(J.tj) * kGemmJ + quarter * 32 + lane;
             const int64_t mm = J.I->m, nn = J.I->n;
             uint8_t* rowj = RES ? J.I->resid + J.gt * J.I->rstride + j * 32 : nullptr;  // + (i / 32) * 32 n
@@ -332,7 +333,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
 #pragma unroll
                                 for (int b = 0; b < 4; ++b) {
                                     const uint32_t u = cur[4 * q + b] + kbias30;  // in [0, 2^31)
-                                    r4[b] = u - (__umulhi(u, mx31) >> 7) * m;    // in [0, m)
+                                    r4[b] = u - (__umulhi(u, mx31) >> mxs) * m;  // in [0, m)
                                 }
                                 w[q] = __byte_perm(__byte_perm(r4[0], r4[1], 0x0040),
                                                    __byte_perm(r4[2], r4[3], 0x0040), 0x5410);

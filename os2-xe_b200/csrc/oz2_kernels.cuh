@@ -89,6 +89,7 @@ struct GemmItem {
     int tiles_i, tiles_j, s, groups;
     uint32_t mod_m[kMaxModuliExt], mod_mu[kMaxModuliExt], mod_kbias[kMaxModuliExt];
     uint32_t mod_kbias30[kMaxModuliExt], mod_mx31[kMaxModuliExt];  // exact quotient, kb_total <= kExactKB
+    uint32_t mod_mxs[kMaxModuliExt];                                // its shift (oz2_plan.hpp)
     // Ozaki-I mode only: job index t is the digit pair (pair_a[t], pair_b[t]) on anti-diagonal
     // pair_d[t]; the int32 products are added into acc[d][i acc_ld + j] (int64)
     int64_t* acc;
@@ -114,6 +115,10 @@ struct CrtItem {
     double* C;
     int64_t block0, iblocks;  // blocks = ceil(n / jb) * iblocks
     int tq, jb;               // a block: tq threads (4 rows each) along i x jb columns, tq * jb = 256
+    // mma: the tensor-core CRT (real items of 8-limb plans, s = 30..32): block0 is the first tile
+    // of 32 rows x 4 columns (128 entries, one tcgen05 MMA) and iblocks the tiles along i;
+    // otherwise the dp2a kernel's geometry
+    int mma;
 };
 
 // host-side helpers filling the launch-geometry fields; they return the blocks of the item
@@ -147,8 +152,14 @@ void launch_oz1_horner(const int64_t* acc, int64_t m, int64_t n, int L, const un
                        const unsigned long long* maxB, int tk, double* C, int64_t ldc, cudaStream_t st);
 int64_t gemm_tiles_i(int64_t m, int bn);
 
-// all items of one CRT launch share s (the CRT table is a kernel parameter)
-void launch_crt(const CrtItem* d_items, int count, int64_t blocks, const Plan& plan, bool cplx, cudaStream_t st);
+// whether launch_crt runs the tensor-core CRT for this plan: real items with 8 limbs (s = 30..32),
+// where it measured faster than the dp2a kernel (B200, 4096^2: 0.60 against 0.77 ms at s = 32,
+// slower below: 1.96 against 0.73 ms at 8192^2, s = 16); the item's `mma` flag must match
+inline bool crt_uses_mma(const Plan& plan, bool cplx) { return !cplx && plan.nl == 8; }
+// all items of one CRT launch share s (the CRT table is a kernel parameter); err: the device error
+// word for the real kernel's bounded wait on its MMA (may be null)
+void launch_crt(const CrtItem* d_items, int count, int64_t blocks, const Plan& plan, bool cplx, int* err,
+                cudaStream_t st);
 
 // sets the GEMM kernels' shared-memory attribute (once per device, before any graph capture)
 cudaError_t prepare_gemm_kernels();

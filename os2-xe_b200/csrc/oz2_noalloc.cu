@@ -222,6 +222,7 @@ extern "C" int oz2_dgemm_noalloc(void* stream, char ta, char tb, int64_t m, int6
         g.mod_kbias[t] = mc[t].kbias;
         g.mod_kbias30[t] = mc[t].kbias30;
         g.mod_mx31[t] = mc[t].mx31;
+        g.mod_mxs[t] = mc[t].mxs;
     }
     CrtItem& c = T.c;
     c.resid = resid;
@@ -247,7 +248,7 @@ extern "C" int oz2_dgemm_noalloc(void* stream, char ta, char tb, int64_t m, int6
     for (int side = 1; side >= 0; --side)
         launch_split(&D->sp[side], &T.sp[side], 1, T.sp[side].rblocks * T.sp[side].kblocks, st);
     launch_gemm(&D->g, 1, g.tiles * s, cfg, num_sms, err, st);
-    launch_crt(&D->c, 1, crt_blocks, p, false, st);
+    launch_crt(&D->c, 1, crt_blocks, p, false, err, st);
     e = cudaGetLastError();
     return e == cudaSuccess ? OZ2_OK : reject(OZ2_ECUDA, std::string("oz2_dgemm_noalloc: ") + cudaGetErrorString(e));
 }

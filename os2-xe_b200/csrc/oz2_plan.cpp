@@ -204,9 +204,12 @@ void mod_constants(const Plan& p, ModConst* out) {
         c.koff7 = (h + m - pow2_mod(125, m)) % m;
         c.kbias = m * static_cast<uint32_t>(((uint64_t{1} << 31) + m - 1) / m);
         c.kbias30 = m * ((kExactSum + m - 1) / m);
-        // Granlund and Montgomery (1994): with M = ceil(2^39 / m) = (2^39 + e) / m, e < m <= 2^8,
-        // floor(v M / 2^39) = floor(v / m) for every v < 2^31 (v e / (m 2^39) < 1 / m)
-        c.mx31 = static_cast<uint32_t>(((uint64_t{1} << 39) + m - 1) / m);
+        // Granlund and Montgomery (1994): with M = ceil(2^(32 + x) / m) = (2^(32 + x) + e) / m, e < m,
+        // floor(v M / 2^(32 + x)) = floor(v / m) for every v < 2^31 when v e < 2^(32 + x), which
+        // x = 7 gives for m <= 256 and x = 6 for m < 128 (e <= 126); M fits 32 bits for m > 128
+        // with x = 7 and for m > 64 with x = 6
+        c.mxs = m > 128 ? 7u : 6u;
+        c.mx31 = static_cast<uint32_t>(((uint64_t{1} << (32 + c.mxs)) + m - 1) / m);
         for (int w = 0; w < 4; ++w) {
             c.cb[w] = 0;
             for (int b = 0; b < 4; ++b) c.cb[w] |= pow2_mod(8 * (4 * w + b), m) << (8 * b);

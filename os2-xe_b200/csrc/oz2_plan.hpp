@@ -53,7 +53,9 @@ struct ModConst {
                      // (|c| < 2^31 - 2^21) and congruent to c modulo m
     uint32_t kbias30;  // m ceil(kExactSum / m): c + kbias30 is in [0, 2^31) for every int32 GEMM sum
                        // c of at most kExactKB k-blocks (|c| <= kExactSum) and congruent to c
-    uint32_t mx31;     // ceil(2^39 / m): floor(v / m) = umulhi(v, mx31) >> 7 exactly for v < 2^31
+    uint32_t mx31;     // ceil(2^(32 + mxs) / m): floor(v / m) = umulhi(v, mx31) >> mxs exactly for v < 2^31
+    uint32_t mxs;      // 7, or 6 for m < 128 (the moduli of the extended sets from s = 29), where
+                       // ceil(2^39 / m) would not fit 32 bits
     uint32_t cb[4];  // bytes 2^(8 l) mod m, l = 0..15, four per word (byte-limb weights)
     uint32_t m32;    // ceil(2^32 / m): floor(v / m) = umulhi(v, m32) exactly for v < 2^24
 };
