@@ -65,6 +65,14 @@ def parse():
     ap.add_argument("--s", type=int, default=16, help="moduli of the DGEMM extra")
     ap.add_argument("--k", type=int, default=0, help="inner dimension of the DGEMM extra (default: --size)")
     ap.add_argument("--no-extras", action="store_true", help="skip the DGEMM, grouped and CPU legs")
+    ap.add_argument("--split-kernel", type=int, default=0, choices=(0, 1),
+                    help="real split kernel: 0 integer pipe (dp4a, default), 1 tensor core")
+    ap.add_argument("--crt-kernel", type=int, default=2, choices=(0, 1, 2),
+                    help="real CRT kernel: 2 auto (default: tensor core for 8-limb plans), 1 tensor core, 0 dp2a")
+    ap.add_argument("--scale-fusion", type=int, default=1, choices=(0, 1),
+                    help="scale pass fused into the split for k <= 2048 (1, default) or separate (0)")
+    ap.add_argument("--crt-fusion", type=int, default=0, choices=(0, 1),
+                    help="CRT in the GEMM epilogue for s <= 8 (1) or a separate CRT launch (0, default)")
     ap.add_argument("--dgemm-only", action="store_true",
                     help="time only the DGEMM of --size and --s (a profiling aid; not the headline)")
     return ap.parse_args()
@@ -773,6 +781,10 @@ def main():
     import torch
     import torch.distributed as dist
     import oz2
+    oz2.set_split_kernel(a.split_kernel)
+    oz2.set_crt_kernel(a.crt_kernel)
+    oz2.set_scale_fusion(a.scale_fusion)
+    oz2.set_crt_fusion(a.crt_fusion)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -222,6 +222,36 @@ int oz2_check_device_error(oz2_handle h);
  * returns OZ2_ETIMEOUT. Calls after oz2_set_failure_test(0, 0) compute normally. */
 int oz2_set_failure_test(int64_t wait_limit_ns, int stall_mma);
 
+/* Kernel of the real split (no counterpart in the reference; process-wide, read when a call
+ * builds its launches, so set it only while no other call is being made): 0 (default) the
+ * integer-pipe (dp4a) split; 1 the tensor-core split, which computes the byte dot products of
+ * every residue with one tcgen05 u8 x u8 MMA per 512 elements (measured slower on B200: it is
+ * bound by per-element instruction overhead, not by the dot products). Both write identical
+ * planes. Complex operands always use the integer-pipe split. OZ2_EINVAL for other values. */
+int oz2_set_split_kernel(int kind);
+
+/* Kernel of the real CRT (no counterpart in the reference; process-wide, read when a call builds
+ * its launches): 0 the dp2a kernel; 1 the tensor-core CRT, whose limb sums are one tcgen05 u8 x
+ * u8 MMA per 128 entries; 2 (default) the tensor-core CRT for 8-limb plans (s = 30..32), the dp2a
+ * kernel below. All produce identical C. Complex operands always use the dp2a kernel. OZ2_EINVAL
+ * for other values. */
+int oz2_set_crt_kernel(int kind);
+
+/* Scale pass fused into the split (no counterpart in the reference, which runs them as two passes
+ * over A and B; process-wide, read when a call builds its launches): with on != 0 (default) a real
+ * operand of oz2_dgemm / oz2_dgemm_grouped whose k is at most 2048 (1024 when its plane rows are
+ * contiguous in memory: op(A) = A, op(B) = B^T) is scaled and split by one kernel that owns whole
+ * rows, takes their maxima and splits them while they are still in L2. Results are identical. */
+int oz2_set_scale_fusion(int on);
+
+/* CRT in the GEMM's epilogue (no counterpart in the reference; process-wide, read when a call
+ * builds its launches): with on != 0 real problems of oz2_dgemm / oz2_dgemm_grouped with s <= 8
+ * and k <= 65408 run one GEMM launch per plan whose epilogue keeps each 128 x 128 tile's residues
+ * of all s moduli in tensor memory and reconstructs C there: no residue planes in HBM and no CRT
+ * launch. Results are identical. Default off: on B200 it measured slower than the GEMM followed by
+ * the CRT launch (the reconstruction runs on the GEMM's eight epilogue warps). */
+int oz2_set_crt_fusion(int on);
+
 /* Emulated DGEMM for callers that cannot allocate device memory. No counterpart in the
  * reference. Same arguments, checks and results as oz2_dgemm, but no handle: it works on the
  * given stream and the current device and allocates nothing. Its scratch is a 64 MiB static

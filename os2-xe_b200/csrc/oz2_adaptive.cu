@@ -46,7 +46,8 @@ __global__ void __launch_bounds__(256) panel_stats_kernel(const StatItem* __rest
     __syncthreads();
     const StatItem* I = items + find_block_item(items, count, blockIdx.x);
     const int64_t local = static_cast<int64_t>(blockIdx.x) - I->block0;
-    const int64_t rb = local % I->rblocks, kc = local / I->rblocks;
+    int64_t rb, kc;
+    divmod_index(local, I->rblocks, kc, rb);
     const unsigned long long* X = reinterpret_cast<const unsigned long long*>(I->X);
     const int64_t rows = I->rows, k = I->k, ldx = I->ldx;
     const int64_t p0 = kc * I->kchunk, p1 = min(k, p0 + I->kchunk);

@@ -37,7 +37,7 @@ constexpr int kRing = 4;
 // A call is planned on the host into a descriptor blob and a list of operations, then issued
 // on the stream (or captured into a CUDA graph and replayed).
 struct Op {
-    enum Kind { Memset, Scale, Split, Gemm, Crt, ScaleC, Mark, Slice, GemmOz1 } kind;
+    enum Kind { Memset, Scale, Split, Gemm, Crt, ScaleC, Mark, Slice, GemmOz1, GemmCrt } kind;
     size_t off = 0;    // descriptor offset in the blob
     int count = 0;     // items
     int64_t blocks = 0;
@@ -347,7 +347,13 @@ struct Task {
     int8_t *planesA, *planesB;
     uint8_t* resid;
     int64_t ldr;
+    bool fuse_a = false, fuse_b = false;  // the side's scale pass runs inside its split
 };
+
+// whether a side's scale pass is fused into its split (the split kernel then writes its maxima)
+bool fuse_side(const Prob& p, bool a_side) {
+    return fuse_scale(p.G == 3, a_side ? is_n(p.ta) : !is_n(p.tb), p.k);
+}
 
 template <class Item>
 void add_grouped(Program& prog, std::vector<Item>& items, Op::Kind kind, int64_t (*geom)(Item&, int64_t),
@@ -364,12 +370,12 @@ void add_grouped(Program& prog, std::vector<Item>& items, Op::Kind kind, int64_t
     prog.ops.push_back(op);
 }
 
-int64_t split_geom(SplitItem& it, int64_t b0) { return split_item_blocks(it, b0); }
+int64_t split_geom(SplitItem& it, int64_t b0) { return split_geometry(it, b0); }
 int64_t crt_geom(CrtItem& it, int64_t b0) { return crt_item_blocks(it, b0); }
 
 // Appends split, GEMM and CRT operations for a list of tasks (launches grouped by kernel variant)
 void plan_tasks(Program& prog, const std::vector<Task>& tasks, const GemmConfig& cfg) {
-    // split: group by (row_contig, complex, limb path: narrow, wide, widest)
+    // split: group by (row_contig, complex / fused scale, limb path: narrow, wide, widest)
     std::map<std::tuple<int, int, int>, std::vector<SplitItem>> split_groups;
     for (const Task& t : tasks) {
         const Prob& p = *t.p;
@@ -377,11 +383,13 @@ void plan_tasks(Program& prog, const std::vector<Task>& tasks, const GemmConfig&
         const int wide = p.plan->tk > kWideScaleBits ? 2 : (p.plan->tk > kNarrowScaleBits ? 1 : 0);
         if (t.split_b) {
             SplitItem it = side_item(p, false, t.j0, t.nb, t.maxB, t.planesB, mc);
-            split_groups[{it.row_contig, it.cplx, wide}].push_back(it);
+            it.fuse = t.fuse_b;
+            split_groups[{it.row_contig, it.cplx + 2 * it.fuse, wide}].push_back(it);
         }
         if (t.split_a) {
             SplitItem it = side_item(p, true, t.i0, t.mb, t.maxA, t.planesA, mc);
-            split_groups[{it.row_contig, it.cplx, wide}].push_back(it);
+            it.fuse = t.fuse_a;
+            split_groups[{it.row_contig, it.cplx + 2 * it.fuse, wide}].push_back(it);
         }
     }
     for (auto& kv : split_groups) add_grouped(prog, kv.second, Op::Split, split_geom, nullptr, false);
@@ -390,8 +398,14 @@ void plan_tasks(Program& prog, const std::vector<Task>& tasks, const GemmConfig&
     mk.stage = kSplit;
     prog.ops.push_back(mk);
 
-    // GEMM: one persistent launch over every task; largest work first
+    // GEMM: one persistent launch over every task; largest work first. Real tasks of s <= 8 with
+    // one exact k chunk take the GEMM with the CRT in its epilogue instead (one launch per plan)
+    auto crt_in_gemm = [](const Task& t) {
+        const Prob& p = *t.p;
+        return crt_fusion() && p.G == 1 && p.plan->s <= kCrtFusedMaxS && ceil_div(p.k, kTileK) <= kExactKB;
+    };
     std::vector<GemmItem> gi;
+    std::map<const Plan*, std::pair<int64_t, std::vector<GemmItem>>> fused;  // plan -> (jobs, items)
     std::vector<size_t> order(tasks.size());
     for (size_t i = 0; i < tasks.size(); ++i) order[i] = i;
     auto work = [&](size_t i) {
@@ -404,6 +418,8 @@ void plan_tasks(Program& prog, const std::vector<Task>& tasks, const GemmConfig&
     for (size_t oi : order) {
         const Task& t = tasks[oi];
         const Prob& p = *t.p;
+        const bool fz = crt_in_gemm(t);
+        const int bn = fz ? 128 : cfg.bn;
         GemmItem g{};
         g.planes_i = t.planesA;
         g.planes_j = t.planesB;
@@ -415,7 +431,7 @@ void plan_tasks(Program& prog, const std::vector<Task>& tasks, const GemmConfig&
         g.m = t.mb;
         g.n = t.nb;
         g.kb_total = ceil_div(p.k, kTileK);
-        g.tiles_i = static_cast<int>(gemm_tiles_i(t.mb, cfg.bn));
+        g.tiles_i = static_cast<int>(gemm_tiles_i(t.mb, bn));
         g.tiles_j = static_cast<int>(ceil_div(t.nb, kGemmJ));
         g.tiles = static_cast<int64_t>(g.tiles_i) * g.tiles_j;
         g.s = p.plan->s;
@@ -430,22 +446,49 @@ void plan_tasks(Program& prog, const std::vector<Task>& tasks, const GemmConfig&
             g.mod_mx31[q] = mc[q].mx31;
             g.mod_mxs[q] = mc[q].mxs;
         }
+        if (fz) {  // one job per tile; the epilogue writes C
+            auto& f = fused[p.plan];
+            g.job0 = f.first;
+            g.C = p.C + t.i0 + t.j0 * p.ldc;
+            g.ldc = p.ldc;
+            g.crt_maxA = t.maxA + t.i0;
+            g.crt_maxB = t.maxB + t.j0;
+            g.crt_tk = p.plan->tk;
+            g.crt_alpha = p.alpha[0];
+            g.crt_beta = p.beta[0];
+            f.first += g.tiles;
+            f.second.push_back(g);
+            continue;
+        }
         jobs += g.tiles * p.G * g.s;
         gi.push_back(g);
     }
-    Op go;
-    go.kind = Op::Gemm;
-    go.count = static_cast<int>(gi.size());
-    go.jobs = jobs;
-    go.cfg = cfg;
-    go.off = prog.add(gi.data(), gi.size() * sizeof(GemmItem));
-    prog.ops.push_back(go);
+    if (!gi.empty()) {
+        Op go;
+        go.kind = Op::Gemm;
+        go.count = static_cast<int>(gi.size());
+        go.jobs = jobs;
+        go.cfg = cfg;
+        go.off = prog.add(gi.data(), gi.size() * sizeof(GemmItem));
+        prog.ops.push_back(go);
+    }
+    for (auto& kv : fused) {
+        Op go;
+        go.kind = Op::GemmCrt;
+        go.count = static_cast<int>(kv.second.second.size());
+        go.jobs = kv.second.first;
+        go.cfg = cfg;
+        go.plan = kv.first;
+        go.off = prog.add(kv.second.second.data(), kv.second.second.size() * sizeof(GemmItem));
+        prog.ops.push_back(go);
+    }
     mk.stage = kGemm;
     prog.ops.push_back(mk);
 
     // CRT: group by (s, complex); the CRT table of s is a kernel parameter
     std::map<std::pair<int, int>, std::pair<const Plan*, std::vector<CrtItem>>> crt_groups;
     for (const Task& t : tasks) {
+        if (crt_in_gemm(t)) continue;
         const Prob& p = *t.p;
         const bool cplx = p.G == 3;
         const int w = cplx ? 2 : 1;
@@ -606,11 +649,15 @@ void issue(oz2_context* h, const Program& prog, const unsigned char* dev) {
                 break;
             case Op::Split:
                 launch_split(reinterpret_cast<const SplitItem*>(dev + op.off), reinterpret_cast<const SplitItem*>(hb + op.off),
-                             op.count, op.blocks, h->stream);
+                             op.count, op.blocks, h->d_err, h->stream);
                 break;
             case Op::Gemm:
                 launch_gemm(reinterpret_cast<const GemmItem*>(dev + op.off), op.count, op.jobs, op.cfg, h->num_sms, h->d_err,
                             h->stream);
+                break;
+            case Op::GemmCrt:
+                launch_gemm_crt(reinterpret_cast<const GemmItem*>(dev + op.off), op.count, op.jobs, *op.plan,
+                                op.cfg.group_j, h->num_sms, h->d_err, h->stream);
                 break;
             case Op::Slice:
                 launch_slice(reinterpret_cast<const SplitItem*>(dev + op.off), reinterpret_cast<const SplitItem*>(hb + op.off),
@@ -761,13 +808,16 @@ int run_single(oz2_context* h, const Prob& p) {
     ms.ptr = maxA;
     ms.bytes = reinterpret_cast<unsigned char*>(planesA) - reinterpret_cast<unsigned char*>(maxA);
     prog.ops.push_back(ms);
-    std::vector<ScaleItem> sc{scale_item(p, true, maxA), scale_item(p, false, maxB)};
+    const bool fa = fuse_side(p, true), fb = fuse_side(p, false);
+    std::vector<ScaleItem> sc;
+    if (!fa) sc.push_back(scale_item(p, true, maxA));
+    if (!fb) sc.push_back(scale_item(p, false, maxB));
     plan_scale(h, prog, sc);
     const int64_t ldr = round_up(L.mb, 32);
     for (int64_t j0 = 0; j0 < p.n; j0 += L.nb) {
         for (int64_t i0 = 0; i0 < p.m; i0 += L.mb) {
             Task t{&p, i0, j0, std::min(L.mb, p.m - i0), std::min(L.nb, p.n - j0), L.pm > 1 || j0 == 0, i0 == 0,
-                   maxA, maxB, planesA, planesB, resid, ldr};
+                   maxA, maxB, planesA, planesB, resid, ldr, fa, fb};
             plan_tasks(prog, {t}, cfg);
         }
     }
@@ -840,10 +890,11 @@ int run_grouped(oz2_context* h, std::vector<Prob>& probs) {
             auto* pa = reinterpret_cast<int8_t*>(carve(z.planesA));
             auto* pb = reinterpret_cast<int8_t*>(carve(z.planesB));
             auto* rs = carve(z.resid);
+            const bool fa = fuse_side(p, true), fb = fuse_side(p, false);
             tasks.push_back(Task{&p, 0, 0, p.m, p.n, true, true, mx[q].first, mx[q].second, pa, pb, rs,
-                                 round_up(p.m, 32)});
-            sc.push_back(scale_item(p, true, mx[q].first));
-            sc.push_back(scale_item(p, false, mx[q].second));
+                                 round_up(p.m, 32), fa, fb});
+            if (!fa) sc.push_back(scale_item(p, true, mx[q].first));
+            if (!fb) sc.push_back(scale_item(p, false, mx[q].second));
         }
         unsigned char* dev_desc = carve(0);
         Program prog;
@@ -2499,6 +2550,28 @@ int oz2_check_device_error(oz2_handle h) {
 int oz2_set_failure_test(int64_t wait_limit_ns, int stall_mma) {
     if (wait_limit_ns < 0) return fail(nullptr, OZ2_EINVAL, "oz2: negative wait limit");
     set_gemm_failure_test(static_cast<uint64_t>(wait_limit_ns), stall_mma);
+    return OZ2_OK;
+}
+
+int oz2_set_split_kernel(int kind) {
+    if (kind != 0 && kind != 1) return fail(nullptr, OZ2_EINVAL, "oz2: split kernel must be 0 (dp4a) or 1 (tensor core)");
+    set_split_path(kind);
+    return OZ2_OK;
+}
+
+int oz2_set_crt_kernel(int kind) {
+    if (kind < 0 || kind > 2) return fail(nullptr, OZ2_EINVAL, "oz2: CRT kernel must be 0 (dp2a), 1 (tensor core) or 2 (auto)");
+    set_crt_path(kind);
+    return OZ2_OK;
+}
+
+int oz2_set_scale_fusion(int on) {
+    set_scale_fusion(on);
+    return OZ2_OK;
+}
+
+int oz2_set_crt_fusion(int on) {
+    set_crt_fusion(on);
     return OZ2_OK;
 }
 

@@ -7,9 +7,11 @@
 // Bandwidth-bound: s bytes of residues per entry in (3s for complex), 8 (16) bytes of C out,
 // plus 8 (16) in when beta != 0. Each thread handles 4 consecutive rows of one column.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 
 #include "oz2_kernels.cuh"
+#include "oz2_crt_math.cuh"
 #include "oz2_ptx.cuh"
 
 namespace oz2 {
@@ -22,109 +24,6 @@ struct CrtParams {
     uint32_t mod_m[kMaxModuliExt];
 };
 
-__device__ __forceinline__ int exponent_of(unsigned long long b, int tk) {
-    if (b >= 0x7FF0000000000000ull) return kNonFinite;
-    if (b == 0) return 0;
-    const int be = static_cast<int>(b >> 52);
-    const int e2 = be ? be - 1022 : -1010 - __clzll(static_cast<long long>(b));
-    return tk - e2;
-}
-
-// 2^E * d for d in [2^63, 2^64]: exponent arithmetic on the bits while the result stays normal
-// (exact), ldexp otherwise (overflow, or one rounding into the subnormal range)
-__device__ __forceinline__ double scale_pow2(double d, int E) {
-    if (E >= -1022 - 63 && E <= 1023 - 64)
-        return __longlong_as_double(__double_as_longlong(d) + (static_cast<long long>(E) << 52));
-    return ldexp(d, E);
-}
-
-// Exact reconstruction + single rounding. R[g] holds the residues r_t in [0, m_t) of the moduli
-// 4g..4g+3 as bytes (zero past s). Every sum is a chain of two-way byte dot products (dp2a):
-// q = round(Sum r_t y_t / m_t) from the 16-bit fractions F16_t (error below 24 * 255 * 2^-16 <
-// 0.1, inside the 1/4 margin that |x| <= M/4 leaves, so q is the reference's FP32 quotient),
-// and Sum r_t W_t limb by limb over 16-bit limbs of W_t (each limb sum below 24 * 255 * 2^16 <
-// 2^29), then x = Sum r_t W_t - q M modulo 2^(32 NL) in 64-bit words, rounded once to double.
-template <int NL>
-__device__ __forceinline__ double crt_finish(const uint64_t (&acc)[NL], int64_t q, const uint32_t* Mw, int shift);
-
-template <int S, int NL>
-__device__ __forceinline__ double crt_value(const uint32_t (&R)[(S + 3) / 4], const CrtConst& cc, int shift) {
-    constexpr int Q = (S + 3) / 4;
-    uint32_t uf = 1u << 15;  // rounding offset of the quotient
-#pragma unroll
-    for (int g = 0; g < Q; ++g) {
-        uf = __dp2a_lo(cc.Fq[g][0], R[g], uf);
-        uf = __dp2a_hi(cc.Fq[g][1], R[g], uf);
-    }
-    const int64_t q = static_cast<int64_t>(uf >> 16);
-    uint64_t acc[NL];
-#pragma unroll
-    for (int l = 0; l < NL; ++l) {
-        uint32_t a0 = 0, a1 = 0;  // 16-bit limbs 2l and 2l + 1
-#pragma unroll
-        for (int g = 0; g < Q; ++g) {
-            a0 = __dp2a_lo(cc.Wq[g][2 * l][0], R[g], a0);
-            a0 = __dp2a_hi(cc.Wq[g][2 * l][1], R[g], a0);
-            a1 = __dp2a_lo(cc.Wq[g][2 * l + 1][0], R[g], a1);
-            a1 = __dp2a_hi(cc.Wq[g][2 * l + 1][1], R[g], a1);
-        }
-        acc[l] = static_cast<uint64_t>(a0) + (static_cast<uint64_t>(a1) << 16);
-    }
-    return crt_finish<NL>(acc, q, cc.M, shift);
-}
-
-// From the 32-bit limb sums acc[l] = sum_t r_t W_t[l] (below 2^46) and the quotient q: x = sum_t
-// r_t W_t - q M modulo 2^(32 NL) in 64-bit words (|x| <= M/4, two's complement), its magnitude's
-// leading 64 bits with a sticky bit for the rest, one RNE to double, 2^-shift.
-template <int NL>
-__device__ __forceinline__ double crt_finish(const uint64_t (&acc)[NL], int64_t q, const uint32_t* Mw, int shift) {
-    uint32_t w[NL];
-    int64_t carry = 0;
-#pragma unroll
-    for (int l = 0; l < NL; ++l) {
-        const int64_t v = static_cast<int64_t>(acc[l]) - q * static_cast<int64_t>(Mw[l]) + carry;
-        w[l] = static_cast<uint32_t>(v);
-        carry = v >> 32;
-    }
-    // 64-bit words, two's complement -> sign and magnitude
-    constexpr int NW = (NL + 1) / 2;
-    uint64_t X[NW];
-#pragma unroll
-    for (int i = 0; i < NW; ++i)
-        X[i] = static_cast<uint64_t>(w[2 * i]) | (2 * i + 1 < NL ? static_cast<uint64_t>(w[2 * i + 1]) << 32 : 0);
-    if (NL % 2)  // odd word count: sign-extend the top word into the last 64-bit word
-        X[NW - 1] = static_cast<uint64_t>(static_cast<int64_t>(static_cast<int32_t>(w[NL - 1])));
-    const bool neg = static_cast<int64_t>(X[NW - 1]) < 0;
-    if (neg) {
-        uint64_t borrow = 1;
-#pragma unroll
-        for (int i = 0; i < NW; ++i) {
-            const uint64_t nv = ~X[i] + borrow;
-            borrow = (borrow && nv == 0) ? 1 : 0;
-            X[i] = nv;
-        }
-    }
-    // leading 64 bits with a sticky bit for everything below
-    uint64_t hiw = 0, low = 0;
-    bool sticky = false;
-    int tw = -1;
-#pragma unroll
-    for (int i = NW - 1; i >= 0; --i)
-        if (tw < 0 && X[i]) tw = i;
-    if (tw < 0) return 0.0;
-#pragma unroll
-    for (int i = 0; i < NW; ++i) {
-        if (i == tw) hiw = X[i];
-        else if (i == tw - 1) low = X[i];
-        else if (i < tw - 1) sticky |= X[i] != 0;
-    }
-    const int z = __clzll(static_cast<long long>(hiw));
-    const uint64_t top = z ? (hiw << z) | (low >> (64 - z)) : hiw;
-    sticky |= (z ? (low << z) : low) != 0;
-    const double val = scale_pow2(__ull2double_rn(top | (sticky ? 1u : 0u)), 64 * tw - z - shift);
-    return neg ? -val : val;
-}
-
 __device__ __forceinline__ uint32_t sub_mod(uint32_t a, uint32_t b, uint32_t m) {  // (a - b) mod m, a,b < m
     uint32_t r = a + m - b;
     return min(r, r - m);
@@ -133,17 +32,6 @@ __device__ __forceinline__ uint32_t sub_mod(uint32_t a, uint32_t b, uint32_t m) 
 // low bytes of a, b, c, d as one little-endian word
 __device__ __forceinline__ uint32_t pack4(uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
     return __byte_perm(__byte_perm(a, b, 0x0040), __byte_perm(c, d, 0x0040), 0x5410);
-}
-
-// 4 x 4 byte transpose: word t of `in` holds entries e = 0..3 of modulus 4g + t; word e of `out`
-// holds moduli 4g..4g+3 of entry e
-__device__ __forceinline__ void transpose4(uint32_t a, uint32_t b, uint32_t c, uint32_t d, uint32_t (&out)[4]) {
-    const uint32_t t0 = __byte_perm(a, b, 0x5140), t1 = __byte_perm(a, b, 0x7362);
-    const uint32_t t2 = __byte_perm(c, d, 0x5140), t3 = __byte_perm(c, d, 0x7362);
-    out[0] = __byte_perm(t0, t2, 0x5410);
-    out[1] = __byte_perm(t0, t2, 0x7632);
-    out[2] = __byte_perm(t1, t3, 0x5410);
-    out[3] = __byte_perm(t1, t3, 0x7632);
 }
 
 template <int S, bool CPLX>
@@ -157,7 +45,8 @@ __global__ void __launch_bounds__(256) crt_kernel(const __grid_constant__ CrtPar
     }
     const CrtItem* __restrict__ I = P.items + lo;
     const int64_t local = static_cast<int64_t>(blockIdx.x) - I->block0;
-    const int64_t jblk = local / I->iblocks, ib = local - jblk * I->iblocks;
+    int64_t jblk, ib;
+    divmod_index(local, I->iblocks, jblk, ib);
     const int tq = I->tq;
     const int64_t j = jblk * I->jb + threadIdx.x / tq;
     const int64_t i0 = (ib * tq + threadIdx.x % tq) * 4;
@@ -243,43 +132,53 @@ __global__ void __launch_bounds__(256) crt_kernel(const __grid_constant__ CrtPar
     }
 }
 
-// ---------------------------------------------------------------- tensor-core CRT (real, 8 limbs)
+// ---------------------------------------------------------------- tensor-core CRT (real)
 // The limb sums sum_t r_t W_t are a small integer matrix product: per entry e, D[e][b] = sum_t
 // r_et Wb[t][b] with r_et the residue bytes and Wb[t][b] byte b of W_t (b < 4 NL), plus two
 // columns of the 16-bit quotient fractions F16_t (low and high byte). One tcgen05.mma kind::i8
-// (unsigned bytes, M = 128 entries, N = 64 columns, K = 32 moduli, zero-padded) computes them
-// for 128 entries: every sum is below 32 * 255^2 < 2^21, exact in the int32 accumulators. The
-// threads then do only the carry chain and the rounding of the dp2a kernel (crt_finish), so the
-// results are the same bits; the integer-multiply pipe, which bounds the dp2a kernel, is left
-// to the few 64-bit products of the carry chain.
-// A CTA is 4 warps; a tile is 32 rows i x 4 columns j (warp q: column j0 + q, its lanes the
-// rows: TMEM lane 32 q + l is entry (i0 + l, j0 + q), so each warp stores 32 consecutive C
-// entries of a column). Persistent over the tiles of all items of the launch.
-constexpr int kCrtN = 64;                               // MMA N: 4 NL limb bytes + 2 quotient bytes
-constexpr uint32_t kCrtIdesc = (2u << 4)                  // D: s32; A, B: unsigned 8-bit, K-major
-                               | (static_cast<uint32_t>(kCrtN >> 3) << 17) | (static_cast<uint32_t>(128 >> 4) << 24);
-constexpr int kCrtSmem = 1024 + 2 * 128 * 128 + kCrtN * 128 + 64;  // align slack, two A tiles, B, barriers + slot
+// (unsigned bytes, M = 128 entries, N = NC columns, K = 32 moduli, zero-padded) computes them
+// for 128 entries; every sum is below 32 * 255^2 < 2^21, exact in the int32 accumulators. The
+// threads then do only the byte-to-limb combination, the carry chain and the rounding of the
+// dp2a kernel (crt_finish), so the results are the same bits, with 4 NL + 2 TMEM columns read
+// per entry in place of 2 Q (2 NL + 1) dp2a.
+// A super-tile is 32 rows i x 16 columns j, four MMA tiles g of 32 rows x 4 columns; their
+// residues share one 128-byte swizzled A tile (tile g in K bytes 32 g .. 32 g + 31 of each row,
+// row 32 c + l = entry (i0 + crt_tc_row(l), j0 + 4 g + c)). 8 warps: for the loads, warp w takes columns w and
+// w + 8 of the super-tile; for the epilogue, warp w reads TMEM lane quarter w % 4 of tiles
+// w / 4 and w / 4 + 2, so each thread finishes two entries and each warp stores 32 consecutive
+// entries of a column. Double-buffered (two A tiles, 2 x 4 NC TMEM columns), persistent, two
+// CTAs per SM (NC = 32: 4 NL + 2 <= 32, so NL <= 7) or one (NC = 64, NL = 8).
+constexpr int kCrtThreads = 256;
+template <int NL>
+struct CrtTc {
+    static constexpr int NC = 4 * NL + 2 <= 32 ? 32 : 64;  // MMA N and TMEM columns per MMA tile
+    static constexpr uint32_t kTmemCols = 2 * 4 * NC;
+    static constexpr uint32_t kIdesc = (2u << 4)             // D: s32; A, B: unsigned 8-bit, K-major
+                                       | (static_cast<uint32_t>(NC >> 3) << 17) | (static_cast<uint32_t>(128 >> 4) << 24);
+    static constexpr int kSmem = 1024 + 2 * 128 * 128 + NC * 128 + 64;  // align slack, two A tiles, B, barriers + slot
+    static constexpr int kSmemLaunch = NC == 32 ? 100 * 1024 : 120 * 1024;  // CTAs per SM as TMEM allows
+};
 
-struct CrtMmaParams {
+struct CrtTcParams {
     const CrtItem* items;
     int count;
-    int64_t tiles;
+    int64_t tiles;  // super-tiles
     int s, nl;
     uint32_t M[kMaxLimbs];
-    alignas(16) uint8_t wb[kCrtN][32];  // B operand rows: byte b of W_t for t = 0..31 (zero past s); F16 bytes at 4 nl, 4 nl + 1
+    alignas(16) uint8_t wb[64][32];  // B operand rows: byte b of W_t for t = 0..31 (zero past s); F16 bytes at 4 nl, 4 nl + 1
     int* err;
     uint64_t wait_ns;
 };
 
-// the residue words of one tile for this thread: column j0 + warp, rows i0 + 4 (lane % 8) .. + 3,
-// moduli 8 (lane / 8) .. + 7 (one 32-bit word = 4 rows per modulus; zero past s or n)
-struct TileRef {
+struct SuperTile {
     const CrtItem* I;
     int64_t i0, j0;
 };
-__device__ __forceinline__ void crt_tile_load(const TileRef& T, int s, uint32_t (&wv)[8]) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t j = T.j0 + warp, n = T.I->n;
+// the residue words of super-tile column c (0..15) for this thread: rows i0 + 4 (lane % 8) .. + 3,
+// moduli 8 (lane / 8) .. + 7 (one 32-bit word = 4 rows of one modulus; zero past s or n)
+__device__ __forceinline__ void crt_tc_load(const SuperTile& T, int c, int s, uint32_t (&wv)[8]) {
+    const int lane = threadIdx.x & 31;
+    const int64_t j = T.j0 + c, n = T.I->n;
     const int rq = lane & 7, mg = lane >> 3;
     const uint8_t* base = T.I->resid + (T.i0 >> 5) * (32 * n) + j * 32 + 4 * rq;
 #pragma unroll
@@ -288,36 +187,42 @@ __device__ __forceinline__ void crt_tile_load(const TileRef& T, int s, uint32_t 
         wv[u] = j < n && t < s ? __ldg(reinterpret_cast<const uint32_t*>(base + t * T.I->rstride)) : 0u;
     }
 }
-// the words regrouped per entry (4 x 4 byte transposes), 8 bytes per entry into its 128-byte
-// swizzled K-major row (K bytes 8 (lane / 8) .. + 7)
-__device__ __forceinline__ void crt_tile_store(uint8_t* sA, const uint32_t (&wv)[8]) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int rq = lane & 7, mg = lane >> 3;
+// Entry rows within a 32-row group are permuted in the A tile (and so in the TMEM lanes): row
+// l = 4 a + u sits in lane a + 8 u, so the eight row quads of one store instruction land in eight
+// different swizzle phases (no bank conflicts); lane -> row is crt_tc_row.
+__device__ __forceinline__ int crt_tc_row(int lane) { return 4 * (lane & 7) + (lane >> 3); }
+// the words of column c regrouped per entry (4 x 4 byte transposes): 8 bytes per entry into row
+// 32 (c % 4) + (lane % 8) + 8 u of the A tile, K bytes 32 (c / 4) + 8 (lane / 8) .. + 7
+__device__ __forceinline__ void crt_tc_store(uint8_t* sA, int c, const uint32_t (&wv)[8]) {
+    const int lane = threadIdx.x & 31;
+    const int rq = lane & 7, mg = lane >> 3, g = c >> 2;
     uint32_t lo[4], hi[4];
     transpose4(wv[0], wv[1], wv[2], wv[3], lo);
     transpose4(wv[4], wv[5], wv[6], wv[7], hi);
+    const int chunk = 2 * g + (mg >> 1);  // 16-byte chunk of the row's 128 K bytes
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
-        const int e = 32 * warp + 4 * rq + u;
-        const int c = mg >> 1;  // 16-byte chunk of the 32 K bytes
-        *reinterpret_cast<uint2*>(sA + e * 128 + ((c ^ (e & 7)) << 4) + 8 * (mg & 1)) = make_uint2(lo[u], hi[u]);
+        const int e = 32 * (c & 3) + rq + 8 * u;  // entry row 4 rq + u of the group
+        *reinterpret_cast<uint2*>(sA + e * 128 + ((chunk ^ (e & 7)) << 4) + 8 * (mg & 1)) = make_uint2(lo[u], hi[u]);
     }
 }
 
-// Software-pipelined over the CTA's tiles: while the MMA of tile k runs, the threads load tile
-// k + 1's residues into registers and finish tile k - 1 from the other accumulator (two A tiles,
-// two 64-column accumulators, two barriers).
+// Software-pipelined over the CTA's super-tiles: while the MMAs of super-tile k run, the threads
+// load super-tile k + 1's residues into registers and finish super-tile k - 1 from the other
+// accumulators.
 template <int NL>
-__global__ void __launch_bounds__(128) crt_mma_kernel(const __grid_constant__ CrtMmaParams P) {
+__global__ void __launch_bounds__(kCrtThreads) crt_tc_kernel(const __grid_constant__ CrtTcParams P) {
+    using T = CrtTc<NL>;
+    constexpr int NC = T::NC;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t{1023});
-    uint8_t* sA0 = smem;                      // two 128 rows x 128 B tiles, K-major, 128-byte swizzle
-    uint8_t* sB = smem + 2 * 128 * 128;       // kCrtN rows x 128 B
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sB + kCrtN * 128);
+    uint8_t* sA0 = smem;                 // two 128 rows x 128 B tiles, K-major, 128-byte swizzle
+    uint8_t* sB = smem + 2 * 128 * 128;  // NC rows x 128 B
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sB + NC * 128);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 2);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (threadIdx.x < kCrtN) {  // B: the W bytes of the plan (only the 32 K bytes of each row are read)
+    if (threadIdx.x < NC) {  // B: the W bytes of the plan (only the 32 K bytes of each row are read)
         const int b = threadIdx.x;
         const uint4* src = reinterpret_cast<const uint4*>(P.wb[b]);
 #pragma unroll
@@ -330,15 +235,16 @@ __global__ void __launch_bounds__(128) crt_mma_kernel(const __grid_constant__ Cr
         dev::fence_barrier_init();
     }
     if (warp == 0) {
-        dev::tmem_alloc(dev::smem_addr(tmem_slot), 2 * kCrtN);
+        dev::tmem_alloc(dev::smem_addr(tmem_slot), T::kTmemCols);
         dev::tmem_relinquish();
     }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     dev::tc_fence_before();
     __syncthreads();
     dev::tc_fence_after();
     const uint32_t tmem = *tmem_slot;
     int item = 0;
-    {  // the item of this CTA's first tile; later tiles only move forward
+    {  // the item of this CTA's first super-tile; later ones only move forward
         int hi = P.count - 1;
         while (item < hi) {
             const int mid = (item + hi + 1) >> 1;
@@ -350,77 +256,88 @@ __global__ void __launch_bounds__(128) crt_mma_kernel(const __grid_constant__ Cr
         while (item + 1 < P.count && P.items[item + 1].block0 <= tile) ++item;
         const CrtItem* I = P.items + item;
         const int64_t local = tile - I->block0;
-        return TileRef{I, (local % I->iblocks) * 32, (local / I->iblocks) * 4};
+        int64_t qd, rm;
+        divmod_index(local, I->iblocks, qd, rm);
+        return SuperTile{I, rm * 32, qd * 16};
     };
     const int64_t ntiles = P.tiles > blockIdx.x ? (P.tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
-    uint32_t wv[8];
-    TileRef cur{}, prev{};
+    uint32_t wv[2][8];
+    SuperTile cur{}, prev{};
     if (ntiles > 0) {
         cur = tile_ref(blockIdx.x);
-        crt_tile_load(cur, P.s, wv);
+        crt_tc_load(cur, warp, P.s, wv[0]);
+        crt_tc_load(cur, warp + 8, P.s, wv[1]);
     }
     bool ok = true;
     for (int64_t kk = 0; kk <= ntiles && ok; ++kk) {
         const int buf = static_cast<int>(kk & 1);
         if (kk < ntiles) {
-            crt_tile_store(sA0 + buf * 128 * 128, wv);
+            crt_tc_store(sA0 + buf * 128 * 128, warp, wv[0]);
+            crt_tc_store(sA0 + buf * 128 * 128, warp + 8, wv[1]);
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         }
         dev::tc_fence_before();
         __syncthreads();
         if (kk < ntiles && threadIdx.x == 0) {
             dev::tc_fence_after();
-            dev::mma_i8(tmem + static_cast<uint32_t>(buf * kCrtN),
-                        dev::sw128_kmajor_desc(dev::smem_addr(sA0 + buf * 128 * 128)),
-                        dev::sw128_kmajor_desc(dev::smem_addr(sB)), kCrtIdesc, 0u);
+            const uint32_t a0 = dev::smem_addr(sA0 + buf * 128 * 128);
+#pragma unroll
+            for (int g = 0; g < 4; ++g)
+                dev::mma_i8(tmem + static_cast<uint32_t>((4 * buf + g) * NC), dev::sw128_kmajor_desc(a0 + 32 * g),
+                            dev::sw128_kmajor_desc(dev::smem_addr(sB)), T::kIdesc, 0u);
             dev::tc_commit(dev::smem_addr(bar + buf));
         }
-        TileRef nxt{};
-        if (kk + 1 < ntiles) {  // the next tile's loads run under this iteration's waits and arithmetic
+        SuperTile nxt{};
+        if (kk + 1 < ntiles) {  // the next super-tile's loads run under this iteration's waits and arithmetic
             nxt = tile_ref(blockIdx.x + (kk + 1) * gridDim.x);
-            crt_tile_load(nxt, P.s, wv);
+            crt_tc_load(nxt, warp, P.s, wv[0]);
+            crt_tc_load(nxt, warp + 8, P.s, wv[1]);
         }
-        if (kk > 0) {  // finish tile kk - 1
+        if (kk > 0) {  // finish super-tile kk - 1
             const int pb = buf ^ 1;
             const uint32_t parity = static_cast<uint32_t>(((kk - 1) >> 1) & 1);
-            const int w_ok = dev::mbar_wait(dev::smem_addr(bar + pb), parity, abort_flag, P.err,
-                                            dev::kErrTimeoutAccFull, P.wait_ns) ? 1 : 0;
+            int w_ok = 1;  // one thread waits; the others sleep in the block barrier
+            if (threadIdx.x == 0)
+                w_ok = dev::mbar_wait(dev::smem_addr(bar + pb), parity, abort_flag, P.err, dev::kErrTimeoutAccFull,
+                                      P.wait_ns) ? 1 : 0;
             if (!__syncthreads_and(w_ok)) {
                 ok = false;
                 break;
             }
             dev::tc_fence_after();
-            uint32_t d0[32], d1[32];
-            const uint32_t taddr = tmem + (static_cast<uint32_t>(32 * warp) << 16) + static_cast<uint32_t>(pb * kCrtN);
-            dev::tmem_load_32x32(taddr, d0);
-            dev::tmem_load_32x32(taddr + 32, d1);
-            dev::tmem_load_wait();
             const CrtItem* __restrict__ I = prev.I;
-            const int64_t i = prev.i0 + lane, j = prev.j0 + warp;
-            if (i < I->m && j < I->n) {
-                uint64_t acc[NL];
+            const int q = warp & 3, h = warp >> 2;
+            const int64_t i = prev.i0 + crt_tc_row(lane);
+            const int tk = I->tk;
+            const int De = i < I->m ? exponent_of(I->maxA[i], tk) : 0;
 #pragma unroll
-                for (int l = 0; l < NL; ++l) {
-                    const uint32_t b0 = 4 * l < 32 ? d0[(4 * l) & 31] : d1[(4 * l) & 31];
-                    const uint32_t b1 = 4 * l + 1 < 32 ? d0[(4 * l + 1) & 31] : d1[(4 * l + 1) & 31];
-                    const uint32_t b2 = 4 * l + 2 < 32 ? d0[(4 * l + 2) & 31] : d1[(4 * l + 2) & 31];
-                    const uint32_t b3 = 4 * l + 3 < 32 ? d0[(4 * l + 3) & 31] : d1[(4 * l + 3) & 31];
-                    acc[l] = static_cast<uint64_t>(b0) + (static_cast<uint64_t>(b1) << 8) +
-                             (static_cast<uint64_t>(b2) << 16) + (static_cast<uint64_t>(b3) << 24);
+            for (int gg = 0; gg < 2; ++gg) {
+                const int g = h + 2 * gg;
+                uint32_t d[NC];
+                const uint32_t taddr = tmem + (static_cast<uint32_t>(32 * q) << 16) + static_cast<uint32_t>((4 * pb + g) * NC);
+                dev::tmem_load_32x32(taddr, *reinterpret_cast<uint32_t(*)[32]>(d));
+                if constexpr (NC == 64) dev::tmem_load_32x32(taddr + 32, *reinterpret_cast<uint32_t(*)[32]>(d + 32));
+                dev::tmem_load_wait();
+                const int64_t j = prev.j0 + 4 * g + q;
+                if (i < I->m && j < I->n) {
+                    uint64_t acc[NL];
+#pragma unroll
+                    for (int l = 0; l < NL; ++l) {
+                        const uint32_t lo = d[4 * l] + (d[4 * l + 1] << 8);      // < 2^30
+                        const uint32_t hi = d[4 * l + 2] + (d[4 * l + 3] << 8);  // < 2^30
+                        acc[l] = static_cast<uint64_t>(lo) + (static_cast<uint64_t>(hi) << 16);
+                    }
+                    const uint32_t uf = (1u << 15) + d[4 * NL] + (d[4 * NL + 1] << 8);
+                    const int64_t qv = static_cast<int64_t>(uf >> 16);
+                    const int Ej = exponent_of(I->maxB[j], tk);
+                    const bool nonfinite = De == kNonFinite || Ej == kNonFinite;
+                    double v = crt_finish<NL>(acc, qv, P.M, nonfinite ? 0 : De + Ej);
+                    if (nonfinite) v = __longlong_as_double(0x7FF8000000000000ll);
+                    double* cp = I->C + i + j * I->ldc;
+                    // the reference's unfused alpha*v + beta*c, one rounding per operation
+                    const double av = __dmul_rn(I->ar, v);
+                    *cp = I->br == 0.0 ? av : __dadd_rn(av, __dmul_rn(I->br, *cp));
                 }
-                const uint32_t f0 = 4 * NL < 32 ? d0[(4 * NL) & 31] : d1[(4 * NL) & 31];
-                const uint32_t f1 = 4 * NL + 1 < 32 ? d0[(4 * NL + 1) & 31] : d1[(4 * NL + 1) & 31];
-                const uint32_t uf = (1u << 15) + f0 + (f1 << 8);
-                const int64_t q = static_cast<int64_t>(uf >> 16);
-                const int tk = I->tk;
-                const int Ej = exponent_of(I->maxB[j], tk), De = exponent_of(I->maxA[i], tk);
-                const bool nonfinite = De == kNonFinite || Ej == kNonFinite;
-                double v = crt_finish<NL>(acc, q, P.M, nonfinite ? 0 : De + Ej);
-                if (nonfinite) v = __longlong_as_double(0x7FF8000000000000ll);
-                double* cp = I->C + i + j * I->ldc;
-                // the reference's unfused alpha*v + beta*c, one rounding per operation
-                const double av = __dmul_rn(I->ar, v);
-                *cp = I->br == 0.0 ? av : __dadd_rn(av, __dmul_rn(I->br, *cp));
             }
         }
         prev = cur;
@@ -430,7 +347,7 @@ __global__ void __launch_bounds__(128) crt_mma_kernel(const __grid_constant__ Cr
     __syncthreads();
     if (warp == 0) {
         dev::tc_fence_after();
-        dev::tmem_dealloc(tmem, 2 * kCrtN);
+        dev::tmem_dealloc(tmem, T::kTmemCols);
     }
 }
 
@@ -578,9 +495,9 @@ __global__ void __launch_bounds__(256) oz1_horner_kernel(const int64_t* __restri
 
 int64_t crt_item_blocks(CrtItem& it, int64_t block0) {
     it.block0 = block0;
-    if (it.mma) {  // tensor-core CRT: tiles of 32 rows x 4 columns
+    if (it.mma) {  // tensor-core CRT: super-tiles of 32 rows x 16 columns
         it.iblocks = ceil_div(it.m, 32);
-        return it.m > 0 ? it.iblocks * ceil_div(it.n, 4) : 0;
+        return it.m > 0 ? it.iblocks * ceil_div(it.n, 16) : 0;
     }
     const int64_t quads = ceil_div(it.m, 4);
     int tq = 1;
@@ -602,14 +519,48 @@ int sm_count() {
     }
     return cached[dev];
 }
+
+std::atomic<int> g_crt_path{2};
+
+template <int NL>
+void crt_tc_launch(const CrtTcParams& P, int64_t blocks, cudaStream_t st) {
+    using T = CrtTc<NL>;
+    const int per_sm = 512 / static_cast<int>(T::kTmemCols);
+    const int grid = static_cast<int>(std::min<int64_t>(blocks, static_cast<int64_t>(sm_count()) * per_sm));
+    crt_tc_kernel<NL><<<grid, kCrtThreads, T::kSmemLaunch, st>>>(P);
+}
+
 }  // namespace
+
+void set_crt_path(int path) { g_crt_path.store(path); }
+int crt_path() { return g_crt_path.load(); }
+
+bool crt_uses_mma(const Plan& plan, bool cplx) {
+    const int path = g_crt_path.load();
+    return !cplx && (path == 1 || (path == 2 && plan.nl >= kCrtTcMinLimbs));
+}
+
+cudaError_t prepare_crt_kernels() {
+    cudaError_t e = cudaSuccess;
+    auto set = [&](const void* f, int bytes) {
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    };
+    set(reinterpret_cast<const void*>(crt_tc_kernel<2>), CrtTc<2>::kSmemLaunch);
+    set(reinterpret_cast<const void*>(crt_tc_kernel<3>), CrtTc<3>::kSmemLaunch);
+    set(reinterpret_cast<const void*>(crt_tc_kernel<4>), CrtTc<4>::kSmemLaunch);
+    set(reinterpret_cast<const void*>(crt_tc_kernel<5>), CrtTc<5>::kSmemLaunch);
+    set(reinterpret_cast<const void*>(crt_tc_kernel<6>), CrtTc<6>::kSmemLaunch);
+    set(reinterpret_cast<const void*>(crt_tc_kernel<7>), CrtTc<7>::kSmemLaunch);
+    set(reinterpret_cast<const void*>(crt_tc_kernel<8>), CrtTc<8>::kSmemLaunch);
+    return e;
+}
 
 void launch_crt(const CrtItem* d_items, int count, int64_t blocks, const Plan& plan, bool cplx, int* err,
                 cudaStream_t st) {
     if (crt_uses_mma(plan, cplx)) {
         if (count <= 0 || blocks <= 0) return;
-        static thread_local CrtMmaParams P;
-        P = CrtMmaParams{};
+        static thread_local CrtTcParams P;
+        P = CrtTcParams{};
         P.items = d_items;
         P.count = count;
         P.tiles = blocks;
@@ -626,9 +577,15 @@ void launch_crt(const CrtItem* d_items, int count, int64_t blocks, const Plan& p
         }
         P.err = err;
         P.wait_ns = dev::kWaitLimitNs;
-        // four CTAs per SM: 4 x 128 of the 512 TMEM columns (and 4 x 41 KB of shared memory)
-        const int grid = static_cast<int>(std::min<int64_t>(blocks, static_cast<int64_t>(sm_count()) * 4));
-        crt_mma_kernel<8><<<grid, 128, kCrtSmem, st>>>(P);  // crt_uses_mma: 8 limbs only
+        switch (plan.nl) {
+            case 2: crt_tc_launch<2>(P, blocks, st); break;
+            case 3: crt_tc_launch<3>(P, blocks, st); break;
+            case 4: crt_tc_launch<4>(P, blocks, st); break;
+            case 5: crt_tc_launch<5>(P, blocks, st); break;
+            case 6: crt_tc_launch<6>(P, blocks, st); break;
+            case 7: crt_tc_launch<7>(P, blocks, st); break;
+            default: crt_tc_launch<8>(P, blocks, st); break;
+        }
         return;
     }
     if (count <= 0 || blocks <= 0) return;

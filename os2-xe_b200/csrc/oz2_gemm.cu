@@ -24,6 +24,7 @@
 #include <atomic>
 #include <cstdio>
 
+#include "oz2_crt_math.cuh"
 #include "oz2_kernels.cuh"
 #include "oz2_ptx.cuh"
 
@@ -54,6 +55,7 @@ struct GemmParams {
     int* err;
     uint64_t wait_ns;  // limit of every bounded mbarrier wait
     int stall;         // failure-path test: the MMA issuer issues nothing, so the waits run out
+    CrtConst cc;       // kKindCrt: the plan's CRT constants (all items of the launch share the plan)
 };
 
 struct Job {
@@ -62,7 +64,8 @@ struct Job {
     int ti, tj;
     int64_t nch;  // k chunks
 };
-__device__ __forceinline__ Job decode(const GemmParams& P, int64_t job) {
+// per_tile: the job is a tile and runs every modulus (kKindCrt); otherwise (group, modulus, tile)
+__device__ __forceinline__ Job decode(const GemmParams& P, int64_t job, bool per_tile = false) {
     int lo = 0, hi = P.count - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
@@ -76,7 +79,7 @@ __device__ __forceinline__ Job decode(const GemmParams& P, int64_t job) {
     // several times a 32-bit one, and every warp decodes every job)
     const uint32_t local = static_cast<uint32_t>(job - J.I->job0);
     const uint32_t tiles = static_cast<uint32_t>(J.I->tiles);
-    const uint32_t gt = local / tiles;
+    const uint32_t gt = per_tile ? 0u : local / tiles;
     J.gt = static_cast<int>(gt);
     const uint32_t tile = local - gt * tiles;
     const uint32_t tiles_i = static_cast<uint32_t>(J.I->tiles_i), tiles_j = static_cast<uint32_t>(J.I->tiles_j);
@@ -96,12 +99,18 @@ __device__ __forceinline__ Job decode(const GemmParams& P, int64_t job) {
 // baseline (job t = digit pair, int64 atomic sums per anti-diagonal instead of residues);
 // kKindCert the certificate (bf16 planes of scaled magnitudes, kind::f16 MMAs, the largest
 // (R'_i + S'_j) / G_ij and 1 / G_ij per adaptive tile instead of residues)
-constexpr int kKindResidue = 0, kKindOz1 = 1, kKindCert = 2;
+// kKindCrt the Ozaki-II GEMM with the CRT in the epilogue (a job is a tile and all its s <= 8
+// moduli: each modulus's residues go to tensor memory as packed bytes, columns 2 BN + 128 h + 16 t
+// + w for epilogue half h, modulus t and word w; after the last modulus the epilogue reconstructs
+// its 64 entries per lane and writes C)
+constexpr int kKindResidue = 0, kKindOz1 = 1, kKindCert = 2, kKindCrt = 3;
 
 template <int BN, int KIND>
 __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __grid_constant__ GemmParams P) {
-    constexpr bool OZ1 = KIND == kKindOz1, CERT = KIND == kKindCert;
+    constexpr bool OZ1 = KIND == kKindOz1, CERT = KIND == kKindCert, CRTF = KIND == kKindCrt;
+    static_assert(!CRTF || BN == 128, "the fused CRT keeps its residues beside two 128-column accumulators");
     using C = Cfg<BN>;
+    constexpr uint32_t kTmemCols = CRTF ? 512u : C::kTmemCols;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t{1023});
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + C::kStages * C::kStageBytes);
@@ -130,7 +139,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
         dev::fence_barrier_init();
     }
     if (warp == 1) {
-        dev::tmem_alloc(dev::smem_addr(tmem_slot), C::kTmemCols);
+        dev::tmem_alloc(dev::smem_addr(tmem_slot), kTmemCols);
         dev::tmem_relinquish();
     }
     dev::tc_fence_before();
@@ -146,9 +155,12 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
             uint32_t issued_mask = 0, issued_phase = 0;
             bool ok = true;
             for (int64_t job = blockIdx.x; ok && job < P.jobs; job += nprog) {
-                const Job J = decode(P, job);
+                const Job J = decode(P, job, CRTF);
                 const int64_t kb_total = J.I->kb_total, row_block = kb_total * kTileBytes;
-                const int pj = OZ1 ? J.I->pair_b[J.gt] : J.gt, pi = OZ1 ? J.I->pair_a[J.gt] : J.gt;
+                const int nt = CRTF ? J.I->s : 1;
+                for (int tt = 0; ok && tt < nt; ++tt) {
+                const int gt = CRTF ? tt : J.gt;
+                const int pj = OZ1 ? J.I->pair_b[gt] : gt, pi = OZ1 ? J.I->pair_a[gt] : gt;
                 const int8_t* srcJ = J.I->planes_j + pj * J.I->pstride_j + J.tj * row_block;
                 const int8_t* srcI = J.I->planes_i + pi * J.I->pstride_i + (static_cast<int64_t>(J.ti) * (BN / 128)) * row_block;
                 for (int64_t kb = 0; ok && kb < kb_total; ++kb) {
@@ -170,6 +182,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
                         phase ^= 1u;
                     }
                 }
+                }
             }
             if (!ok) {  // let every copy that was issued land before the CTA exits
                 for (int i = 0; i < C::kStages; ++i)
@@ -183,8 +196,10 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
             bool ok = !P.stall, issued = false;
             int local = 0;  // (job, chunk) pairs processed: selects the accumulator
             for (int64_t job = blockIdx.x; ok && job < P.jobs; job += nprog) {
-                const Job J = decode(P, job);
+                const Job J = decode(P, job, CRTF);
                 const int64_t kb_total = J.I->kb_total;
+                const int nt = CRTF ? J.I->s : 1;
+                for (int tt = 0; ok && tt < nt; ++tt)
                 for (int64_t c = 0; ok && c < J.nch; ++c, ++local) {
                     const int acc = local & 1;
                     const uint32_t use = static_cast<uint32_t>(local >> 1);
@@ -239,9 +254,11 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
         int local = 0;
         bool ok = true;
         for (int64_t job = blockIdx.x; ok && job < P.jobs; job += nprog) {
-            const Job J = decode(P, job);
-            const int t = J.gt % J.I->s;
-            constexpr bool RES = KIND == kKindResidue;
+            const Job J = decode(P, job, CRTF);
+            const int nt = CRTF ? J.I->s : 1;
+            for (int tt = 0; ok && tt < nt; ++tt) {
+            const int t = CRTF ? tt : J.gt % J.I->s;
+            constexpr bool RES = KIND == kKindResidue || CRTF;
             const uint32_t m = RES ? J.I->mod_m[t] : 1u, mu = RES ? J.I->mod_mu[t] : 0u,
                            kbias = RES ? J.I->mod_kbias[t] : 0u;
             // at most kExactKB k-blocks (one chunk): |c| <= kExactSum, so u = c + kbias30 < 2^31 and
@@ -251,7 +268,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
             const uint32_t mxs = RES ? J.I->mod_mxs[t] : 7u;
             const int64_t j = static_cast<int64_t>(J.tj) * kGemmJ + quarter * 32 + lane;
             const int64_t mm = J.I->m, nn = J.I->n;
-            uint8_t* rowj = RES ? J.I->resid + J.gt * J.I->rstride + j * 32 : nullptr;  // + (i / 32) * 32 n
+            uint8_t* rowj = RES && !CRTF ? J.I->resid + J.gt * J.I->rstride + j * 32 : nullptr;  // + (i / 32) * 32 n
             // certificate: this lane's column sum (zero for a padding column or an all-zero column,
             // whose entries are skipped)
             const float sj = CERT && j < nn ? static_cast<float>(J.I->cert_sb[j]) : 0.0f;
@@ -324,6 +341,23 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
                                     atomicAdd(dst + (i0 + b) * ld, static_cast<unsigned long long>(
                                                                        static_cast<long long>(static_cast<int32_t>(cur[b]))));
                         }
+                    } else if constexpr (CRTF) {
+                        // residues of this modulus as packed bytes into tensor memory (every lane
+                        // and chunk: padding entries are never read back)
+                        uint32_t w[8];
+#pragma unroll
+                        for (int q = 0; q < 8; ++q) {
+                            uint32_t r4[4];
+#pragma unroll
+                            for (int b = 0; b < 4; ++b) {
+                                const uint32_t u = cur[4 * q + b] + kbias30;
+                                r4[b] = u - (__umulhi(u, mx31) >> mxs) * m;
+                            }
+                            w[q] = __byte_perm(__byte_perm(r4[0], r4[1], 0x0040), __byte_perm(r4[2], r4[3], 0x0040), 0x5410);
+                        }
+                        dev::tmem_store_32x8(tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) +
+                                                 static_cast<uint32_t>(2 * BN + 128 * half + 16 * tt + 8 * cc),
+                                             w);
                     } else if (exact) {
                         if (j < nn && i0 < mm) {
                             uint32_t w[8];
@@ -375,6 +409,57 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
                 __syncwarp();
                 if (lane == 0) dev::mbar_arrive(acc_empty(acc));
             }
+            }
+            if constexpr (CRTF) {
+                // every modulus of the tile is in: reconstruct this lane's column j for the 64 rows
+                // i of this warp's half, four entries per word, eight words per pass
+                if (ok) {
+                    dev::tmem_store_wait();
+                    const GemmItem* __restrict__ I = J.I;
+                    const int tk = I->crt_tk, s_ = I->s;
+                    const int64_t j = static_cast<int64_t>(J.tj) * kGemmJ + quarter * 32 + lane;
+                    const int64_t mm = I->m, nn = I->n;
+                    const int Ej = j < nn ? exponent_of(I->crt_maxB[j], tk) : 0;
+                    const uint32_t rbase = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) +
+                                           static_cast<uint32_t>(2 * BN + 128 * half);
+#pragma unroll 1
+                    for (int wb = 0; wb < 2; ++wb) {
+                        uint32_t R8[kCrtFusedMaxS][8];
+#pragma unroll
+                        for (int t2 = 0; t2 < kCrtFusedMaxS; ++t2) {
+                            if (t2 < s_) {
+                                dev::tmem_load_32x8(rbase + 16 * t2 + 8 * wb, R8[t2]);
+                            } else {
+#pragma unroll
+                                for (int q = 0; q < 8; ++q) R8[t2][q] = 0;
+                            }
+                        }
+                        dev::tmem_load_wait();
+#pragma unroll
+                        for (int q = 0; q < 8; ++q) {
+                            uint32_t lo[4], hi[4];  // moduli 0..3 and 4..7 of the word's four entries
+                            transpose4(R8[0][q], R8[1][q], R8[2][q], R8[3][q], lo);
+                            transpose4(R8[4][q], R8[5][q], R8[6][q], R8[7][q], hi);
+#pragma unroll
+                            for (int e = 0; e < 4; ++e) {
+                                const int64_t i = static_cast<int64_t>(J.ti) * BN + half * 64 + 4 * (8 * wb + q) + e;
+                                if (i < mm && j < nn) {
+                                    const int De = exponent_of(I->crt_maxA[i], tk);
+                                    const bool nonfinite = De == kNonFinite || Ej == kNonFinite;
+                                    const uint32_t R[2] = {lo[e], hi[e]};
+                                    double v = crt_value<kCrtFusedMaxS, 2>(R, P.cc, nonfinite ? 0 : De + Ej);
+                                    if (nonfinite) v = __longlong_as_double(0x7FF8000000000000ll);
+                                    double* cp = I->C + i + j * I->ldc;
+                                    // the reference's unfused alpha*v + beta*c, one rounding per operation
+                                    const double av = __dmul_rn(I->crt_alpha, v);
+                                    *cp = I->crt_beta == 0.0 ? av : __dadd_rn(av, __dmul_rn(I->crt_beta, *cp));
+                                }
+                            }
+                        }
+                    }
+                    dev::tc_fence_before();
+                }
+            }
         }
     }
     __syncwarp();
@@ -382,7 +467,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
     __syncthreads();
     if (warp == 1) {
         dev::tc_fence_after();
-        dev::tmem_dealloc(tmem_base, C::kTmemCols);
+        dev::tmem_dealloc(tmem_base, kTmemCols);
     }
 }
 
@@ -413,6 +498,11 @@ cudaError_t prepare_gemm_kernels() {
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(gemm_i8_modm_kernel<256, kKindCert>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  Cfg<256>::kSmemBytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(gemm_i8_modm_kernel<128, kKindCrt>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 Cfg<128>::kSmemBytes);
+    if (e == cudaSuccess) e = prepare_split_kernels();
+    if (e == cudaSuccess) e = prepare_crt_kernels();
     return e;
 }
 
@@ -439,6 +529,22 @@ void launch_gemm_oz1(const GemmItem* d_items, int count, int64_t jobs, const Gem
     const GemmParams P = make_params(d_items, count, cfg.group_j > 0 ? cfg.group_j : 16, jobs, err);
     const int grid = static_cast<int>(std::min<int64_t>(num_sms, jobs));
     launch_bn<256, kKindOz1>(P, grid, st);
+}
+
+namespace {
+std::atomic<int> g_crt_fusion{0};
+}  // namespace
+
+void set_crt_fusion(int on) { g_crt_fusion.store(on ? 1 : 0); }
+int crt_fusion() { return g_crt_fusion.load(); }
+
+void launch_gemm_crt(const GemmItem* d_items, int count, int64_t jobs, const Plan& plan, int group_j, int num_sms,
+                     int* err, cudaStream_t st) {
+    if (count <= 0 || jobs <= 0) return;
+    GemmParams P = make_params(d_items, count, group_j > 0 ? group_j : 16, jobs, err);
+    crt_constants(plan, P.cc);
+    const int grid = static_cast<int>(std::min<int64_t>(num_sms, jobs));
+    launch_bn<128, kKindCrt>(P, grid, st);
 }
 
 void launch_gemm_cert(const GemmItem* d_items, int count, int64_t jobs, int num_sms, int* err, cudaStream_t st) {

@@ -35,6 +35,7 @@ constexpr int kGemmIPad = 256;
 constexpr int kChunkKB = 1023;
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
 inline int64_t round_up(int64_t a, int64_t b) { return ceil_div(a, b) * b; }
 
 // plane geometry of one side
@@ -70,12 +71,22 @@ struct SplitItem {
     int64_t ldx, rows, k;
     int row_contig, cplx, conj;
     int tk, s;
-    const unsigned long long* maxbits;  // of the panel's rows
+    const unsigned long long* maxbits;  // of the panel's rows (written by the fused scale + split)
     int8_t* planes;                     // s planes (complex: 3 groups of s)
     int64_t plane_bytes, kb_total, rows_pad;
     int64_t block0, rblocks, kblocks;   // blocks = rblocks * kblocks
     ModConst mc[kMaxModuliExt];
+    // tc: the tensor-core split runs this item (real operands); block0 is then its first unit of
+    // 512 elements (4 rows x 128 inner indices, or 16 x 32 when rows are contiguous), rblocks x
+    // kblocks its units
+    int tc;
+    // fuse: the scale pass is fused into this item's split (real operands, k <= kFuseMaxK): the
+    // kernel takes the row maxima itself and writes them to maxbits; rblocks blocks of whole rows
+    int fuse;
 };
+// largest k for which the scale pass is fused into the split (k contiguous / rows contiguous)
+constexpr int64_t kFuseMaxK = 2048;
+constexpr int64_t kFuseMaxKRowc = 1024;
 
 // ---- gemm: one item per problem; jobs = groups * s * tiles, each job runs all k chunks
 constexpr int kMaxOz1Pairs = 45;  // Ozaki Scheme I: L (L + 1) / 2 digit pairs, L <= 9
@@ -102,7 +113,18 @@ struct GemmItem {
     const double* cert_sb;
     unsigned int* cert_q;
     int64_t cert_tile, cert_na;
+    // CRT in the epilogue (launch_gemm_crt): C (rows i, columns j of this item) and its alpha /
+    // beta update, the maxima of op(A)'s rows and op(B)'s columns for the unscaling
+    double* C;
+    int64_t ldc;
+    const unsigned long long* crt_maxA;
+    const unsigned long long* crt_maxB;
+    int crt_tk;
+    double crt_alpha, crt_beta;
 };
+// largest s whose residues fit in tensor memory beside the two accumulators (BN = 128: 8 x 32
+// columns of packed bytes), so that the GEMM's epilogue can run the CRT itself
+constexpr int kCrtFusedMaxS = 8;
 
 // ---- crt: one item per problem; all items of a launch share s
 struct CrtItem {
@@ -115,8 +137,8 @@ struct CrtItem {
     double* C;
     int64_t block0, iblocks;  // blocks = ceil(n / jb) * iblocks
     int tq, jb;               // a block: tq threads (4 rows each) along i x jb columns, tq * jb = 256
-    // mma: the tensor-core CRT (real items of 8-limb plans, s = 30..32): block0 is the first tile
-    // of 32 rows x 4 columns (128 entries, one tcgen05 MMA) and iblocks the tiles along i;
+    // mma: the tensor-core CRT (real items, crt_uses_mma): block0 is the first super-tile of 32
+    // rows x 16 columns (four tcgen05 MMAs of 128 entries) and iblocks the super-tiles along i;
     // otherwise the dp2a kernel's geometry
     int mma;
 };
@@ -124,12 +146,25 @@ struct CrtItem {
 // host-side helpers filling the launch-geometry fields; they return the blocks of the item
 int64_t scale_item_blocks(ScaleItem& it, int num_sms, int64_t block0);
 int64_t split_item_blocks(SplitItem& it, int64_t block0);
+// the split's geometry for the kernel that will run the item: the tensor-core split for real
+// items while it is selected, else split_item_blocks; sets it.tc
+int64_t split_geometry(SplitItem& it, int64_t block0);
+// process-wide selection of the real split: 0 the dp4a kernel (default), 1 the tensor-core split
+void set_split_path(int tc);
+int split_path();
+// process-wide: whether real operands with k <= kFuseMaxK (kFuseMaxKRowc when rows are contiguous)
+// take the fused scale + split (default on); fuse_scale tells whether an operand qualifies
+void set_scale_fusion(int on);
+bool fuse_scale(bool cplx, bool row_contig, int64_t k);
 int64_t crt_item_blocks(CrtItem& it, int64_t block0);
 
 // launches over device tables (d_items) whose host copies (h_items) give the geometry
 void launch_scale(const ScaleItem* d_items, const ScaleItem* h_items, int count, int64_t blocks, cudaStream_t st);
-// all items of one split launch share row_contig, cplx and the narrow/wide limb path
-void launch_split(const SplitItem* d_items, const SplitItem* h_items, int count, int64_t blocks, cudaStream_t st);
+// all items of one split launch share row_contig, cplx, tc and the narrow/wide/widest limb path;
+// err: the device error word for the tensor-core split's bounded wait on its MMA (may be null
+// only for launches without tc items)
+void launch_split(const SplitItem* d_items, const SplitItem* h_items, int count, int64_t blocks, int* err,
+                  cudaStream_t st);
 
 struct GemmConfig {
     int bn = 256;        // tile width along i (MMA N): 256 or 128
@@ -141,6 +176,16 @@ void launch_gemm(const GemmItem* d_items, int count, int64_t jobs, const GemmCon
 // the same GEMM on bf16 planes of scaled magnitudes, with the certificate's maxima in the
 // epilogue instead of residues (one job per tile; items as for launch_gemm with s = 1)
 void launch_gemm_cert(const GemmItem* d_items, int count, int64_t jobs, int num_sms, int* err, cudaStream_t st);
+// the same GEMM with the CRT in its epilogue (real items of one plan with s <= kCrtFusedMaxS and
+// at most kExactKB k blocks): one job per 128 x 128 tile runs all s moduli, keeps the residues in
+// tensor memory and writes C; no residue planes and no CRT launch. BN is 128.
+void launch_gemm_crt(const GemmItem* d_items, int count, int64_t jobs, const Plan& plan, int group_j, int num_sms,
+                     int* err, cudaStream_t st);
+// process-wide: whether fixed-s real problems that qualify take launch_gemm_crt (default off:
+// measured slower than the GEMM followed by the CRT launch, since the reconstruction of a tile's
+// 16384 entries runs on the GEMM's eight epilogue warps while the MMA pipeline waits)
+void set_crt_fusion(int on);
+int crt_fusion();
 // the same GEMM for the Ozaki Scheme I baseline: digit-pair jobs, int64 atomic sums per diagonal
 void launch_gemm_oz1(const GemmItem* d_items, int count, int64_t jobs, const GemmConfig& cfg, int num_sms, int* err,
                      cudaStream_t st);
@@ -152,17 +197,24 @@ void launch_oz1_horner(const int64_t* acc, int64_t m, int64_t n, int L, const un
                        const unsigned long long* maxB, int tk, double* C, int64_t ldc, cudaStream_t st);
 int64_t gemm_tiles_i(int64_t m, int bn);
 
-// whether launch_crt runs the tensor-core CRT for this plan: real items with 8 limbs (s = 30..32),
-// where it measured faster than the dp2a kernel (B200, 4096^2: 0.60 against 0.77 ms at s = 32,
-// slower below: 1.96 against 0.73 ms at 8192^2, s = 16); the item's `mma` flag must match
-inline bool crt_uses_mma(const Plan& plan, bool cplx) { return !cplx && plan.nl == 8; }
+// whether launch_crt runs the tensor-core CRT for this plan (real items only): process-wide path
+// 0 the dp2a kernel, 1 the tensor-core CRT, 2 (default) the tensor-core CRT from
+// kCrtTcMinLimbs limbs on (8 limbs: s = 30..32); the items' `mma` flag must match
+constexpr int kCrtTcMinLimbs = 8;
+bool crt_uses_mma(const Plan& plan, bool cplx);
+void set_crt_path(int path);
+int crt_path();
+// sets the tensor-core CRT kernels' shared-memory attribute (with prepare_gemm_kernels)
+cudaError_t prepare_crt_kernels();
 // all items of one CRT launch share s (the CRT table is a kernel parameter); err: the device error
 // word for the real kernel's bounded wait on its MMA (may be null)
 void launch_crt(const CrtItem* d_items, int count, int64_t blocks, const Plan& plan, bool cplx, int* err,
                 cudaStream_t st);
 
-// sets the GEMM kernels' shared-memory attribute (once per device, before any graph capture)
+// sets the shared-memory attribute of the GEMM and tensor-core split kernels (once per device,
+// before any graph capture)
 cudaError_t prepare_gemm_kernels();
+cudaError_t prepare_split_kernels();
 // Failure-path test of the GEMM's bounded waits (process-wide, read at each launch): wait_ns
 // limits every mbarrier wait (0 = the 2 s default); with stall set the MMA issuer of every CTA
 // issues nothing, so the other roles' waits run out, record their code in the error word, drain

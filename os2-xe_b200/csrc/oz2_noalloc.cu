@@ -195,7 +195,7 @@ extern "C" int oz2_dgemm_noalloc(void* stream, char ta, char tb, int64_t m, int6
         sp.kb_total = gg.kb_total;
         sp.rows_pad = gg.rows_pad;
         for (int t = 0; t < s; ++t) sp.mc[t] = mc[t];
-        split_item_blocks(sp, 0);
+        split_geometry(sp, 0);
     }
     GemmConfig cfg;
     cfg.bn = m <= 384 ? 128 : 256;
@@ -238,6 +238,7 @@ extern "C" int oz2_dgemm_noalloc(void* stream, char ta, char tb, int64_t m, int6
     c.ar = alpha;
     c.br = beta;
     c.C = C;
+    c.mma = crt_uses_mma(p, false) ? 1 : 0;
     const int64_t crt_blocks = crt_item_blocks(c, 0);
     static_assert(sizeof(Tables) <= 8 * 1024, "item tables exceed their scratch region");
     unsigned char* dtab = scratch + o_D;
@@ -246,7 +247,7 @@ extern "C" int oz2_dgemm_noalloc(void* stream, char ta, char tb, int64_t m, int6
     for (int side = 0; side < 2; ++side)
         launch_scale(&D->sc[side], &T.sc[side], 1, T.sc[side].rblocks * ceil_div(k, T.sc[side].kchunk), st);
     for (int side = 1; side >= 0; --side)
-        launch_split(&D->sp[side], &T.sp[side], 1, T.sp[side].rblocks * T.sp[side].kblocks, st);
+        launch_split(&D->sp[side], &T.sp[side], 1, T.sp[side].rblocks * T.sp[side].kblocks, err, st);
     launch_gemm(&D->g, 1, g.tiles * s, cfg, num_sms, err, st);
     launch_crt(&D->c, 1, crt_blocks, p, false, err, st);
     e = cudaGetLastError();

@@ -30,6 +30,14 @@ constexpr int kWideScaleBits = 92;
 constexpr int kNonFinite = -2147483647 - 1;
 
 // 32-bit limbs of M per s: max(2, floor(log2 M / 32) + 1) (ref src/ozaki2_gpu.hpp:55-59, :168)
+// a = q b + r for the block and unit indices of a launch (below 2^31, which the host checks for
+// every grid): 32-bit division, several times cheaper than the 64-bit one
+OZ2_HD inline void divmod_index(int64_t a, int64_t b, int64_t& q, int64_t& r) {
+    const uint32_t qq = static_cast<uint32_t>(a) / static_cast<uint32_t>(b);
+    q = qq;
+    r = a - static_cast<int64_t>(qq) * b;
+}
+
 OZ2_HD constexpr int limbs_for(int s) {
     constexpr int t[kMaxModuliExt + 1] = {0, 0, 2, 2, 2, 2, 2, 2, 2, 3, 3, 3, 3, 4, 4, 4, 4,
                                           5, 5, 5, 5, 6, 6, 6, 6, 6, 7, 7, 7, 7, 8, 8, 8};

@@ -8,8 +8,10 @@
 //        modulo each m_t in [-h_t, m_t-1-h_t] (ref :407-455, complex 3M form :457-520),
 //        stored as int8 in the pre-tiled plane layout of oz2_kernels.cuh.
 #include <algorithm>
+#include <atomic>
 
 #include "oz2_kernels.cuh"
+#include "oz2_ptx.cuh"
 
 namespace oz2 {
 namespace {
@@ -44,7 +46,8 @@ template <bool CPLX, bool ROWC>
 __global__ void __launch_bounds__(256) scale_kernel(const ScaleItem* __restrict__ items, int count) {
     const ScaleItem* I = items + find_item(items, count, blockIdx.x);
     const int64_t local = static_cast<int64_t>(blockIdx.x) - I->block0;
-    const int64_t rb = local % I->rblocks, kc = local / I->rblocks;
+    int64_t rb, kc;
+    divmod_index(local, I->rblocks, kc, rb);
     const unsigned long long* X = reinterpret_cast<const unsigned long long*>(I->X);
     const int64_t rows = I->rows, k = I->k, ldx = I->ldx, kchunk = I->kchunk;
     if (ROWC) {
@@ -191,17 +194,14 @@ __device__ __forceinline__ void split_coords(int64_t bx, int64_t by, int64_t& r,
     }
 }
 
+// The EPT elements (r, k0 .. k0 + EPT - 1) of every plane, r < rows_pad and k0 < the padded k:
+// maxb is the row's maximum bits (read only for r < rows).
 template <int NLIMB, bool CPLX, bool ROWC>
-__global__ void __launch_bounds__(256) split_kernel(const SplitItem* __restrict__ items, int count) {
+__device__ __forceinline__ void split_piece(const SplitItem* __restrict__ I, int64_t r, int64_t k0,
+                                            unsigned long long maxb) {
     constexpr int EPT = split_ept<NLIMB, CPLX>();
-    const SplitItem* __restrict__ I = items + find_item(items, count, blockIdx.x);
-    const int64_t local = static_cast<int64_t>(blockIdx.x) - I->block0;
-    const int64_t bx = local % I->rblocks, by = local / I->rblocks;
-    int64_t r, k0;
-    split_coords<EPT, ROWC>(bx, by, r, k0);
     const int64_t kb_total = I->kb_total, plane_bytes = I->plane_bytes, ldx = I->ldx, k = I->k;
     const int64_t rows = I->rows;
-    if (r >= I->rows_pad || k0 >= kb_total * kTileK) return;
     const double* X = I->X;
     const int conj = I->conj, nmod = I->s;
     const int64_t rb = r >> 7;
@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(256) split_kernel(const SplitItem* __restrict_
         }
         return;
     }
-    const int e = exponent_of(I->maxbits[r], I->tk);
+    const int e = exponent_of(maxb, I->tk);
     const bool live = e != kNonFinite;
 
     constexpr int NG = CPLX ? 2 : 1;
@@ -307,6 +307,375 @@ __global__ void __launch_bounds__(256) split_kernel(const SplitItem* __restrict_
     }
 }
 
+template <int NLIMB, bool CPLX, bool ROWC>
+__global__ void __launch_bounds__(256) split_kernel(const SplitItem* __restrict__ items, int count) {
+    constexpr int EPT = split_ept<NLIMB, CPLX>();
+    const SplitItem* __restrict__ I = items + find_item(items, count, blockIdx.x);
+    const int64_t local = static_cast<int64_t>(blockIdx.x) - I->block0;
+    int64_t bx, by;
+    divmod_index(local, I->rblocks, by, bx);
+    int64_t r, k0;
+    split_coords<EPT, ROWC>(bx, by, r, k0);
+    if (r >= I->rows_pad || k0 >= I->kb_total * kTileK) return;
+    split_piece<NLIMB, CPLX, ROWC>(I, r, k0, r < I->rows && k0 < I->k ? I->maxbits[r] : 0ull);
+}
+
+// ------------------------------------------------------------------ scale fused into the split
+// One launch for both phases of a real operand (ref src/ozaki2_gpu.hpp:974-989 then :1004-1022
+// run them as two passes over A and B): a block owns whole plane rows, takes their maxima over
+// all of k (and writes them for the CRT), then splits the same rows. The second read of the rows
+// follows the first within the block, so it is served by L2 while the rows that all resident
+// blocks have in flight fit there (the launcher uses it for k up to kFuseMaxK: at most 8 rows of
+// 16 KiB, or 16 rows of 4 KiB, per block). k contiguous: 8 rows per block, a warp per row, lanes
+// over k. Rows contiguous: EPT rows per block (a 128-byte line per inner index), the 256 / EPT
+// thread groups over k, then the split's own warp layout over 256-wide k blocks.
+template <int NLIMB, bool ROWC>
+__global__ void __launch_bounds__(256) scale_split_kernel(const SplitItem* __restrict__ items, int count) {
+    constexpr int EPT = split_ept<NLIMB, false>();
+    constexpr int RB = ROWC ? EPT : 8;  // rows per block
+    __shared__ unsigned long long smax[RB];
+    const SplitItem* __restrict__ I = items + find_item(items, count, blockIdx.x);
+    const int64_t r0 = (static_cast<int64_t>(blockIdx.x) - I->block0) * RB;
+    const unsigned long long* X = reinterpret_cast<const unsigned long long*>(I->X);
+    const int64_t rows = I->rows, k = I->k, ldx = I->ldx, kpad = I->kb_total * kTileK;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid < RB) smax[tid] = 0;
+    __syncthreads();
+    if (ROWC) {
+        const int64_t r = r0 + tid % RB;
+        unsigned long long best = 0;
+        if (r < rows)
+            for (int64_t p = tid / RB; p < k; p += 256 / RB) best = max(best, __ldg(X + r + p * ldx) & kAbsMask);
+        if (best) atomicMax(&smax[tid % RB], best);
+    } else {
+        const int64_t r = r0 + warp;
+        unsigned long long best = 0;
+        if (r < rows)
+            for (int64_t p = lane; p < k; p += 32) best = max(best, __ldg(X + p + r * ldx) & kAbsMask);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) best = max(best, __shfl_xor_sync(0xFFFFFFFFu, best, o));
+        if (lane == 0) smax[warp] = best;
+    }
+    __syncthreads();
+    if (tid < RB && r0 + tid < rows) const_cast<unsigned long long*>(I->maxbits)[r0 + tid] = smax[tid];  // for the CRT
+    if (ROWC) {
+        for (int64_t by = 0; by * kSplitRowcK < kpad; ++by) {
+            int64_t r, k0;
+            split_coords<EPT, true>(blockIdx.x - I->block0, by, r, k0);  // bx: this block's EPT rows
+            if (r < I->rows_pad && k0 < kpad) split_piece<NLIMB, false, true>(I, r, k0, smax[r - r0]);
+        }
+    } else {
+        const int64_t r = r0 + warp;
+        if (r < I->rows_pad)
+            for (int64_t k0 = lane * EPT; k0 < kpad; k0 += 32 * EPT) split_piece<NLIMB, false, false>(I, r, k0, smax[warp]);
+    }
+}
+
+// ------------------------------------------------------------------ tensor-core split
+// The byte dot products of byte_residue, v_t = Sum_l byte_l (2^(8 l) mod m_t), form a small
+// matrix product: (moduli x bytes) times (bytes x elements). One tcgen05.mma kind::i8 (unsigned
+// A and B, M = 128, N = 256, K = 32, int32 in TMEM) computes them for a unit of 512 elements:
+//   B (N x K, K-major): column n holds two elements, segment g = 0, 1 in bytes 16 g .. 16 g + 15
+//     (the offset integer's 8 / 12 / 16 bytes, zero-filled);
+//   A (M x K, K-major): row 32 q + l is the slot sigma = 32 (q % Qa) + l, sigma < 2 s: segment
+//     sigma / s, modulus sigma % s, the weights 2^(8 l) mod m in that segment's bytes. With
+//     Qa = 1 (s <= 16) all four TMEM lane quarters hold the same 32 slots, with Qa = 2 (s <= 32)
+//     quarters 0, 1 hold the 2 s slots and 2, 3 repeat them, so every epilogue warp reads its own
+//     lane quarter (a hardware rule) and the quarters split the 256 columns between them.
+// The epilogue turns v + koff into the residue (x + h) mod m by the exact multiply-high quotient
+// (v < 2^20), subtracts h modulo 256 and stores the 32 residues of one slot's 32 consecutive
+// inner indices as one 32-byte piece of its plane. The integer pipe keeps one multiply-high and
+// one multiply-subtract per residue; the dp4a of byte_residue move to the tensor core.
+// Persistent, one CTA per SM with 16 warps, software-pipelined over the CTA's units: while the
+// MMA of unit k runs, the threads finish unit k - 1 from the other accumulator (two A and two B
+// tiles, 2 x 256 TMEM columns); a unit's FP64 loads are issued kTcAhead units ahead, into
+// registers.
+constexpr int kTcThreads = 512;
+constexpr int kTcAhead = 3;
+constexpr int kTcSmem = 1024 + 2 * 16384 + 2 * 32768 + 64;  // two A tiles, two B tiles, barriers + TMEM slot
+constexpr int kTcSmemLaunch = 160 * 1024;                   // one CTA per SM (TMEM: 2 x 256 columns)
+constexpr uint32_t kTcIdesc = (2u << 4)                     // D: s32; A, B: unsigned 8-bit, K-major
+                              | (static_cast<uint32_t>(256 >> 3) << 17) | (static_cast<uint32_t>(128 >> 4) << 24);
+
+template <bool ROWC>
+struct TcGeom {
+    static constexpr int UR = ROWC ? 16 : 4;    // rows per unit
+    static constexpr int UK = ROWC ? 32 : 128;  // inner indices per unit
+    // element f = 0..511 of a unit -> row offset, inner offset (loads: coalesced along the
+    // contiguous index), segment and column
+    __device__ static void element(int f, int& ro, int& po, int& seg, int& n) {
+        if (ROWC) {
+            ro = f & 15;
+            po = f >> 4;
+            seg = ro >> 3;
+            n = ((ro & 7) << 5) | po;
+        } else {
+            ro = f >> 7;
+            po = f & 127;
+            seg = ro >> 1;
+            n = ((ro & 1) << 7) | po;
+        }
+    }
+    // the 32 columns n0 .. n0 + 31 of segment seg -> row offset and first inner offset
+    __device__ static void chunk(int seg, int n0, int& ro, int& po) {
+        if (ROWC) {
+            ro = 8 * seg + (n0 >> 5);
+            po = 0;
+        } else {
+            ro = 2 * seg + (n0 >> 7);
+            po = n0 & 127;
+        }
+    }
+};
+
+template <int NW>
+__device__ __forceinline__ void offset_words(double v, double s1, double s2, uint32_t (&W)[4]) {
+    if constexpr (NW == 2) {
+        uint32_t w[2];
+        offset_words_fp(v, s1, s2, w);
+        W[0] = w[0], W[1] = w[1], W[2] = 0, W[3] = 0;
+    } else if constexpr (NW == 3) {
+        uint32_t w[3];
+        offset_words_fp_wide(v, s1, s2, w);
+        W[0] = w[0], W[1] = w[1], W[2] = w[2], W[3] = 0;
+    } else {
+        offset_words_fp_widest(v, s1, s2, W);
+    }
+}
+
+template <int NW, bool ROWC>
+__global__ void __launch_bounds__(kTcThreads, 1) split_tc_kernel(const SplitItem* __restrict__ items, int count,
+                                                                int64_t units, int* err) {
+    using G = TcGeom<ROWC>;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t{1023});
+    uint8_t* sA0 = smem;              // two 128 rows x 128 bytes (swizzled; the first two chunks used)
+    uint8_t* sB0 = smem + 2 * 16384;  // two 256 rows x 128 bytes
+    uint64_t* bar_p = reinterpret_cast<uint64_t*>(smem + 2 * 16384 + 2 * 32768);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar_p + 2);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        dev::mbar_init(dev::smem_addr(bar_p), 1);
+        dev::mbar_init(dev::smem_addr(bar_p + 1), 1);
+        *abort_flag = 0;
+        dev::fence_barrier_init();
+    }
+    if (warp == 0) {
+        dev::tmem_alloc(dev::smem_addr(tmem_slot), 512);
+        dev::tmem_relinquish();
+    }
+    dev::tc_fence_before();
+    __syncthreads();
+    dev::tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const int64_t stride = gridDim.x;
+    const int64_t nmine = units > blockIdx.x ? (units - 1 - blockIdx.x) / stride + 1 : 0;
+    int ro_l, po_l, seg_l, n_l;  // this thread's element of every unit
+    G::element(tid, ro_l, po_l, seg_l, n_l);
+
+    int first = 0;
+    {  // the item of this CTA's first unit; later units only move forward
+        int hi = count - 1;
+        const int64_t u = blockIdx.x;
+        while (first < hi) {
+            const int mid = (first + hi + 1) >> 1;
+            if (items[mid].block0 <= u) first = mid;
+            else hi = mid - 1;
+        }
+    }
+    auto advance = [&](int& cur, int64_t u) {
+        while (cur + 1 < count && items[cur + 1].block0 <= u) ++cur;
+    };
+    // the element's value (0 outside the item's rows and k, and for non-finite rows, whose
+    // residues are then zero like the padding's) and its row's maximum bits
+    int cur_l = first;
+    auto load_elem = [&](int64_t kk, double& v, unsigned long long& mb) {
+        v = 0.0;
+        mb = 0;
+        if (kk >= nmine) return;
+        const int64_t u = blockIdx.x + kk * stride;
+        advance(cur_l, u);
+        const SplitItem* I = items + cur_l;
+        const int64_t local = u - I->block0;
+        int64_t qd, rm;
+        divmod_index(local, I->rblocks, qd, rm);
+        const int64_t r = rm * G::UR + ro_l, p = qd * G::UK + po_l;
+        if (r < I->rows && p < I->k) {
+            mb = __ldg(I->maxbits + r);
+            if (mb < 0x7FF0000000000000ull) v = __ldg(I->X + (ROWC ? r + p * I->ldx : p + r * I->ldx));
+        }
+    };
+    double pv[kTcAhead];
+    unsigned long long pm[kTcAhead];
+#pragma unroll
+    for (int a = 0; a < kTcAhead; ++a) load_elem(a, pv[a], pm[a]);
+
+    int cur_w = first, cur_e = first;  // items of the unit being written and of the one being finished
+    int a_item0 = -1, a_item1 = -1;    // item whose weights are in A tile 0 / 1
+    int e_item = -1;                   // item of the epilogue lane constants
+    bool valid = false;
+    int seg = 0, qa = 1;
+    uint32_t m = 1, m32 = 0, koff = 0, c256h = 0;
+    int8_t* plane = nullptr;
+    bool ok = true;
+    uint32_t committed = 0, last_par = 0;  // (thread 0) per accumulator: a commit issued, its parity
+    for (int64_t kb = 0; ok && kb <= nmine; kb += kTcAhead) {
+#pragma unroll
+        for (int a = 0; a < kTcAhead; ++a) {
+            const int64_t kk = kb + a;  // unit kk is written, unit kk - 1 finished
+            if (!ok || kk > nmine) break;
+            const int buf = static_cast<int>(kk & 1);
+            if (kk < nmine) {
+                const int64_t u = blockIdx.x + kk * stride;
+                advance(cur_w, u);
+                const SplitItem* __restrict__ I = items + cur_w;
+                if ((buf ? a_item1 : a_item0) != cur_w) {  // unit kk - 2's MMA, this tile's last reader, is complete
+                    if (buf) a_item1 = cur_w;
+                    else a_item0 = cur_w;
+                    if (tid < 128) {
+                        const int s = I->s, q2 = s <= 16 ? 1 : 2;
+                        const int sigma = 32 * ((tid >> 5) % q2) + (tid & 31);
+                        uint4 w0 = make_uint4(0, 0, 0, 0), w1 = w0;
+                        if (sigma < 2 * s) {
+                            const ModConst& c = I->mc[sigma % s];
+                            const uint4 cw = make_uint4(c.cb[0], c.cb[1], NW > 2 ? c.cb[2] : 0u, NW > 3 ? c.cb[3] : 0u);
+                            if (sigma < s) w0 = cw;
+                            else w1 = cw;
+                        }
+                        uint8_t* row = sA0 + buf * 16384 + tid * 128;
+                        *reinterpret_cast<uint4*>(row + ((0 ^ (tid & 7)) << 4)) = w0;
+                        *reinterpret_cast<uint4*>(row + ((1 ^ (tid & 7)) << 4)) = w1;
+                    }
+                }
+                const int e = exponent_of(pm[a], I->tk);
+                const bool live = e != kNonFinite;
+                const int e1 = e >> 1;
+                const double s1 = pow2(live ? e1 : 0), s2 = pow2(live ? e - e1 : 0);
+                uint32_t W[4];
+                offset_words<NW>(pv[a], s1, s2, W);
+                *reinterpret_cast<uint4*>(sB0 + buf * 32768 + n_l * 128 + ((seg_l ^ (n_l & 7)) << 4)) =
+                    make_uint4(W[0], W[1], W[2], W[3]);
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            }
+            dev::tc_fence_before();
+            __syncthreads();
+            if (kk < nmine && tid == 0) {
+                dev::tc_fence_after();
+                dev::mma_i8(tmem + static_cast<uint32_t>(buf * 256), dev::sw128_kmajor_desc(dev::smem_addr(sA0 + buf * 16384)),
+                            dev::sw128_kmajor_desc(dev::smem_addr(sB0 + buf * 32768)), kTcIdesc, 0u);
+                dev::tc_commit(dev::smem_addr(bar_p + buf));
+                committed |= 1u << buf;
+                last_par = (last_par & ~(1u << buf)) | (static_cast<uint32_t>((kk >> 1) & 1) << buf);
+            }
+            if (kk < nmine) load_elem(kk + kTcAhead, pv[a], pm[a]);
+            if (kk > 0) {  // finish unit kk - 1
+                const int pb = buf ^ 1;
+                const uint32_t parity = static_cast<uint32_t>(((kk - 1) >> 1) & 1);
+                int got = 1;  // one thread waits; the others sleep in the block barrier
+                if (tid == 0)
+                    got = dev::mbar_wait(dev::smem_addr(bar_p + pb), parity, abort_flag, err, dev::kErrTimeoutAccFull,
+                                         dev::kWaitLimitNs) ? 1 : 0;
+                if (!__syncthreads_and(got)) {
+                    ok = false;
+                    break;
+                }
+                dev::tc_fence_after();
+                const int64_t u = blockIdx.x + (kk - 1) * stride;
+                advance(cur_e, u);
+                const SplitItem* __restrict__ I = items + cur_e;
+                if (cur_e != e_item) {
+                    e_item = cur_e;
+                    const int s = I->s;
+                    qa = s <= 16 ? 1 : 2;
+                    const int sigma = 32 * ((warp & 3) % qa) + lane;
+                    valid = sigma < 2 * s;
+                    if (valid) {
+                        const int t = sigma % s;
+                        const ModConst& c = I->mc[t];
+                        seg = sigma / s;
+                        m = c.m;
+                        m32 = c.m32;
+                        koff = NW == 2 ? c.koff3 : (NW == 3 ? c.koff5 : c.koff7);
+                        c256h = 256u - c.h;
+                        plane = I->planes + t * I->plane_bytes;
+                    }
+                }
+                const int64_t local = u - I->block0;
+                int64_t qd, rm;
+                divmod_index(local, I->rblocks, qd, rm);
+                const int64_t r0 = rm * G::UR, p0 = qd * G::UK;
+                // warp (quarter q, part pt) reads lane quarter q: with qa = 1 (four copies of the
+                // slots) 16 columns, with qa = 2 (two copies) 32 columns
+                const int q = warp & 3, pt = warp >> 2;
+                const uint32_t taddr = tmem + (static_cast<uint32_t>(32 * q) << 16) + static_cast<uint32_t>(pb * 256);
+                if (qa == 1) {
+                    const int n0 = 16 * (4 * q + pt);
+                    uint32_t d[16];
+                    dev::tmem_load_32x16(taddr + n0, d);
+                    dev::tmem_load_wait();
+                    if (valid) {
+                        int ro, po;
+                        G::chunk(seg, n0 & ~31, ro, po);
+                        const int64_t r = r0 + ro, pk = p0 + po + (n0 & 31);
+                        const int rr = static_cast<int>(r & 127);
+                        const int c = static_cast<int>((pk & 127) >> 4);
+                        int8_t* tile = plane + ((r >> 7) * I->kb_total + (pk >> 7)) * kTileBytes + rr * kTileK;
+                        uint32_t w[4];
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            uint32_t r4[4];
+#pragma unroll
+                            for (int b = 0; b < 4; ++b) {
+                                const uint32_t v = d[4 * j + b] + koff;     // < 2^20 + 2^8
+                                r4[b] = v - __umulhi(v, m32) * m + c256h;  // low byte: (x mod m, symmetric)
+                            }
+                            w[j] = pack_bytes(r4[0], r4[1], r4[2], r4[3]);
+                        }
+                        *reinterpret_cast<uint4*>(tile + ((c ^ (rr & 7)) << 4)) = make_uint4(w[0], w[1], w[2], w[3]);
+                    }
+                } else {
+                    const int n0 = 32 * (4 * (q >> 1) + pt);
+                    uint32_t d[32];
+                    dev::tmem_load_32x32(taddr + n0, d);
+                    dev::tmem_load_wait();
+                    if (valid) {
+                        int ro, po;
+                        G::chunk(seg, n0, ro, po);
+                        const int64_t r = r0 + ro, pk = p0 + po;
+                        const int rr = static_cast<int>(r & 127);
+                        const int c = static_cast<int>((pk & 127) >> 4);
+                        int8_t* tile = plane + ((r >> 7) * I->kb_total + (pk >> 7)) * kTileBytes + rr * kTileK;
+                        uint32_t w[8];
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            uint32_t r4[4];
+#pragma unroll
+                            for (int b = 0; b < 4; ++b) {
+                                const uint32_t v = d[4 * j + b] + koff;
+                                r4[b] = v - __umulhi(v, m32) * m + c256h;
+                            }
+                            w[j] = pack_bytes(r4[0], r4[1], r4[2], r4[3]);
+                        }
+                        *reinterpret_cast<uint4*>(tile + ((c ^ (rr & 7)) << 4)) = make_uint4(w[0], w[1], w[2], w[3]);
+                        *reinterpret_cast<uint4*>(tile + (((c + 1) ^ (rr & 7)) << 4)) = make_uint4(w[4], w[5], w[6], w[7]);
+                    }
+                }
+            }
+        }
+    }
+    if (!ok && tid == 0) {  // the last MMA of each accumulator completes before TMEM is freed
+        for (int b = 0; b < 2; ++b)
+            if (committed & (1u << b)) dev::mbar_wait_drain(dev::smem_addr(bar_p + b), (last_par >> b) & 1u);
+    }
+    dev::tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        dev::tc_fence_after();
+        dev::tmem_dealloc(tmem, 512);
+    }
+}
+
 // Ozaki Scheme I digits (the reference's comparison baseline, benchmarks/ozaki1_gpu.hpp:31-40):
 // x = RNE(v 2^e) as on the narrow split path (tk = 7L - 2 <= 61), then L balanced base-128
 // digits in [-64, 63], most significant in plane 0, written in the same plane layout and with
@@ -316,7 +685,8 @@ __global__ void __launch_bounds__(256) slice_kernel(const SplitItem* __restrict_
     constexpr int EPT = 16;
     const SplitItem* __restrict__ I = items + find_item(items, count, blockIdx.x);
     const int64_t local = static_cast<int64_t>(blockIdx.x) - I->block0;
-    const int64_t bx = local % I->rblocks, by = local / I->rblocks;
+    int64_t bx, by;
+    divmod_index(local, I->rblocks, by, bx);
     int64_t r, k0;
     split_coords<EPT, ROWC>(bx, by, r, k0);
     const int64_t kb_total = I->kb_total, plane_bytes = I->plane_bytes, ldx = I->ldx, k = I->k;
@@ -355,6 +725,29 @@ __global__ void __launch_bounds__(256) slice_kernel(const SplitItem* __restrict_
         for (int q = 0; q < 4; ++q) w[q] = pack_bytes(b[4 * q], b[4 * q + 1], b[4 * q + 2], b[4 * q + 3]);
         *reinterpret_cast<uint4*>(out + i * plane_bytes) = make_uint4(w[0], w[1], w[2], w[3]);
     }
+}
+
+template <int NW>
+void split_tc_dispatch(const SplitItem* d, int count, int64_t units, bool rowc, int* err, cudaStream_t st) {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    const unsigned grid = static_cast<unsigned>(std::min<int64_t>(units, static_cast<int64_t>(sms)));
+    if (rowc) split_tc_kernel<NW, true><<<grid, kTcThreads, kTcSmemLaunch, st>>>(d, count, units, err);
+    else split_tc_kernel<NW, false><<<grid, kTcThreads, kTcSmemLaunch, st>>>(d, count, units, err);
+}
+
+std::atomic<int> g_split_tc{0};
+std::atomic<int> g_scale_fusion{1};
+
+template <int NLIMB>
+void scale_split_dispatch(const SplitItem* d, int count, int64_t blocks, bool rowc, cudaStream_t st) {
+    if (rowc) scale_split_kernel<NLIMB, true><<<static_cast<unsigned>(blocks), 256, 0, st>>>(d, count);
+    else scale_split_kernel<NLIMB, false><<<static_cast<unsigned>(blocks), 256, 0, st>>>(d, count);
 }
 
 template <int NLIMB, bool CPLX>
@@ -401,6 +794,46 @@ int64_t split_item_blocks(SplitItem& it, int64_t block0) {
     return it.rblocks * it.kblocks;
 }
 
+int64_t split_geometry(SplitItem& it, int64_t block0) {
+    if (it.fuse) {  // whole rows per block
+        it.tc = 0;
+        it.block0 = block0;
+        const int rb = it.row_contig ? (it.tk > kNarrowScaleBits ? 8 : 16) : 8;
+        it.rblocks = it.rows_pad / rb;
+        it.kblocks = 1;
+        return it.rblocks;
+    }
+    it.tc = !it.cplx && g_split_tc.load() ? 1 : 0;
+    if (!it.tc) return split_item_blocks(it, block0);
+    it.block0 = block0;
+    const int ur = it.row_contig ? TcGeom<true>::UR : TcGeom<false>::UR;
+    const int uk = it.row_contig ? TcGeom<true>::UK : TcGeom<false>::UK;
+    it.rblocks = it.rows_pad / ur;              // rows_pad is a multiple of 128
+    it.kblocks = it.kb_total * (kTileK / uk);
+    return it.rblocks * it.kblocks;
+}
+
+void set_split_path(int tc) { g_split_tc.store(tc ? 1 : 0); }
+void set_scale_fusion(int on) { g_scale_fusion.store(on ? 1 : 0); }
+bool fuse_scale(bool cplx, bool row_contig, int64_t k) {
+    return g_scale_fusion.load() && !cplx && k > 0 && k <= (row_contig ? kFuseMaxKRowc : kFuseMaxK);
+}
+int split_path() { return g_split_tc.load(); }
+
+cudaError_t prepare_split_kernels() {
+    cudaError_t e = cudaSuccess;
+    auto set = [&](const void* f) {
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemLaunch);
+    };
+    set(reinterpret_cast<const void*>(split_tc_kernel<2, false>));
+    set(reinterpret_cast<const void*>(split_tc_kernel<2, true>));
+    set(reinterpret_cast<const void*>(split_tc_kernel<3, false>));
+    set(reinterpret_cast<const void*>(split_tc_kernel<3, true>));
+    set(reinterpret_cast<const void*>(split_tc_kernel<4, false>));
+    set(reinterpret_cast<const void*>(split_tc_kernel<4, true>));
+    return e;
+}
+
 void launch_scale(const ScaleItem* d, const ScaleItem* h, int count, int64_t blocks, cudaStream_t st) {
     if (count <= 0 || blocks <= 0) return;
     const bool rowc = h[0].row_contig != 0, cplx = h[0].cplx != 0;
@@ -420,9 +853,21 @@ void launch_slice(const SplitItem* d, const SplitItem* h, int count, int64_t blo
     else slice_kernel<false><<<static_cast<unsigned>(blocks), 256, 0, st>>>(d, count);
 }
 
-void launch_split(const SplitItem* d, const SplitItem* h, int count, int64_t blocks, cudaStream_t st) {
+void launch_split(const SplitItem* d, const SplitItem* h, int count, int64_t blocks, int* err, cudaStream_t st) {
     if (count <= 0 || blocks <= 0) return;
     const bool wide = h[0].tk > kNarrowScaleBits, rowc = h[0].row_contig != 0;
+    if (h[0].fuse) {
+        if (h[0].tk > kWideScaleBits) scale_split_dispatch<7>(d, count, blocks, rowc, st);
+        else if (wide) scale_split_dispatch<5>(d, count, blocks, rowc, st);
+        else scale_split_dispatch<3>(d, count, blocks, rowc, st);
+        return;
+    }
+    if (h[0].tc) {
+        if (h[0].tk > kWideScaleBits) split_tc_dispatch<4>(d, count, blocks, rowc, err, st);
+        else if (wide) split_tc_dispatch<3>(d, count, blocks, rowc, err, st);
+        else split_tc_dispatch<2>(d, count, blocks, rowc, err, st);
+        return;
+    }
     if (h[0].tk > kWideScaleBits) {  // extended sets: real operands only
         split_dispatch<7, false>(d, count, blocks, rowc, st);
         return;

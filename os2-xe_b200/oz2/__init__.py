@@ -46,6 +46,10 @@ _lib.oz2_last_tiling.argtypes = [_vp, C.POINTER(_i64)]
 _lib.oz2_set_tuning.argtypes = [_vp, _i32, _i32, _i32]
 _lib.oz2_check_device_error.argtypes = [_vp]
 _lib.oz2_set_failure_test.argtypes = [_i64, _i32]
+_lib.oz2_set_split_kernel.argtypes = [_i32]
+_lib.oz2_set_crt_kernel.argtypes = [_i32]
+_lib.oz2_set_scale_fusion.argtypes = [_i32]
+_lib.oz2_set_crt_fusion.argtypes = [_i32]
 
 
 class DgemmProblem(C.Structure):
@@ -90,6 +94,48 @@ def set_failure_test(wait_limit_ns=0, stall_mma=False):
     every wait (0 = the 2 s default); with stall_mma the MMA issuer issues nothing, so the waits
     run out and check_device_error raises TimeoutError. set_failure_test() restores normal runs."""
     _raise(_lib.oz2_set_failure_test(int(wait_limit_ns), 1 if stall_mma else 0))
+
+
+SPLIT_DP4A = 0
+SPLIT_TENSOR_CORE = 1
+
+
+SPLIT_DEFAULT = SPLIT_DP4A
+
+
+def set_split_kernel(kind):
+    """Kernel of the real split (process-wide): SPLIT_DP4A (default, integer pipe) or
+    SPLIT_TENSOR_CORE (the residues' byte dot products as one tcgen05 u8 x u8 MMA per 512
+    elements; measured slower). Both write identical planes."""
+    _raise(_lib.oz2_set_split_kernel(int(kind)))
+
+
+CRT_DP2A = 0
+CRT_TENSOR_CORE = 1
+CRT_AUTO = 2
+
+
+CRT_DEFAULT = CRT_AUTO
+
+
+def set_crt_kernel(kind):
+    """Kernel of the real CRT (process-wide): CRT_AUTO (default; the tensor-core CRT for 8-limb
+    plans, s = 30..32, dp2a below), CRT_TENSOR_CORE (limb sums as one tcgen05 u8 x u8 MMA per 128
+    entries) or CRT_DP2A. All produce identical C."""
+    _raise(_lib.oz2_set_crt_kernel(int(kind)))
+
+
+def set_scale_fusion(on):
+    """Scale pass fused into the split for real operands with k <= 2048 (1024 when the plane rows
+    are contiguous), process-wide, default on. Results are identical either way."""
+    _raise(_lib.oz2_set_scale_fusion(1 if on else 0))
+
+
+def set_crt_fusion(on):
+    """CRT in the GEMM's epilogue for real problems with s <= 8 and k <= 65408 (process-wide,
+    default off: measured slower): the residues stay in tensor memory and the GEMM writes C.
+    Results are identical."""
+    _raise(_lib.oz2_set_crt_fusion(1 if on else 0))
 
 
 def mlp_info():

@@ -75,3 +75,20 @@ def test_cpp_header_compiles():
     assert os.path.exists(src)
     assert r.returncode == 0, r.stderr
     assert subprocess.run([exe], timeout=60).returncode == 0
+
+
+def test_split_kernel_selector():
+    """process-wide choice of the real split's kernel: host-only, checked values"""
+    import oz2
+    oz2.set_split_kernel(oz2.SPLIT_DP4A)
+    oz2.set_split_kernel(oz2.SPLIT_TENSOR_CORE)
+    with pytest.raises(ValueError, match="split kernel"):
+        oz2.set_split_kernel(7)
+
+
+def test_crt_kernel_selector():
+    import oz2
+    for kind in (oz2.CRT_DP2A, oz2.CRT_TENSOR_CORE, oz2.CRT_AUTO):
+        oz2.set_crt_kernel(kind)
+    with pytest.raises(ValueError, match="CRT kernel"):
+        oz2.set_crt_kernel(3)
