@@ -68,9 +68,9 @@ def parse():
     ap.add_argument("--split-kernel", type=int, default=0, choices=(0, 1),
                     help="real split kernel: 0 integer pipe (dp4a, default), 1 tensor core")
     ap.add_argument("--crt-kernel", type=int, default=2, choices=(0, 1, 2),
-                    help="real CRT kernel: 2 auto (default: tensor core for 8-limb plans), 1 tensor core, 0 dp2a")
-    ap.add_argument("--scale-fusion", type=int, default=1, choices=(0, 1),
-                    help="scale pass fused into the split for k <= 2048 (1, default) or separate (0)")
+                    help="real CRT kernel: 2 auto (default: tensor core for 7- and 8-limb plans), 1 tensor core, 0 dp2a")
+    ap.add_argument("--scale-fusion", type=int, default=0, choices=(0, 1),
+                    help="scale pass fused into the split for k <= 2048 (1) or separate (0, default)")
     ap.add_argument("--crt-fusion", type=int, default=0, choices=(0, 1),
                     help="CRT in the GEMM epilogue for s <= 8 (1) or a separate CRT launch (0, default)")
     ap.add_argument("--dgemm-only", action="store_true",

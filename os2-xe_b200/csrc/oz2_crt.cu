@@ -34,8 +34,13 @@ __device__ __forceinline__ uint32_t pack4(uint32_t a, uint32_t b, uint32_t c, ui
     return __byte_perm(__byte_perm(a, b, 0x0040), __byte_perm(c, d, 0x0040), 0x5410);
 }
 
+// Occupancy for the latency-bound loads: real plans up to 20 moduli fit 64 registers (four
+// blocks per SM), up to 24 fit 80 (three); larger ones and complex ones take what the
+// reconstruction needs.
 template <int S, bool CPLX>
-__global__ void __launch_bounds__(256) crt_kernel(const __grid_constant__ CrtParams P) {
+constexpr int crt_min_blocks() { return CPLX ? 1 : (S <= 20 ? 4 : (S <= 24 ? 3 : 1)); }
+template <int S, bool CPLX>
+__global__ void __launch_bounds__(256, crt_min_blocks<S, CPLX>()) crt_kernel(const __grid_constant__ CrtParams P) {
     constexpr int NL = limbs_for(S);
     int lo = 0, hi = P.count - 1;
     while (lo < hi) {
@@ -80,17 +85,26 @@ __global__ void __launch_bounds__(256) crt_kernel(const __grid_constant__ CrtPar
                 for (int e = 0; e < 4; ++e) Rq[e][g] = o[e];
             }
         }
+        // real: the sums of two entries together, each weight read once per pair (four entries'
+        // limb sums would cost registers, and so occupancy)
+        constexpr int EG = CPLX ? 1 : 2;
+        uint32_t ufg[EG];
+        uint64_t accg[EG][CPLX ? 1 : NL];
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
             const int64_t i = i0 + e;
             if (i >= m) break;
+            if constexpr (!CPLX) {
+                if (e % EG == 0)
+                    crt_sums<S, NL, EG>(*reinterpret_cast<const uint32_t(*)[EG][Q]>(&Rq[e][0]), P.cc, ufg, accg);
+            }
             const int De = exponent_of(I->maxA[i], tk);
             const bool nonfinite = De == kNonFinite || Ej == kNonFinite;
             const int shift = nonfinite ? 0 : De + Ej;
             const uint32_t sel = 0x4440 + e;  // byte e of a word, zero-extended
             double* cp = I->C + (CPLX ? 2 : 1) * (i + j * I->ldc);
             if constexpr (!CPLX) {
-                double v = crt_value<S, NL>(Rq[e], P.cc, shift);
+                double v = crt_finish<NL>(accg[e % EG], static_cast<int64_t>(ufg[e % EG] >> 16), P.cc.M, shift);
                 if (nonfinite) v = __longlong_as_double(0x7FF8000000000000ll);
                 // the reference's unfused alpha*v + beta*c, one rounding per operation
                 const double av = __dmul_rn(ar, v);

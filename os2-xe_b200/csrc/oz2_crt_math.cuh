@@ -62,6 +62,41 @@ __device__ __forceinline__ double crt_value(const uint32_t (&R)[(S + 3) / 4], co
 // From the 32-bit limb sums acc[l] = sum_t r_t W_t[l] (below 2^46) and the quotient q: x = sum_t
 // r_t W_t - q M modulo 2^(32 NL) in 64-bit words (|x| <= M/4, two's complement), its magnitude's
 // leading 64 bits with a sticky bit for the rest, one RNE to double, 2^-shift.
+// The sums of crt_value for EG entries at once: every weight word is read once and used for all
+// of them (the entries' dot products interleave, and a constant costs one load, not EG). uf[e] is
+// the rounded quotient sum (q = uf >> 16) and acc[e][l] the limb sums of entry e.
+template <int S, int NL, int EG>
+__device__ __forceinline__ void crt_sums(const uint32_t (&R)[EG][(S + 3) / 4], const CrtConst& cc,
+                                         uint32_t (&uf)[EG], uint64_t (&acc)[EG][NL]) {
+    constexpr int Q = (S + 3) / 4;
+#pragma unroll
+    for (int e = 0; e < EG; ++e) uf[e] = 1u << 15;
+#pragma unroll
+    for (int g = 0; g < Q; ++g) {
+        const uint32_t f0 = cc.Fq[g][0], f1 = cc.Fq[g][1];
+#pragma unroll
+        for (int e = 0; e < EG; ++e) uf[e] = __dp2a_hi(f1, R[e][g], __dp2a_lo(f0, R[e][g], uf[e]));
+    }
+#pragma unroll
+    for (int l = 0; l < NL; ++l) {
+        uint32_t a0[EG], a1[EG];  // 16-bit limbs 2l and 2l + 1
+#pragma unroll
+        for (int e = 0; e < EG; ++e) a0[e] = a1[e] = 0;
+#pragma unroll
+        for (int g = 0; g < Q; ++g) {
+            const uint32_t w00 = cc.Wq[g][2 * l][0], w01 = cc.Wq[g][2 * l][1];
+            const uint32_t w10 = cc.Wq[g][2 * l + 1][0], w11 = cc.Wq[g][2 * l + 1][1];
+#pragma unroll
+            for (int e = 0; e < EG; ++e) {
+                a0[e] = __dp2a_hi(w01, R[e][g], __dp2a_lo(w00, R[e][g], a0[e]));
+                a1[e] = __dp2a_hi(w11, R[e][g], __dp2a_lo(w10, R[e][g], a1[e]));
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < EG; ++e) acc[e][l] = static_cast<uint64_t>(a0[e]) + (static_cast<uint64_t>(a1[e]) << 16);
+    }
+}
+
 template <int NL>
 __device__ __forceinline__ double crt_finish(const uint64_t (&acc)[NL], int64_t q, const uint32_t* Mw, int shift) {
     uint32_t w[NL];

@@ -153,7 +153,9 @@ int64_t split_geometry(SplitItem& it, int64_t block0);
 void set_split_path(int tc);
 int split_path();
 // process-wide: whether real operands with k <= kFuseMaxK (kFuseMaxKRowc when rows are contiguous)
-// take the fused scale + split (default on); fuse_scale tells whether an operand qualifies
+// take the fused scale + split (default off: measured neutral on one DGEMM and 2.7 % slower on a
+// group of 512 small DGEMMs, where the separate passes spread over more blocks); fuse_scale tells
+// whether an operand qualifies
 void set_scale_fusion(int on);
 bool fuse_scale(bool cplx, bool row_contig, int64_t k);
 int64_t crt_item_blocks(CrtItem& it, int64_t block0);
@@ -199,8 +201,10 @@ int64_t gemm_tiles_i(int64_t m, int bn);
 
 // whether launch_crt runs the tensor-core CRT for this plan (real items only): process-wide path
 // 0 the dp2a kernel, 1 the tensor-core CRT, 2 (default) the tensor-core CRT from
-// kCrtTcMinLimbs limbs on (8 limbs: s = 30..32); the items' `mma` flag must match
-constexpr int kCrtTcMinLimbs = 8;
+// kCrtTcMinLimbs limbs on (7 and 8 limbs: s = 26..32, where it measured as fast or faster: B200,
+// 4096^2 x 1024, s = 29: 0.56 against 0.67 ms; s = 20: 0.47 against 0.28); the items' `mma` flag
+// must match
+constexpr int kCrtTcMinLimbs = 7;
 bool crt_uses_mma(const Plan& plan, bool cplx);
 void set_crt_path(int path);
 int crt_path();

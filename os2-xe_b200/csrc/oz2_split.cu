@@ -344,14 +344,18 @@ __global__ void __launch_bounds__(256) scale_split_kernel(const SplitItem* __res
     if (ROWC) {
         const int64_t r = r0 + tid % RB;
         unsigned long long best = 0;
-        if (r < rows)
+        if (r < rows) {
+#pragma unroll 4
             for (int64_t p = tid / RB; p < k; p += 256 / RB) best = max(best, __ldg(X + r + p * ldx) & kAbsMask);
+        }
         if (best) atomicMax(&smax[tid % RB], best);
     } else {
         const int64_t r = r0 + warp;
         unsigned long long best = 0;
-        if (r < rows)
+        if (r < rows) {
+#pragma unroll 4
             for (int64_t p = lane; p < k; p += 32) best = max(best, __ldg(X + p + r * ldx) & kAbsMask);
+        }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) best = max(best, __shfl_xor_sync(0xFFFFFFFFu, best, o));
         if (lane == 0) smax[warp] = best;
@@ -742,7 +746,7 @@ void split_tc_dispatch(const SplitItem* d, int count, int64_t units, bool rowc, 
 }
 
 std::atomic<int> g_split_tc{0};
-std::atomic<int> g_scale_fusion{1};
+std::atomic<int> g_scale_fusion{0};
 
 template <int NLIMB>
 void scale_split_dispatch(const SplitItem* d, int count, int64_t blocks, bool rowc, cudaStream_t st) {

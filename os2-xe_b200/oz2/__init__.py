@@ -119,15 +119,15 @@ CRT_DEFAULT = CRT_AUTO
 
 
 def set_crt_kernel(kind):
-    """Kernel of the real CRT (process-wide): CRT_AUTO (default; the tensor-core CRT for 8-limb
-    plans, s = 30..32, dp2a below), CRT_TENSOR_CORE (limb sums as one tcgen05 u8 x u8 MMA per 128
+    """Kernel of the real CRT (process-wide): CRT_AUTO (default; the tensor-core CRT for 7- and
+    8-limb plans, s = 26..32, dp2a below), CRT_TENSOR_CORE (limb sums as one tcgen05 u8 x u8 MMA per 128
     entries) or CRT_DP2A. All produce identical C."""
     _raise(_lib.oz2_set_crt_kernel(int(kind)))
 
 
 def set_scale_fusion(on):
     """Scale pass fused into the split for real operands with k <= 2048 (1024 when the plane rows
-    are contiguous), process-wide, default on. Results are identical either way."""
+    are contiguous), process-wide, default off (measured no faster). Results are identical."""
     _raise(_lib.oz2_set_scale_fusion(1 if on else 0))
 
 

@@ -18,7 +18,7 @@ pytestmark = pytest.mark.gpu
 def fusion():
     import oz2
     yield oz2
-    oz2.set_scale_fusion(True)
+    oz2.set_scale_fusion(False)
 
 
 def run(oz, ta, tb, m, n, k, s, A, B, C0, al=1.5, be=-0.5):
