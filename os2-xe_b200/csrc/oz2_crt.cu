@@ -35,10 +35,10 @@ __device__ __forceinline__ uint32_t pack4(uint32_t a, uint32_t b, uint32_t c, ui
 }
 
 // Occupancy for the latency-bound loads: real plans up to 20 moduli fit 64 registers (four
-// blocks per SM), up to 24 fit 80 (three); larger ones and complex ones take what the
+// blocks per SM), up to 24 fit 80 (three); complex ones 128 (two); larger real ones take what the
 // reconstruction needs.
 template <int S, bool CPLX>
-constexpr int crt_min_blocks() { return CPLX ? 1 : (S <= 20 ? 4 : (S <= 24 ? 3 : 1)); }
+constexpr int crt_min_blocks() { return CPLX ? 2 : (S <= 20 ? 4 : (S <= 24 ? 3 : 1)); }
 template <int S, bool CPLX>
 __global__ void __launch_bounds__(256, crt_min_blocks<S, CPLX>()) crt_kernel(const __grid_constant__ CrtParams P) {
     constexpr int NL = limbs_for(S);
