@@ -70,8 +70,12 @@ typedef struct {
  * grouped scale and split per kernel variant, one persistent tcgen05 GEMM over every
  * (problem, modulus, tile) job, one CRT per distinct s. No counterpart in the reference
  * (equivalent to `count` calls of Ozaki2::gemm, src/ozaki2_gpu.hpp:739-760, with the same
- * results bit for bit). Arguments are checked for every problem before anything runs; C
- * blocks must not overlap. */
+ * results bit for bit). A problem whose num_moduli is OZ2_S_ADAPTIVE (-1) instead takes the
+ * adaptive s per tile of oz2_dgemm_adaptive (mode 0, DGEMM-level target of 53 bits): those
+ * problems run together after the fixed-s ones, and the call then does not run in graph mode
+ * (OZ2_EINVAL), since the adaptive choice reads tile statistics back to the host. Arguments are
+ * checked for every problem before anything runs; C blocks must not overlap. */
+#define OZ2_S_ADAPTIVE (-1)
 int oz2_dgemm_grouped(oz2_handle h, int count, const oz2_dgemm_problem* problems, void* const* deps, int ndeps,
                       void* done);
 /* Grouped calls are captured in a CUDA graph on first use and replayed when the same problem

@@ -41,7 +41,8 @@ struct TileInfo {
 };
 
 // one problem of a grouped or adaptive call (no counterpart in the reference): the arguments of
-// gemm(); num_moduli is ignored by the adaptive modes other than Fixed
+// gemm(); num_moduli is ignored by the adaptive modes other than Fixed, and in gemm_grouped
+// OZ2_S_ADAPTIVE (-1) gives the problem the adaptive s per tile
 struct Problem {
     Trans ta = Trans::N, tb = Trans::N;
     int64_t m = 0, n = 0, k = 0;
@@ -165,7 +166,8 @@ public:
 
     // ---- beyond the reference: many problems in one set of launches, and adaptive s per tile
 
-    // every problem as gemm() would compute it, bit for bit, in one grouped launch
+    // every problem as gemm() would compute it, bit for bit, in one grouped launch (problems with
+    // num_moduli = OZ2_S_ADAPTIVE as gemm_adaptive(Mlp) would)
     void gemm_grouped(const std::vector<Problem>& ps, const std::vector<cudaEvent_t>& deps = {},
                       cudaEvent_t done = nullptr) {
         auto q = detail::problems(ps);

@@ -2115,6 +2115,41 @@ int oz2_dgemm_grouped(oz2_handle h, int count, const oz2_dgemm_problem* problems
     if (count < 0 || (count > 0 && !problems)) return fail(h, OZ2_EINVAL, "oz2: bad problem list");
     h->marks.clear();
     if (h->plans.size() > 8192) h->plans.clear();
+    // num_moduli = -1: the adaptive path (mode 0, DGEMM-level target) for those problems
+    std::vector<oz2_dgemm_problem> fixed_list, adaptive_list;
+    for (int i = 0; i < count; ++i) (problems[i].num_moduli == OZ2_S_ADAPTIVE ? adaptive_list : fixed_list).push_back(problems[i]);
+    if (!adaptive_list.empty()) {
+        if (h->graph_mode)
+            return fail(h, OZ2_EINVAL, "oz2: num_moduli = -1 (adaptive) does not run in graph mode: the adaptive "
+                                       "choice reads tile statistics back to the host");
+        std::vector<Prob> fprobs, aprobs;
+        std::vector<int> afixed;
+        int st = validate_grouped(h, static_cast<int>(fixed_list.size()), fixed_list.data(), fprobs);
+        if (st) return st;
+        if ((st = validate_adaptive(h, static_cast<int>(adaptive_list.size()), adaptive_list.data(), aprobs, afixed,
+                                    false)))
+            return st;
+        if ((st = begin_call(h, deps, ndeps))) return st;
+        for (int i = 0; i < count; ++i) {  // k == 0 or alpha == 0: C = beta C
+            const oz2_dgemm_problem& q = problems[i];
+            if (q.m > 0 && q.n > 0 && (q.k == 0 || q.alpha == 0.0)) {
+                const double be[2] = {q.beta, 0.0};
+                launch_scale_c(q.C, q.ldc, q.m, q.n, be, false, h->stream);
+                ++h->launches;
+            }
+        }
+        if (!fprobs.empty() && (st = run_grouped(h, fprobs))) return st;
+        if (!aprobs.empty()) {
+            for (int q = 0; q < kAdaptiveStats; ++q) h->astats[q] = 0;
+            for (int64_t& g : h->gbytes) g = 0;
+            h->native_ms = 0.0;
+            st = run_adaptive(h, aprobs, afixed, 53, 0);
+            const int sj = native_join(h);
+            if (st) return st;
+            if (sj) return sj;
+        }
+        return end_call(h, done);
+    }
     std::vector<Prob> probs;
     int st = validate_grouped(h, count, problems, probs);
     if (st) return st;

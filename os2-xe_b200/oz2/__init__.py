@@ -96,6 +96,8 @@ def set_failure_test(wait_limit_ns=0, stall_mma=False):
     _raise(_lib.oz2_set_failure_test(int(wait_limit_ns), 1 if stall_mma else 0))
 
 
+S_ADAPTIVE = -1  # num_moduli of a grouped problem that takes the adaptive s per tile
+
 SPLIT_DP4A = 0
 SPLIT_TENSOR_CORE = 1
 
@@ -317,7 +319,8 @@ class Ozaki2:
 
     def gemm_grouped(self, problems, deps=None, done=None):
         """problems: sequence of (ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, num_moduli),
-        the arguments of gemm() per problem; all run in one set of launches"""
+        the arguments of gemm() per problem; all run in one set of launches. num_moduli = S_ADAPTIVE
+        (-1) gives that problem the adaptive s per tile (gemm_adaptive, mode 0, 53-bit target)."""
         arr = self._problems(problems)
         ev, nev = self._events(deps)
         d = done.cuda_event if hasattr(done, "cuda_event") else done
