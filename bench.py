@@ -502,6 +502,28 @@ def dgemm_leg(a, oz2, torch, dev, stream, rank):
            "roofline": {"bound": "tensor", "kernel": "gemm_i8_modm_kernel", "achieved": achieved, "peak": peak,
                         "unit": "TOPS (int8)", "frac": achieved / peak, "peak_note": note,
                         "algorithmic": "2 s m n k int8 ops per call"}}
+    # the bandwidth-side stages against the measured copy bandwidth (algorithmic bytes per call:
+    # scale 8 (mk + kn); split (8 + s)(mk + kn); CRT s mn residue bytes + 8 mn for C out + 8 mn in,
+    # beta != 0)
+    hbm = peaks().get("hbm_gbs") or 6650.0
+    stage_bytes = {"scale": 8.0 * (m * k + k * n), "split": (8.0 + a.s) * (m * k + k * n),
+                   "crt": (a.s + 16.0) * m * n}
+    out["stage_roofline"] = {
+        name: {"bound": "hbm", "algorithmic_bytes": b, "achieved_gbs": b / (st_sum[i] * 1e-3) / 1e9,
+               "peak_gbs": hbm, "frac": b / (st_sum[i] * 1e-3) / 1e9 / hbm}
+        for i, (name, b) in ((0, ("scale", stage_bytes["scale"])), (1, ("split", stage_bytes["split"])),
+                             (3, ("crt", stage_bytes["crt"])))}
+    out["stage_roofline_note"] = "peak: hbm_gbs of MEASURED_PEAKS.json (copy bandwidth); stage times as stage_ms"
+    # the other op pairs at the same shape and s (alpha 1.5, beta -0.5)
+    by_op = {}
+    for ta, tb in (("N", "N"), ("N", "T"), ("T", "N"), ("T", "T")):
+        lda_, ldb_ = (m if ta == "N" else k), (k if tb == "N" else n)
+        oz.gemm(ta, tb, m, n, k, 1.5, A, lda_, B, ldb_, -0.5, C, ldc, a.s)
+        with Timer(torch, stream) as t:
+            for _ in range(5):
+                oz.gemm(ta, tb, m, n, k, 1.5, A, lda_, B, ldb_, -0.5, C, ldc, a.s)
+        by_op[ta + tb] = flops / (t.ms / 5 * 1e-3) / 1e12
+    out["tflops_by_op"] = by_op
     # end to end with host buffers: H2D of A, B, C and D2H of C every step
     hA = torch.empty(m * k, dtype=torch.float64, pin_memory=True)
     hB = torch.empty(k * n, dtype=torch.float64, pin_memory=True)
@@ -551,6 +573,22 @@ def dgemm_leg(a, oz2, torch, dev, stream, rank):
                 oz.gemm("N", "N", m, n, k, 1.5, A, m, B, k, -0.5, C, ldc, sv)
         sweep[str(sv)] = flops / (t.ms / 5 * 1e-3) / 1e12
     out["tflops_by_s"] = sweep
+    # the other DGEMM shapes of the workload table: 1024^3 at s = 16, and the k-split case
+    # 1024 x 1024 x 262144 at s = 16 (three exact int32 chunks of k), NN, alpha 1, beta 0
+    shapes = {}
+    for name, (mm, nn, kk) in (("1024x1024x1024", (1024, 1024, 1024)), ("1024x1024x262144", (1024, 1024, 262144))):
+        As = torch.rand(mm * kk, dtype=torch.float64, device=dev, generator=g) * 2 - 1
+        Bs = torch.rand(kk * nn, dtype=torch.float64, device=dev, generator=g) * 2 - 1
+        Cs = torch.empty(mm * nn, dtype=torch.float64, device=dev)
+        oz.gemm("N", "N", mm, nn, kk, 1.0, As, mm, Bs, kk, 0.0, Cs, mm, 16)
+        with Timer(torch, stream) as t:
+            for _ in range(5):
+                oz.gemm("N", "N", mm, nn, kk, 1.0, As, mm, Bs, kk, 0.0, Cs, mm, 16)
+        shapes[name] = {"s": 16, "tflops": 2.0 * mm * nn * kk / (t.ms / 5 * 1e-3) / 1e12, "ms": t.ms / 5,
+                        "k_chunks": oz.last_tiling().k_chunks,
+                        "l2": "inputs fit in L2 (warm)" if 8 * (mm * kk + kk * nn) < 100e6 else "inputs larger than L2"}
+        del As, Bs, Cs
+    out["other_shapes"] = shapes
     oz.check_device_error()
     oz.close()
     return out
