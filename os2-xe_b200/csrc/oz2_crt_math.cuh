@@ -99,11 +99,14 @@ __device__ __forceinline__ void crt_sums(const uint32_t (&R)[EG][(S + 3) / 4], c
 
 template <int NL>
 __device__ __forceinline__ double crt_finish(const uint64_t (&acc)[NL], int64_t q, const uint32_t* Mw, int shift) {
+    // the quotient is below 2^16 (a 16-bit fraction sum shifted by 16), so q M_l is one
+    // 32 x 32 -> 64-bit product
+    const uint64_t q32 = static_cast<uint32_t>(q);
     uint32_t w[NL];
     int64_t carry = 0;
 #pragma unroll
     for (int l = 0; l < NL; ++l) {
-        const int64_t v = static_cast<int64_t>(acc[l]) - q * static_cast<int64_t>(Mw[l]) + carry;
+        const int64_t v = static_cast<int64_t>(acc[l]) - static_cast<int64_t>(q32 * Mw[l]) + carry;
         w[l] = static_cast<uint32_t>(v);
         carry = v >> 32;
     }
@@ -115,15 +118,14 @@ __device__ __forceinline__ double crt_finish(const uint64_t (&acc)[NL], int64_t 
         X[i] = static_cast<uint64_t>(w[2 * i]) | (2 * i + 1 < NL ? static_cast<uint64_t>(w[2 * i + 1]) << 32 : 0);
     if (NL % 2)  // odd word count: sign-extend the top word into the last 64-bit word
         X[NW - 1] = static_cast<uint64_t>(static_cast<int64_t>(static_cast<int32_t>(w[NL - 1])));
-    const bool neg = static_cast<int64_t>(X[NW - 1]) < 0;
-    if (neg) {
-        uint64_t borrow = 1;
+    // magnitude without a branch: (X xor s) + (s & 1) over the words, s all ones when negative
+    const uint64_t sgn = static_cast<uint64_t>(static_cast<int64_t>(X[NW - 1]) >> 63);
+    uint64_t inc = sgn & 1u;
 #pragma unroll
-        for (int i = 0; i < NW; ++i) {
-            const uint64_t nv = ~X[i] + borrow;
-            borrow = (borrow && nv == 0) ? 1 : 0;
-            X[i] = nv;
-        }
+    for (int i = 0; i < NW; ++i) {
+        const uint64_t t = (X[i] ^ sgn) + inc;
+        inc &= t == 0 ? 1u : 0u;  // the carry goes on only past a word that wrapped to zero
+        X[i] = t;
     }
     // leading 64 bits with a sticky bit for everything below
     uint64_t hiw = 0, low = 0;
@@ -143,7 +145,7 @@ __device__ __forceinline__ double crt_finish(const uint64_t (&acc)[NL], int64_t 
     const uint64_t top = z ? (hiw << z) | (low >> (64 - z)) : hiw;
     sticky |= (z ? (low << z) : low) != 0;
     const double val = scale_pow2(__ull2double_rn(top | (sticky ? 1u : 0u)), 64 * tw - z - shift);
-    return neg ? -val : val;
+    return __longlong_as_double(__double_as_longlong(val) | static_cast<long long>(sgn & 0x8000000000000000ull));
 }
 
 // 4 x 4 byte transpose: word t of `in` holds entries e = 0..3 of modulus 4g + t; word e of `out`
