@@ -66,7 +66,7 @@ struct ProbeItem {
     int64_t block0;
 };
 
-// Freivalds probe of one computed tile (the north star's C x against A (B x) in double-double):
+// Freivalds probe of one computed tile (C x against alpha A (B x) in double-double):
 // kFreivaldsVecs random vectors x_v with x_vj = +-2^-f_j (f_j the frexp exponent of op(B)'s
 // column maximum, 0 for a zero or non-finite column), so every product with x is exact. Pass 1
 // (one block per kFreivaldsP inner indices): u_v = op(B) x_v in double-double and ub_v = |op(B)||x_v|.
