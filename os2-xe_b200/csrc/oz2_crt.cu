@@ -283,6 +283,7 @@ __global__ void __launch_bounds__(kCrtThreads) crt_tc_kernel(const __grid_consta
         crt_tc_load(cur, warp + 8, P.s, wv[1]);
     }
     bool ok = true;
+    uint32_t committed = 0, last_par = 0;  // (thread 0) per accumulator: a commit issued, its parity
     for (int64_t kk = 0; kk <= ntiles && ok; ++kk) {
         const int buf = static_cast<int>(kk & 1);
         if (kk < ntiles) {
@@ -300,6 +301,8 @@ __global__ void __launch_bounds__(kCrtThreads) crt_tc_kernel(const __grid_consta
                 dev::mma_i8(tmem + static_cast<uint32_t>((4 * buf + g) * NC), dev::sw128_kmajor_desc(a0 + 32 * g),
                             dev::sw128_kmajor_desc(dev::smem_addr(sB)), T::kIdesc, 0u);
             dev::tc_commit(dev::smem_addr(bar + buf));
+            committed |= 1u << buf;
+            last_par = (last_par & ~(1u << buf)) | (static_cast<uint32_t>((kk >> 1) & 1) << buf);
         }
         SuperTile nxt{};
         if (kk + 1 < ntiles) {  // the next super-tile's loads run under this iteration's waits and arithmetic
@@ -356,6 +359,10 @@ __global__ void __launch_bounds__(kCrtThreads) crt_tc_kernel(const __grid_consta
         }
         prev = cur;
         cur = nxt;
+    }
+    if (!ok && threadIdx.x == 0) {  // the last MMA of each accumulator completes before TMEM is freed
+        for (int b = 0; b < 2; ++b)
+            if (committed & (1u << b)) dev::mbar_wait_drain(dev::smem_addr(bar + b), (last_par >> b) & 1u);
     }
     dev::tc_fence_before();
     __syncthreads();

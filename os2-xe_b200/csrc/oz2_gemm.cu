@@ -461,6 +461,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_i8_modm_kernel(const __g
                 }
             }
         }
+        if constexpr (CRTF) dev::tmem_store_wait();  // no residue store in flight when TMEM is freed
     }
     __syncwarp();
     dev::tc_fence_before();
