@@ -73,6 +73,8 @@ def parse():
                     help="scale pass fused into the split for k <= 2048 (1) or separate (0, default)")
     ap.add_argument("--crt-fusion", type=int, default=0, choices=(0, 1),
                     help="CRT in the GEMM epilogue for s <= 8 (1) or a separate CRT launch (0, default)")
+    ap.add_argument("--probe-kind", type=int, default=-1, choices=(-1, 0, 1, 2, 3),
+                    help="probe of the MLP tiles: -1 the library default, 0 columns, 1 Freivalds, 2 both, 3 none")
     ap.add_argument("--dgemm-only", action="store_true",
                     help="time only the DGEMM of --size and --s (a profiling aid; not the headline)")
     return ap.parse_args()
@@ -777,6 +779,8 @@ def probe_study(a, oz, torch, dev):
     probe and both; per setting the problems over the bound after the reruns, the probed and rerun
     tiles, and the step time. Prints one JSON line."""
     model = oz.load_model()
+    if a.probe_kind >= 0:
+        oz.set_probe_kind(a.probe_kind)
     steps = step_specs(a, 0)
     rows = []
     for part in steps:
