@@ -114,6 +114,7 @@ struct Templates {
         Big M = Big::of(1);
         for (int t = 0; t < s; ++t) {
             p.m[t] = seq[t];
+            if (seq[t] != 256 && seq[t] % 2 == 0) return 3;  // the split's rounded quotient needs odd m
             if (!M.mul(seq[t])) return 5;
         }
         p.log2M = M.log2();
@@ -218,6 +219,11 @@ void mod_constants(const Plan& p, ModConst* out) {
         // with M = ceil(2^32 / m) = (2^32 + e) / m, 0 <= e < m <= 2^8, floor(v M / 2^32) =
         // floor(v / m) for every v < 2^24 (the added v e / (m 2^32) stays below 1 / m)
         c.m32 = static_cast<uint32_t>(((uint64_t{1} << 32) + m - 1) / m);
+        c.foff3 = 0x4B000000u + (m - pow2_mod(62, m)) % m;
+        c.foff5 = 0x4B000000u + (m - pow2_mod(93, m)) % m;
+        c.foff7 = 0x4B000000u + (m - pow2_mod(125, m)) % m;
+        c.finv = 1.0f / static_cast<float>(m);
+        c.fbias = -8388608.0f * c.finv;
     }
 }
 

@@ -66,6 +66,11 @@ struct ModConst {
                        // ceil(2^39 / m) would not fit 32 bits
     uint32_t cb[4];  // bytes 2^(8 l) mod m, l = 0..15, four per word (byte-limb weights)
     uint32_t m32;    // ceil(2^32 / m): floor(v / m) = umulhi(v, m32) exactly for v < 2^24
+    // the split's start values 0x4B000000 + (-2^62 mod m), (-2^93 mod m), (-2^125 mod m): as
+    // floats, 2^23 plus the offset that cancels the narrow, wide and widest offset integers
+    uint32_t foff3, foff5, foff7;
+    float finv;   // fl(1 / m)
+    float fbias;  // -2^23 fl(1 / m), exact (a power-of-two multiple)
 };
 
 struct Plan {

@@ -146,16 +146,28 @@ __device__ __forceinline__ void offset_words_fp_widest(double v, double s1, doub
     W[3] = static_cast<uint32_t>(oh >> 32);
 }
 
-// (x + h) mod m in [0, m) from the bytes of the offset integer: v = koff + sum_l byte_l (2^(8 l)
-// mod m) by byte dot products (at most 16 bytes, so v < 255 + 16 255^2 < 2^20), then the exact
-// multiply-high quotient by ceil(2^32 / m). Two (three, four) dot products, one multiply-high
-// and one multiply-subtract per residue.
+// The byte dot products of the offset integer: v = 0x4B000000 + koff + sum_l byte_l (2^(8 l) mod m)
+// with koff = -2^62 (-2^93, -2^125) mod m, so that v' = v - 0x4B000000 is congruent to x modulo m
+// and below 2^20 (at most 16 bytes: m + 16 255^2), and v's bits are the float 2^23 + v' exactly.
 template <int NW>
-__device__ __forceinline__ uint32_t byte_residue(const uint32_t (&W)[NW], const ModConst& c) {
-    uint32_t v = NW == 2 ? c.koff3 : (NW == 3 ? c.koff5 : c.koff7);
+__device__ __forceinline__ uint32_t byte_dot(const uint32_t (&W)[NW], const ModConst& c) {
+    uint32_t v = NW == 2 ? c.foff3 : (NW == 3 ? c.foff5 : c.foff7);
 #pragma unroll
     for (int j = 0; j < NW; ++j) v = __dp4a(W[j], c.cb[j], v);
-    return v - __umulhi(v, c.m32) * c.m;
+    return v;
+}
+
+// The symmetric residue v' - q m, q = rint(v' / m), in [-h, h] (m odd), in the low byte of the
+// result (the upper bytes hold a constant of m). One FMA gives fl(v' fl(1/m)): its addend -2^23
+// fl(1/m) cancels the 2^23 of v's float exactly, so only the product and one rounding err, by at
+// most (v'/m) 2^-23 < 2^-2 / m for v' < 2^21. For odd m, v'/m lies at least 1 / (2m) from every
+// half-integer, so adding 1.5 2^23 (round to nearest, ulp 1) gives the float 1.5 2^23 + q with
+// bits 0x4B400000 + q. Then v - bits m = v' - q m + (0x4B000000 - 0x4B400000 m), and both
+// constants are 0 modulo 256. Per residue: two FP32 operations in place of the integer
+// multiply-high quotient, and no shift of [0, m) to [-h, m-1-h] afterwards.
+__device__ __forceinline__ uint32_t sym_residue(uint32_t v, const ModConst& c) {
+    const float t = __fadd_rn(__fmaf_rn(__uint_as_float(v), c.finv, c.fbias), 12582912.0f);
+    return v - __float_as_uint(t) * c.m;
 }
 
 // low bytes of a, b, c, d as one little-endian word
@@ -275,28 +287,23 @@ __device__ __forceinline__ void split_piece(const SplitItem* __restrict__ I, int
         } else {
 #pragma unroll
             for (int q = 0; q < EPT; ++q) {
-                const uint32_t r0 = byte_residue<NW>(L[0][q], mc);
-                b0[q] = r0;
+                const uint32_t v0 = byte_dot<NW>(L[0][q], mc);
+                b0[q] = sym_residue(v0, mc);
                 if (CPLX) {
-                    const uint32_t r1 = byte_residue<NW>(L[NG - 1][q], mc);
-                    // (x0 + x1 + h) mod m from the two shifted residues
-                    uint32_t r2 = r0 + r1 + (mc.m - mc.h);
-                    r2 = min(r2, r2 - mc.m);
-                    r2 = min(r2, r2 - mc.m);
-                    b1[q] = r1;
-                    b2[q] = r2;
+                    const uint32_t v1 = byte_dot<NW>(L[NG - 1][q], mc);
+                    b1[q] = sym_residue(v1, mc);
+                    b2[q] = sym_residue(v0 + v1 - 0x4B000000u, mc);  // x0 + x1: v0' + v1' < 2^21
                 }
             }
         }
-        // bytes r - h modulo 256, four per word (m = 256 stores x mod 256 directly)
-        const uint32_t h4 = mc.m == 256 ? 0u : mc.h * 0x01010101u;
+        // the residue bytes (as int8), four per word
         uint32_t w0[EPT / 4], w1[EPT / 4], w2[EPT / 4];
 #pragma unroll
         for (int q = 0; q < EPT / 4; ++q) {
-            w0[q] = __vsub4(pack_bytes(b0[4 * q], b0[4 * q + 1], b0[4 * q + 2], b0[4 * q + 3]), h4);
+            w0[q] = pack_bytes(b0[4 * q], b0[4 * q + 1], b0[4 * q + 2], b0[4 * q + 3]);
             if (CPLX) {
-                w1[q] = __vsub4(pack_bytes(b1[4 * q], b1[4 * q + 1], b1[4 * q + 2], b1[4 * q + 3]), h4);
-                w2[q] = __vsub4(pack_bytes(b2[4 * q], b2[4 * q + 1], b2[4 * q + 2], b2[4 * q + 3]), h4);
+                w1[q] = pack_bytes(b1[4 * q], b1[4 * q + 1], b1[4 * q + 2], b1[4 * q + 3]);
+                w2[q] = pack_bytes(b2[4 * q], b2[4 * q + 1], b2[4 * q + 2], b2[4 * q + 3]);
             }
         }
         store(out + t * plane_bytes, w0);
