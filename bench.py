@@ -9,7 +9,7 @@ beta = 0, target DGEMM-level error (|C - AB| <= k 2^-53 (|A||B|)_ij). The stream
 at most 512), generated on the device with a seeded generator before the step and timed alone
 with CUDA events, so every timed problem is distinct; each batch (tens of GB) is far larger than
 the 126 MB L2. s is chosen per 512 x 512 tile: certified where a tile needs 23 or more moduli by
-the analytic rule, else by the MLP (probed, rerun at the judge's s on failure); tiles no s <= 24
+the analytic rule, else by the MLP (probed, rerun at the arbiter's s on failure); tiles no s <= 24
 serves run in native FP64. Metric: FP64-equivalent TFLOP/s = sum 2 m n k / t. The fixed-s forms
 of the same batches (per-problem analytic s batched and as plain calls, the certified per-problem
 s, cuBLAS DGEMM for everything, s = 24, the reference's moduli_for_bits(k, 53)) are timed step by
@@ -775,7 +775,7 @@ def e2e_leg(oz, torch, dev, stream, b0, steps):
 
 def probe_study(a, oz, torch, dev):
     """What the probes catch: the MLP mode at lowered decision thresholds (more tiles below their
-    judge's s) over the first batches of the stream, with no probe, the column probe, the Freivalds
+    arbiter's s) over the first batches of the stream, with no probe, the column probe, the Freivalds
     probe and both; per setting the problems over the bound after the reruns, the probed and rerun
     tiles, and the step time. Prints one JSON line."""
     model = oz.load_model()

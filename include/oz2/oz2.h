@@ -98,17 +98,17 @@ int oz2_autotune_grouped(oz2_handle h, int count, const oz2_dgemm_problem* probl
  * FP64 GEMM for target_bits = 53 ("DGEMM-level error"). Per tile of tile x tile entries (default
  * 512), s comes from
  *   mode 0: the MLP (oz2_mlp_set_weights; a tile takes the largest class over itself and its
- *           up to 8 neighbours in the problem), capped by the judge's s, for problems with
- *           beta = 0 and tiles without a certificate (the others take the judge's s); tiles below
- *           the judge's s are probed (C x against A (B x) with x = e_j for 8 columns j, each entry
+ *           up to 8 neighbours in the problem), capped by the arbiter's s, for problems with
+ *           beta = 0 and tiles without a certificate (the others take the arbiter's s); tiles below
+ *           the arbiter's s are probed (C x against A (B x) with x = e_j for 8 columns j, each entry
  *           checked) and rerun at it when the probe fails; without weights it behaves as mode 4
  *   mode 1: the analytic s of the tile: smallest s whose tk >= R + 2 + t - floor(log2(k - 1)),
  *           R the largest exponent gap below the row / column maximum in the tile's panels
  *   mode 2: the analytic s of the whole problem (the largest over its tiles)
  *   mode 3: each problem's own num_moduli, 2..32 (tiled like the other modes)
- *   mode 4: the judge's s of the tile (no MLP, no probe: every tile meets the target)
- *   mode 5: the judge's s of the whole problem (the largest over its tiles)
- * The judge of a tile is the smaller of its analytic s and, for problems with a tile whose analytic
+ *   mode 4: the arbiter's s of the tile (no MLP, no probe: every tile meets the target)
+ *   mode 5: the arbiter's s of the whole problem (the largest over its tiles)
+ * The arbiter of a tile is the smaller of its analytic s and, for problems with a tile whose analytic
  * s is 23 or more (k <= 65472), its certified s: the smallest s for which a rigorous entrywise
  * bound of the emulation's error (row / column sums of |A| and |B| against a bf16 lower bound of
  * |A||B| from a tcgen05 GEMM) meets the target in every entry of the tile. In modes 0 and 4 a
@@ -116,13 +116,13 @@ int oz2_autotune_grouped(oz2_handle h, int count, const oz2_dgemm_problem* probl
  * more than its tiles as chosen, counting a tile task 12 % dearer and native FP64 as 63 moduli.
  * Above s = 24 the adaptive path uses moduli sets of its own (s = 25..32: pairwise-coprime
  * integers <= 256 taken greedily from the top; up to 124 bits per element), so a tile whose
- * judge needs more than the 91 bits of 24 moduli still runs emulated; the MLP's last class means
+ * arbiter needs more than the 91 bits of 24 moduli still runs emulated; the MLP's last class means
  * "more than 24" and answers 25. In modes 0-2, 4 and 5 a tile that no s <= 32 brings to the
  * target runs as a native FP64 GEMM (cuBLAS DGEMM), the whole problem in one call when all its
  * tiles do; the analytic rule sends a tile there when a gap reaches 63 binades (its histogram's
  * last bin).
  * stats (may be NULL, 10 entries): tiles, sum of s over emulated tiles (reruns included), probed
- * tiles, rerun tiles, sum of s of the reruns (33 for native), sum of the judge's s (33 for native),
+ * tiles, rerun tiles, sum of s of the reruns (33 for native), sum of the arbiter's s (33 for native),
  * MLP used, int8 multiply-adds of the emulated tiles (s m_t n_t k summed, reruns included),
  * native tiles, native FP64 multiply-adds. The host waits in the middle of the call for the tile
  * statistics (and in mode 0 for the probe). Those reads, and the uploads of item tables, are copy
@@ -141,7 +141,7 @@ int oz2_set_adaptive_options(oz2_handle h, int tile, float threshold);
  * x_j = +-2^-f_j (f_j the exponent of op(B)'s column maximum), row by row against alpha k 2^-t
  * (|A| (|B| |x|))_i; 2 runs both (a tile fails when either fails); 3 runs none, so the MLP's s
  * stands unchecked (for measuring what the probes catch). A tile that meets the target passes
- * every kind; a failing tile is rerun at its judge's s. */
+ * every kind; a failing tile is rerun at its arbiter's s. */
 int oz2_set_probe_kind(oz2_handle h, int kind);
 /* with profiling on: device time of the last oz2_dgemm_adaptive's probe and of its native FP64
  * tiles (out2 = {probe_ms, native_ms}) */

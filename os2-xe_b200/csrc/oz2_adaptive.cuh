@@ -19,7 +19,7 @@ constexpr int kHidden = 32;
 // s <= 32 brings to the target, run as a native FP64 GEMM
 constexpr int kNativeS = kMaxModuliExt + 1;
 // the MLP's classes: s = 2..24 and one for "more than 24" (s = 25 as its answer: a lower bound
-// that the probe checks, or the judge's s where a certificate takes the tile)
+// that the probe checks, or the arbiter's s where a certificate takes the tile)
 constexpr int kClasses = kMaxModuli;
 // per-call statistics of oz2_dgemm_adaptive
 constexpr int kAdaptiveStats = 10;

@@ -1225,10 +1225,10 @@ int certify_tiles(oz2_context* h, const std::vector<Prob>& base, const std::vect
     return OZ2_OK;
 }
 
-// mode: 0 MLP per tile for tiles without a certificate (judge cap, probe, rerun at the judge's s;
-// certified tiles take the judge's s), 1 analytic per tile,
+// mode: 0 MLP per tile for tiles without a certificate (arbiter cap, probe, rerun at the arbiter's s;
+// certified tiles take the arbiter's s), 1 analytic per tile,
 // 2 analytic per problem (the largest of its tiles), 3 the problems' own num_moduli, 4 certified
-// per tile, 5 certified per problem. The judge of a tile is the smaller of its analytic and
+// per tile, 5 certified per problem. The arbiter of a tile is the smaller of its analytic and
 // certified s (modes 0, 4, 5; the analytic s alone in modes 1 and 2).
 int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>& fixed_s, int target_bits,
                  int mode, float* feat_out = nullptr, int* sa_out = nullptr, int64_t* ntiles_out = nullptr) {
@@ -1430,7 +1430,7 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
         }
         s_ml.swap(pooled);
     }
-    // the judge: the smaller of the analytic and the certified s (both meet the target)
+    // the arbiter: the smaller of the analytic and the certified s (both meet the target)
     std::vector<int> s_jd(ntiles);
     for (int64_t t = 0; t < ntiles; ++t) s_jd[t] = certify ? std::min(s_an[t], std::max(s_ce[t], 2)) : s_an[t];
     std::vector<int> s_tile(ntiles);
@@ -1441,7 +1441,7 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
         int sv;
         switch (mode) {
             // the probe and the rerun need C's old values gone (beta = 0): other problems keep
-            // the judge's s
+            // the arbiter's s
             // a tile with a certificate takes it (rigorous, within about a modulus of the smallest
             // s that meets the target); the MLP chooses for the others, below the analytic s
             case 0:
@@ -1742,7 +1742,7 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
             const TileRef& r = tiles[t];
             const Prob& p = base[r.prob];
             if (h->probe_kind == 3) break;  // no probe: the MLP's s stands (for measurements)
-            if (p.beta[0] != 0.0 || s_tile[t] >= s_jd[t]) continue;  // the judge's s needs no probe
+            if (p.beta[0] != 0.0 || s_tile[t] >= s_jd[t]) continue;  // the arbiter's s needs no probe
             ProbeItem it{};
             it.a_rowc = is_n(p.ta);
             it.b_rowc = !is_n(p.tb);

@@ -355,7 +355,7 @@ class Ozaki2:
     def gemm_adaptive(self, problems, target_bits=53, mode=0):
         """problems as for gemm_grouped (num_moduli is used by mode 3 only). Returns the stats
         dict: tiles, sum_s (emulated tiles, reruns included), probed, rerun, rerun_sum_s,
-        analytic_sum_s (the judge's s summed: the analytic s, or in modes 0, 4 and 5 the smaller of
+        analytic_sum_s (the arbiter's s summed: the analytic s, or in modes 0, 4 and 5 the smaller of
         the analytic and certified s; 33 counts a native tile), mlp, int8_macs (sum of s m_t n_t k
         over emulated tiles), native_tiles, native_macs (tiles run as native FP64 GEMMs)."""
         arr = self._problems(problems)

@@ -5,7 +5,7 @@ fewer rows or columns, of a problem with inputs (u - 0.5) exp(phi g), per-row / 
 exponent offsets), the label is the smallest s whose result meets the DGEMM-level target, every
 entry within k 2^-53 (|A||B|)_ij of the exact product, measured against the library's
 double-double reference (oz2_dd_reference); 25 when no s <= 24 does (the MLP's last class: "more
-than 24", which the library resolves with its judge, up to the extended sets' s = 32 or native
+than 24", which the library resolves with its arbiter, up to the extended sets' s = 32 or native
 FP64). Features are the
 library's own tile features (oz2_tile_features). Training runs the hand-written CUDA kernel
 (oz2_mlp_train). The model is saved as JSON: parameters, decision threshold, tile, provenance.

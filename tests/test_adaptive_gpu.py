@@ -188,7 +188,7 @@ def test_analytic_modes_meet_the_target(az, phi, offsets):
 
 def test_probe_reruns_tiles_run_at_too_few_moduli(az):
     """an MLP that always answers s = 2 (on tiles whose analytic s stays below 23, so that no
-    certificate takes them over): every tile is probed, fails and is rerun at its judge's s, and
+    certificate takes them over): every tile is probed, fails and is rerun at its arbiter's s, and
     the result meets the target"""
     import torch
     m, n, k = 1030, 600, 700
@@ -242,7 +242,7 @@ def test_probe_passes_tiles_that_meet_the_target(az):
         st = az.gemm_adaptive([("N", "N", m, n, k, 1.0, dA, m, dB, k, 0.0, dC, m, 16)], 53, az.ADAPTIVE_MLP)
     finally:
         az.set_mlp_weights(None)
-    # probed when s_min is below the judge (the certified s is within a modulus or two of s_min)
+    # probed when s_min is below the arbiter (the certified s is within a modulus or two of s_min)
     assert st["analytic_sum_s"] >= s_min
     assert st["probed"] == (1 if st["analytic_sum_s"] > s_min else 0)
     assert st["rerun"] == 0 and st["sum_s"] == s_min
@@ -421,7 +421,7 @@ def test_whole_problem_and_tile_tasks_agree(az):
                                                (600, 1100, 1500, 6.0, 40), (520, 520, 300, 8.0, 40)])
 def test_certified_modes_meet_the_target(az, m, n, k, phi, offsets):
     """modes 4 (certified s per tile) and 5 (per problem): every output within the target, the
-    judge never above the analytic rule, the same result on every run, and op(A) = T / op(B) = T
+    arbiter never above the analytic rule, the same result on every run, and op(A) = T / op(B) = T
     on explicitly transposed copies (the k-contiguous certificate layouts) equal to NN bit for bit"""
     import torch
     A, B = nn_problem(300 + m, m, n, k, phi, offsets)
@@ -450,9 +450,9 @@ def test_certified_modes_meet_the_target(az, m, n, k, phi, offsets):
                                           (4, 400, 333, 6.0), (5, 512, 512, 1.0), (6, 500, 700, 5.0),
                                           (7, 384, 1500, 7.0)])
 def test_certified_s_matches_the_restatement(oracle, az, seed, n, k, phi):
-    """one tile per problem: where the analytic s is 23 or more the device's judge lies between
+    """one tile per problem: where the analytic s is 23 or more the device's arbiter lies between
     the restated certificate (FP64 |A||B|) and one modulus above it (the device's bf16 lower
-    bound is a little smaller); below 23 no certificate runs and the judge is the analytic s"""
+    bound is a little smaller); below 23 no certificate runs and the arbiter is the analytic s"""
     import torch
     A, B = nn_problem(700 + seed, n, n, k, phi, 30)
     dA, dB = to_dev(A), to_dev(B)
@@ -554,7 +554,7 @@ def test_gemm_bytes_count_planes_once_and_residues(az):
 def test_freivalds_probe_reruns_tiles_run_at_too_few_moduli(az, kind):
     """the Freivalds test (C x against alpha A (B x) in double-double), alone and beside the column
     probe: an MLP that always answers s = 2 leaves every tile far off, every tile fails and is rerun
-    at its judge's s, and the result meets the target"""
+    at its arbiter's s, and the result meets the target"""
     import torch
     m, n, k = 1030, 600, 700
     A, B = nn_problem(73, m, n, k, 1.0, 10)
@@ -582,12 +582,12 @@ def test_freivalds_probe_passes_tiles_that_meet_the_target(az, phi, offsets):
     dA, dB = to_dev(A), to_dev(B)
     s_min = smallest_s(az, dA, dB, m, n, k)
     dC = torch.zeros(m * n, dtype=torch.float64, device="cuda")
-    judge = az.gemm_adaptive([("N", "N", m, n, k, 1.0, dA, m, dB, k, 0.0, dC, m, 16)], 53,
+    arbiter = az.gemm_adaptive([("N", "N", m, n, k, 1.0, dA, m, dB, k, 0.0, dC, m, 16)], 53,
                              az.ADAPTIVE_CERTIFIED_TILE)["analytic_sum_s"]
     _, s_an = az.tile_features([("N", "N", m, n, k, 1.0, dA, m, dB, k, 0.0, dC, m, 16)])
     assert int(s_an[0]) < 23, "a tile the certificate would take over is never probed"
-    if s_min >= judge or s_min > 24:
-        pytest.skip("no s below the judge's meets the target here: nothing to probe")
+    if s_min >= arbiter or s_min > 24:
+        pytest.skip("no s below the arbiter's meets the target here: nothing to probe")
     az.set_mlp_weights(const_class_params(s_min - 2))
     az.set_probe_kind(1)
     try:
