@@ -221,6 +221,24 @@ __device__ __forceinline__ void crt_tc_store(uint8_t* sA, int c, const uint32_t 
     }
 }
 
+// The row and column maxima this thread needs to finish its two entries of a super-tile: row
+// i0 + crt_tc_row(lane), columns j0 + 4 (warp / 4) + warp % 4 and 8 further (zero outside the
+// problem). Loaded with the super-tile's residues, a loop iteration before they are used, so
+// finishing waits on no global load.
+struct TcMaxima {
+    unsigned long long a, b0, b1;
+};
+__device__ __forceinline__ TcMaxima crt_tc_maxima(const SuperTile& T) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t i = T.i0 + crt_tc_row(lane);
+    const int64_t j0 = T.j0 + 4 * (warp >> 2) + (warp & 3), j1 = j0 + 8;
+    TcMaxima r;
+    r.a = i < T.I->m ? __ldg(T.I->maxA + i) : 0ull;
+    r.b0 = j0 < T.I->n ? __ldg(T.I->maxB + j0) : 0ull;
+    r.b1 = j1 < T.I->n ? __ldg(T.I->maxB + j1) : 0ull;
+    return r;
+}
+
 // Software-pipelined over the CTA's super-tiles: while the MMAs of super-tile k run, the threads
 // load super-tile k + 1's residues into registers and finish super-tile k - 1 from the other
 // accumulators.
@@ -277,10 +295,12 @@ __global__ void __launch_bounds__(kCrtThreads) crt_tc_kernel(const __grid_consta
     const int64_t ntiles = P.tiles > blockIdx.x ? (P.tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
     uint32_t wv[2][8];
     SuperTile cur{}, prev{};
+    TcMaxima mcur{}, mprev{};
     if (ntiles > 0) {
         cur = tile_ref(blockIdx.x);
         crt_tc_load(cur, warp, P.s, wv[0]);
         crt_tc_load(cur, warp + 8, P.s, wv[1]);
+        mcur = crt_tc_maxima(cur);
     }
     bool ok = true;
     uint32_t committed = 0, last_par = 0;  // (thread 0) per accumulator: a commit issued, its parity
@@ -305,10 +325,12 @@ __global__ void __launch_bounds__(kCrtThreads) crt_tc_kernel(const __grid_consta
             last_par = (last_par & ~(1u << buf)) | (static_cast<uint32_t>((kk >> 1) & 1) << buf);
         }
         SuperTile nxt{};
+        TcMaxima mnxt{};
         if (kk + 1 < ntiles) {  // the next super-tile's loads run under this iteration's waits and arithmetic
             nxt = tile_ref(blockIdx.x + (kk + 1) * gridDim.x);
             crt_tc_load(nxt, warp, P.s, wv[0]);
             crt_tc_load(nxt, warp + 8, P.s, wv[1]);
+            mnxt = crt_tc_maxima(nxt);
         }
         if (kk > 0) {  // finish super-tile kk - 1
             const int pb = buf ^ 1;
@@ -326,7 +348,7 @@ __global__ void __launch_bounds__(kCrtThreads) crt_tc_kernel(const __grid_consta
             const int q = warp & 3, h = warp >> 2;
             const int64_t i = prev.i0 + crt_tc_row(lane);
             const int tk = I->tk;
-            const int De = i < I->m ? exponent_of(I->maxA[i], tk) : 0;
+            const int De = i < I->m ? exponent_of(mprev.a, tk) : 0;
 #pragma unroll
             for (int gg = 0; gg < 2; ++gg) {
                 const int g = h + 2 * gg;
@@ -346,7 +368,7 @@ __global__ void __launch_bounds__(kCrtThreads) crt_tc_kernel(const __grid_consta
                     }
                     const uint32_t uf = (1u << 15) + d[4 * NL] + (d[4 * NL + 1] << 8);
                     const int64_t qv = static_cast<int64_t>(uf >> 16);
-                    const int Ej = exponent_of(I->maxB[j], tk);
+                    const int Ej = exponent_of(gg ? mprev.b1 : mprev.b0, tk);
                     const bool nonfinite = De == kNonFinite || Ej == kNonFinite;
                     double v = crt_finish<NL>(acc, qv, P.M, nonfinite ? 0 : De + Ej);
                     if (nonfinite) v = __longlong_as_double(0x7FF8000000000000ll);
@@ -359,6 +381,8 @@ __global__ void __launch_bounds__(kCrtThreads) crt_tc_kernel(const __grid_consta
         }
         prev = cur;
         cur = nxt;
+        mprev = mcur;
+        mcur = mnxt;
     }
     if (!ok && threadIdx.x == 0) {  // the last MMA of each accumulator completes before TMEM is freed
         for (int b = 0; b < 2; ++b)
