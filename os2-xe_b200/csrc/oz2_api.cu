@@ -575,9 +575,11 @@ int put_blob(oz2_context* h, const void* data, size_t bytes, unsigned char* dev)
     if (h->ring_used[slot]) OZ2_CUDA(h, cudaEventSynchronize(h->ring_ev[slot]));
     if (!h->ring_ev[slot]) OZ2_CUDA(h, cudaEventCreateWithFlags(&h->ring_ev[slot], cudaEventDisableTiming));
     if (h->ring_cap[slot] < bytes) {
-        // pinned allocations are slow and synchronise: grow in powers of two from 1 MiB
+        // pinned allocations are slow and synchronise: grow in powers of two from 1 MiB, to at
+        // least twice this blob, so that the next calls' blobs (which vary with the problem list)
+        // rarely grow a slot again
         size_t cap = std::max(h->ring_cap[slot] * 2, size_t{1} << 20);
-        while (cap < bytes) cap *= 2;
+        while (cap < 2 * bytes) cap *= 2;
         if (h->ring_host[slot]) cudaFreeHost(h->ring_host[slot]);
         h->ring_host[slot] = h->ring_dev[slot] = nullptr;
         h->ring_cap[slot] = 0;

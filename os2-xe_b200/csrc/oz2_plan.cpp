@@ -141,6 +141,22 @@ const Templates& templates() {
 }
 }  // namespace
 
+// floor(M / 2^e) for e >= 0, or 2^64 - 1 when that does not fit 64 bits
+static uint64_t shr_saturated(const Big& M, int e) {
+    for (int i = kBigWords - 1; i >= 0; --i) {
+        if (!M.w[i]) continue;
+        if (32 * i + 31 - __builtin_clz(M.w[i]) >= e + 64) return ~uint64_t{0};
+        break;
+    }
+    uint64_t r = 0;
+    for (int i = 0; i < kBigWords; ++i) {
+        const int sh = 32 * i - e;  // where bit 0 of word i lands
+        if (!M.w[i] || sh <= -32) continue;
+        r |= sh >= 0 ? uint64_t{M.w[i]} << sh : uint64_t{M.w[i]} >> -sh;
+    }
+    return r;
+}
+
 int plan_tk(int s, int64_t k) {
     if (s < 2 || s > kMaxModuliExt || k < 1) return 0;
     const Templates& T = templates();
@@ -155,9 +171,8 @@ int plan_tk(int s, int64_t k) {
     if (tk > cap) tk = cap;
     for (;; --tk) {
         if (tk < 1) return 0;
-        Big lhs = Big::of(static_cast<uint64_t>(k));
-        if (!lhs.shl(2 * tk + 2)) continue;
-        if (lhs.cmp(M) <= 0) return tk;
+        // k 2^e <= M exactly when k <= floor(M / 2^e), M shifted right by e and saturated to 64 bits
+        if (static_cast<uint64_t>(k) <= shr_saturated(M, 2 * tk + 2)) return tk;
     }
 }
 
