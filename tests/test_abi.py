@@ -46,6 +46,27 @@ def test_planning_entry_points_match_oracle(oracle):
         oz2.Ozaki2.precision_bits(100, 1)
 
 
+def test_precision_bits_at_the_edges_of_k(oracle):
+    """tk changes where k 2^(2 tk + 2) crosses M: k on both sides of every power of two up to 2^40
+    and of M / 2^(2 t + 2) for each plan, against the oracle's plan"""
+    import oz2
+    ks = {2 ** e + d for e in range(41) for d in (-2, -1, 0, 1, 2) if 2 ** e + d >= 1}
+    for s in range(2, 25):
+        M = oracle.plan(s, 1).Mint
+        for t in range(20, 101, 7):
+            edge = M >> (2 * t + 2)
+            ks.update(x for x in (edge - 1, edge, edge + 1) if 1 <= x < 2 ** 62)
+    for s in range(2, 25):
+        for k in sorted(ks):
+            try:
+                want = oracle.precision_bits(k, s)
+            except ValueError:
+                with pytest.raises(ValueError, match="too small"):
+                    oz2.Ozaki2.precision_bits(k, s)
+                continue
+            assert oz2.Ozaki2.precision_bits(k, s) == want, (s, k)
+
+
 def test_null_handle_is_rejected():
     import oz2
     lib = oz2.lib()
