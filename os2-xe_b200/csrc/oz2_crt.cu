@@ -34,11 +34,11 @@ __device__ __forceinline__ uint32_t pack4(uint32_t a, uint32_t b, uint32_t c, ui
     return __byte_perm(__byte_perm(a, b, 0x0040), __byte_perm(c, d, 0x0040), 0x5410);
 }
 
-// Occupancy for the latency-bound loads: real plans up to 20 moduli fit 64 registers (four
-// blocks per SM), up to 24 fit 80 (three); complex ones 128 (two); larger real ones take what the
-// reconstruction needs.
+// Occupancy for the latency-bound loads: real plans of up to 5 limbs (20 moduli) fit 64 registers
+// (four blocks per SM), of 6 limbs (21 to 25 moduli) 80 (three); complex ones 128 (two); larger
+// real ones take what the reconstruction needs.
 template <int S, bool CPLX>
-constexpr int crt_min_blocks() { return CPLX ? 2 : (S <= 20 ? 4 : (S <= 24 ? 3 : 1)); }
+constexpr int crt_min_blocks() { return CPLX ? 2 : (limbs_for(S) <= 5 ? 4 : (limbs_for(S) <= 6 ? 3 : 1)); }
 template <int S, bool CPLX>
 __global__ void __launch_bounds__(256, crt_min_blocks<S, CPLX>()) crt_kernel(const __grid_constant__ CrtParams P) {
     constexpr int NL = limbs_for(S);
