@@ -24,6 +24,7 @@ Under torchrun every rank runs its own stream (weak scaling, no collective on th
 value = all ranks' work / the sum over steps of the slowest rank's step time.
 """
 import argparse
+import gc
 import json
 import math
 import os
@@ -332,8 +333,23 @@ def int8_peak():
     return 2.0 * 1590.0, "2 x fallback bf16 1.59 PF"
 
 
+class NoGC:
+    """Python's cyclic garbage collector off inside a timed region, as timeit does: a collection
+    there stalls the host thread that issues the launches (tens to hundreds of ms in a process
+    holding this many objects); it runs at the next allocation after the region instead"""
+
+    def __enter__(self):
+        self.was = gc.isenabled()
+        gc.disable()
+        return self
+
+    def __exit__(self, *exc):
+        if self.was:
+            gc.enable()
+
+
 class Timer:
-    """CUDA events on the launching stream around a region"""
+    """CUDA events on the launching stream around a region (garbage collector off)"""
 
     def __init__(self, torch, stream):
         self.torch, self.stream = torch, stream
@@ -341,6 +357,7 @@ class Timer:
         self.e1 = torch.cuda.Event(enable_timing=True)
 
     def __enter__(self):
+        self.nogc = NoGC().__enter__()
         self.torch.cuda.synchronize()
         self.e0.record(self.stream)
         return self
@@ -349,6 +366,7 @@ class Timer:
         self.e1.record(self.stream)
         self.torch.cuda.synchronize()
         self.ms = self.e0.elapsed_time(self.e1)
+        self.nogc.__exit__()
 
 
 def sharded_leg(a, oz2, torch, dev, stream, dist, world, rank):
@@ -910,11 +928,12 @@ def main():
         CUDA events on the launching stream; the slowest rank's time"""
         if world > 1:
             dist.barrier()
-        torch.cuda.synchronize()
-        e0.record(stream)
-        ret = fn(batch)
-        e1.record(stream)
-        torch.cuda.synchronize()
+        with NoGC():
+            torch.cuda.synchronize()
+            e0.record(stream)
+            ret = fn(batch)
+            e1.record(stream)
+            torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         if world > 1:
             x = torch.tensor([ms], dtype=torch.float64, device=dev)
