@@ -84,6 +84,66 @@ __global__ void __launch_bounds__(256) panel_stats_kernel(const StatItem* __rest
         if (hist[i]) atomicAdd(I->hist + i, hist[i]);
 }
 
+// Scale and statistics in one pass over DRAM. ROWC: 32 rows per block (one per lane), the 8 warps
+// interleave the inner index, the row maximum is combined through shared memory; otherwise one
+// warp per row (8 rows per block), lanes over the inner index. The second read of the rows
+// (the histogram against the row maximum) comes from the L2. Same maxima and counts as
+// scale_kernel followed by panel_stats_kernel.
+template <bool ROWC>
+__global__ void __launch_bounds__(256) scale_stats_kernel(const StatItem* __restrict__ items, int count) {
+    __shared__ unsigned int hist[kGapBins + 1];
+    __shared__ unsigned long long part[8][32];
+    for (int i = threadIdx.x; i <= kGapBins; i += blockDim.x) hist[i] = 0;
+    const StatItem* I = items + find_block_item(items, count, blockIdx.x);
+    const int64_t rb = static_cast<int64_t>(blockIdx.x) - I->block0;
+    const unsigned long long* X = reinterpret_cast<const unsigned long long*>(I->X);
+    const int64_t rows = I->rows, k = I->k, ldx = I->ldx;
+    const int warp = static_cast<int>(threadIdx.x >> 5), lane = static_cast<int>(threadIdx.x & 31);
+    auto add = [&](unsigned long long bits, int erow) {
+        bits &= 0x7FFFFFFFFFFFFFFFull;
+        if (bits == 0) {
+            atomicAdd(&hist[kGapBins], 1u);
+        } else if (bits < 0x7FF0000000000000ull) {
+            const int g = min(max(erow - frexp_exp_bits(bits), 0), kGapBins - 1);
+            atomicAdd(&hist[g], 1u);
+        }
+    };
+    unsigned long long mb = 0;  // the row maximum (bits of |x|)
+    int64_t r;
+    if (ROWC) {
+        r = rb * 32 + lane;
+        unsigned long long best = 0;
+        if (r < rows)
+            for (int64_t p = warp; p < k; p += 8) best = max(best, __ldg(X + r + p * ldx) & 0x7FFFFFFFFFFFFFFFull);
+        part[warp][lane] = best;
+        __syncthreads();
+#pragma unroll
+        for (int w = 0; w < 8; ++w) mb = max(mb, part[w][lane]);
+        if (warp == 0 && r < rows) I->maxbits[r] = mb;
+    } else {
+        r = rb * 8 + warp;
+        unsigned long long best = 0;
+        if (r < rows)
+            for (int64_t p = lane; p < k; p += 32) best = max(best, __ldg(X + p + r * ldx) & 0x7FFFFFFFFFFFFFFFull);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) best = max(best, __shfl_xor_sync(0xFFFFFFFFu, best, o));
+        mb = best;
+        if (lane == 0 && r < rows) I->maxbits[r] = mb;
+        __syncthreads();  // the histogram's zeroing is visible
+    }
+    if (r < rows && mb != 0 && mb < 0x7FF0000000000000ull) {
+        const int erow = frexp_exp_bits(mb);
+        if (ROWC) {
+            for (int64_t p = warp; p < k; p += 8) add(__ldg(X + r + p * ldx), erow);
+        } else {
+            for (int64_t p = lane; p < k; p += 32) add(__ldg(X + p + r * ldx), erow);
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i <= kGapBins; i += blockDim.x)
+        if (hist[i]) atomicAdd(I->hist + i, hist[i]);
+}
+
 // ---------------------------------------------------------------- features + analytic s
 __device__ float gap_quantile(const unsigned int* h, unsigned long long nonzero, float q) {
     if (nonzero == 0) return 0.0f;
@@ -560,6 +620,19 @@ int64_t stat_item_blocks(StatItem& it, int64_t block0) {
     const int64_t chunks = (it.k + 2047) / 2048;
     it.kchunk = (it.k + chunks - 1) / chunks;
     return it.rblocks * chunks;
+}
+
+int64_t scale_stat_item_blocks(StatItem& it, int64_t block0) {
+    it.block0 = block0;
+    it.kchunk = it.k;
+    it.rblocks = it.rows <= 0 || it.k <= 0 ? 0 : (it.row_contig ? (it.rows + 31) / 32 : (it.rows + 7) / 8);
+    return it.rblocks;
+}
+
+void launch_scale_stats(const StatItem* d, const StatItem* h, int count, int64_t blocks, cudaStream_t st) {
+    if (count <= 0 || blocks <= 0) return;
+    if (h[0].row_contig) scale_stats_kernel<true><<<static_cast<unsigned>(blocks), 256, 0, st>>>(d, count);
+    else scale_stats_kernel<false><<<static_cast<unsigned>(blocks), 256, 0, st>>>(d, count);
 }
 
 void launch_panel_stats(const StatItem* d, const StatItem* h, int count, int64_t blocks, cudaStream_t st) {

@@ -36,7 +36,7 @@ struct StatItem {
     const double* X;
     int64_t ldx, rows, k;
     int row_contig;
-    const unsigned long long* maxbits;  // row maxima of the panel rows
+    unsigned long long* maxbits;        // row maxima of the panel rows (written by scale_stats)
     unsigned int* hist;                 // kGapBins + 1 counters, zeroed before the launch
     int64_t kchunk, block0, rblocks;
 };
@@ -126,6 +126,12 @@ void launch_cert_tiles(const CertTileItem* d, int count, cudaStream_t st);
 
 int64_t stat_item_blocks(StatItem& it, int64_t block0);
 void launch_panel_stats(const StatItem* d, const StatItem* h, int count, int64_t blocks, cudaStream_t st);
+// the scale pass and the panel statistics in one launch: a block owns whole rows, takes their
+// maxima (written to maxbits) and then reads the same rows again, from the L2, for the gap
+// histogram; for problems with k up to kFusedStatsMaxK (a row then stays well inside the L2)
+constexpr int64_t kFusedStatsMaxK = 16384;
+int64_t scale_stat_item_blocks(StatItem& it, int64_t block0);
+void launch_scale_stats(const StatItem* d, const StatItem* h, int count, int64_t blocks, cudaStream_t st);
 void launch_tile_features(const FeatureItem* d, int count, float* feat, int* s_analytic, cudaStream_t st);
 int64_t probe_item_blocks(ProbeItem& it, int64_t block0);
 void launch_probe(const ProbeItem* d, int count, int64_t blocks, int* fail, cudaStream_t st);

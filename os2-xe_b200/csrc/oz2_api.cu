@@ -1294,8 +1294,13 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
     ++h->launches;
 
     Program ph1;
+    // with every k up to kFusedStatsMaxK one launch per layout takes the row maxima and the panel
+    // statistics together (one read of A and B from DRAM); otherwise the scale pass runs first
+    int64_t kmax = 0;
+    for (const Prob& p : base) kmax = std::max(kmax, p.k);
+    const bool fused_stats = kmax <= kFusedStatsMaxK;
     std::vector<ScaleItem> sc;
-    for (size_t q = 0; q < base.size(); ++q) {
+    for (size_t q = 0; q < base.size() && !fused_stats; ++q) {
         sc.push_back(scale_item(base[q], true, maxA(static_cast<int>(q))));
         sc.push_back(scale_item(base[q], false, maxB(static_cast<int>(q))));
     }
@@ -1330,7 +1335,8 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
     std::vector<StatOp> stat_ops;
     for (auto& kv : stat_groups) {
         int64_t blocks = 0;
-        for (auto& it : kv.second) blocks += stat_item_blocks(it, blocks);
+        for (auto& it : kv.second)
+            blocks += fused_stats ? scale_stat_item_blocks(it, blocks) : stat_item_blocks(it, blocks);
         stat_ops.push_back({ph1.add(kv.second.data(), kv.second.size() * sizeof(StatItem)),
                             static_cast<int>(kv.second.size()), blocks});
     }
@@ -1363,9 +1369,10 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
     mark(h, kBegin);
     issue(h, ph1, dd);  // scale (its mark closes the scale stage)
     for (const StatOp& so : stat_ops) {
-        launch_panel_stats(reinterpret_cast<const StatItem*>(dd + so.off),
-                           reinterpret_cast<const StatItem*>(ph1.blob.data() + so.off), so.count, so.blocks,
-                           h->stream);
+        const StatItem* d_items = reinterpret_cast<const StatItem*>(dd + so.off);
+        const StatItem* h_items = reinterpret_cast<const StatItem*>(ph1.blob.data() + so.off);
+        if (fused_stats) launch_scale_stats(d_items, h_items, so.count, so.blocks, h->stream);
+        else launch_panel_stats(d_items, h_items, so.count, so.blocks, h->stream);
         ++h->launches;
     }
     launch_tile_features(reinterpret_cast<const FeatureItem*>(dd + ofi), static_cast<int>(ntiles), d_feat, d_sa,

@@ -100,14 +100,19 @@ def test_mlp_training_fits_a_learnable_rule(az):
     assert (s - labels).abs().le(1).float().mean().item() > 0.9
 
 
-def test_tile_features_and_analytic_s_match_host_restatement(oracle, az):
+# the first list takes the fused scale + statistics pass (every k up to 16384), the second, with
+# one longer k, the scale pass followed by the statistics pass
+FEATURE_CASES = [[("N", "N", 700, 600, 300, 1.0, 10), ("T", "N", 513, 1030, 999, 4.0, 40),
+                  ("N", "T", 128, 200, 5000, 0.0, 0), ("T", "T", 600, 520, 64, 8.0, 20)],
+                 [("N", "N", 300, 130, 20000, 2.0, 30), ("T", "T", 90, 520, 700, 4.0, 10)]]
+
+
+@pytest.mark.parametrize("case", range(len(FEATURE_CASES)))
+def test_tile_features_and_analytic_s_match_host_restatement(oracle, az, case):
     import torch
     rng = np.random.default_rng(9)
     probs, dev = [], []
-    for q, (ta, tb, m, n, k, phi, offs) in enumerate([("N", "N", 700, 600, 300, 1.0, 10),
-                                                      ("T", "N", 513, 1030, 999, 4.0, 40),
-                                                      ("N", "T", 128, 200, 5000, 0.0, 0),
-                                                      ("T", "T", 600, 520, 64, 8.0, 20)]):
+    for q, (ta, tb, m, n, k, phi, offs) in enumerate(FEATURE_CASES[case]):
         Ar, Ac = op_shape(ta, m, k)
         Br, Bc = op_shape(tb, k, n)
         A = wide_rows(100 + q, Ar, Ac, phi, offs)
