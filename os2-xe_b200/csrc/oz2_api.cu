@@ -613,8 +613,8 @@ int read_back(oz2_context* h, std::initializer_list<HostRead> reads) {
         if (h->rb_host) cudaFreeHost(h->rb_host);
         h->rb_host = h->rb_dev = nullptr;
         h->rb_cap = 0;
-        size_t cap = size_t{1} << 16;
-        while (cap < total) cap *= 2;
+        size_t cap = size_t{1} << 20;  // pinned allocations are slow: room for twice the request
+        while (cap < 2 * total) cap *= 2;
         OZ2_CUDA(h, cudaHostAlloc(&h->rb_host, cap, cudaHostAllocMapped));
         OZ2_CUDA(h, cudaHostGetDevicePointer(&h->rb_dev, h->rb_host, 0));
         h->rb_cap = cap;
@@ -1278,7 +1278,9 @@ int run_adaptive(oz2_context* h, std::vector<Prob>& base, const std::vector<int>
                               ntiles * (sizeof(FeatureItem) + sizeof(ProbeItem) + 2 * sizeof(FreivaldsItem)) +
                               16 * 256;
     const size_t odesc = carve1(desc_bytes);
-    int st = ensure_workspace(h, off);
+    // a quarter of headroom: the phase-1 data grows with the tile count, which varies from call to
+    // call, and each regrowth drains the stream and reallocates
+    int st = h->ws_size >= off ? OZ2_OK : ensure_workspace(h, off + off / 4);
     if (st) return st;
     auto* ws = h->ws;
     auto maxA = [&](int q) { return reinterpret_cast<unsigned long long*>(ws + omaxA[q]); };
